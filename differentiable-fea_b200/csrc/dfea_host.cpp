@@ -1,0 +1,90 @@
+// dfea_host.cpp -- host side of the C ABI: error reporting, device queries and the greedy element
+// colouring that orders the deterministic scatter of every element kernel.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "difffea_b200.h"
+
+namespace dfea {
+
+static thread_local char g_error[512] = "no error";
+
+int set_error(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int check_cuda(cudaError_t err, const char* what) {
+    if (err == cudaSuccess) return DFEA_OK;
+    return set_error(DFEA_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(err), cudaGetErrorName(err));
+}
+
+int launch_check(const char* what) { return check_cuda(cudaGetLastError(), what); }
+
+// Kernels this library has launched in the process (direct launches when issued, graph-executed
+// kernels when the graph's solve returns): the evidence behind a benchmark's "gpu_launches".
+static std::atomic<long long> g_launches{0};
+void note_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int device_sm_count() {
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (cache[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
+}  // namespace dfea
+
+using namespace dfea;
+
+extern "C" const char* dfea_last_error(void) { return g_error; }
+
+extern "C" int dfea_version(void) { return 10000; }
+
+extern "C" int64_t dfea_launch_count(void) { return (int64_t)g_launches.load(std::memory_order_relaxed); }
+
+extern "C" int dfea_element_supported(int32_t nen, int32_t n_q) {
+    return (nen == 4 && n_q == 4) || (nen == 9 && n_q == 9) || (nen == 3 && n_q == 1) || (nen == 6 && n_q == 6) ||
+           (nen == 8 && n_q == 9);
+}
+
+extern "C" int dfea_colour_elements(const int64_t* conn, int64_t n_el, int32_t nen, int64_t n_nodes, int32_t* colour,
+                                    int32_t* n_colours) {
+    if (n_el < 0 || nen < 1 || n_nodes < 1 || !n_colours || (n_el > 0 && (!conn || !colour)))
+        return set_error(DFEA_ERR_INVALID, "dfea_colour_elements: bad arguments");
+    // used[node]: bit c set when an element of colour c touches the node
+    std::vector<uint64_t> used((size_t)n_nodes, 0ull);
+    int32_t n_used = 0;
+    for (int64_t e = 0; e < n_el; ++e) {
+        uint64_t taken = 0ull;
+        for (int a = 0; a < nen; ++a) {
+            const int64_t node = conn[e * nen + a];
+            if (node < 0 || node >= n_nodes)
+                return set_error(DFEA_ERR_INVALID, "element %lld references node %lld outside [0, %lld)", (long long)e,
+                                 (long long)node, (long long)n_nodes);
+            taken |= used[(size_t)node];
+        }
+        if (taken == ~0ull) return set_error(DFEA_ERR_COLOURS, "element %lld needs more than %d colours", (long long)e,
+                                             DFEA_MAX_COLOURS);
+        int c = 0;
+        while (taken & (1ull << c)) ++c;
+        colour[e] = c;
+        if (c + 1 > n_used) n_used = c + 1;
+        for (int a = 0; a < nen; ++a) used[(size_t)conn[e * nen + a]] |= (1ull << c);
+    }
+    *n_colours = n_used > 0 ? n_used : 1;
+    return DFEA_OK;
+}

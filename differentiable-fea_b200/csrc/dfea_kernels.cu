@@ -1,0 +1,579 @@
+// dfea_kernels.cu -- mesh packing, kernel (a) (Gauss-point moduli + Jacobi diagonal), the tangent
+// product entry point, the FP64 residual / strain energy, norms, kernel (d) (element sensitivity)
+// and small vector helpers.  All entry points are `extern "C"` (include/difffea_b200.h).
+#include <cstdio>
+
+#include "dfea_apply.cuh"
+#include "dfea_common.cuh"
+
+namespace dfea {
+
+// ------------------------------------------------------------------------------------------
+// validation shared by the entry points
+// ------------------------------------------------------------------------------------------
+int validate_mesh(const dfea_mesh_view* mv, bool need_grad32) {
+    if (mv == nullptr) return set_error(DFEA_ERR_INVALID, "mesh view is NULL");
+    if (mv->n_el < 0 || mv->n_nodes <= 0) return set_error(DFEA_ERR_INVALID, "bad sizes n_el=%lld n_nodes=%lld",
+                                                             (long long)mv->n_el, (long long)mv->n_nodes);
+    if (mv->stride < mv->n_el || mv->stride % 32 != 0)
+        return set_error(DFEA_ERR_INVALID, "stride %lld must be a multiple of 32 and >= n_el %lld",
+                         (long long)mv->stride, (long long)mv->n_el);
+    if (!dfea_element_supported(mv->nen, mv->n_q))
+        return set_error(DFEA_ERR_UNSUPPORTED, "element with nen=%d n_q=%d is not built", mv->nen, mv->n_q);
+    if (mv->n_colours < 1 || mv->n_colours > DFEA_MAX_COLOURS)
+        return set_error(DFEA_ERR_INVALID, "n_colours %d out of [1, %d]", mv->n_colours, DFEA_MAX_COLOURS);
+    if (mv->colour_begin[0] != 0 || mv->colour_begin[mv->n_colours] != mv->n_el)
+        return set_error(DFEA_ERR_INVALID, "colour ranges must cover [0, n_el)");
+    for (int c = 0; c < mv->n_colours; ++c)
+        if (mv->colour_begin[c + 1] < mv->colour_begin[c]) return set_error(DFEA_ERR_INVALID, "colour ranges not sorted");
+    if (!mv->conn || !mv->orig || !mv->grad || !mv->wdet || !mv->node_fix)
+        return set_error(DFEA_ERR_INVALID, "mesh view has a NULL device pointer");
+    if (need_grad32 && !mv->grad32) return set_error(DFEA_ERR_INVALID, "FP32 operator needs mesh->grad32");
+    if (mv->n_nodes >= (int64_t(1) << 29)) return set_error(DFEA_ERR_INVALID, "too many nodes for the packed connectivity");
+    return DFEA_OK;
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// ------------------------------------------------------------------------------------------
+// mesh packing
+// ------------------------------------------------------------------------------------------
+__global__ void k_pack(int64_t n_el, int64_t S, int nen, int nq, const int64_t* __restrict__ perm,
+                       const int64_t* __restrict__ conn_ref, const double* __restrict__ dN,
+                       const double* __restrict__ wd, const double* __restrict__ mask,
+                       int32_t* __restrict__ conn, int32_t* __restrict__ orig, double* __restrict__ grad,
+                       double* __restrict__ wdet) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n_el; s += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = perm[s];
+        orig[s] = (int32_t)o;
+        for (int a = 0; a < nen; ++a) {
+            const int64_t node = conn_ref[o * nen + a];
+            const int fix = (mask[2 * node] == 0.0 ? 1 : 0) | (mask[2 * node + 1] == 0.0 ? 2 : 0);
+            conn[a * S + s] = (int32_t)((node << 2) | fix);
+        }
+        for (int q = 0; q < nq; ++q) {
+            wdet[q * S + s] = wd[o * nq + q];
+            for (int a = 0; a < nen; ++a) {
+                const double* src = dN + ((o * nq + q) * nen + a) * 2;
+                reinterpret_cast<double2*>(grad)[(int64_t)(q * nen + a) * S + s] = make_double2(src[0], src[1]);
+            }
+        }
+    }
+}
+
+__global__ void k_node_fix(int64_t n_nodes, const double* __restrict__ mask, uint8_t* __restrict__ node_fix) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_nodes; n += (int64_t)gridDim.x * blockDim.x)
+        node_fix[n] = (uint8_t)((mask[2 * n] == 0.0 ? 1 : 0) | (mask[2 * n + 1] == 0.0 ? 2 : 0));
+}
+
+__global__ void k_to_f32(int64_t n, const double* __restrict__ x, float* __restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = (float)x[i];
+}
+
+__global__ void k_to_f64(int64_t n, const float* __restrict__ x, double* __restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = (double)x[i];
+}
+
+// ------------------------------------------------------------------------------------------
+// kernel (a): moduli + element diagonals, one colour per launch
+// ------------------------------------------------------------------------------------------
+template <int NEN, int NQ, typename CT>
+__global__ void __launch_bounds__(128)
+k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const double* __restrict__ theta,
+         double mu0, double lam0, CT* __restrict__ Cout, double* __restrict__ diag) {
+    const int64_t S = m.stride;
+    const double2* u2 = reinterpret_cast<const double2*>(u);
+    for (int64_t e = e0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < e1; e += (int64_t)gridDim.x * blockDim.x) {
+        int node[NEN];
+        double ux[NEN], uy[NEN], dx[NEN], dy[NEN];
+#pragma unroll
+        for (int a = 0; a < NEN; ++a) {
+            node[a] = m.conn[a * S + e] >> 2;
+            const double2 t = __ldg(u2 + node[a]);
+            ux[a] = t.x;
+            uy[a] = t.y;
+            dx[a] = 0.0;
+            dy[a] = 0.0;
+        }
+        const double th = theta[m.orig[e]];
+        const double mu = mu0 * th, lam = lam0 * th;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double gx[NEN], gy[NEN];
+            double F[4] = {1.0, 0.0, 0.0, 1.0};
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                const double2 g = load_grad(m.grad, (int64_t)(q * NEN + a) * S + e);
+                gx[a] = g.x;
+                gy[a] = g.y;
+                F[0] += ux[a] * g.x;
+                F[1] += ux[a] * g.y;
+                F[2] += uy[a] * g.x;
+                F[3] += uy[a] * g.y;
+            }
+            const NHPoint p = nh_point(F);
+            double Cq[16];
+            nh_moduli(p, mu, lam, m.wdet[q * S + e], Cq);
+            if (Cout != nullptr) store_moduli(Cout, S, q, e, Cq);
+            if (diag != nullptr) {
+                // e_k^T K_e e_k for the unit DOF (a, i): sum_{J,L} C[(iJ),(iL)] dN_aJ dN_aL
+#pragma unroll
+                for (int a = 0; a < NEN; ++a) {
+                    dx[a] += Cq[0] * gx[a] * gx[a] + (Cq[1] + Cq[4]) * gx[a] * gy[a] + Cq[5] * gy[a] * gy[a];
+                    dy[a] += Cq[10] * gx[a] * gx[a] + (Cq[11] + Cq[14]) * gx[a] * gy[a] + Cq[15] * gy[a] * gy[a];
+                }
+            }
+        }
+        if (diag != nullptr) {
+            double2* d2 = reinterpret_cast<double2*>(diag);
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                double2 t = d2[node[a]];
+                t.x += dx[a];
+                t.y += dy[a];
+                d2[node[a]] = t;
+            }
+        }
+    }
+}
+
+__global__ void k_zero(int64_t n, double* __restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] = 0.0;
+}
+
+// diag = where(m > 0, clamp(diag, min=1e-6), 1)   (operators.py:555-556)
+__global__ void k_diag_finalize(Mesh m, double* __restrict__ diag) {
+    double2* d2 = reinterpret_cast<double2*>(diag);
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fix = m.node_fix[n];
+        double2 t = d2[n];
+        t.x = (fix & 1) ? 1.0 : fmax(t.x, 1e-6);
+        t.y = (fix & 2) ? 1.0 : fmax(t.y, 1e-6);
+        d2[n] = t;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 residual and strain energy, one colour per launch
+// ------------------------------------------------------------------------------------------
+// R = -load_factor * f on free DOFs, 0 on fixed DOFs (the colour passes then add R_int).
+__global__ void k_residual_init(Mesh m, const double* __restrict__ f, double lf, double* __restrict__ R) {
+    const double2* f2 = reinterpret_cast<const double2*>(f);
+    double2* R2 = reinterpret_cast<double2*>(R);
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fix = m.node_fix[n];
+        const double2 t = f ? f2[n] : make_double2(0.0, 0.0);
+        R2[n] = make_double2((fix & 1) ? 0.0 : -lf * t.x, (fix & 2) ? 0.0 : -lf * t.y);
+    }
+}
+
+template <int NEN, int NQ, bool ENERGY>
+__global__ void __launch_bounds__(128)
+k_residual(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const double* __restrict__ theta,
+           double mu0, double lam0, double* __restrict__ R, RedSite site) {
+    const int64_t S = m.stride;
+    const double2* u2 = reinterpret_cast<const double2*>(u);
+    double2* R2 = reinterpret_cast<double2*>(R);
+    double energy = 0.0;
+    for (int64_t e = e0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < e1; e += (int64_t)gridDim.x * blockDim.x) {
+        int node[NEN], fix[NEN];
+        double ux[NEN], uy[NEN], fx[NEN], fy[NEN];
+#pragma unroll
+        for (int a = 0; a < NEN; ++a) {
+            const int c = m.conn[a * S + e];
+            node[a] = c >> 2;
+            fix[a] = c & 3;
+            const double2 t = __ldg(u2 + node[a]);
+            ux[a] = t.x;
+            uy[a] = t.y;
+            fx[a] = 0.0;
+            fy[a] = 0.0;
+        }
+        const double th = theta ? theta[m.orig[e]] : 1.0;
+        const double mu = mu0 * th, lam = lam0 * th;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double gx[NEN], gy[NEN];
+            double F[4] = {1.0, 0.0, 0.0, 1.0};
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                const double2 g = load_grad(m.grad, (int64_t)(q * NEN + a) * S + e);
+                gx[a] = g.x;
+                gy[a] = g.y;
+                F[0] += ux[a] * g.x;
+                F[1] += ux[a] * g.y;
+                F[2] += uy[a] * g.x;
+                F[3] += uy[a] * g.y;
+            }
+            const NHPoint p = nh_point(F);
+            double P[4];
+            nh_stress(F, p, mu, lam, P);
+            const double w = m.wdet[q * S + e];
+            if (ENERGY) energy += w * nh_energy(F, p, mu, lam);
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                fx[a] += w * (P[0] * gx[a] + P[1] * gy[a]);
+                fy[a] += w * (P[2] * gx[a] + P[3] * gy[a]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < NEN; ++a) {
+            double2 t = R2[node[a]];
+            if (!(fix[a] & 1)) t.x += fx[a];
+            if (!(fix[a] & 2)) t.y += fy[a];
+            R2[node[a]] = t;
+        }
+    }
+    if (ENERGY) {
+        const double vals[1] = {block_sum<128>(energy)};
+        double tot[1];
+        if (last_block_sum<128, 1>(vals, site, tot) && threadIdx.x == 0) site.result[0] = tot[0];
+    }
+}
+
+// sum x^2 over 2N entries; the last block also adds up per-colour energies (if any) in colour order.
+__global__ void __launch_bounds__(kThreads)
+k_norm2(int64_t n, const double* __restrict__ x, RedSite site, double* __restrict__ out,
+        const double* __restrict__ colour_energy, int n_colours, double* __restrict__ out_energy) {
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double t = x[i];
+        s += t * t;
+    }
+    const double vals[1] = {block_sum<kThreads>(s)};
+    double tot[1];
+    if (last_block_sum<kThreads, 1>(vals, site, tot) && threadIdx.x == 0) {
+        if (out) *out = tot[0];
+        if (out_energy) {
+            double E = 0.0;
+            for (int c = 0; c < n_colours; ++c) E += colour_energy[c];
+            *out_energy = E;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// kernel (d): per-element sensitivity g_e = -lambda_e . f_e(u; p0)
+// ------------------------------------------------------------------------------------------
+template <int NEN, int NQ>
+__global__ void __launch_bounds__(128)
+k_sensitivity(Mesh m, const double* __restrict__ u, const double* __restrict__ lam_adj, double mu0, double lam0,
+              double* __restrict__ g) {
+    const int64_t S = m.stride;
+    const double2* u2 = reinterpret_cast<const double2*>(u);
+    const double2* l2 = reinterpret_cast<const double2*>(lam_adj);
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m.n_el; e += (int64_t)gridDim.x * blockDim.x) {
+        double ux[NEN], uy[NEN], lx[NEN], ly[NEN];
+#pragma unroll
+        for (int a = 0; a < NEN; ++a) {
+            const int c = m.conn[a * S + e];
+            const int node = c >> 2, fix = c & 3;
+            const double2 t = __ldg(u2 + node);
+            const double2 l = __ldg(l2 + node);
+            ux[a] = t.x;
+            uy[a] = t.y;
+            lx[a] = (fix & 1) ? 0.0 : l.x;
+            ly[a] = (fix & 2) ? 0.0 : l.y;
+        }
+        double ge = 0.0;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double gx[NEN], gy[NEN];
+            double F[4] = {1.0, 0.0, 0.0, 1.0};
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                const double2 gg = load_grad(m.grad, (int64_t)(q * NEN + a) * S + e);
+                gx[a] = gg.x;
+                gy[a] = gg.y;
+                F[0] += ux[a] * gg.x;
+                F[1] += ux[a] * gg.y;
+                F[2] += uy[a] * gg.x;
+                F[3] += uy[a] * gg.y;
+            }
+            const NHPoint p = nh_point(F);
+            double P[4];
+            nh_stress(F, p, mu0, lam0, P);
+            const double w = m.wdet[q * S + e];
+            // lambda_e : (P dN^T) integrated, i.e. sum_a lambda_a . f_a
+            double lgx = 0.0, lgy = 0.0, lgx2 = 0.0, lgy2 = 0.0;
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                lgx += lx[a] * gx[a];
+                lgy += lx[a] * gy[a];
+                lgx2 += ly[a] * gx[a];
+                lgy2 += ly[a] * gy[a];
+            }
+            ge += w * (P[0] * lgx + P[1] * lgy + P[2] * lgx2 + P[3] * lgy2);
+        }
+        g[m.orig[e]] = -ge;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// small vector kernels
+// ------------------------------------------------------------------------------------------
+__global__ void k_axpy(int64_t n, double a, const double* __restrict__ x, double* __restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += a * x[i];
+}
+
+__global__ void k_add_scaled(int64_t n, const double* __restrict__ a, double alpha, const double* __restrict__ b,
+                             double* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] + alpha * b[i];
+}
+
+// Scratch layout of dfea_residual / dfea_vec_norm2:
+//   [0, DFEA_MAX_COLOURS + 1) reduction sites of kMaxBlocks partials, then tickets, then results.
+struct ReduceWork {
+    double* partials;   // n_sites x kMaxBlocks
+    unsigned* tickets;  // kTicketSlots >= n_sites
+    double* results;    // n_sites
+    static constexpr int n_sites = DFEA_MAX_COLOURS + 1;
+    static constexpr int kTicketSlots = 128;
+    static int64_t bytes() {
+        return (int64_t)n_sites * kMaxBlocks * 8 + kTicketSlots * 4 + (int64_t)n_sites * 8 + 256;
+    }
+    explicit ReduceWork(void* base) {
+        char* p = static_cast<char*>(base);
+        partials = reinterpret_cast<double*>(p);
+        p += (int64_t)n_sites * kMaxBlocks * 8;
+        tickets = reinterpret_cast<unsigned*>(p);
+        p += kTicketSlots * 4;
+        results = reinterpret_cast<double*>(p);
+    }
+    RedSite site(int i) const { return RedSite{partials + (int64_t)i * kMaxBlocks, tickets + i, results + i}; }
+};
+
+__global__ void k_zero_tickets(unsigned* t, int n, double* results, int nr) {
+    // one block of >= max(n, nr) threads; n <= ReduceWork::kTicketSlots
+    const int i = threadIdx.x;
+    if (i < n) t[i] = 0u;
+    if (i < nr) results[i] = 0.0;
+}
+
+}  // namespace dfea
+
+using namespace dfea;
+
+// ==========================================================================================
+// C ABI
+// ==========================================================================================
+extern "C" int dfea_mesh_pack(int64_t n_el, int64_t stride, int32_t nen, int32_t n_q, int64_t n_nodes,
+                              const int64_t* perm, const int64_t* conn_ref, const double* dN_dX,
+                              const double* w_detJ, const double* m, int32_t* conn_out, int32_t* orig_out,
+                              double* grad_out, double* wdet_out, uint8_t* node_fix_out, void* stream) {
+    if (n_el < 0 || n_nodes <= 0 || stride < n_el || stride % 32 != 0)
+        return set_error(DFEA_ERR_INVALID, "dfea_mesh_pack: bad sizes");
+    if (!dfea_element_supported(nen, n_q))
+        return set_error(DFEA_ERR_UNSUPPORTED, "element with nen=%d n_q=%d is not built", nen, n_q);
+    if (n_nodes >= (int64_t(1) << 29)) return set_error(DFEA_ERR_INVALID, "too many nodes for the packed connectivity");
+    if (!m || !node_fix_out || (n_el > 0 && (!perm || !conn_ref || !dN_dX || !w_detJ || !conn_out || !orig_out ||
+                                             !grad_out || !wdet_out)))
+        return set_error(DFEA_ERR_INVALID, "dfea_mesh_pack: NULL pointer");
+    if (!aligned16(grad_out)) return set_error(DFEA_ERR_INVALID, "dfea_mesh_pack: grad_out must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n_el > 0) {
+        k_pack<<<grid_for(n_el, kThreads, 8), kThreads, 0, s>>>(n_el, stride, nen, n_q, perm, conn_ref, dN_dX, w_detJ, m,
+                                                                  conn_out, orig_out, grad_out, wdet_out);
+        note_launches(1);
+    }
+    k_node_fix<<<grid_for(n_nodes, kThreads, 8), kThreads, 0, s>>>(n_nodes, m, node_fix_out);
+    note_launches(1);
+    return launch_check("dfea_mesh_pack");
+}
+
+extern "C" int dfea_mesh_grad_to_f32(const dfea_mesh_view* mesh, float* grad32_out, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!grad32_out || !aligned16(grad32_out)) return set_error(DFEA_ERR_INVALID, "grad32_out must be 16-byte aligned");
+    const int64_t n = (int64_t)mesh->n_q * mesh->nen * mesh->stride * 2;
+    k_to_f32<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, mesh->grad, grad32_out);
+    note_launches(1);
+    return launch_check("dfea_mesh_grad_to_f32");
+}
+
+extern "C" int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                              double lambda0, void* moduli, int32_t moduli_dtype, double* diag, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!u || !theta || (!moduli && !diag)) return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: NULL pointer");
+    if (!aligned16(u) || (moduli && !aligned16(moduli)) || (diag && !aligned16(diag)))
+        return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: u, moduli and diag must be 16-byte aligned");
+    if (moduli_dtype != DFEA_F64 && moduli_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad moduli dtype");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const Mesh m = kernel_mesh(*mesh);
+    if (diag) {
+        k_zero<<<grid_for(2 * mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(2 * mesh->n_nodes, diag);
+        note_launches(1);
+    }
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        for (int c = 0; c < mesh->n_colours; ++c) {
+            const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
+            if (e1 <= e0) continue;
+            const int grid = grid_for(e1 - e0, 128, 12);
+            if (moduli_dtype == DFEA_F64)
+                k_moduli<NEN, NQ, double><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
+                                                                static_cast<double*>(moduli), diag);
+            else
+                k_moduli<NEN, NQ, float><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
+                                                               static_cast<float*>(moduli), diag);
+            note_launches(1);
+        }
+        return DFEA_OK;
+    });
+    if (rc) return rc;
+    if (diag) {
+        k_diag_finalize<<<grid_for(mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(m, diag);
+        note_launches(1);
+    }
+    return launch_check("dfea_qp_moduli");
+}
+
+extern "C" int dfea_tangent_apply(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype, const void* v,
+                                  void* y, int32_t vec_dtype, void* stream) {
+    int rc = validate_mesh(mesh, vec_dtype == DFEA_F32);
+    if (rc) return rc;
+    if (!moduli || !v || !y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: NULL pointer");
+    if (v == y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: y must not alias v");
+    if (!aligned16(moduli) || !aligned16(v) || !aligned16(y))
+        return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: moduli, v and y must be 16-byte aligned");
+    if (vec_dtype == DFEA_F64 && moduli_dtype != DFEA_F64)
+        return set_error(DFEA_ERR_INVALID, "FP64 vectors need FP64 moduli");
+    if (vec_dtype == DFEA_F32 && moduli_dtype != DFEA_F32)
+        return set_error(DFEA_ERR_INVALID, "FP32 vectors need FP32 moduli");
+    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const Mesh m = kernel_mesh(*mesh);
+    const int gn = grid_for(mesh->n_nodes, kThreads, 8);
+    return dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        if (vec_dtype == DFEA_F64) {
+            k_pivot_init<double><<<gn, kThreads, 0, s>>>(m, static_cast<const double*>(v), static_cast<double*>(y));
+            note_launches(1);
+            return launch_apply_colours<NEN, NQ, double, false>(*mesh, static_cast<const double*>(moduli), mesh->grad,
+                                                               static_cast<const double*>(v), static_cast<double*>(y),
+                                                               nullptr, nullptr, s);
+        }
+        k_pivot_init<float><<<gn, kThreads, 0, s>>>(m, static_cast<const float*>(v), static_cast<float*>(y));
+        note_launches(1);
+        return launch_apply_colours<NEN, NQ, float, false>(*mesh, static_cast<const float*>(moduli), mesh->grad32,
+                                                          static_cast<const float*>(v), static_cast<float*>(y),
+                                                          nullptr, nullptr, s);
+    });
+}
+
+extern "C" int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh) {
+    (void)mesh;
+    return ReduceWork::bytes();
+}
+
+extern "C" int dfea_residual(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                             double lambda0, const double* f, double load_factor, double* R, double* out_norm2,
+                             double* out_energy, void* work, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!u || !R) return set_error(DFEA_ERR_INVALID, "dfea_residual: NULL pointer");
+    if ((out_norm2 || out_energy) && !work) return set_error(DFEA_ERR_INVALID, "dfea_residual: reductions need work");
+    if (!aligned16(u) || !aligned16(R) || (f && !aligned16(f)) || (work && !aligned16(work)))
+        return set_error(DFEA_ERR_INVALID, "dfea_residual: vectors must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const Mesh m = kernel_mesh(*mesh);
+    ReduceWork w(work);
+    if (work) {
+        k_zero_tickets<<<1, 128, 0, s>>>(w.tickets, ReduceWork::n_sites, w.results, ReduceWork::n_sites);
+        note_launches(1);
+    }
+    k_residual_init<<<grid_for(mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(m, f, load_factor, R);
+    note_launches(1);
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        for (int c = 0; c < mesh->n_colours; ++c) {
+            const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
+            if (e1 <= e0) continue;
+            const int grid = grid_for(e1 - e0, 128, 12);
+            if (out_energy)
+                k_residual<NEN, NQ, true><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0, R, w.site(1 + c));
+            else
+                k_residual<NEN, NQ, false><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0, R, RedSite{});
+            note_launches(1);
+        }
+        return DFEA_OK;
+    });
+    if (rc) return rc;
+    if (out_norm2 || out_energy) {
+        const int64_t n = 2 * mesh->n_nodes;
+        k_norm2<<<grid_for(n, kThreads, 4), kThreads, 0, s>>>(n, R, w.site(0), out_norm2, w.results + 1,
+                                                             mesh->n_colours, out_energy);
+        note_launches(1);
+    }
+    return launch_check("dfea_residual");
+}
+
+extern "C" int dfea_vec_norm2(const dfea_mesh_view* mesh, const double* x, double* out, void* work, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!x || !out || !work) return set_error(DFEA_ERR_INVALID, "dfea_vec_norm2: NULL pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ReduceWork w(work);
+    k_zero_tickets<<<1, 128, 0, s>>>(w.tickets, ReduceWork::n_sites, w.results, ReduceWork::n_sites);
+    note_launches(1);
+    const int64_t n = 2 * mesh->n_nodes;
+    k_norm2<<<grid_for(n, kThreads, 4), kThreads, 0, s>>>(n, x, w.site(0), out, nullptr, 0, nullptr);
+    note_launches(1);
+    return launch_check("dfea_vec_norm2");
+}
+
+extern "C" int dfea_element_sensitivity(const dfea_mesh_view* mesh, const double* u, const double* lam, double mu0,
+                                        double lambda0, double* g, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!u || !lam || !g) return set_error(DFEA_ERR_INVALID, "dfea_element_sensitivity: NULL pointer");
+    if (!aligned16(u) || !aligned16(lam)) return set_error(DFEA_ERR_INVALID, "u and lambda must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const Mesh m = kernel_mesh(*mesh);
+    if (mesh->n_el == 0) return DFEA_OK;
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        k_sensitivity<NEN, NQ><<<grid_for(mesh->n_el, 128, 12), 128, 0, s>>>(m, u, lam, mu0, lambda0, g);
+        note_launches(1);
+        return DFEA_OK;
+    });
+    if (rc) return rc;
+    return launch_check("dfea_element_sensitivity");
+}
+
+extern "C" int dfea_axpy(int64_t n, double a, const double* x, double* y, void* stream) {
+    if (n < 0 || (n > 0 && (!x || !y))) return set_error(DFEA_ERR_INVALID, "dfea_axpy: bad arguments");
+    if (n == 0) return DFEA_OK;
+    k_axpy<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, a, x, y);
+    note_launches(1);
+    return launch_check("dfea_axpy");
+}
+
+extern "C" int dfea_add_scaled(int64_t n, const double* a, double alpha, const double* b, double* out, void* stream) {
+    if (n < 0 || (n > 0 && (!a || !b || !out))) return set_error(DFEA_ERR_INVALID, "dfea_add_scaled: bad arguments");
+    if (n == 0) return DFEA_OK;
+    k_add_scaled<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, a, alpha, b, out);
+    note_launches(1);
+    return launch_check("dfea_add_scaled");
+}
+
+extern "C" int dfea_f64_to_f32(int64_t n, const double* x, float* y, void* stream) {
+    if (n < 0 || (n > 0 && (!x || !y))) return set_error(DFEA_ERR_INVALID, "dfea_f64_to_f32: bad arguments");
+    if (n == 0) return DFEA_OK;
+    k_to_f32<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, x, y);
+    note_launches(1);
+    return launch_check("dfea_f64_to_f32");
+}
+
+extern "C" int dfea_f32_to_f64(int64_t n, const float* x, double* y, void* stream) {
+    if (n < 0 || (n > 0 && (!x || !y))) return set_error(DFEA_ERR_INVALID, "dfea_f32_to_f64: bad arguments");
+    if (n == 0) return DFEA_OK;
+    k_to_f64<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, x, y);
+    note_launches(1);
+    return launch_check("dfea_f32_to_f64");
+}

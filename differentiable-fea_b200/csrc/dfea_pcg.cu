@@ -1,0 +1,435 @@
+// dfea_pcg.cu -- kernel (c): Jacobi-preconditioned CG resident on the device.
+//
+// The reference runs PCG in Python with three host synchronisations per iteration
+// (newton_krylov.py:28-88).  Here one iteration is
+//     colour passes of k_apply<DOT>   Ap = A p  and  p.Ap (energy form, per colour, fixed order)
+//     k_pcg_update1                   alpha = rz / pAp;  x += alpha p;  r -= alpha Ap;
+//                                     |r|^2 and r.z with z = r / diag   (z is never stored)
+//     k_pcg_update2                   convergence test; beta; p = z + beta p; Ap := (1 - m) p
+//                                     (the pivot term of the next product); sum of fixed p^2
+//     k_pcg_cond                      sets the condition of the graph's while-loop node
+// captured once in a CUDA graph whose conditional WHILE node repeats it on the device, so that a
+// whole solve is one graph launch and one read-back.  Scalars (rz, |r|^2, status, k) live in a
+// device state block; every reduction is a fixed-order two-level sum (no float atomics).
+//
+// Termination does not depend on the numerics: k_pcg_update2 stops at max_iter and k_pcg_cond keeps
+// an independent execution counter that ends the loop after max_iter + 4 bodies in any case.
+#include <cstring>
+#include <new>
+#include <type_traits>
+
+#include "dfea_apply.cuh"
+#include "dfea_common.cuh"
+
+namespace dfea {
+
+int validate_mesh(const dfea_mesh_view* mv, bool need_grad32);
+
+struct PcgState {
+    double rz;      // r.z of the current iterate
+    double rr;      // |r|^2 after the last update   (result[0] of the update-1 site)
+    double rz_new;  // r.z after the last update     (result[1] of the update-1 site)
+    double norm_b;
+    double rtol;
+    double pfix;    // sum of p^2 over fixed DOFs (identity rows of A)
+    double curv;    // last p.Ap
+    double spare;
+    double curv_c[DFEA_MAX_COLOURS];
+    int32_t k;
+    int32_t max_iter;
+    int32_t done;
+    int32_t iters;
+    int32_t guard;
+    int32_t spare_i[3];
+    unsigned tickets[DFEA_MAX_COLOURS + 8];
+};
+
+// Work buffer: [r | p | Ap] vectors (2N each, 256-byte aligned), partials, state.
+struct PcgLayout {
+    int64_t off_r, off_p, off_y, off_part, off_state, total;
+    PcgLayout(int64_t n_nodes, int vec_bytes, int n_colours) {
+        auto up = [](int64_t x) { return (x + 255) / 256 * 256; };
+        const int64_t vb = up(2 * n_nodes * vec_bytes);
+        off_r = 0;
+        off_p = vb;
+        off_y = 2 * vb;
+        off_part = 3 * vb;
+        const int64_t n_sites = n_colours + 3;
+        off_state = off_part + up(n_sites * 3 * (int64_t)kMaxBlocks * 8);
+        total = off_state + up(sizeof(PcgState));
+    }
+};
+
+__global__ void k_pcg_reset(PcgState* st) {
+    const int i = threadIdx.x;
+    if (i < DFEA_MAX_COLOURS + 8) st->tickets[i] = 0u;
+    if (i < DFEA_MAX_COLOURS) st->curv_c[i] = 0.0;
+    if (i == 0) {
+        st->done = DFEA_PCG_RUNNING;
+        st->k = 0;
+        st->iters = 0;
+        st->guard = 0;
+    }
+}
+
+// x = 0, r = b, z = b / d, p = z, Ap := (1 - m) p;  rz = r.z, |b|, pfix.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_pcg_setup(Mesh m, const T* __restrict__ b, const T* __restrict__ d, T* __restrict__ x, T* __restrict__ r,
+            T* __restrict__ p, T* __restrict__ y, PcgState* st, RedSite site, double rtol, int max_iter) {
+    using T2 = v2_t<T>;
+    double rz = 0.0, bb = 0.0, pf = 0.0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fix = m.node_fix[n];
+        const T2 bn = reinterpret_cast<const T2*>(b)[n];
+        const T2 dn = reinterpret_cast<const T2*>(d)[n];
+        const T zx = bn.x / dn.x, zy = bn.y / dn.y;
+        reinterpret_cast<T2*>(x)[n] = make_v2<T>(T(0), T(0));
+        reinterpret_cast<T2*>(r)[n] = bn;
+        reinterpret_cast<T2*>(p)[n] = make_v2<T>(zx, zy);
+        reinterpret_cast<T2*>(y)[n] = make_v2<T>((fix & 1) ? zx : T(0), (fix & 2) ? zy : T(0));
+        rz += (double)bn.x * zx + (double)bn.y * zy;
+        bb += (double)bn.x * bn.x + (double)bn.y * bn.y;
+        if (fix & 1) pf += (double)zx * zx;
+        if (fix & 2) pf += (double)zy * zy;
+    }
+    const double vals[3] = {block_sum<kThreads>(rz), block_sum<kThreads>(bb), block_sum<kThreads>(pf)};
+    double tot[3];
+    if (last_block_sum<kThreads, 3>(vals, site, tot) && threadIdx.x == 0) {
+        st->rz = tot[0];
+        st->norm_b = sqrt(tot[1]);
+        st->pfix = tot[2];
+        st->rtol = rtol;
+        st->max_iter = max_iter;
+        st->k = 0;
+        st->iters = 0;
+        st->guard = 0;
+        st->done = (st->norm_b == 0.0) ? DFEA_PCG_ZERO_RHS : DFEA_PCG_RUNNING;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restrict__ y, const T* __restrict__ d,
+              T* __restrict__ x, T* __restrict__ r, PcgState* st, RedSite site) {
+    using T2 = v2_t<T>;
+    if (st->done) return;
+    double curv = st->pfix;
+    for (int c = 0; c < n_colours; ++c) curv += st->curv_c[c];
+    const int k = st->k;
+    if (curv <= 0.0) {
+        // not SPD along p: return z at k = 0 and x otherwise (newton_krylov.py:69-70)
+        if (k == 0) {
+            for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+                const T2 rn = reinterpret_cast<const T2*>(r)[n];
+                const T2 dn = reinterpret_cast<const T2*>(d)[n];
+                reinterpret_cast<T2*>(x)[n] = make_v2<T>(rn.x / dn.x, rn.y / dn.y);
+            }
+        }
+        const double vals[1] = {0.0};
+        double tot[1];
+        if (last_block_sum<kThreads, 1>(vals, site, tot) && threadIdx.x == 0) {
+            st->curv = curv;
+            st->iters = k;
+            st->done = DFEA_PCG_NEG_CURV;
+        }
+        return;
+    }
+    const double alpha = st->rz / curv;
+    const T a = (T)alpha;
+    double rr = 0.0, rz = 0.0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const T2 pn = reinterpret_cast<const T2*>(p)[n];
+        const T2 yn = reinterpret_cast<const T2*>(y)[n];
+        const T2 dn = reinterpret_cast<const T2*>(d)[n];
+        T2 xn = reinterpret_cast<const T2*>(x)[n];
+        T2 rn = reinterpret_cast<const T2*>(r)[n];
+        xn.x += a * pn.x;
+        xn.y += a * pn.y;
+        rn.x -= a * yn.x;
+        rn.y -= a * yn.y;
+        reinterpret_cast<T2*>(x)[n] = xn;
+        reinterpret_cast<T2*>(r)[n] = rn;
+        rr += (double)rn.x * rn.x + (double)rn.y * rn.y;
+        rz += (double)rn.x * (rn.x / dn.x) + (double)rn.y * (rn.y / dn.y);
+    }
+    const double vals[2] = {block_sum<kThreads>(rr), block_sum<kThreads>(rz)};
+    double tot[2];
+    if (last_block_sum<kThreads, 2>(vals, site, tot) && threadIdx.x == 0) {
+        st->rr = tot[0];
+        st->rz_new = tot[1];
+        st->curv = curv;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __restrict__ p, T* __restrict__ y,
+              PcgState* st, RedSite site) {
+    using T2 = v2_t<T>;
+    if (st->done) return;
+    const int k = st->k;
+    if (sqrt(st->rr) <= st->rtol * st->norm_b) {
+        // converged: ||r|| <= rtol ||b||  (newton_krylov.py:77-79)
+        const double vals[1] = {0.0};
+        double tot[1];
+        if (last_block_sum<kThreads, 1>(vals, site, tot) && threadIdx.x == 0) {
+            st->iters = k + 1;
+            st->done = DFEA_PCG_CONVERGED;
+        }
+        return;
+    }
+    const double beta = st->rz_new / st->rz;
+    const T bt = (T)beta;
+    double pf = 0.0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fix = m.node_fix[n];
+        const T2 rn = reinterpret_cast<const T2*>(r)[n];
+        const T2 dn = reinterpret_cast<const T2*>(d)[n];
+        T2 pn = reinterpret_cast<const T2*>(p)[n];
+        pn.x = rn.x / dn.x + bt * pn.x;
+        pn.y = rn.y / dn.y + bt * pn.y;
+        reinterpret_cast<T2*>(p)[n] = pn;
+        reinterpret_cast<T2*>(y)[n] = make_v2<T>((fix & 1) ? pn.x : T(0), (fix & 2) ? pn.y : T(0));
+        if (fix & 1) pf += (double)pn.x * pn.x;
+        if (fix & 2) pf += (double)pn.y * pn.y;
+    }
+    const double vals[1] = {block_sum<kThreads>(pf)};
+    double tot[1];
+    if (last_block_sum<kThreads, 1>(vals, site, tot) && threadIdx.x == 0) {
+        st->rz = st->rz_new;
+        st->pfix = tot[0];
+        st->k = k + 1;
+        if (k + 1 >= st->max_iter) {
+            st->iters = st->max_iter;
+            st->done = DFEA_PCG_MAX_ITER;
+        }
+    }
+}
+
+__global__ void k_pcg_cond(PcgState* st, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0) return;
+    const int g = ++st->guard;
+    if (st->done == DFEA_PCG_RUNNING && g >= st->max_iter + 4) {
+        st->iters = st->max_iter;
+        st->done = DFEA_PCG_MAX_ITER;
+    }
+    cudaGraphSetConditional(h, st->done == DFEA_PCG_RUNNING ? 1u : 0u);
+}
+
+}  // namespace dfea
+
+using namespace dfea;
+
+struct dfea_pcg {
+    dfea_mesh_view mesh;
+    const void* moduli;
+    const void* diag;
+    const void* b;
+    void* x;
+    int vec_dtype;
+    char* work;
+    PcgLayout layout{1, 8, 1};
+    int use_graph;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int32_t* host_status = nullptr;  // pinned: [done, iters]
+
+    PcgState* state() const { return reinterpret_cast<PcgState*>(work + layout.off_state); }
+    RedSite site(int i, int k_slot_results) const {
+        double* parts = reinterpret_cast<double*>(work + layout.off_part) + (int64_t)i * 3 * kMaxBlocks;
+        PcgState* st = state();
+        (void)k_slot_results;
+        double* res = nullptr;
+        if (i < mesh.n_colours) res = st->curv_c + i;          // colour curvature
+        else if (i == mesh.n_colours) res = &st->rr;            // update 1: rr, rz_new
+        return RedSite{parts, st->tickets + i, res};
+    }
+};
+
+namespace {
+
+template <typename T>
+int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHandle cond, bool with_cond) {
+    const dfea_mesh_view& mv = h.mesh;
+    const Mesh m = kernel_mesh(mv);
+    const T* C = static_cast<const T*>(h.moduli);
+    const T* G = std::is_same<T, float>::value ? reinterpret_cast<const T*>(mv.grad32) : reinterpret_cast<const T*>(mv.grad);
+    T* r = reinterpret_cast<T*>(h.work + h.layout.off_r);
+    T* p = reinterpret_cast<T*>(h.work + h.layout.off_p);
+    T* y = reinterpret_cast<T*>(h.work + h.layout.off_y);
+    const T* d = static_cast<const T*>(h.diag);
+    T* x = static_cast<T*>(h.x);
+    PcgState* st = h.state();
+    RedSite sites[DFEA_MAX_COLOURS];
+    for (int c = 0; c < mv.n_colours; ++c) sites[c] = h.site(c, 1);
+    int rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        return launch_apply_colours<NEN, NQ, T, true>(mv, C, G, p, y, sites, &st->done, s, !with_cond);
+    });
+    if (rc) return rc;
+    const int gn = grid_for(mv.n_nodes, kThreads, 4);
+    k_pcg_update1<T><<<gn, kThreads, 0, s>>>(m, mv.n_colours, p, y, d, x, r, st, h.site(mv.n_colours, 2));
+    k_pcg_update2<T><<<gn, kThreads, 0, s>>>(m, r, d, p, y, st, h.site(mv.n_colours + 1, 1));
+    if (with_cond) k_pcg_cond<<<1, 32, 0, s>>>(st, cond);
+    else note_launches(2);  // graph-captured kernels are counted when the graph's solve returns
+    return launch_check("pcg iteration");
+}
+
+template <typename T>
+int launch_setup(const dfea_pcg& h, cudaStream_t s, double rtol, int max_iter) {
+    const dfea_mesh_view& mv = h.mesh;
+    const Mesh m = kernel_mesh(mv);
+    T* r = reinterpret_cast<T*>(h.work + h.layout.off_r);
+    T* p = reinterpret_cast<T*>(h.work + h.layout.off_p);
+    T* y = reinterpret_cast<T*>(h.work + h.layout.off_y);
+    PcgState* st = h.state();
+    k_pcg_reset<<<1, 128, 0, s>>>(st);
+    k_pcg_setup<T><<<grid_for(mv.n_nodes, kThreads, 4), kThreads, 0, s>>>(
+        m, static_cast<const T*>(h.b), static_cast<const T*>(h.diag), static_cast<T*>(h.x), r, p, y, st,
+        h.site(mv.n_colours + 2, 3), rtol, max_iter);
+    note_launches(2);
+    return launch_check("pcg setup");
+}
+
+int build_graph(dfea_pcg* h) {
+    int rc;
+    if ((rc = check_cuda(cudaGraphCreate(&h->graph, 0), "cudaGraphCreate"))) return rc;
+    cudaGraphConditionalHandle cond;
+    if ((rc = check_cuda(cudaGraphConditionalHandleCreate(&cond, h->graph, 1u, cudaGraphCondAssignDefault),
+                         "cudaGraphConditionalHandleCreate")))
+        return rc;
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};  // aggregate init: the rest is zero
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if ((rc = check_cuda(cudaGraphAddNode(&node, h->graph, nullptr, 0, &cp), "cudaGraphAddNode(while)"))) return rc;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if ((rc = check_cuda(cudaStreamBeginCaptureToGraph(h->capture_stream, body, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal),
+                         "cudaStreamBeginCaptureToGraph")))
+        return rc;
+    rc = (h->vec_dtype == DFEA_F64) ? launch_iteration<double>(*h, h->capture_stream, cond, true)
+                                    : launch_iteration<float>(*h, h->capture_stream, cond, true);
+    cudaGraph_t captured = body;
+    const int rc_end = check_cuda(cudaStreamEndCapture(h->capture_stream, &captured), "cudaStreamEndCapture");
+    if (rc) return rc;
+    if (rc_end) return rc_end;
+    return check_cuda(cudaGraphInstantiate(&h->exec, h->graph, 0), "cudaGraphInstantiate");
+}
+
+void release(dfea_pcg* h) {
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
+    if (h->host_status) cudaFreeHost(h->host_status);
+    delete h;
+}
+
+}  // namespace
+
+extern "C" int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype) {
+    if (!mesh || (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32)) return -1;
+    return PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F64 ? 8 : 4, mesh->n_colours).total;
+}
+
+extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, const void* diag, const void* b,
+                               void* x, int32_t vec_dtype, void* work, int32_t use_graph, dfea_pcg** out) {
+    if (!out) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: out is NULL");
+    *out = nullptr;
+    int rc = validate_mesh(mesh, vec_dtype == DFEA_F32);
+    if (rc) return rc;
+    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
+    if (!moduli || !diag || !b || !x || !work) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: NULL pointer");
+    auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 255u) == 0; };
+    auto al16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    if (!al(work)) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: work must be 256-byte aligned");
+    if (!al16(moduli) || !al16(diag) || !al16(b) || !al16(x))
+        return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: moduli, diag, b and x must be 16-byte aligned");
+    if (x == b) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: x must not alias b");
+
+    dfea_pcg* h = new (std::nothrow) dfea_pcg;
+    if (!h) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: out of host memory");
+    h->mesh = *mesh;
+    h->moduli = moduli;
+    h->diag = diag;
+    h->b = b;
+    h->x = x;
+    h->vec_dtype = vec_dtype;
+    h->work = static_cast<char*>(work);
+    h->layout = PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F64 ? 8 : 4, mesh->n_colours);
+    h->use_graph = use_graph ? 1 : 0;
+    (void)device_sm_count();  // cache the device query before any stream capture
+    if ((rc = check_cuda(cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (rc = check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&h->host_status), 4 * sizeof(int32_t), cudaHostAllocDefault),
+                         "cudaHostAlloc"))) {
+        release(h);
+        return rc;
+    }
+    // zero the partial sums, tickets and state once (later solves reset what they use)
+    if ((rc = check_cuda(cudaMemsetAsync(h->work + h->layout.off_part, 0, h->layout.total - h->layout.off_part,
+                                         h->capture_stream), "cudaMemsetAsync")) ||
+        (rc = check_cuda(cudaStreamSynchronize(h->capture_stream), "cudaStreamSynchronize"))) {
+        release(h);
+        return rc;
+    }
+    if (h->use_graph && (rc = build_graph(h))) {
+        release(h);
+        return rc;
+    }
+    *out = h;
+    return DFEA_OK;
+}
+
+extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_t* iters, int32_t* status,
+                              void* stream) {
+    if (!h) return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve: NULL handle");
+    if (max_iter < 1 || max_iter > 100000000) return set_error(DFEA_ERR_INVALID, "max_iter %d out of [1, 1e8]", max_iter);
+    if (!(rtol >= 0.0)) return set_error(DFEA_ERR_INVALID, "rtol must be >= 0");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = (h->vec_dtype == DFEA_F64) ? launch_setup<double>(*h, s, rtol, max_iter)
+                                        : launch_setup<float>(*h, s, rtol, max_iter);
+    if (rc) return rc;
+    PcgState* st = h->state();
+    if (h->use_graph) {
+        if ((rc = check_cuda(cudaGraphLaunch(h->exec, s), "cudaGraphLaunch"))) return rc;
+        if ((rc = check_cuda(cudaMemcpyAsync(h->host_status, &st->done, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+                             "cudaMemcpyAsync")) ||
+            (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+            return rc;
+        // each executed body ran the non-empty colour passes, two updates and the loop condition
+        int nonempty = 0;
+        for (int c = 0; c < h->mesh.n_colours; ++c) nonempty += h->mesh.colour_begin[c + 1] > h->mesh.colour_begin[c];
+        note_launches((long long)h->host_status[2] * (nonempty + 3));
+    } else {
+        // the same kernels launched directly; the host reads the status every 16 iterations
+        const int chunk = 16;
+        int launched = 0;
+        h->host_status[0] = DFEA_PCG_RUNNING;
+        while (true) {
+            for (int i = 0; i < chunk; ++i) {
+                rc = (h->vec_dtype == DFEA_F64) ? launch_iteration<double>(*h, s, 0, false)
+                                                : launch_iteration<float>(*h, s, 0, false);
+                if (rc) return rc;
+            }
+            launched += chunk;
+            if ((rc = check_cuda(cudaMemcpyAsync(h->host_status, &st->done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+                                 "cudaMemcpyAsync")) ||
+                (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+                return rc;
+            if (h->host_status[0] != DFEA_PCG_RUNNING || launched > max_iter + chunk) break;
+        }
+    }
+    if (h->host_status[0] == DFEA_PCG_RUNNING)
+        return set_error(DFEA_ERR_INVALID, "PCG ended without a status (internal error)");
+    if (status) *status = h->host_status[0];
+    if (iters) *iters = h->host_status[1];
+    return DFEA_OK;
+}
+
+extern "C" int dfea_pcg_destroy(dfea_pcg* h) {
+    if (h) release(h);
+    return DFEA_OK;
+}

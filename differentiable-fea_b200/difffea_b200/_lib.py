@@ -1,0 +1,102 @@
+"""
+ctypes binding of libdifffea_b200.so (the C ABI declared in include/difffea_b200.h).
+
+The library is built in-tree by ``differentiable-fea_b200/build.py``.  There is no fallback: if it is
+missing or does not load, every compute entry point raises ``RuntimeError`` -- the package never
+computes on the CPU or through another implementation behind the caller's back.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libdifffea_b200.so")
+
+DFEA_OK = 0
+DFEA_F64 = 0
+DFEA_F32 = 1
+MAX_COLOURS = 64
+
+PCG_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "negative_curvature", 4: "zero_rhs"}
+
+c_i32, c_i64, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+
+class MeshView(ctypes.Structure):
+    """Mirror of ``dfea_mesh_view``."""
+    _fields_ = [
+        ("n_el", c_i64), ("stride", c_i64), ("n_nodes", c_i64),
+        ("nen", c_i32), ("n_q", c_i32), ("n_colours", c_i32), ("reserved", c_i32),
+        ("colour_begin", c_i64 * (MAX_COLOURS + 1)),
+        ("conn", c_vp), ("orig", c_vp), ("grad", c_vp), ("wdet", c_vp), ("grad32", c_vp), ("node_fix", c_vp),
+    ]
+
+
+_PROTOS = {
+    "dfea_last_error": (ctypes.c_char_p, []),
+    "dfea_version": (ctypes.c_int, []),
+    "dfea_launch_count": (c_i64, []),
+    "dfea_element_supported": (ctypes.c_int, [c_i32, c_i32]),
+    "dfea_colour_elements": (ctypes.c_int, [c_vp, c_i64, c_i32, c_i64, c_vp, c_vp]),
+    "dfea_mesh_pack": (ctypes.c_int, [c_i64, c_i64, c_i32, c_i32, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                      c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "dfea_mesh_grad_to_f32": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp]),
+    "dfea_qp_moduli": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp, c_vp]),
+    "dfea_tangent_apply": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_i32, c_vp, c_vp, c_i32, c_vp]),
+    "dfea_reduce_work_bytes": (c_i64, [ctypes.POINTER(MeshView)]),
+    "dfea_residual": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_f64, c_vp, c_vp,
+                                     c_vp, c_vp, c_vp]),
+    "dfea_vec_norm2": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp]),
+    "dfea_element_sensitivity": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_vp]),
+    "dfea_pcg_work_bytes": (c_i64, [ctypes.POINTER(MeshView), c_i32]),
+    "dfea_pcg_create": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_i32,
+                                       ctypes.POINTER(c_vp)]),
+    "dfea_pcg_solve": (ctypes.c_int, [c_vp, c_f64, c_i32, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_vp]),
+    "dfea_pcg_destroy": (ctypes.c_int, [c_vp]),
+    "dfea_axpy": (ctypes.c_int, [c_i64, c_f64, c_vp, c_vp, c_vp]),
+    "dfea_add_scaled": (ctypes.c_int, [c_i64, c_vp, c_f64, c_vp, c_vp, c_vp]),
+    "dfea_f64_to_f32": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp]),
+    "dfea_f32_to_f64": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp]),
+}
+
+_lib = None
+_load_error = None
+
+
+def exported_symbols():
+    """Names of the C entry points this binding expects (the declarations of include/difffea_b200.h)."""
+    return sorted(_PROTOS)
+
+
+def load():
+    """Load the library once; raise RuntimeError with the reason if it is not there."""
+    global _lib, _load_error
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        _load_error = (f"{LIB_PATH} is missing: build it with `python differentiable-fea_b200/build.py` "
+                       "(the CUDA kernels have no fallback)")
+        raise RuntimeError(_load_error)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _PROTOS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error():
+    return load().dfea_last_error().decode(errors="replace")
+
+
+def check(rc, what):
+    """Raise RuntimeError for a non-zero return code of a C entry point."""
+    if rc != DFEA_OK:
+        raise RuntimeError(f"{what} failed (code {rc}): {last_error()}")
+
+
+def call(name, *args):
+    """Call a C entry point by name and check its return code."""
+    rc = getattr(load(), name)(*args)
+    check(rc, name)
+    return rc

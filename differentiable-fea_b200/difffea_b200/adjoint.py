@@ -1,0 +1,30 @@
+"""
+Adjoint sensitivities on the GPU (the reference's adjoint.py API).
+
+    solve_adjoint(u_star, theta, params, dL_du, rtol=1e-6, max_iter=500)      adjoint.py:31-69
+    compute_implicit_vjp(u_star, theta, params, lambda_adj)                     adjoint.py:75-106
+
+The adjoint system A^T lambda = m * dL/du is solved by the device PCG with the stored-moduli operator
+(the hyperelastic tangent is symmetric, so A^T = A).  The implicit VJP  dL/dtheta = -lambda^T dR/dtheta
+is kernel (d): one thread per element evaluates f_e(u*; mu0, lambda0) and contracts it with the masked
+adjoint, which is exact because R_int is linear in theta_e.
+"""
+import torch
+
+from difffea_b200 import ops
+from difffea_b200.newton_krylov import pcg
+from difffea_b200.operators import _f64c, _prepare, make_AT_operator, make_jacobi_preconditioner
+
+
+def solve_adjoint(u_star, theta, params, dL_du, rtol=1e-6, max_iter=500):
+    """(lambda (2N,), PCG iterations) of A^T lambda = m * dL/du at the converged state u_star."""
+    AT = make_AT_operator(u_star, theta, params)
+    Minv = make_jacobi_preconditioner(u_star, theta, params)
+    b = (params["m"] * dL_du).to(torch.float64).contiguous()
+    return pcg(AT, b, Minv, rtol=rtol, max_iter=max_iter)
+
+
+def compute_implicit_vjp(u_star, theta, params, lambda_adj):
+    """dL/dtheta (n_el,) = -lambda^T dR/dtheta (theta enters linearly, so no theta dependence remains)."""
+    mesh, mid, mu0, lam0 = _prepare(u_star, theta, params)
+    return ops.element_sensitivity(mid, _f64c(u_star), _f64c(lambda_adj), mu0, lam0)

@@ -1,0 +1,48 @@
+"""
+Differentiable equilibrium: u*(theta) as a torch.autograd.Function whose backward is the adjoint.
+
+    u = equilibrium(theta, params, **solver_options)      forward: device Newton-Krylov solve
+    L = compliance(theta, params, **solver_options)       f . u*(theta)
+    L.backward()                                          theta.grad = dL/dtheta by the adjoint kernels
+
+The backward pass receives dL/du*, solves A^T lambda = m * dL/du* with the device PCG at u* and returns
+-lambda^T dR/dtheta from the per-element sensitivity kernel.  No graph of the Newton iterations is
+recorded.  (The reference removed its class-based autograd bridge in favour of compute_sensitivity,
+adjoint.py:18-20; this restores the torch.autograd interface on top of the same mathematics.)
+"""
+import torch
+
+from difffea_b200.adjoint import compute_implicit_vjp, solve_adjoint
+from difffea_b200.newton_krylov import solve_newton_krylov
+
+
+class EquilibriumSolve(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, theta, params, options):
+        opts = dict(options)
+        adj = {k: opts.pop(k) for k in ("adjoint_rtol", "adjoint_max_iter") if k in opts}
+        opts.setdefault("verbose", False)
+        u = solve_newton_krylov(params, theta.detach(), **opts)
+        ctx.save_for_backward(theta.detach(), u)
+        ctx.params = params
+        ctx.adjoint = adj
+        return u
+
+    @staticmethod
+    def backward(ctx, grad_u):
+        theta, u = ctx.saved_tensors
+        lam, iters = solve_adjoint(u, theta, ctx.params, grad_u.contiguous(),
+                                   rtol=ctx.adjoint.get("adjoint_rtol", 1e-10),
+                                   max_iter=ctx.adjoint.get("adjoint_max_iter", 500))
+        ctx.adjoint_iterations = iters
+        return compute_implicit_vjp(u, theta, ctx.params, lam).to(theta.dtype), None, None
+
+
+def equilibrium(theta, params, **options):
+    """u*(theta), differentiable w.r.t. theta through the adjoint."""
+    return EquilibriumSolve.apply(theta, params, options)
+
+
+def compliance(theta, params, **options):
+    """L(theta) = f . u*(theta), differentiable w.r.t. theta."""
+    return torch.dot(params["f"].to(torch.float64), equilibrium(theta, params, **options))

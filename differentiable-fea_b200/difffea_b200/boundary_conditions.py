@@ -1,0 +1,68 @@
+"""
+Boundary selection, DOF masks and consistent edge loads (host set-up).
+
+Same semantics as the reference's builders (boundary_conditions.py:141-277): nodes on a side of the
+bounding box within a relative tolerance; node-major DOFs (dof = 2 * node + component); boundary edges
+are the edges that belong to exactly one element, kept in element order; a uniform traction whose
+total is given is integrated against the edge shape functions with a 3-point Gauss rule (work-
+equivalent nodal forces).
+"""
+import torch
+
+from difffea_b200.elements import edge_shape, gauss_1d
+
+
+def select_boundary_nodes(nodes, side, tol=1e-6):
+    """(N,) bool mask of the nodes on side "left" | "right" | "bottom" | "top" of the bounding box."""
+    x, y = nodes[:, 0], nodes[:, 1]
+    eps = tol * torch.max(x.max() - x.min(), y.max() - y.min())
+    if side == "left":
+        return x <= x.min() + eps
+    if side == "right":
+        return x >= x.max() - eps
+    if side == "bottom":
+        return y <= y.min() + eps
+    if side == "top":
+        return y >= y.max() - eps
+    raise ValueError("side must be 'left', 'right', 'bottom' or 'top'")
+
+
+def dofs_from_node_mask(node_mask, components=(0, 1)):
+    """Expand a node mask (N,) to a DOF mask (2N,) for the given components (0 = x, 1 = y)."""
+    out = torch.zeros(node_mask.shape[0], 2, dtype=torch.bool, device=node_mask.device)
+    for c in components:
+        out[:, c] = node_mask
+    return out.reshape(-1)
+
+
+def boundary_edges(conn, edge_local_nodes):
+    """Edges used by exactly one element, as (E, k) global node ids [start, end(, mid)], element order."""
+    k = len(edge_local_nodes[0])
+    all_edges = conn[:, torch.tensor(edge_local_nodes, device=conn.device)].reshape(-1, k)
+    lo = torch.minimum(all_edges[:, 0], all_edges[:, 1])
+    hi = torch.maximum(all_edges[:, 0], all_edges[:, 1])
+    key = lo * (int(conn.max()) + 1) + hi
+    _, inverse, counts = torch.unique(key, return_inverse=True, return_counts=True)
+    return all_edges[counts[inverse] == 1]
+
+
+def edge_traction_load(nodes, edges, order, node_mask, total_force, n_gauss=3):
+    """
+    Consistent nodal forces (N, 2) of a uniform traction of total (Fx, Fy) on the boundary edges whose
+    nodes all lie in ``node_mask``; ``order`` is the edge interpolation order (1 or 2).
+    """
+    dtype, device = nodes.dtype, nodes.device
+    f = torch.zeros_like(nodes)
+    edges = edges[node_mask[edges].all(dim=1)]
+    if edges.shape[0] == 0:
+        return f
+    s, w = gauss_1d(n_gauss, dtype, device)
+    N, dN = edge_shape(order, s)                                   # (g, k)
+    Xe = nodes[edges]                                              # (E, k, 2)
+    tangent = torch.einsum("gk,ekd->egd", dN, Xe)                  # dX/ds at every Gauss point
+    speed = torch.linalg.norm(tangent, dim=-1)                     # (E, g)
+    length = torch.einsum("eg,g->", speed, w)
+    t = torch.as_tensor(total_force, dtype=dtype, device=device) / length
+    f_edge = torch.einsum("g,ga,eg,i->eai", w, N, speed, t)        # (E, k, 2)
+    f.index_add_(0, edges.reshape(-1), f_edge.reshape(-1, 2))
+    return f

@@ -1,0 +1,68 @@
+"""
+Device-resident Jacobi-PCG (kernel (c)) bound to fixed buffers.
+
+``DevicePCG`` owns a ``dfea_pcg`` handle: one PCG iteration (the colour passes of the tangent product
+with the curvature fused in, two fused vector-update kernels, the loop condition) captured once in a
+CUDA graph with a device-side while-loop, so a whole solve is one graph launch and one read-back of
+(status, iterations).  The buffers it binds (moduli, diagonal, right-hand side, solution and a work
+area for the Krylov vectors and partial sums) stay allocated for the life of the object; their
+contents may change between solves.
+"""
+import ctypes
+import warnings
+
+import torch
+
+from difffea_b200 import _lib
+from difffea_b200.cuda_mesh import ptr, stream_handle
+
+
+class DevicePCG:
+    def __init__(self, mesh, C, diag, b, x, use_graph=True):
+        dt = _lib.DFEA_F64 if C.dtype == torch.float64 else _lib.DFEA_F32
+        vt = torch.float64 if dt == _lib.DFEA_F64 else torch.float32
+        for name, t in (("diag", diag), ("b", b), ("x", x)):
+            if t.dtype != vt or t.numel() != mesh.n_dof or not t.is_contiguous() or t.device != mesh.device:
+                raise ValueError(f"{name} must be a contiguous ({mesh.n_dof},) {vt} tensor on {mesh.device}")
+        if dt == _lib.DFEA_F32:
+            mesh.ensure_grad32()
+        self.mesh, self.C, self.diag, self.b, self.x = mesh, C, diag, b, x
+        self.vec_dtype = vt
+        nbytes = int(_lib.load().dfea_pcg_work_bytes(mesh.view_ref, dt))
+        self.work = torch.empty(nbytes, dtype=torch.uint8, device=mesh.device)
+        self._h = ctypes.c_void_p(0)
+        with torch.cuda.device(mesh.device):
+            # the handle zeroes its work area on an internal stream: order it after torch's stream
+            torch.cuda.current_stream().synchronize()
+            rc = _lib.load().dfea_pcg_create(mesh.view_ref, ptr(C), ptr(diag), ptr(b), ptr(x), dt, ptr(self.work),
+                                             1 if use_graph else 0, ctypes.byref(self._h))
+            if rc != _lib.DFEA_OK and use_graph:
+                # the conditional-graph path could not be built on this device/driver: same kernels,
+                # launched directly (host-polled), rather than failing the solve
+                warnings.warn(f"PCG graph unavailable ({_lib.last_error()}); using direct launches")
+                use_graph = False
+                rc = _lib.load().dfea_pcg_create(mesh.view_ref, ptr(C), ptr(diag), ptr(b), ptr(x), dt,
+                                                 ptr(self.work), 0, ctypes.byref(self._h))
+            _lib.check(rc, "dfea_pcg_create")
+        self.use_graph = use_graph
+        self.last_status = None
+
+    def solve(self, rtol, max_iter=500):
+        """Run PCG on the bound buffers; returns (iterations, status string).  Blocks until done."""
+        iters, status = ctypes.c_int32(0), ctypes.c_int32(0)
+        with torch.cuda.device(self.mesh.device):
+            _lib.call("dfea_pcg_solve", self._h, float(rtol), int(max_iter), ctypes.byref(iters), ctypes.byref(status),
+                      stream_handle())
+        self.last_status = _lib.PCG_STATUS.get(status.value, str(status.value))
+        return iters.value, self.last_status
+
+    def close(self):
+        if self._h and self._h.value:
+            _lib.load().dfea_pcg_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

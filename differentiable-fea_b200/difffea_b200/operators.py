@@ -1,0 +1,200 @@
+"""
+Residual, tangent-operator and preconditioner closures on the GPU (the reference's operators.py API).
+
+    global_residual(u, theta, params, load_factor=1.0)          operators.py:159-220
+    make_tangent_operator(kind, u, theta, params)               operators.py:415-435, kind "cuda" / "auto"
+    make_AT_operator(u, theta, params)                          operators.py:441-471
+    compute_jacobi_diagonal / make_jacobi_preconditioner        operators.py:477-570
+    make_preconditioner(kind, u, theta, params)                 operators.py:702-710, kind "jacobi"
+    precompute_geometry(params)                                 operators.py:85-120
+
+Every closure has the reference's semantics -- A(v) = m * J(u)(m * v) + (1 - m) * v, symmetric, the
+identity on fixed DOFs -- and runs on the device of ``u`` through the kernels of libdifffea_b200.so.
+``"cuda"`` is the stored-moduli variant: kernel (a) evaluates the Gauss-point moduli C once per
+linearisation point, kernel (b) applies them.  The reference's own variants (jvp, linearize, qp, qp_ew)
+are PyTorch programs of the reference package and are not re-implemented here.
+"""
+import weakref
+
+import torch
+
+from difffea_b200 import ops
+from difffea_b200.cuda_mesh import _require_cuda, cuda_mesh
+from difffea_b200.materials import neo_hookean_parameters
+from difffea_b200.problem import precompute_geometry  # noqa: F401  (re-exported, as in the reference)
+
+TANGENT_OPERATORS = ("auto", "cuda")
+REFERENCE_TANGENT_VARIANTS = ("jvp", "linearize", "qp", "qp_ew")
+PRECONDITIONERS = ("jacobi",)
+
+
+def _prepare(u, theta, params):
+    _require_cuda(u, theta)
+    mesh = cuda_mesh(params)
+    if u.device != mesh.device:
+        raise RuntimeError("u and params must be on the same device")
+    mu0, lam0 = neo_hookean_parameters(params)
+    return mesh, ops.register_mesh(mesh), mu0, lam0
+
+
+def _f64c(t):
+    return t.detach().to(torch.float64).contiguous()
+
+
+# ---------------------------------------------------------------------------------------------
+# residual
+# ---------------------------------------------------------------------------------------------
+def global_residual(u, theta, params, load_factor=1.0):
+    """R(u) = m * (R_int(u, theta) - load_factor * f), shape (2N,)."""
+    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    R, _, _ = ops.residual(mid, _f64c(u), _f64c(theta), mu0, lam0, _f64c(params["f"]), float(load_factor))
+    return R
+
+
+def residual_and_norm(u, theta, params, load_factor=1.0):
+    """(R, ||R||) with the norm reduced on the device in fixed order (one scalar read-back)."""
+    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    R, n2, _ = ops.residual(mid, _f64c(u), _f64c(theta), mu0, lam0, _f64c(params["f"]), float(load_factor))
+    return R, float(n2) ** 0.5
+
+
+def strain_energy(u, theta, params):
+    """Total strain energy sum_e sum_q w detJ psi(F), the ``strain_energy`` of compute_fields."""
+    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    _, _, W = ops.residual(mid, _f64c(u), _f64c(theta), mu0, lam0, _f64c(params["f"]), 0.0)
+    return W
+
+
+# ---------------------------------------------------------------------------------------------
+# tangent operator
+# ---------------------------------------------------------------------------------------------
+class CudaTangentOperator:
+    """
+    v -> A(v) from moduli stored at the Gauss points (kernel (b)).  Holds the moduli C of its
+    linearisation point and the Jacobi diagonal computed in the same pass of kernel (a).
+    """
+
+    def __init__(self, mesh, mesh_id, C, diag, precision="fp64"):
+        self.mesh, self.mesh_id, self.C, self.diag, self.precision = mesh, mesh_id, C, diag, precision
+        self._pcg = None
+        self._pcg_diag_src = None
+        self.last_status = None
+
+    def __call__(self, v):
+        if v.dtype != self.C.dtype:
+            raise ValueError(f"this operator applies {self.C.dtype} vectors, got {v.dtype}")
+        return ops.tangent_apply(self.mesh_id, self.C, v.contiguous())
+
+    @property
+    def dtype(self):
+        return self.C.dtype
+
+    def pcg_solve(self, b, diag, rtol, max_iter):
+        """Jacobi-PCG on the device (kernel (c)) with this operator; returns (x in b's dtype, iterations)."""
+        from difffea_b200.krylov import DevicePCG
+        vt = self.C.dtype
+        if self._pcg is None or self._pcg_diag_src is not diag:
+            d = diag.detach().to(vt).contiguous()
+            n = self.mesh.n_dof
+            bb = torch.empty(n, dtype=vt, device=self.mesh.device)
+            xx = torch.empty(n, dtype=vt, device=self.mesh.device)
+            if self._pcg is not None:
+                self._pcg.close()
+            self._pcg = DevicePCG(self.mesh, self.C, d, bb, xx)
+            self._pcg_diag_src = diag
+        self._pcg.b.copy_(b)
+        iters, status = self._pcg.solve(rtol, max_iter)
+        self.last_status = status
+        return self._pcg.x.to(b.dtype, copy=True), iters
+
+
+# (weakref(u), u._version, weakref(theta), theta._version, mesh id) -> diag of the last linearisation,
+# so that make_preconditioner right after make_tangent_operator at the same point reuses kernel (a)'s pass
+_LAST_DIAG = {}
+
+
+def _diag_key(u, theta, mesh):
+    return (id(u), u._version, id(theta), theta._version, id(mesh))
+
+
+def make_A_operator_cuda(u, theta, params, precision="fp64"):
+    """The stored-moduli tangent operator at (u, theta); precision "fp64" or "fp32" (moduli and vectors)."""
+    if precision not in ("fp64", "fp32"):
+        raise ValueError("precision must be 'fp64' or 'fp32'")
+    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    if precision == "fp32":
+        mesh.ensure_grad32()
+    C, diag = ops.qp_moduli(mid, _f64c(u), _f64c(theta), mu0, lam0, precision == "fp32", True)
+    _LAST_DIAG.clear()
+    _LAST_DIAG[_diag_key(u, theta, mesh)] = (weakref.ref(u), weakref.ref(theta), diag)
+    return CudaTangentOperator(mesh, mid, C, diag, precision)
+
+
+def make_tangent_operator(kind, u, theta, params):
+    """
+    Build the forward tangent operator by name: one of ``TANGENT_OPERATORS``.  "auto" picks "cuda"
+    for CUDA tensors (the reference picks qp_ew there and qp on the CPU; its CPU variants stay in the
+    reference package).
+    """
+    if kind == "auto":
+        if not u.is_cuda:
+            raise RuntimeError("'auto' on a CPU tensor selects the reference's CPU variant 'qp', which lives "
+                               "in the reference package; difffea_b200 runs on CUDA devices only")
+        kind = "cuda"
+    if kind == "cuda":
+        return make_A_operator_cuda(u, theta, params)
+    if kind in REFERENCE_TANGENT_VARIANTS:
+        raise ValueError(f"tangent '{kind}' is one of the reference's PyTorch variants; difffea_b200 provides "
+                         f"{TANGENT_OPERATORS}")
+    raise ValueError(f"Unknown tangent operator '{kind}'. Choose one of {TANGENT_OPERATORS}.")
+
+
+def make_AT_operator(u, theta, params):
+    """A^T: the hyperelastic tangent is symmetric, so this is the same stored-moduli operator."""
+    return make_A_operator_cuda(u, theta, params)
+
+
+# ---------------------------------------------------------------------------------------------
+# Jacobi preconditioner
+# ---------------------------------------------------------------------------------------------
+class CudaJacobiPreconditioner:
+    """r -> r / diag(K) with diag clamped to >= 1e-6 on free DOFs and 1 on fixed DOFs."""
+
+    def __init__(self, mesh, diag):
+        self.mesh, self.diag = mesh, diag
+
+    def __call__(self, r):
+        return r / self.diag.to(r.dtype)
+
+
+def compute_jacobi_diagonal(u, theta, params):
+    """diag(K) without forming K (kernel (a)'s element diagonals, scattered by colour), shape (2N,)."""
+    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    hit = _LAST_DIAG.get(_diag_key(u, theta, mesh))
+    if hit is not None and hit[0]() is u and hit[1]() is theta:
+        return hit[2]
+    return _diag_only(mesh, u, theta, mu0, lam0)
+
+
+def _diag_only(mesh, u, theta, mu0, lam0):
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr, stream_handle
+    u64, th64 = _f64c(u), _f64c(theta)
+    diag = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
+    _lib.call("dfea_qp_moduli", mesh.view_ref, ptr(u64), ptr(th64), mu0, lam0, ptr(None), _lib.DFEA_F64, ptr(diag),
+              stream_handle())
+    return diag
+
+
+def make_jacobi_preconditioner(u, theta, params):
+    mesh = cuda_mesh(params)
+    return CudaJacobiPreconditioner(mesh, compute_jacobi_diagonal(u, theta, params))
+
+
+def make_preconditioner(kind, u, theta, params):
+    """Build a preconditioner by name: one of ``PRECONDITIONERS``."""
+    if kind == "jacobi":
+        return make_jacobi_preconditioner(u, theta, params)
+    if kind in ("block_jacobi", "ilu"):
+        raise ValueError(f"preconditioner '{kind}' is not built on the device; use 'jacobi'")
+    raise ValueError(f"Unknown preconditioner '{kind}'. Choose one of {PRECONDITIONERS}.")

@@ -1,0 +1,105 @@
+"""
+Per-problem device workspace of the Newton-Krylov solver.
+
+A ``NewtonWorkspace`` keeps everything a solve touches in HBM for the whole solve: the state and
+trial vectors, the residual, the Gauss-point moduli (FP64, or FP32 for the mixed-precision inner
+solver), the Jacobi diagonal, and one graph-captured ``DevicePCG`` bound to them.  The solver loop
+calls the C ABI directly on these buffers (no allocation per Newton step), reading back only the
+scalars the algorithm branches on: ||R|| per residual evaluation and (status, iterations) per PCG.
+"""
+import ctypes
+
+import torch
+
+from difffea_b200 import _lib
+from difffea_b200.cuda_mesh import _require_cuda, cuda_mesh, ptr, stream_handle
+from difffea_b200.krylov import DevicePCG
+from difffea_b200.materials import neo_hookean_parameters
+
+
+class NewtonWorkspace:
+    def __init__(self, params, precision="fp64", use_graph=True):
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")
+        self.params = params
+        self.mesh = mesh = cuda_mesh(params)
+        self.mu0, self.lam0 = neo_hookean_parameters(params)
+        self.precision = precision
+        dev, n = mesh.device, mesh.n_dof
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.f = params["f"].detach().to(**f64).contiguous()
+        self.R = torch.empty(n, **f64)
+        self.Rc = torch.empty(n, **f64)
+        self.uc = torch.empty(n, **f64)
+        self.du = torch.empty(n, **f64)
+        self.diag = torch.empty(n, **f64)
+        self.scal = torch.zeros(4, **f64)
+        self.scal_host = torch.zeros(4, dtype=torch.float64).pin_memory()
+        vt = torch.float64 if precision == "fp64" else torch.float32
+        self.C = torch.empty(mesh.moduli_numel(), dtype=vt, device=dev)
+        if precision == "fp64":
+            # the PCG writes its solution straight into du
+            self.diag_v, self.b, self.x = self.diag, torch.empty(n, **f64), self.du
+        else:
+            mesh.ensure_grad32()
+            self.diag_v = torch.empty(n, dtype=vt, device=dev)
+            self.b = torch.empty(n, dtype=vt, device=dev)
+            self.x = torch.empty(n, dtype=vt, device=dev)
+        self.pcg = DevicePCG(mesh, self.C, self.diag_v, self.b, self.x, use_graph=use_graph)
+        self.work = mesh.reduce_work()
+        self.theta = None
+        self.n_launch_groups = 0
+
+    # ---------------------------------------------------------------------------------------------
+    def set_theta(self, theta):
+        _require_cuda(theta)
+        if theta.numel() != self.mesh.n_el or theta.device != self.mesh.device:
+            raise ValueError(f"theta must have one entry per element ({self.mesh.n_el}) on {self.mesh.device}")
+        self.theta = theta.detach().to(torch.float64).contiguous()
+
+    def residual(self, u, load_factor, out, energy=False):
+        """out = R(u) (FP64); returns ||R|| (and the strain energy if asked) as Python floats."""
+        _lib.call("dfea_residual", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0, ptr(self.f),
+                  float(load_factor), ptr(out), ptr(self.scal), ptr(self.scal[1:]) if energy else ptr(None),
+                  ptr(self.work), stream_handle())
+        self.scal_host.copy_(self.scal, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        rn = float(self.scal_host[0]) ** 0.5
+        return (rn, float(self.scal_host[1])) if energy else rn
+
+    def linearize(self, u):
+        """Kernel (a): moduli C and Jacobi diagonal at u (into the buffers the PCG graph is bound to)."""
+        dt = _lib.DFEA_F64 if self.precision == "fp64" else _lib.DFEA_F32
+        _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0, ptr(self.C), dt,
+                  ptr(self.diag), stream_handle())
+        if self.precision == "fp32":
+            _lib.call("dfea_f64_to_f32", self.mesh.n_dof, ptr(self.diag), ptr(self.diag_v), stream_handle())
+
+    def solve(self, R, rtol, max_iter):
+        """du = PCG(A, -R) to relative tolerance rtol; returns (du (FP64 buffer), iterations, status)."""
+        if self.precision == "fp64":
+            torch.neg(R, out=self.b)
+        else:
+            _lib.call("dfea_f64_to_f32", self.mesh.n_dof, ptr(R), ptr(self.b), stream_handle())
+            self.b.neg_()
+        iters, status = self.pcg.solve(rtol, max_iter)
+        if self.precision == "fp32":
+            _lib.call("dfea_f32_to_f64", self.mesh.n_dof, ptr(self.x), ptr(self.du), stream_handle())
+        return self.du, iters, status
+
+    def trial(self, u, alpha, du, out):
+        _lib.call("dfea_add_scaled", self.mesh.n_dof, ptr(u), float(alpha), ptr(du), ptr(out), stream_handle())
+        return out
+
+
+def workspace_for(params, precision="fp64", cache=None):
+    """A workspace for ``params`` (reused through ``cache`` if given: a dict kept by the caller)."""
+    if cache is not None:
+        key = (id(params["conn"]), id(params["m"]), id(params["f"]), precision)
+        ws = cache.get(key)
+        if ws is not None and ws.params["conn"] is params["conn"]:
+            return ws
+        ws = NewtonWorkspace(params, precision)
+        cache[key] = ws
+        return ws
+    return NewtonWorkspace(params, precision)

@@ -1,0 +1,214 @@
+/*
+ * difffea_b200.h -- C ABI of the B200 (sm_100a) matrix-free Newton-Krylov kernels.
+ *
+ * Every entry point takes plain pointers and sizes; device pointers point to memory the caller
+ * owns (the Python host layer passes torch tensors from the caching allocator).  Nothing here
+ * allocates device memory: scratch space for reductions and Krylov vectors is a caller buffer
+ * whose size the matching *_work_bytes query returns.  Streams are passed as `void*`
+ * (a cudaStream_t); every launch is asynchronous on that stream unless the comment says otherwise.
+ *
+ * Return value: DFEA_OK (0) or one of the DFEA_ERR_* codes below; dfea_last_error() gives a
+ * human-readable message for the calling thread.
+ *
+ * Layouts (all "SoA": the element index runs fastest so that a warp reads 32 consecutive elements):
+ *   stride             element stride of every per-element row, a multiple of 32 that is >= n_el
+ *   conn   int32       [nen][stride]   node << 2 | fix bits (bit 0: x DOF fixed, bit 1: y DOF fixed)
+ *   orig   int32       [stride]        original (reference) element id of a colour-sorted slot
+ *   grad   f64 (f32)   [n_q][nen][stride][2]  (dN_a/dX, dN_a/dY) at Gauss point q
+ *   wdet   f64         [n_q][stride]   Gauss weight * det(dX/dxi)
+ *   moduli f64         [n_q][8][stride][2]   entry pair k holds C[2k], C[2k+1] of the row-major 4x4
+ *          f32         [n_q][4][stride][4]   row r holds C[4r .. 4r+3]
+ *   vectors            (2 * n_nodes) node-major DOF vectors, dof = 2 * node + component,
+ *                      as in the reference (boundary_conditions.py:171-179)
+ * Elements are stored sorted by colour: no two elements of one colour share a node, so the
+ * scatter of one colour needs neither atomics nor a fixed summation order to be deterministic.
+ */
+#ifndef DIFFFEA_B200_H
+#define DIFFFEA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFEA_OK 0
+#define DFEA_ERR_INVALID 1     /* a size, pointer or option is out of range */
+#define DFEA_ERR_UNSUPPORTED 2 /* (nen, n_q) pair of an element type the library does not build */
+#define DFEA_ERR_CUDA 3        /* a CUDA call failed; dfea_last_error() has the CUDA message */
+#define DFEA_ERR_COLOURS 4     /* the element graph needs more than DFEA_MAX_COLOURS colours */
+
+#define DFEA_F64 0
+#define DFEA_F32 1
+
+#define DFEA_MAX_COLOURS 64
+
+/* Status words of the device-resident PCG (dfea_pcg_solve). */
+#define DFEA_PCG_RUNNING 0
+#define DFEA_PCG_CONVERGED 1   /* ||r|| <= rtol ||b||                                  */
+#define DFEA_PCG_MAX_ITER 2    /* max_iter iterations without convergence             */
+#define DFEA_PCG_NEG_CURV 3    /* p.Ap <= 0: the operator is not SPD along p           */
+#define DFEA_PCG_ZERO_RHS 4    /* ||b|| == 0: x = 0 after zero iterations              */
+
+/* A mesh in device memory, colour-sorted.  Sizes are host values, pointers are device pointers. */
+typedef struct dfea_mesh_view {
+    int64_t n_el;        /* number of elements                                           */
+    int64_t stride;      /* element stride of every SoA row (multiple of 32, >= n_el)     */
+    int64_t n_nodes;     /* number of nodes N; DOF vectors have 2N entries                */
+    int32_t nen;         /* nodes per element                                             */
+    int32_t n_q;         /* Gauss points per element                                      */
+    int32_t n_colours;   /* number of colour classes                                      */
+    int32_t reserved;
+    int64_t colour_begin[DFEA_MAX_COLOURS + 1]; /* elements [colour_begin[c], colour_begin[c+1]) */
+    const int32_t* conn;     /* [nen][stride]                                              */
+    const int32_t* orig;     /* [stride]                                                   */
+    const double* grad;      /* [n_q][nen][stride][2]                                      */
+    const double* wdet;      /* [n_q][stride]                                              */
+    const float* grad32;     /* optional FP32 copy of grad (NULL if not built)              */
+    const uint8_t* node_fix; /* [n_nodes] fix bits of every node                           */
+} dfea_mesh_view;
+
+/* ---------------------------------------------------------------- library --------------------- */
+
+/* Message of the last error of the calling thread (static storage, never NULL). */
+const char* dfea_last_error(void);
+
+/* Library version as major * 10000 + minor * 100 + patch. */
+int dfea_version(void);
+
+/* Number of kernels this library has launched in the process so far (kernels run by a captured
+ * PCG graph are added when its solve returns).  A diagnostic for benchmarks. */
+int64_t dfea_launch_count(void);
+
+/* 1 if the (nen, n_q) pair is built: (3,1) tri3, (6,6) tri6, (4,4) quad4, (8,9) quad8, (9,9) quad9. */
+int dfea_element_supported(int32_t nen, int32_t n_q);
+
+/* ---------------------------------------------------------------- mesh set-up ----------------- */
+
+/*
+ * Greedy element colouring (host function, host pointers).  conn is the reference connectivity
+ * (n_el, nen) int64 (problem.py:180-190 `conn`).  On return colour[e] in [0, *n_colours) and no
+ * two elements that share a node have the same colour.  Elements are visited in id order; each
+ * takes the smallest colour unused at its nodes, which gives 4 colours on structured Q4/Q8/Q9 grids.
+ */
+int dfea_colour_elements(const int64_t* conn, int64_t n_el, int32_t nen, int64_t n_nodes,
+                         int32_t* colour, int32_t* n_colours);
+
+/*
+ * Copy the reference-layout mesh arrays (device pointers) into the colour-sorted SoA layout of a
+ * dfea_mesh_view.  perm[s] = original element id stored in slot s (n_el entries).  dN_dX is
+ * (n_el, n_q, nen, 2) and w_detJ (n_el, n_q), as precompute_geometry returns them
+ * (operators.py:85-120); m is the (2N) Dirichlet mask of 0.0/1.0 entries (operators.py:29).
+ * Outputs: conn_out [nen][stride], orig_out [stride], grad_out [n_q][nen][stride][2],
+ * wdet_out [n_q][stride], node_fix_out [n_nodes].
+ */
+int dfea_mesh_pack(int64_t n_el, int64_t stride, int32_t nen, int32_t n_q, int64_t n_nodes,
+                   const int64_t* perm, const int64_t* conn_ref, const double* dN_dX,
+                   const double* w_detJ, const double* m, int32_t* conn_out, int32_t* orig_out,
+                   double* grad_out, double* wdet_out, uint8_t* node_fix_out, void* stream);
+
+/* FP32 copy of the packed gradients (the geometry of the FP32 inner operator). */
+int dfea_mesh_grad_to_f32(const dfea_mesh_view* mesh, float* grad32_out, void* stream);
+
+/* ---------------------------------------------------------------- kernels (a), (b) ------------ */
+
+/*
+ * Kernel (a): Gauss-point tangent moduli and Jacobi diagonal at state u.
+ * Replaces `_qp_setup` (operators.py:316-342) and `compute_jacobi_diagonal` (operators.py:477-556):
+ *   F = I + sum_a u_a (x) dN_a,  C[(iJ),(kL)] = w detJ d2psi/dF_iJ dF_kL  (neo-Hookean, plane strain,
+ *   materials.py:209-217 with mu = mu0 theta_e, lambda = lambda0 theta_e, materials.py:383-390),
+ *   diag = where(m > 0, max(sum_e diag(K_e), 1e-6), 1).
+ * theta is indexed by ORIGINAL element id.  moduli_dtype selects the moduli layout (DFEA_F64 or
+ * DFEA_F32).  diag (2N, f64) is written; it may be NULL to skip the diagonal, and moduli may be NULL
+ * to compute the diagonal alone (the Jacobi preconditioner of operators.py:562-570).
+ */
+int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                   double lambda0, void* moduli, int32_t moduli_dtype, double* diag, void* stream);
+
+/*
+ * Kernel (b): y = m * J(u) (m * v) + (1 - m) * v from the stored moduli, i.e. the `qp`/`qp_ew`
+ * tangent product (operators.py:345-412).  One fused gather-contract-scatter launch per colour;
+ * no atomics.  vec_dtype selects f64 or f32 vectors; with f32 vectors the moduli must be f32 and
+ * mesh->grad32 must be set.  y must not alias v.
+ */
+int dfea_tangent_apply(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype,
+                       const void* v, void* y, int32_t vec_dtype, void* stream);
+
+/* ---------------------------------------------------------------- residual, energy ------------ */
+
+/* Bytes of scratch that dfea_residual and dfea_vec_norm2 need for their reductions. */
+int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh);
+
+/*
+ * R = m * (R_int(u) - load_factor * f), R_int = scatter(sum_q w detJ P(F) dN)  (global_residual,
+ * operators.py:159-220).  If out_norm2 is not NULL, *out_norm2 (device) = sum R^2 (fixed-order,
+ * deterministic).  If out_energy is not NULL, *out_energy (device) = sum_e sum_q w detJ psi(F_q),
+ * the strain energy of compute_fields (postprocess.py:102).  f may be NULL (zero load).
+ * work: dfea_reduce_work_bytes(mesh) bytes of scratch.
+ */
+int dfea_residual(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                  double lambda0, const double* f, double load_factor, double* R, double* out_norm2,
+                  double* out_energy, void* work, void* stream);
+
+/* *out (device) = sum_i x_i^2 over 2N entries, fixed-order reduction.  work as for dfea_residual. */
+int dfea_vec_norm2(const dfea_mesh_view* mesh, const double* x, double* out, void* work, void* stream);
+
+/* ---------------------------------------------------------------- kernel (d) ------------------ */
+
+/*
+ * Per-element compliance sensitivity, the implicit VJP of adjoint.py:75-106:
+ *   g_e = -sum_{a,i} (m * lambda)[dof(e,a,i)] f_e[a,i](u; mu0, lambda0),
+ * exact because R_int is linear in theta_e when theta scales every parameter (neo-Hookean mu and
+ * lambda, materials.py:308-312).  g has n_el entries in ORIGINAL element order.
+ */
+int dfea_element_sensitivity(const dfea_mesh_view* mesh, const double* u, const double* lam,
+                             double mu0, double lambda0, double* g, void* stream);
+
+/* ---------------------------------------------------------------- kernel (c): PCG ------------- */
+
+typedef struct dfea_pcg dfea_pcg; /* opaque: a captured CUDA graph of one PCG iteration */
+
+/* Bytes of the caller buffer that dfea_pcg_create binds (Krylov vectors, partial sums, state). */
+int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
+
+/*
+ * Bind a Jacobi-PCG solver to fixed buffers and capture one iteration in a CUDA graph whose
+ * while-loop node repeats it on the device until convergence (newton_krylov.py:28-88 semantics:
+ * x0 = 0, stop when ||r|| <= rtol ||b|| or at max_iter, early exit on p.Ap <= 0 returning z at
+ * k = 0 and x otherwise).  moduli/diag/b/x are device buffers that stay bound to the handle;
+ * their CONTENTS may change between solves.  vec_dtype DFEA_F64 needs f64 moduli; DFEA_F32 needs
+ * f32 moduli and mesh->grad32, and then diag, b and x are f32.  The graph is captured on an internal
+ * stream; `use_graph` = 0 launches the same kernels directly (host-polled every 16 iterations).
+ */
+int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, const void* diag,
+                    const void* b, void* x, int32_t vec_dtype, void* work, int32_t use_graph,
+                    dfea_pcg** out);
+
+/*
+ * Solve on `stream`.  Blocks the host until the solve ends (it reads back the iteration count);
+ * *iters and *status receive the result (DFEA_PCG_* status word).
+ */
+int dfea_pcg_solve(dfea_pcg* pcg, double rtol, int32_t max_iter, int32_t* iters, int32_t* status,
+                   void* stream);
+
+/* Release the graph and the handle (not the bound buffers). */
+int dfea_pcg_destroy(dfea_pcg* pcg);
+
+/* ---------------------------------------------------------------- vector helpers -------------- */
+
+/* y = a * x + y  on n entries (f64). */
+int dfea_axpy(int64_t n, double a, const double* x, double* y, void* stream);
+
+/* out = a + alpha * b  on n entries (f64): the Newton trial state of the line search. */
+int dfea_add_scaled(int64_t n, const double* a, double alpha, const double* b, double* out,
+                    void* stream);
+
+/* Element-wise conversions between f64 and f32 vectors (n entries). */
+int dfea_f64_to_f32(int64_t n, const double* x, float* y, void* stream);
+int dfea_f32_to_f64(int64_t n, const float* x, double* y, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIFFFEA_B200_H */

@@ -1,0 +1,114 @@
+"""
+Generate the golden vectors of the reference implementation (run in the build container, where the
+reference package is importable; the GPU box only reads the .npz files this writes).
+
+    python tests/golden/make_golden.py [/path/to/reference/src]
+
+Every fixture is produced by calling the reference's own public functions on small seeded inputs:
+problem dictionaries from build_problem (structured rectangle meshes, as in the reference's
+tests/helpers.py small_problem), moduli from _qp_setup, products from the qp / qp_ew / jvp tangent
+variants, residuals, Jacobi diagonals, strain energies, complete Newton-Krylov solves and adjoint
+sensitivities.  File names say what each fixture holds.
+"""
+import os
+import sys
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+sys.path.insert(0, REF_SRC)
+
+from difffea.newton_krylov import newton_krylov_solve  # noqa: E402
+from difffea.operators import (_qp_setup, compute_jacobi_diagonal, global_residual,  # noqa: E402
+                               make_tangent_operator)
+from difffea.postprocess import compute_fields  # noqa: E402
+from difffea.problem import build_problem, default_spec  # noqa: E402
+from difffea.sensitivity import compute_sensitivity  # noqa: E402
+
+torch.set_num_threads(min(8, os.cpu_count() or 1))
+DT = torch.float64
+KEYS = ("nodes", "conn", "dN_dX", "w_detJ", "f", "m", "fixed", "u_D", "mat_p")
+
+
+def problem(element_type, h=0.5, load=(60.0, 0.0), E=2600.0, nu=0.3, **over):
+    spec = default_spec("rectangle", element_type, h)
+    spec.update(mesher="structured", load_value=load, E=E, nu=nu)
+    spec.update(over)
+    return build_problem(spec)
+
+
+def arrays(params):
+    return {k: params[k].numpy() for k in KEYS}
+
+
+def save(name, **arrs):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **{k: np.asarray(v) for k, v in arrs.items()})
+    print("wrote", os.path.relpath(path), {k: np.asarray(v).shape for k, v in arrs.items()})
+
+
+def operator_case(element_type, h, seed, nonuniform_theta):
+    p = problem(element_type, h)
+    n_el = p["conn"].shape[0]
+    g = torch.Generator().manual_seed(seed)
+    n = p["f"].shape[0]
+    # 0.02 at h = 0.5 (the reference's tests/test_tangent_operators.py state), scaled with h so that no
+    # element of the finer meshes is inverted
+    u = 0.04 * h * torch.randn(n, dtype=DT, generator=g) * p["m"]
+    v = torch.randn(n, dtype=DT, generator=g)
+    theta = (0.5 + torch.rand(n_el, dtype=DT, generator=g)) if nonuniform_theta else torch.ones(n_el, dtype=DT)
+    C, _ = _qp_setup(u, theta, p)
+    out = dict(arrays(p), u=u.numpy(), v=v.numpy(), theta=theta.numpy(), C=C.numpy(),
+               Av_qp_ew=make_tangent_operator("qp_ew", u, theta, p)(v).numpy(),
+               Av_qp=make_tangent_operator("qp", u, theta, p)(v).numpy(),
+               Av_jvp=make_tangent_operator("jvp", u, theta, p)(v).numpy(),
+               R=global_residual(u, theta, p).numpy(),
+               R_half=global_residual(u, theta, p, load_factor=0.5).numpy(),
+               diag=compute_jacobi_diagonal(u, theta, p).numpy(),
+               energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])))
+    tag = "theta" if nonuniform_theta else "unit"
+    save(f"operator_{element_type}_h{h}_{tag}", **out)
+
+
+def solve_case(element_type, h, load, n_steps, tol_rel, name):
+    p = problem(element_type, h, load=load)
+    theta = torch.ones(p["conn"].shape[0], dtype=DT)
+    tol = tol_rel * float(torch.norm(p["f"]))
+    u, info = newton_krylov_solve(p, theta, n_steps, tol, verbose=False, preconditioner="jacobi", tangent="qp")
+    assert info["converged"]
+    hist = info["history"]
+    save(name, **arrays(p), theta=theta.numpy(), u_star=u.numpy(), tol=np.array(tol),
+         n_load_steps=np.array(n_steps), total_newton=np.array(info["total_newton"]),
+         total_cg=np.array(info["total_cg"]), residuals=np.array([r["residual"] for r in hist]),
+         cg_iters=np.array([r["cg_iters"] for r in hist]), alphas=np.array([r["alpha"] for r in hist]),
+         energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])))
+
+
+def sensitivity_case(element_type, h, name):
+    p = problem(element_type, h, load=(50.0, 0.0))
+    n_el = p["conn"].shape[0]
+    theta = 1.0 + 0.2 * torch.sin(torch.arange(n_el, dtype=DT))
+    loss_fn = lambda u: torch.dot(p["f"], u)  # noqa: E731  compliance
+    u, g = compute_sensitivity(p, theta, loss_fn, n_load_steps=2, tol=1e-12)
+    save(name, **arrays(p), theta=theta.numpy(), u_star=u.numpy(), dL_dtheta=g.numpy())
+
+
+def main():
+    for et in ("quad4", "quad8", "quad9", "tri3", "tri6"):
+        operator_case(et, 0.5, seed=0, nonuniform_theta=False)
+        operator_case(et, 0.25, seed=1, nonuniform_theta=True)
+    operator_case("quad4", 0.1, seed=3, nonuniform_theta=True)          # 20 x 10 cells
+    # complete solves (the reference's jacobi-PCG path, tangent qp)
+    solve_case("quad4", 0.25, (0.0, -40.0), 3, 1e-11, "solve_quad4_h0.25_cantilever")   # dolfinx case
+    solve_case("tri6", 0.5, (0.0, -40.0), 3, 1e-11, "solve_tri6_h0.5_cantilever")       # dolfinx case
+    solve_case("quad9", 0.5, (0.0, -40.0), 3, 1e-9, "solve_quad9_h0.5_cantilever")
+    solve_case("quad4", 0.2, (60.0, 0.0), 2, 1e-10, "solve_quad4_h0.2_tension")
+    sensitivity_case("quad4", 1.0, "sensitivity_quad4_h1")
+    sensitivity_case("tri3", 1.0, "sensitivity_tri3_h1")
+    sensitivity_case("quad4", 0.25, "sensitivity_quad4_h0.25")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,80 @@
+"""The C-ABI library loads and exports every declared symbol; host-side entry points work without a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from difffea_b200 import _lib
+from difffea_b200.cuda_mesh import colour_elements
+from difffea_b200.mesh import create_rectangle_mesh
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "difffea_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dfea_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared_symbols()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(_lib.exported_symbols())     # the binding declares exactly the header
+
+
+def test_version_and_element_table():
+    lib = _lib.load()
+    assert lib.dfea_version() >= 10000
+    for nen, nq in ((4, 4), (9, 9), (3, 1), (6, 6), (8, 9)):
+        assert lib.dfea_element_supported(nen, nq) == 1
+    assert lib.dfea_element_supported(4, 9) == 0
+
+
+def _valid_colouring(conn, colour):
+    conn = np.asarray(conn)
+    for c in np.unique(colour):
+        nodes = conn[colour == c].reshape(-1)
+        assert len(np.unique(nodes)) == len(nodes), f"colour {c} shares a node"
+
+
+@pytest.mark.parametrize("et,expected", [("quad4", 4), ("quad8", 4), ("quad9", 4), ("tri3", None), ("tri6", None)])
+def test_greedy_colouring(et, expected):
+    _, conn = create_rectangle_mesh(et, 3.0, 2.0, 13, 7)
+    colour, nc = colour_elements(conn)
+    _valid_colouring(conn, colour)
+    assert colour.min() == 0 and colour.max() == nc - 1
+    if expected:
+        assert nc == expected
+    else:
+        assert nc <= 8
+
+
+def test_colouring_rejects_bad_node_ids():
+    lib = _lib.load()
+    conn = np.array([[0, 1, 2, 7]], dtype=np.int64)
+    col = np.zeros(1, dtype=np.int32)
+    nc = ctypes.c_int32(0)
+    rc = lib.dfea_colour_elements(conn.ctypes.data_as(ctypes.c_void_p), 1, 4, 5, col.ctypes.data_as(ctypes.c_void_p),
+                                  ctypes.byref(nc))
+    assert rc == 1 and "outside" in _lib.last_error()
+
+
+def test_pcg_work_size_query_is_host_only():
+    view = _lib.MeshView()
+    view.n_nodes, view.n_colours = 1000, 4
+    n64 = _lib.load().dfea_pcg_work_bytes(ctypes.byref(view), _lib.DFEA_F64)
+    n32 = _lib.load().dfea_pcg_work_bytes(ctypes.byref(view), _lib.DFEA_F32)
+    assert n64 > n32 > 3 * 2 * 1000 * 4
+
+
+def test_compute_entry_points_validate_before_touching_the_gpu():
+    view = _lib.MeshView()            # all zero: invalid
+    rc = _lib.load().dfea_tangent_apply(ctypes.byref(view), None, 0, None, None, 0, None)
+    assert rc != 0

@@ -1,0 +1,147 @@
+"""
+Parity of kernels (a) and (b), the residual and the strain energy with the reference (golden vectors)
+and the oracle, FP64 and FP32, plus determinism, symmetry and linearity at larger sizes.
+"""
+import pytest
+import torch
+
+import oracle
+from difffea_b200 import ops
+from difffea_b200.cuda_mesh import cuda_mesh
+from difffea_b200.materials import neo_hookean_parameters
+from difffea_b200.operators import global_residual, make_A_operator_cuda, make_tangent_operator, strain_energy
+from difffea_b200.problem import build_rectangle_problem, to_device
+from golden_utils import golden_names, load, params_from, rel
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+OPERATOR_CASES = golden_names("operator_")
+
+
+def unpack_moduli(mesh, C):
+    """(n_el, n_q, 4, 4) in original element order from the colour-sorted SoA layout of kernel (a)."""
+    S, nq, n = mesh.stride, mesh.n_q, mesh.n_el
+    if C.dtype == torch.float64:
+        slot = C.view(nq, 8, S, 2)[:, :, :n, :].permute(2, 0, 1, 3).reshape(n, nq, 4, 4)
+    else:
+        slot = C.view(nq, 4, S, 4)[:, :, :n, :].permute(2, 0, 1, 3).reshape(n, nq, 4, 4)
+    out = torch.empty_like(slot)
+    out[mesh.perm] = slot
+    return out
+
+
+def golden_case(name):
+    d = load(name)
+    p = params_from(d, DEV)
+    t = lambda k: torch.as_tensor(d[k], dtype=torch.float64, device=DEV)  # noqa: E731
+    return d, p, t("u"), t("v"), t("theta")
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES)
+def test_moduli_and_diagonal_match_reference(name):
+    d, p, u, v, th = golden_case(name)
+    A = make_A_operator_cuda(u, th, p)
+    assert rel(unpack_moduli(A.mesh, A.C), d["C"]) < 1e-12
+    assert rel(A.diag, d["diag"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES)
+def test_tangent_product_matches_qp_ew(name):
+    d, p, u, v, th = golden_case(name)
+    y = make_tangent_operator("cuda", u, th, p)(v)
+    assert rel(y, d["Av_qp_ew"]) < 1e-11           # the parity bar of the north star (per product)
+    assert rel(y, d["Av_jvp"]) < 1e-11
+    assert make_tangent_operator("auto", u, th, p)(v).equal(y)
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES)
+def test_residual_and_energy_match_reference(name):
+    d, p, u, v, th = golden_case(name)
+    assert rel(global_residual(u, th, p), d["R"]) < 1e-12
+    assert rel(global_residual(u, th, p, load_factor=0.5), d["R_half"]) < 1e-12
+    W = float(strain_energy(u, th, p))
+    assert abs(W - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES)
+def test_fp32_operator_is_close(name):
+    d, p, u, v, th = golden_case(name)
+    A32 = make_A_operator_cuda(u, th, p, precision="fp32")
+    y = A32(v.float())
+    assert y.dtype == torch.float32
+    assert rel(y.double(), d["Av_qp_ew"]) < 2e-5
+    assert rel(unpack_moduli(A32.mesh, A32.C).double(), d["C"]) < 1e-6
+
+
+def _random_state(p, h, seed):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    n = p["f"].shape[0]
+    u = ((torch.rand(n, dtype=torch.float64, generator=g) * 2 - 1) * 0.05 * h).to(DEV) * p["m"]
+    v = torch.randn(n, dtype=torch.float64, generator=g).to(DEV)
+    w = torch.randn(n, dtype=torch.float64, generator=g).to(DEV)
+    th = torch.exp(0.3 * torch.randn(p["conn"].shape[0], dtype=torch.float64, generator=g)).to(DEV)
+    return u, v, w, th
+
+
+@pytest.mark.parametrize("et,nx,ny", [("quad4", 120, 60), ("quad9", 40, 20), ("tri6", 30, 20), ("tri3", 60, 30),
+                                      ("quad8", 30, 15)])
+def test_larger_meshes_against_oracle(et, nx, ny):
+    p = build_rectangle_problem(et, nx, ny, float(nx), float(ny), load=(0.0, 1e-3), device=DEV)
+    u, v, w, th = _random_state(p, 1.0, 7)
+    P = oracle.as_problem(p)
+    A = make_tangent_operator("cuda", u, th, p)
+    uc, thc, vc = u.cpu(), th.cpu(), v.cpu()
+    C_ref = oracle.moduli(uc, thc, P)
+    assert rel(A(v), oracle.apply_qp_ew(C_ref, vc, P)) < 1e-11
+    assert rel(global_residual(u, th, p, 0.7), oracle.residual(uc, thc, P, 0.7)) < 1e-12
+    assert rel(A.diag, oracle.jacobi_diagonal(uc, thc, P)) < 1e-12
+
+
+@pytest.mark.parametrize("et", ["quad4", "quad9"])
+def test_product_is_deterministic_symmetric_and_linear(et):
+    n = 160 if et == "quad4" else 80
+    p = build_rectangle_problem(et, n, n, float(n), float(n), device=DEV)
+    u, v, w, th = _random_state(p, 1.0, 3)
+    A = make_tangent_operator("cuda", u, th, p)
+    y1, y2 = A(v), A(v)
+    assert torch.equal(y1, y2)                                       # colour-ordered scatter: bitwise
+    Aw = A(w)
+    assert abs(float(w @ y1) - float(v @ Aw)) <= 1e-12 * abs(float(v @ Aw))
+    assert rel(A(2.5 * v - 0.5 * w), 2.5 * y1 - 0.5 * Aw) < 1e-13
+    fixed = ~p["m"].bool()
+    e = torch.zeros_like(v)
+    e[fixed] = v[fixed]
+    assert torch.equal(A(e), e)                                      # identity pivot on fixed DOFs
+
+
+def test_inverted_element_propagates_nan_like_the_reference():
+    p = build_rectangle_problem("quad4", 4, 4, 4.0, 4.0, device=DEV)
+    u = torch.zeros(p["f"].shape[0], dtype=torch.float64, device=DEV)
+    th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV)
+    node = int(p["conn"][5, 2])
+    u[2 * node] = -3.0                                               # fold one element over itself
+    R = global_residual(u, th, p)
+    R_ref = oracle.residual(u.cpu(), th.cpu(), oracle.as_problem(p))
+    assert torch.equal(torch.isnan(R).cpu(), torch.isnan(R_ref))
+    assert torch.isnan(R).any()
+
+
+def test_custom_ops_are_registered():
+    assert hasattr(torch.ops.difffea_b200, "tangent_apply")
+    assert hasattr(torch.ops.difffea_b200, "qp_moduli")
+    d, p, u, v, th = golden_case("operator_quad4_h0.5_unit")
+    mesh = cuda_mesh(p)
+    mid = ops.register_mesh(mesh)
+    mu0, lam0 = neo_hookean_parameters(p)
+    C, _ = torch.ops.difffea_b200.qp_moduli(mid, u, th, mu0, lam0, False, False)
+    assert rel(torch.ops.difffea_b200.tangent_apply(mid, C, v), d["Av_qp_ew"]) < 1e-11
+
+
+def test_reference_built_dictionary_on_device_is_accepted():
+    """A params dict moved with to_device (reference layout) runs unchanged."""
+    d = load("operator_tri6_h0.5_unit")
+    p = to_device(params_from(d), DEV)
+    u = torch.as_tensor(d["u"], device=DEV)
+    y = make_tangent_operator("cuda", u, torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV), p)(
+        torch.as_tensor(d["v"], device=DEV))
+    assert rel(y, d["Av_qp_ew"]) < 1e-11

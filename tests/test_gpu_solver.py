@@ -1,0 +1,123 @@
+"""
+Kernel (c) and the Newton-Krylov driver: complete solves against the reference's, the device PCG
+against the oracle's PCG (same recurrences), its edge cases, and the mixed-precision solve.
+"""
+import pytest
+import torch
+
+import oracle
+from difffea_b200.krylov import DevicePCG
+from difffea_b200.newton_krylov import newton_krylov_solve, pcg
+from difffea_b200.operators import make_jacobi_preconditioner, make_tangent_operator, strain_energy
+from difffea_b200.problem import build_rectangle_problem
+from golden_utils import golden_names, load, params_from, rel
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+SOLVE_CASES = golden_names("solve_")
+
+
+def _t(d, k):
+    return torch.as_tensor(d[k], dtype=torch.float64, device=DEV)
+
+
+@pytest.mark.parametrize("name", SOLVE_CASES)
+def test_complete_solve_matches_reference(name):
+    d = load(name)
+    p = params_from(d, DEV)
+    u, info = newton_krylov_solve(p, _t(d, "theta"), int(d["n_load_steps"]), float(d["tol"]), verbose=False)
+    assert info["converged"] and info["load_factor"] == 1.0
+    assert rel(u, d["u_star"]) < 1e-9                      # complete solutions: the north star's bar
+    assert info["total_newton"] == int(d["total_newton"])
+    assert abs(info["total_cg"] - int(d["total_cg"])) <= max(3, 0.03 * int(d["total_cg"]))
+    assert abs(float(strain_energy(u, _t(d, "theta"), p)) - float(d["energy"])) <= 1e-9 * abs(float(d["energy"]))
+
+
+def test_dolfinx_known_answers_on_the_gpu():
+    for name, known in (("solve_quad4_h0.25_cantilever", 0.5168860494403356),
+                        ("solve_tri6_h0.5_cantilever", 0.5321248641215832)):
+        d = load(name)
+        p = params_from(d, DEV)
+        u, info = newton_krylov_solve(p, _t(d, "theta"), 3, float(d["tol"]), verbose=False)
+        assert abs(float(u.abs().max()) - known) <= 1e-10 * known
+
+
+def _linear_system(name="operator_quad4_h0.1_theta"):
+    d = load(name)
+    p = params_from(d, DEV)
+    u, th = _t(d, "u"), _t(d, "theta")
+    P = oracle.as_problem(p)
+    A = make_tangent_operator("cuda", u, th, p)
+    M = make_jacobi_preconditioner(u, th, p)
+    A_ref = oracle.make_operator("qp_ew", u.cpu(), th.cpu(), P)
+    d_ref = oracle.jacobi_diagonal(u.cpu(), th.cpu(), P)
+    b = p["m"] * _t(d, "v")
+    return p, A, M, A_ref, d_ref, b
+
+
+@pytest.mark.parametrize("rtol,max_iter", [(1e-10, 2000), (1e-4, 500), (1e-12, 5)])
+def test_device_pcg_follows_the_reference_recurrences(rtol, max_iter):
+    p, A, M, A_ref, d_ref, b = _linear_system()
+    x, k = pcg(A, b, M, rtol=rtol, max_iter=max_iter)
+    x_ref, k_ref = oracle.pcg(A_ref, b.cpu(), lambda r: r / d_ref, rtol=rtol, max_iter=max_iter)
+    assert abs(k - k_ref) <= 1
+    assert rel(x, x_ref) < (1e-9 if rtol < 1e-6 else 1e-6)
+
+
+def test_device_pcg_zero_rhs_and_status():
+    p, A, M, *_ = _linear_system()
+    x, k = pcg(A, torch.zeros(A.mesh.n_dof, dtype=torch.float64, device=DEV), M)
+    assert k == 0 and float(x.abs().max()) == 0.0 and A.last_status == "zero_rhs"
+
+
+def test_device_pcg_negative_curvature_returns_z_at_first_iteration():
+    d = load("operator_quad4_h0.25_theta")
+    p = params_from(d, DEV)
+    u, th = _t(d, "u"), -_t(d, "theta")                     # negated stiffness: p.Ap < 0 at once
+    A = make_tangent_operator("cuda", u, th, p)
+    M = make_jacobi_preconditioner(u, th, p)
+    b = p["m"] * _t(d, "v")
+    x, k = pcg(A, b, M)
+    P = oracle.as_problem(p)
+    x_ref, k_ref = oracle.pcg(oracle.make_operator("qp_ew", u.cpu(), th.cpu(), P), b.cpu(),
+                              lambda r: r / oracle.jacobi_diagonal(u.cpu(), th.cpu(), P))
+    assert k == k_ref == 0 and A.last_status == "negative_curvature"
+    assert rel(x, x_ref) < 1e-12
+
+
+def test_graph_and_direct_launch_give_identical_iterates():
+    p, A, M, A_ref, d_ref, b = _linear_system()
+    res = []
+    for use_graph in (True, False):
+        bb, xx = b.clone(), torch.empty_like(b)
+        solver = DevicePCG(A.mesh, A.C, M.diag, bb, xx, use_graph=use_graph)
+        k, status = solver.solve(1e-9, 1000)
+        res.append((k, status, xx.clone()))
+        solver.close()
+    assert res[0][0] == res[1][0] and res[0][1] == res[1][1] == "converged"
+    assert torch.equal(res[0][2], res[1][2])
+
+
+def test_mixed_precision_solve_meets_1e8():
+    p = build_rectangle_problem("quad4", 40, 20, 2.0, 1.0, E=2600.0, load=(60.0, 0.0), device=DEV)
+    th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV)
+    tol = 1e-12 * float(torch.norm(p["f"]))
+    u64, i64 = newton_krylov_solve(p, th, 2, tol, verbose=False, pcg_max_iter=5000)
+    u32, i32 = newton_krylov_solve(p, th, 2, tol, verbose=False, pcg_max_iter=5000, precision="fp32")
+    assert i64["converged"] and i32["converged"]
+    assert rel(u32, u64) <= 1e-8
+    W64, W32 = float(strain_energy(u64, th, p)), float(strain_energy(u32, th, p))
+    assert abs(W32 - W64) <= 1e-8 * abs(W64)
+
+
+def test_load_cutbacks_recover():
+    """One nominal step of a large tip load needs cut-backs (the continuation logic of the reference)."""
+    p = build_rectangle_problem("quad4", 20, 4, 5.0, 1.0, E=1.0, load=(0.0, -0.08), device=DEV)
+    th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV)
+    u, info = newton_krylov_solve(p, th, 1, 1e-9, max_newton=8, verbose=False, pcg_max_iter=2000)
+    P = oracle.as_problem(p)
+    u_ref, info_ref = oracle.newton_krylov_solve(P, th.cpu(), 1, 1e-9, max_newton=8, pcg_max_iter=2000)
+    assert info["converged"] == info_ref["converged"]
+    assert info["n_cutbacks"] == info_ref["n_cutbacks"]
+    if info["converged"]:
+        assert rel(u, u_ref) < 1e-7

@@ -1,0 +1,59 @@
+"""
+Pin the oracle (the CPU restatement used as the parity checker) to the reference's own outputs:
+every golden vector in tests/golden was produced by the reference package (make_golden.py).
+"""
+import pytest
+import torch
+
+import oracle
+from golden_utils import golden_names, load, params_from, rel
+
+OPERATOR_CASES = golden_names("operator_")
+SOLVE_CASES = golden_names("solve_")
+SENS_CASES = golden_names("sensitivity_")
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES)
+def test_oracle_operator_quantities_match_reference(name):
+    d = load(name)
+    P = oracle.as_problem(params_from(d))
+    u, v, th = (torch.as_tensor(d[k]) for k in ("u", "v", "theta"))
+    C = oracle.moduli(u, th, P)
+    assert rel(C, d["C"]) < 1e-13
+    assert rel(oracle.apply_qp_ew(C, v, P), d["Av_qp_ew"]) < 1e-13
+    assert rel(oracle.apply_qp(C, v, P), d["Av_qp"]) < 1e-13
+    assert rel(oracle.make_operator("jvp", u, th, P)(v), d["Av_jvp"]) < 1e-12
+    assert rel(oracle.residual(u, th, P), d["R"]) < 1e-13
+    assert rel(oracle.residual(u, th, P, 0.5), d["R_half"]) < 1e-13
+    assert rel(oracle.jacobi_diagonal(u, th, P), d["diag"]) < 1e-13
+    assert abs(float(oracle.strain_energy(u, th, P)) - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))
+
+
+@pytest.mark.parametrize("name", SOLVE_CASES)
+def test_oracle_solve_matches_reference(name):
+    d = load(name)
+    P = oracle.as_problem(params_from(d))
+    th = torch.as_tensor(d["theta"])
+    u, info = oracle.newton_krylov_solve(P, th, int(d["n_load_steps"]), float(d["tol"]), tangent="qp")
+    assert info["converged"]
+    assert rel(u, d["u_star"]) < 1e-9
+    assert info["total_newton"] == int(d["total_newton"])
+    assert abs(info["total_cg"] - int(d["total_cg"])) <= max(2, 0.02 * int(d["total_cg"]))
+
+
+@pytest.mark.parametrize("name", SENS_CASES)
+def test_oracle_sensitivity_matches_reference(name):
+    d = load(name)
+    P = oracle.as_problem(params_from(d))
+    th = torch.as_tensor(d["theta"])
+    u, g = oracle.compute_sensitivity(P, th, lambda w: torch.dot(P["f"], w), n_load_steps=2, tol=1e-12)
+    assert rel(u, d["u_star"]) < 1e-9
+    assert rel(g, d["dL_dtheta"]) < 1e-8
+
+
+def test_dolfinx_known_answers():
+    """Published dolfinx max |u| of the structured rectangle cases (benchmarks/results/validate_dolfinx.json)."""
+    for name, known in (("solve_quad4_h0.25_cantilever", 0.5168860494403356),
+                        ("solve_tri6_h0.5_cantilever", 0.5321248641215832)):
+        d = load(name)
+        assert abs(abs(d["u_star"]).max() - known) <= 1e-12 * known
