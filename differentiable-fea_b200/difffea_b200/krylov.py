@@ -9,6 +9,7 @@ area for the Krylov vectors and partial sums) stay allocated for the life of the
 contents may change between solves.
 """
 import ctypes
+import os
 import warnings
 
 import torch
@@ -18,7 +19,13 @@ from difffea_b200.cuda_mesh import ptr, stream_handle
 
 
 class DevicePCG:
+    """
+    use_graph=False (or DFEA_PCG_GRAPH=0 in the environment) launches the same kernels directly and
+    polls the status every 16 iterations -- for profilers that trace individual launches.
+    """
+
     def __init__(self, mesh, C, diag, b, x, use_graph=True):
+        use_graph = use_graph and os.environ.get("DFEA_PCG_GRAPH", "1") != "0"
         dt = _lib.DFEA_F64 if C.dtype == torch.float64 else _lib.DFEA_F32
         vt = torch.float64 if dt == _lib.DFEA_F64 else torch.float32
         for name, t in (("diag", diag), ("b", b), ("x", x)):
