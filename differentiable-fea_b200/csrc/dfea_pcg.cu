@@ -15,6 +15,7 @@
 // Termination does not depend on the numerics: k_pcg_update2 stops at max_iter and k_pcg_cond keeps
 // an independent execution counter that ends the loop after max_iter + 4 bodies in any case.
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <type_traits>
 
@@ -431,5 +432,103 @@ extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_
 
 extern "C" int dfea_pcg_destroy(dfea_pcg* h) {
     if (h) release(h);
+    return DFEA_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Allocation-free PCG: the work area is a file-scope device array instead of a caller buffer.
+// ------------------------------------------------------------------------------------------------
+// Reserved in each GPU's memory when the library's module is loaded there; kept until exit.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[DFEA_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxColours = 16;
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch for the current device.  In host code the symbol itself is a
+// host-side stand-in, so the address is looked up once per device, with that device current.
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    int rc = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    if (dev < 0 || dev >= kNoallocMaxDevices) return set_error(DFEA_ERR_INVALID, "device ordinal %d unsupported", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_address[dev] == nullptr) {
+        void* p = nullptr;
+        rc = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(g_noalloc_scratch)");
+        if (rc) return rc;
+        g_noalloc_address[dev] = p;
+    }
+    *out = g_noalloc_address[dev];
+    return DFEA_OK;
+}
+
+}  // namespace
+
+extern "C" int dfea_pcg_solve_noalloc(const dfea_mesh_view* mesh, const void* moduli, const void* diag, const void* b,
+                                      void* x, int32_t vec_dtype, double rtol, int32_t max_iter, int32_t* iters,
+                                      int32_t* status, void* stream) {
+    int rc = validate_mesh(mesh, vec_dtype == DFEA_F32);
+    if (rc) return rc;
+    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
+    if (!moduli || !diag || !b || !x) return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve_noalloc: NULL pointer");
+    auto al16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    if (!al16(moduli) || !al16(diag) || !al16(b) || !al16(x))
+        return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve_noalloc: moduli, diag, b and x must be 16-byte aligned");
+    if (x == b) return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve_noalloc: x must not alias b");
+    if (mesh->n_nodes > DFEA_NOALLOC_MAX_NODES)
+        return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve_noalloc: %lld nodes exceed the fixed scratch limit of %d nodes",
+                         (long long)mesh->n_nodes, DFEA_NOALLOC_MAX_NODES);
+    if (mesh->n_colours > kNoallocMaxColours)
+        return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve_noalloc: %d colours exceed the limit of %d", mesh->n_colours,
+                         kNoallocMaxColours);
+    if (max_iter < 1 || max_iter > 100000000) return set_error(DFEA_ERR_INVALID, "max_iter %d out of [1, 1e8]", max_iter);
+    if (!(rtol >= 0.0)) return set_error(DFEA_ERR_INVALID, "rtol must be >= 0");
+    const PcgLayout layout(mesh->n_nodes, vec_dtype == DFEA_F64 ? 8 : 4, mesh->n_colours);
+    if (layout.total > DFEA_NOALLOC_SCRATCH_BYTES)
+        return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve_noalloc: needs %lld scratch bytes, the fixed array has %d",
+                         (long long)layout.total, DFEA_NOALLOC_SCRATCH_BYTES);
+    void* scratch = nullptr;
+    if ((rc = noalloc_scratch(&scratch))) return rc;
+
+    // A handle on the stack bound to the fixed scratch: no graph, no stream, no pinned buffer.
+    dfea_pcg h;
+    int32_t host_status[4] = {DFEA_PCG_RUNNING, 0, 0, 0};
+    h.mesh = *mesh;
+    h.moduli = moduli;
+    h.diag = diag;
+    h.b = b;
+    h.x = x;
+    h.vec_dtype = vec_dtype;
+    h.work = static_cast<char*>(scratch);
+    h.layout = layout;
+    h.use_graph = 0;
+    h.host_status = host_status;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    (void)device_sm_count();
+    // k_pcg_reset (first kernel of the setup) clears the tickets and state the previous call left behind
+    rc = (vec_dtype == DFEA_F64) ? launch_setup<double>(h, s, rtol, max_iter) : launch_setup<float>(h, s, rtol, max_iter);
+    if (rc) return rc;
+    PcgState* st = h.state();
+    const int chunk = 16;
+    int launched = 0;
+    while (true) {
+        for (int i = 0; i < chunk; ++i) {
+            rc = (vec_dtype == DFEA_F64) ? launch_iteration<double>(h, s, 0, false) : launch_iteration<float>(h, s, 0, false);
+            if (rc) return rc;
+        }
+        launched += chunk;
+        if ((rc = check_cuda(cudaMemcpyAsync(host_status, &st->done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+                             "cudaMemcpyAsync")) ||
+            (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+            return rc;
+        if (host_status[0] != DFEA_PCG_RUNNING || launched > max_iter + chunk) break;
+    }
+    if (host_status[0] == DFEA_PCG_RUNNING) return set_error(DFEA_ERR_INVALID, "PCG ended without a status (internal error)");
+    if (status) *status = host_status[0];
+    if (iters) *iters = host_status[1];
     return DFEA_OK;
 }

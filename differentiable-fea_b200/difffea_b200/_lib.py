@@ -52,6 +52,8 @@ _PROTOS = {
                                        ctypes.POINTER(c_vp)]),
     "dfea_pcg_solve": (ctypes.c_int, [c_vp, c_f64, c_i32, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_vp]),
     "dfea_pcg_destroy": (ctypes.c_int, [c_vp]),
+    "dfea_pcg_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp, c_i32, c_f64, c_i32,
+                                              ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_vp]),
     "dfea_axpy": (ctypes.c_int, [c_i64, c_f64, c_vp, c_vp, c_vp]),
     "dfea_add_scaled": (ctypes.c_int, [c_i64, c_vp, c_f64, c_vp, c_vp, c_vp]),
     "dfea_f64_to_f32": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp]),

@@ -194,6 +194,28 @@ int dfea_pcg_solve(dfea_pcg* pcg, double rtol, int32_t max_iter, int32_t* iters,
 /* Release the graph and the handle (not the bound buffers). */
 int dfea_pcg_destroy(dfea_pcg* pcg);
 
+/*
+ * Jacobi-PCG without any device allocation.  This entry point has no counterpart in the reference.
+ *
+ * It is for callers that cannot allocate GPU memory themselves: a solver embedded in a host
+ * application whose memory manager owns the device (a plug-in that must not call cudaMalloc), or a
+ * caller on a latency-critical path where cudaMalloc/cudaFree would block or synchronise the device.
+ * Such a caller passes only its inputs and outputs (moduli, diag, b, x as in dfea_pcg_create) and
+ * gets the same iterates as dfea_pcg_solve with the kernels launched directly.  The Krylov vectors,
+ * partial sums and solver state live in one fixed scratch array of DFEA_NOALLOC_SCRATCH_BYTES that
+ * the library reserves in every GPU's memory when the library is loaded there, for the life of the
+ * process.  Limits: mesh->n_nodes <= DFEA_NOALLOC_MAX_NODES and mesh->n_colours <= 16; larger meshes
+ * are rejected with DFEA_ERR_INVALID and a message.  The first call on a device looks up the
+ * scratch array's device address once (with that device current); make that first call before any
+ * stream capture.  All calls share the one array, so calls that overlap on the GPU (two host threads,
+ * two streams) race and must be serialised by the caller.  Blocks the host until the solve ends.
+ */
+#define DFEA_NOALLOC_SCRATCH_BYTES (8 * 1024 * 1024)
+#define DFEA_NOALLOC_MAX_NODES 131072
+int dfea_pcg_solve_noalloc(const dfea_mesh_view* mesh, const void* moduli, const void* diag,
+                           const void* b, void* x, int32_t vec_dtype, double rtol, int32_t max_iter,
+                           int32_t* iters, int32_t* status, void* stream);
+
 /* ---------------------------------------------------------------- vector helpers -------------- */
 
 /* y = a * x + y  on n entries (f64). */
