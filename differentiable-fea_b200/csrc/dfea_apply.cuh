@@ -1,6 +1,6 @@
 // dfea_apply.cuh -- kernel (b): the stored-moduli tangent product, one colour per launch.
 //
-// For every element e of one colour (one thread per element, grid-stride):
+// For every element e of one colour (one thread per element):
 //     gather     v_e[a,i] = (m * v)[dof(e,a,i)]                      (fix bits in conn, no mask reads)
 //     contract   dgrad_iJ = sum_a v_e[a,i] dN_aJ ;  dP = C_q dgrad ;  f_e[a,i] += sum_J dP_iJ dN_aJ
 //     scatter    y[dof] += f_e  on free DOFs                         (read-modify-write, no atomics)
@@ -12,16 +12,68 @@
 //     sum_e sum_q dgrad_q . C_q dgrad_q = (m p)^T J (m p),
 // reduced per colour in fixed order: the curvature of PCG fused into the operator epilogue.
 //
-// Moduli and gradients are read once with streaming (evict-first) loads, so that the DOF vectors
-// (a few % of the traffic, gathered ~nen times) stay resident in the 126 MB L2.
+// Memory pipeline.  The kernel is persistent (a grid of a few blocks per SM walks tiles of 128
+// elements) and streams the moduli and gradients through shared memory with cp.async: the unit of
+// the pipeline is one (tile, Gauss point) item -- 8 x 16 B of moduli and nen x 16 B of gradients per
+// element in FP64 -- and STAGES items are in flight per thread, so each SM keeps ~100 KB of loads
+// outstanding without spending registers on them.  Each thread copies and later reads only its own
+// element's slots (layout [row][thread], conflict-free), so the pipeline needs no block barrier.
+// The copies bypass L1 and stream through L2 once.  The DOF vectors (a few % of the traffic, but
+// gathered and scattered once per colour pass) are kept in L2 across the passes by an access-policy
+// window on the launch that marks them persisting (see `l2_window`).
 #pragma once
 
 #include "dfea_common.cuh"
 
 namespace dfea {
 
-template <int NEN>
-__host__ __device__ constexpr int apply_threads() { return NEN <= 4 ? 256 : 128; }
+// ------------------------------------------------------------------------------------------
+// cp.async helpers (asynchronous global -> shared copies)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const size_t g = __cvta_generic_to_global(gmem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const size_t g = __cvta_generic_to_global(gmem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const size_t g = __cvta_generic_to_global(gmem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <typename T> struct ApplyUnits;
+template <> struct ApplyUnits<double> {
+    using CU = double2;              // one pair of moduli entries
+    using GU = double2;              // (dN/dX, dN/dY)
+    static constexpr int CROWS = 8;  // CU units per Gauss point
+};
+template <> struct ApplyUnits<float> {
+    using CU = float4;               // one row of the 4x4 moduli
+    using GU = float2;
+    static constexpr int CROWS = 4;
+};
+
+template <int NEN, typename T>
+struct ApplyCfg {
+    using CU = typename ApplyUnits<T>::CU;
+    using GU = typename ApplyUnits<T>::GU;
+    static constexpr int NT = 128;
+    static constexpr int CROWS = ApplyUnits<T>::CROWS;
+    static constexpr int STAGES = (sizeof(T) == 8 && NEN > 4) ? 3 : 4;
+    static constexpr int C_BYTES = CROWS * 16 * NT;                 // moduli of one item
+    static constexpr int G_BYTES = NEN * (int)sizeof(GU) * NT;      // gradients of one item
+    static constexpr int N_BYTES = NEN * 4 * NT;                    // connectivity (tile's first item)
+    static constexpr int STAGE_BYTES = C_BYTES + G_BYTES + N_BYTES;
+    static constexpr int SMEM = STAGES * STAGE_BYTES;
+};
 
 // y = (1 - m) * v : the Dirichlet identity pivot, written before the colour passes add m * J (m v).
 template <typename T>
@@ -38,71 +90,144 @@ __global__ void __launch_bounds__(kThreads) k_pivot_init(Mesh m, const T* __rest
 }
 
 template <int NEN, int NQ, typename T, bool DOT>
-__global__ void __launch_bounds__(apply_threads<NEN>())
+__global__ void __launch_bounds__(128)
 k_apply(Mesh m, int64_t e0, int64_t e1, const T* __restrict__ C, const T* __restrict__ G,
         const T* __restrict__ v, T* __restrict__ y, RedSite site, const int* __restrict__ done) {
-    constexpr int NT = apply_threads<NEN>();
+    using Cfg = ApplyCfg<NEN, T>;
+    using CU = typename Cfg::CU;
+    using GU = typename Cfg::GU;
     using T2 = v2_t<T>;
+    constexpr int NT = Cfg::NT, ST = Cfg::STAGES, CR = Cfg::CROWS;
+    extern __shared__ __align__(16) unsigned char smem[];
+
     if (DOT && done != nullptr && *done) return;  // solve finished: no-op iteration of the graph
 
+    const int tid = threadIdx.x;
     const int64_t S = m.stride;
+    const int64_t n_tiles = (e1 - e0 + NT - 1) / NT;
+    const int64_t my_tiles = (n_tiles > (int64_t)blockIdx.x) ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int64_t n_items = my_tiles * NQ;
+    const CU* Cg = reinterpret_cast<const CU*>(C);
+    const GU* Gg = reinterpret_cast<const GU*>(G);
+
+    auto element_of = [&](int64_t item) -> int64_t {
+        return e0 + ((int64_t)blockIdx.x + (item / NQ) * (int64_t)gridDim.x) * NT + tid;
+    };
+    auto c_slot = [&](int s, int k) -> CU* {
+        return reinterpret_cast<CU*>(smem + s * Cfg::STAGE_BYTES) + k * NT + tid;
+    };
+    auto g_slot = [&](int s, int a) -> GU* {
+        return reinterpret_cast<GU*>(smem + s * Cfg::STAGE_BYTES + Cfg::C_BYTES) + a * NT + tid;
+    };
+    auto n_slot = [&](int s, int a) -> int* {
+        return reinterpret_cast<int*>(smem + s * Cfg::STAGE_BYTES + Cfg::C_BYTES + Cfg::G_BYTES) + a * NT + tid;
+    };
+    // prefetch item `it` (its moduli, gradients, and at a tile's first point its connectivity)
+    auto issue = [&](int64_t it) {
+        if (it < n_items) {
+            const int64_t e = element_of(it);
+            if (e < e1) {
+                const int q = (int)(it % NQ), s = (int)(it % ST);
+#pragma unroll
+                for (int k = 0; k < CR; ++k) cp_async16(c_slot(s, k), Cg + (int64_t)(q * CR + k) * S + e);
+#pragma unroll
+                for (int a = 0; a < NEN; ++a) {
+                    if (sizeof(GU) == 16) cp_async16(g_slot(s, a), Gg + (int64_t)(q * NEN + a) * S + e);
+                    else cp_async8(g_slot(s, a), Gg + (int64_t)(q * NEN + a) * S + e);
+                }
+                if (q == 0) {
+#pragma unroll
+                    for (int a = 0; a < NEN; ++a) cp_async4(n_slot(s, a), m.conn + (int64_t)a * S + e);
+                }
+            }
+        }
+        cp_async_commit();  // empty groups keep the group count uniform
+    };
+
+#pragma unroll
+    for (int i = 0; i < ST - 1; ++i) issue(i);
+
     const T2* v2 = reinterpret_cast<const T2*>(v);
     T2* y2 = reinterpret_cast<T2*>(y);
     double curv = 0.0;
+    int node[NEN], fix[NEN];
+    T vx[NEN], vy[NEN], fx[NEN], fy[NEN];
+#pragma unroll
+    for (int a = 0; a < NEN; ++a) {
+        node[a] = 0;
+        fix[a] = 3;
+        vx[a] = vy[a] = fx[a] = fy[a] = T(0);
+    }
 
-    for (int64_t e = e0 + blockIdx.x * (int64_t)NT + threadIdx.x; e < e1; e += (int64_t)gridDim.x * NT) {
-        int node[NEN], fix[NEN];
-        T vx[NEN], vy[NEN], fx[NEN], fy[NEN];
+    for (int64_t it = 0; it < n_items; ++it) {
+        issue(it + ST - 1);
+        cp_async_wait<ST - 1>();  // item `it` has landed (groups complete in order)
+        const int64_t e = element_of(it);
+        if (e >= e1) continue;
+        const int q = (int)(it % NQ), s = (int)(it % ST);
+        if (q == 0) {
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                const int c = *n_slot(s, a);
+                node[a] = c >> 2;
+                fix[a] = c & 3;
+            }
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                const T2 t = __ldg(v2 + node[a]);
+                vx[a] = (fix[a] & 1) ? T(0) : t.x;
+                vy[a] = (fix[a] & 2) ? T(0) : t.y;
+                fx[a] = T(0);
+                fy[a] = T(0);
+            }
+        }
+        T gx[NEN], gy[NEN];
 #pragma unroll
         for (int a = 0; a < NEN; ++a) {
-            const int c = __ldcs(m.conn + a * S + e);
-            node[a] = c >> 2;
-            fix[a] = c & 3;
-            const T2 t = __ldg(v2 + node[a]);
-            vx[a] = (fix[a] & 1) ? T(0) : t.x;
-            vy[a] = (fix[a] & 2) ? T(0) : t.y;
-            fx[a] = T(0);
-            fy[a] = T(0);
+            const GU g = *g_slot(s, a);
+            gx[a] = g.x;
+            gy[a] = g.y;
         }
+        T d[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            T gx[NEN], gy[NEN];
-#pragma unroll
-            for (int a = 0; a < NEN; ++a) {
-                const T2 g = load_grad(G, (int64_t)(q * NEN + a) * S + e);
-                gx[a] = g.x;
-                gy[a] = g.y;
-            }
-            T d[4] = {T(0), T(0), T(0), T(0)};
-#pragma unroll
-            for (int a = 0; a < NEN; ++a) {
-                d[0] += vx[a] * gx[a];
-                d[1] += vx[a] * gy[a];
-                d[2] += vy[a] * gx[a];
-                d[3] += vy[a] * gy[a];
-            }
-            T dP[4];
+        for (int a = 0; a < NEN; ++a) {
+            d[0] += vx[a] * gx[a];
+            d[1] += vx[a] * gy[a];
+            d[2] += vy[a] * gx[a];
+            d[3] += vy[a] * gy[a];
+        }
+        T dP[4];
+        if constexpr (sizeof(T) == 8) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                T row[4];
-                load_moduli_row(C, S, q, r, e, row);
-                dP[r] = row[0] * d[0] + row[1] * d[1] + row[2] * d[2] + row[3] * d[3];
+                const double2 a = *reinterpret_cast<const double2*>(c_slot(s, 2 * r));
+                const double2 b = *reinterpret_cast<const double2*>(c_slot(s, 2 * r + 1));
+                dP[r] = (T)a.x * d[0] + (T)a.y * d[1] + (T)b.x * d[2] + (T)b.y * d[3];
             }
-            if (DOT) curv += (double)(d[0] * dP[0] + d[1] * dP[1] + d[2] * dP[2] + d[3] * dP[3]);
+        } else {
 #pragma unroll
-            for (int a = 0; a < NEN; ++a) {
-                fx[a] += dP[0] * gx[a] + dP[1] * gy[a];
-                fy[a] += dP[2] * gx[a] + dP[3] * gy[a];
+            for (int r = 0; r < 4; ++r) {
+                const float4 a = *reinterpret_cast<const float4*>(c_slot(s, r));
+                dP[r] = (T)a.x * d[0] + (T)a.y * d[1] + (T)a.z * d[2] + (T)a.w * d[3];
             }
         }
+        if (DOT) curv += (double)(d[0] * dP[0] + d[1] * dP[1] + d[2] * dP[2] + d[3] * dP[3]);
 #pragma unroll
         for (int a = 0; a < NEN; ++a) {
-            T2 t = y2[node[a]];
-            if (!(fix[a] & 1)) t.x += fx[a];
-            if (!(fix[a] & 2)) t.y += fy[a];
-            y2[node[a]] = t;
+            fx[a] += dP[0] * gx[a] + dP[1] * gy[a];
+            fy[a] += dP[2] * gx[a] + dP[3] * gy[a];
+        }
+        if (q == NQ - 1) {
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                T2 t = y2[node[a]];
+                if (!(fix[a] & 1)) t.x += fx[a];
+                if (!(fix[a] & 2)) t.y += fy[a];
+                y2[node[a]] = t;
+            }
         }
     }
+    cp_async_wait<0>();
 
     if (DOT) {
         const double vals[1] = {block_sum<NT>(curv)};
@@ -111,22 +236,94 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const T* __restrict__ C, const T* __rest
     }
 }
 
+// Persistent grid of k_apply for one colour: as many blocks as fit on the GPU at once (occupancy of the
+// instantiation with its shared memory), never more than there are tiles or kMaxBlocks.
+template <int NEN, int NQ, typename T, bool DOT>
+int apply_grid(int64_t n_elements) {
+    using Cfg = ApplyCfg<NEN, T>;
+    static unsigned long long configured = 0ull;  // one bit per device ordinal
+    static int blocks_per_sm[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+    if (!(configured & (1ull << dev))) {
+        cudaFuncSetAttribute(k_apply<NEN, NQ, T, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_apply<NEN, NQ, T, DOT>, Cfg::NT, Cfg::SMEM) != cudaSuccess ||
+            b < 1)
+            b = 1;
+        blocks_per_sm[dev] = b;
+        configured |= (1ull << dev);
+    }
+    const int64_t tiles = (n_elements + Cfg::NT - 1) / Cfg::NT;
+    int64_t grid = (int64_t)device_sm_count() * blocks_per_sm[dev];
+    if (grid > kMaxBlocks) grid = kMaxBlocks;
+    if (grid > tiles) grid = tiles;
+    return (int)(grid < 1 ? 1 : grid);
+}
+
+// The byte range of the DOF vectors a product gathers (v) and scatters (y): both when they are
+// adjacent (one allocation, as in the PCG work buffer), else y alone.
+struct L2Window {
+    const void* base = nullptr;
+    size_t bytes = 0;
+};
+inline L2Window l2_window(const void* v, const void* y, size_t vec_bytes) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(v), b = reinterpret_cast<uintptr_t>(y);
+    const uintptr_t lo = a < b ? a : b, hi = (a < b ? b : a) + vec_bytes;
+    if (hi - lo <= 2 * vec_bytes + 4096) return L2Window{reinterpret_cast<const void*>(lo), hi - lo};
+    return L2Window{y, vec_bytes};
+}
+
 // Launch the colour passes of one product on `stream` (the pivot init is launched by the caller).
 // With DOT, colour c reduces into sites[c] (result = curvature of that colour).
 template <int NEN, int NQ, typename T, bool DOT>
 int launch_apply_colours(const dfea_mesh_view& mv, const T* C, const T* G, const T* v, T* y,
                          const RedSite* sites, const int* done, cudaStream_t stream, bool count = true) {
-    constexpr int NT = apply_threads<NEN>();
+    using Cfg = ApplyCfg<NEN, T>;
     const Mesh m = kernel_mesh(mv);
+    long long max_window = 0;
+    const long long setaside = persisting_l2_bytes(&max_window);
+    L2Window w = l2_window(v, y, (size_t)(2 * mv.n_nodes) * sizeof(T));
+    if ((long long)w.bytes > max_window) w.bytes = (size_t)max_window;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(w.base);
+    attr[0].val.accessPolicyWindow.num_bytes = w.bytes;
+    attr[0].val.accessPolicyWindow.hitRatio =
+        (setaside > 0 && w.bytes > 0) ? (float)(setaside >= (long long)w.bytes ? 1.0 : (double)setaside / (double)w.bytes) : 0.f;
+    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    const bool use_window = setaside > 0 && w.bytes > 0;
     for (int c = 0; c < mv.n_colours; ++c) {
         const int64_t e0 = mv.colour_begin[c], e1 = mv.colour_begin[c + 1];
         if (e1 <= e0) continue;
-        const int grid = grid_for(e1 - e0, NT, NT == 256 ? 8 : 12);
+        const int grid = apply_grid<NEN, NQ, T, DOT>(e1 - e0);
         const RedSite site = DOT ? sites[c] : RedSite{nullptr, nullptr, nullptr};
-        k_apply<NEN, NQ, T, DOT><<<grid, NT, 0, stream>>>(m, e0, e1, C, G, v, y, site, done);
+        if (use_window) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(grid);
+            cfg.blockDim = dim3(Cfg::NT);
+            cfg.dynamicSmemBytes = Cfg::SMEM;
+            cfg.stream = stream;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            const int rc = check_cuda(cudaLaunchKernelEx(&cfg, k_apply<NEN, NQ, T, DOT>, m, e0, e1, C, G, v, y, site, done),
+                                      "cudaLaunchKernelEx(k_apply)");
+            if (rc) return rc;
+        } else {
+            k_apply<NEN, NQ, T, DOT><<<grid, Cfg::NT, Cfg::SMEM, stream>>>(m, e0, e1, C, G, v, y, site, done);
+        }
         if (count) note_launches(1);
     }
     return launch_check("k_apply");
+}
+
+// Configure the instantiations a solver launches (shared-memory size, occupancy) before any stream capture.
+template <int NEN, int NQ, typename T>
+void prepare_apply() {
+    (void)apply_grid<NEN, NQ, T, true>(1);
+    (void)apply_grid<NEN, NQ, T, false>(1);
+    (void)persisting_l2_bytes(nullptr);
 }
 
 }  // namespace dfea

@@ -27,6 +27,7 @@ int check_cuda(cudaError_t err, const char* what);
 int launch_check(const char* what);
 void note_launches(long long n);
 int device_sm_count();
+long long persisting_l2_bytes(long long* max_window);
 
 // Partial sums per reduction site; grids of reducing kernels never exceed this many blocks.
 constexpr int kMaxBlocks = 2048;

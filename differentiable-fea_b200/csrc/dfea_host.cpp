@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "difffea_b200.h"
@@ -44,6 +45,39 @@ int device_sm_count() {
         cache[dev] = n;
     }
     return cache[dev];
+}
+
+// L2 set-aside for persisting accesses, configured once per device (before any stream capture).
+// The tangent product marks the DOF vectors it gathers and scatters as persisting so that the
+// streamed moduli do not evict them between colour passes.  A context-level limit: it ends with
+// the process.  Returns 0 (no window) where the device or driver does not offer it.
+static std::mutex g_l2_mutex;
+static long long g_l2_setaside[64];
+static long long g_l2_window_max[64];
+static bool g_l2_init[64];
+
+long long persisting_l2_bytes(long long* max_window) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    std::lock_guard<std::mutex> lock(g_l2_mutex);
+    if (!g_l2_init[dev]) {
+        g_l2_init[dev] = true;
+        int max_persist = 0, max_win = 0;
+        if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, dev) == cudaSuccess &&
+            max_persist > 0 && max_win > 0) {
+            size_t cur = 0;
+            if (cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) == cudaSuccess && cur < (size_t)max_persist)
+                cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)max_persist);
+            if (cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
+                g_l2_setaside[dev] = (long long)cur;
+                g_l2_window_max[dev] = max_win;
+            }
+        }
+        cudaGetLastError();  // a refused limit is not an error of the caller
+    }
+    if (max_window) *max_window = g_l2_window_max[dev];
+    return g_l2_setaside[dev];
 }
 
 }  // namespace dfea

@@ -362,7 +362,14 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
     h->work = static_cast<char*>(work);
     h->layout = PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F64 ? 8 : 4, mesh->n_colours);
     h->use_graph = use_graph ? 1 : 0;
-    (void)device_sm_count();  // cache the device query before any stream capture
+    // device queries and kernel attributes are set up before any stream capture
+    (void)device_sm_count();
+    dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        if (vec_dtype == DFEA_F64) prepare_apply<NEN, NQ, double>();
+        else prepare_apply<NEN, NQ, float>();
+        return DFEA_OK;
+    });
     if ((rc = check_cuda(cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
         (rc = check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&h->host_status), 4 * sizeof(int32_t), cudaHostAllocDefault),
                          "cudaHostAlloc"))) {
