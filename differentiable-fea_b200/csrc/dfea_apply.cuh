@@ -100,8 +100,6 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const T* __restrict__ C, const T* __rest
     constexpr int NT = Cfg::NT, ST = Cfg::STAGES, CR = Cfg::CROWS;
     extern __shared__ __align__(16) unsigned char smem[];
 
-    if (DOT && done != nullptr && *done) return;  // solve finished: no-op iteration of the graph
-
     const int tid = threadIdx.x;
     const int64_t S = m.stride;
     const int64_t n_tiles = (e1 - e0 + NT - 1) / NT;
@@ -145,7 +143,15 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const T* __restrict__ C, const T* __rest
     };
 
 #pragma unroll
-    for (int i = 0; i < ST - 1; ++i) issue(i);
+    for (int i = 0; i < ST - 1; ++i) issue(i);  // moduli/gradients/connectivity: no predecessor writes them
+
+    // From here on v, y and the solver state may come from the predecessor (PDL).
+    grid_dependency_wait();
+    if (DOT && done != nullptr && *done) {  // solve finished: no-op iteration of the graph
+        cp_async_wait<0>();
+        return;
+    }
+    grid_dependents_launch();
 
     const T2* v2 = reinterpret_cast<const T2*>(v);
     T2* y2 = reinterpret_cast<T2*>(y);
@@ -285,34 +291,21 @@ int launch_apply_colours(const dfea_mesh_view& mv, const T* C, const T* G, const
     const long long setaside = persisting_l2_bytes(&max_window);
     L2Window w = l2_window(v, y, (size_t)(2 * mv.n_nodes) * sizeof(T));
     if ((long long)w.bytes > max_window) w.bytes = (size_t)max_window;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
-    attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(w.base);
-    attr[0].val.accessPolicyWindow.num_bytes = w.bytes;
-    attr[0].val.accessPolicyWindow.hitRatio =
-        (setaside > 0 && w.bytes > 0) ? (float)(setaside >= (long long)w.bytes ? 1.0 : (double)setaside / (double)w.bytes) : 0.f;
-    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-    const bool use_window = setaside > 0 && w.bytes > 0;
+    LaunchOpts opts;
+    opts.pdl = true;
+    if (setaside > 0 && w.bytes > 0) {
+        opts.win_base = w.base;
+        opts.win_bytes = w.bytes;
+        opts.hit_ratio = setaside >= (long long)w.bytes ? 1.0f : (float)((double)setaside / (double)w.bytes);
+    }
     for (int c = 0; c < mv.n_colours; ++c) {
         const int64_t e0 = mv.colour_begin[c], e1 = mv.colour_begin[c + 1];
         if (e1 <= e0) continue;
         const int grid = apply_grid<NEN, NQ, T, DOT>(e1 - e0);
         const RedSite site = DOT ? sites[c] : RedSite{nullptr, nullptr, nullptr};
-        if (use_window) {
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(grid);
-            cfg.blockDim = dim3(Cfg::NT);
-            cfg.dynamicSmemBytes = Cfg::SMEM;
-            cfg.stream = stream;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            const int rc = check_cuda(cudaLaunchKernelEx(&cfg, k_apply<NEN, NQ, T, DOT>, m, e0, e1, C, G, v, y, site, done),
-                                      "cudaLaunchKernelEx(k_apply)");
-            if (rc) return rc;
-        } else {
-            k_apply<NEN, NQ, T, DOT><<<grid, Cfg::NT, Cfg::SMEM, stream>>>(m, e0, e1, C, G, v, y, site, done);
-        }
+        const int rc = launch_kernel(k_apply<NEN, NQ, T, DOT>, dim3(grid), dim3(Cfg::NT), Cfg::SMEM, stream, opts, m, e0,
+                                     e1, C, G, v, y, site, done);
+        if (rc) return rc;
         if (count) note_launches(1);
     }
     return launch_check("k_apply");

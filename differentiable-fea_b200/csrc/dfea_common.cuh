@@ -76,6 +76,52 @@ inline int grid_for(int64_t n, int threads, int blocks_per_sm) {
 }
 
 // ------------------------------------------------------------------------------------------
+// programmatic dependent launch (PDL) and launches with attributes
+// ------------------------------------------------------------------------------------------
+// A kernel launched with the PDL attribute may start while its predecessor on the stream still
+// runs.  It must not touch anything the predecessor writes before grid_dependency_wait(), which
+// returns once the predecessor has completed and its memory is visible; every block of every PDL
+// kernel calls it before its first dependent access.  Without the attribute both are no-ops.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+struct LaunchOpts {
+    bool pdl = false;               // allow this launch to overlap its predecessor's tail
+    const void* win_base = nullptr; // L2 access-policy window marked persisting (0 bytes: none)
+    size_t win_bytes = 0;
+    float hit_ratio = 0.f;
+};
+
+template <typename... KArgs, typename... Args>
+int launch_kernel(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                  const LaunchOpts& o, Args... args) {
+    cudaLaunchAttribute attr[2];
+    unsigned n = 0;
+    if (o.pdl) {
+        attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[n].val.programmaticStreamSerializationAllowed = 1;
+        ++n;
+    }
+    if (o.win_bytes > 0 && o.hit_ratio > 0.f) {
+        attr[n].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[n].val.accessPolicyWindow.base_ptr = const_cast<void*>(o.win_base);
+        attr[n].val.accessPolicyWindow.num_bytes = o.win_bytes;
+        attr[n].val.accessPolicyWindow.hitRatio = o.hit_ratio;
+        attr[n].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[n].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        ++n;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cfg.attrs = n ? attr : nullptr;
+    cfg.numAttrs = n;
+    return check_cuda(cudaLaunchKernelEx(&cfg, kernel, args...), "cudaLaunchKernelEx");
+}
+
+// ------------------------------------------------------------------------------------------
 // deterministic reductions
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {

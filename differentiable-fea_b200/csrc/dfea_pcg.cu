@@ -114,6 +114,8 @@ __global__ void __launch_bounds__(kThreads)
 k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restrict__ y, const T* __restrict__ d,
               T* __restrict__ x, T* __restrict__ r, PcgState* st, RedSite site) {
     using T2 = v2_t<T>;
+    grid_dependency_wait();  // launched with PDL: everything below reads the predecessors' results
+    grid_dependents_launch();
     if (st->done) return;
     double curv = st->pfix;
     for (int c = 0; c < n_colours; ++c) curv += st->curv_c[c];
@@ -168,6 +170,8 @@ __global__ void __launch_bounds__(kThreads)
 k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __restrict__ p, T* __restrict__ y,
               PcgState* st, RedSite site) {
     using T2 = v2_t<T>;
+    grid_dependency_wait();
+    grid_dependents_launch();
     if (st->done) return;
     const int k = st->k;
     if (sqrt(st->rr) <= st->rtol * st->norm_b) {
@@ -271,8 +275,14 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
     });
     if (rc) return rc;
     const int gn = grid_for(mv.n_nodes, kThreads, 4);
-    k_pcg_update1<T><<<gn, kThreads, 0, s>>>(m, mv.n_colours, p, y, d, x, r, st, h.site(mv.n_colours, 2));
-    k_pcg_update2<T><<<gn, kThreads, 0, s>>>(m, r, d, p, y, st, h.site(mv.n_colours + 1, 1));
+    LaunchOpts pdl;
+    pdl.pdl = true;
+    if ((rc = launch_kernel(k_pcg_update1<T>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mv.n_colours, p,
+                            (const T*)y, d, x, r, st, h.site(mv.n_colours, 2))))
+        return rc;
+    if ((rc = launch_kernel(k_pcg_update2<T>, dim3(gn), dim3(kThreads), 0, s, pdl, m, (const T*)r, d, p, y, st,
+                            h.site(mv.n_colours + 1, 1))))
+        return rc;
     if (with_cond) k_pcg_cond<<<1, 32, 0, s>>>(st, cond);
     else note_launches(2);  // graph-captured kernels are counted when the graph's solve returns
     return launch_check("pcg iteration");
