@@ -149,7 +149,15 @@ def plain_solve(params, theta, ws=None):
 
 
 def matvec_roofline(device, reps=20):
-    """Time kernel (b) (FP64 stored moduli) at 2.56M Q4 elements with CUDA events; algorithmic bytes."""
+    """
+    Time kernel (b) (FP64 stored moduli) at 2.56M Q4 elements with CUDA events on its launch stream.
+    v and y live in one allocation, as the PCG's Krylov vectors do, so the L2 window covers both.
+    Algorithmic bytes per product: n_el*n_q*16*8 (moduli) + n_el*n_q*nen*2*8 (gradients) + n_el*nen*4
+    (connectivity) + 3*2N*8 (v read, y written, mask).
+    """
+    import ctypes
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr, stream_handle
     from difffea_b200.operators import make_tangent_operator
     from difffea_b200.problem import build_rectangle_problem
     n = MATVEC_N
@@ -157,25 +165,34 @@ def matvec_roofline(device, reps=20):
     g = torch.Generator().manual_seed(0)
     N2 = p["f"].shape[0]
     u = (((torch.rand(N2, dtype=torch.float64, generator=g) * 2 - 1) * 0.05).to(device)) * p["m"]
-    v = torch.randn(N2, dtype=torch.float64, generator=g).to(device)
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     A = make_tangent_operator("cuda", u, th, p)
+    pad = (N2 + 3) // 4 * 4
+    buf = torch.empty(2 * pad, dtype=torch.float64, device=device)
+    v, y = buf[:N2], buf[pad:pad + N2]
+    v.copy_(torch.randn(N2, dtype=torch.float64, generator=g).to(device))
     n_el, nen, nq = p["conn"].shape[0], 4, 4
     alg_bytes = n_el * nq * 16 * 8 + n_el * nq * nen * 2 * 8 + n_el * nen * 4 + 3 * N2 * 8
+
+    def product():
+        _lib.call("dfea_tangent_apply", A.mesh.view_ref, ptr(A.C), _lib.DFEA_F64, ptr(v), ptr(y), _lib.DFEA_F64,
+                  stream_handle())
     for _ in range(3):
-        A(v)
+        product()
     torch.cuda.synchronize()
     s = torch.cuda.current_stream()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(s)
     for _ in range(reps):
-        A(v)
+        product()
     t1.record(s)
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1) / reps
-    del A, p
+    y_ref = A(v)
+    ok = bool(torch.equal(y_ref, y))
+    del A, p, buf
     torch.cuda.empty_cache()
-    return dict(n_el=n_el, bytes=alg_bytes, ms=ms, gbs=alg_bytes / (ms * 1e-3) / 1e9)
+    return dict(n_el=n_el, bytes=alg_bytes, ms=ms, gbs=alg_bytes / (ms * 1e-3) / 1e9, same_as_op=ok)
 
 
 def cpu_oracle_solve(params_cpu, theta_cpu):

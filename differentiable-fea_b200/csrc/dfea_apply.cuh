@@ -89,11 +89,13 @@ __global__ void __launch_bounds__(kThreads) k_pivot_init(Mesh m, const T* __rest
     }
 }
 
-template <int NEN, int NQ, typename T, bool DOT>
+// SD: storage type of the moduli and gradients; T: type of the DOF vectors and of the arithmetic
+// (SD = float, T = double is the mixed form: FP32 operator data, FP64 Krylov vectors).
+template <int NEN, int NQ, typename SD, typename T, bool DOT>
 __global__ void __launch_bounds__(128)
-k_apply(Mesh m, int64_t e0, int64_t e1, const T* __restrict__ C, const T* __restrict__ G,
+k_apply(Mesh m, int64_t e0, int64_t e1, const SD* __restrict__ C, const SD* __restrict__ G,
         const T* __restrict__ v, T* __restrict__ y, RedSite site, const int* __restrict__ done) {
-    using Cfg = ApplyCfg<NEN, T>;
+    using Cfg = ApplyCfg<NEN, SD>;
     using CU = typename Cfg::CU;
     using GU = typename Cfg::GU;
     using T2 = v2_t<T>;
@@ -191,8 +193,8 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const T* __restrict__ C, const T* __rest
 #pragma unroll
         for (int a = 0; a < NEN; ++a) {
             const GU g = *g_slot(s, a);
-            gx[a] = g.x;
-            gy[a] = g.y;
+            gx[a] = (T)g.x;
+            gy[a] = (T)g.y;
         }
         T d[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
@@ -203,7 +205,7 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const T* __restrict__ C, const T* __rest
             d[3] += vy[a] * gy[a];
         }
         T dP[4];
-        if constexpr (sizeof(T) == 8) {
+        if constexpr (sizeof(SD) == 8) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 const double2 a = *reinterpret_cast<const double2*>(c_slot(s, 2 * r));
@@ -244,17 +246,17 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const T* __restrict__ C, const T* __rest
 
 // Persistent grid of k_apply for one colour: as many blocks as fit on the GPU at once (occupancy of the
 // instantiation with its shared memory), never more than there are tiles or kMaxBlocks.
-template <int NEN, int NQ, typename T, bool DOT>
+template <int NEN, int NQ, typename SD, typename T, bool DOT>
 int apply_grid(int64_t n_elements) {
-    using Cfg = ApplyCfg<NEN, T>;
+    using Cfg = ApplyCfg<NEN, SD>;
     static unsigned long long configured = 0ull;  // one bit per device ordinal
     static int blocks_per_sm[64] = {0};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
     if (!(configured & (1ull << dev))) {
-        cudaFuncSetAttribute(k_apply<NEN, NQ, T, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+        cudaFuncSetAttribute(k_apply<NEN, NQ, SD, T, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_apply<NEN, NQ, T, DOT>, Cfg::NT, Cfg::SMEM) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_apply<NEN, NQ, SD, T, DOT>, Cfg::NT, Cfg::SMEM) != cudaSuccess ||
             b < 1)
             b = 1;
         blocks_per_sm[dev] = b;
@@ -282,10 +284,10 @@ inline L2Window l2_window(const void* v, const void* y, size_t vec_bytes) {
 
 // Launch the colour passes of one product on `stream` (the pivot init is launched by the caller).
 // With DOT, colour c reduces into sites[c] (result = curvature of that colour).
-template <int NEN, int NQ, typename T, bool DOT>
-int launch_apply_colours(const dfea_mesh_view& mv, const T* C, const T* G, const T* v, T* y,
+template <int NEN, int NQ, typename SD, typename T, bool DOT>
+int launch_apply_colours(const dfea_mesh_view& mv, const SD* C, const SD* G, const T* v, T* y,
                          const RedSite* sites, const int* done, cudaStream_t stream, bool count = true) {
-    using Cfg = ApplyCfg<NEN, T>;
+    using Cfg = ApplyCfg<NEN, SD>;
     const Mesh m = kernel_mesh(mv);
     long long max_window = 0;
     const long long setaside = persisting_l2_bytes(&max_window);
@@ -301,9 +303,9 @@ int launch_apply_colours(const dfea_mesh_view& mv, const T* C, const T* G, const
     for (int c = 0; c < mv.n_colours; ++c) {
         const int64_t e0 = mv.colour_begin[c], e1 = mv.colour_begin[c + 1];
         if (e1 <= e0) continue;
-        const int grid = apply_grid<NEN, NQ, T, DOT>(e1 - e0);
+        const int grid = apply_grid<NEN, NQ, SD, T, DOT>(e1 - e0);
         const RedSite site = DOT ? sites[c] : RedSite{nullptr, nullptr, nullptr};
-        const int rc = launch_kernel(k_apply<NEN, NQ, T, DOT>, dim3(grid), dim3(Cfg::NT), Cfg::SMEM, stream, opts, m, e0,
+        const int rc = launch_kernel(k_apply<NEN, NQ, SD, T, DOT>, dim3(grid), dim3(Cfg::NT), Cfg::SMEM, stream, opts, m, e0,
                                      e1, C, G, v, y, site, done);
         if (rc) return rc;
         if (count) note_launches(1);
@@ -312,10 +314,10 @@ int launch_apply_colours(const dfea_mesh_view& mv, const T* C, const T* G, const
 }
 
 // Configure the instantiations a solver launches (shared-memory size, occupancy) before any stream capture.
-template <int NEN, int NQ, typename T>
+template <int NEN, int NQ, typename SD, typename T>
 void prepare_apply() {
-    (void)apply_grid<NEN, NQ, T, true>(1);
-    (void)apply_grid<NEN, NQ, T, false>(1);
+    (void)apply_grid<NEN, NQ, SD, T, true>(1);
+    (void)apply_grid<NEN, NQ, SD, T, false>(1);
     (void)persisting_l2_bytes(nullptr);
 }
 

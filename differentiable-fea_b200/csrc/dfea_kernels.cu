@@ -435,34 +435,37 @@ extern "C" int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const
 
 extern "C" int dfea_tangent_apply(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype, const void* v,
                                   void* y, int32_t vec_dtype, void* stream) {
-    int rc = validate_mesh(mesh, vec_dtype == DFEA_F32);
+    int rc = validate_mesh(mesh, moduli_dtype == DFEA_F32);
     if (rc) return rc;
     if (!moduli || !v || !y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: NULL pointer");
     if (v == y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: y must not alias v");
     if (!aligned16(moduli) || !aligned16(v) || !aligned16(y))
         return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: moduli, v and y must be 16-byte aligned");
-    if (vec_dtype == DFEA_F64 && moduli_dtype != DFEA_F64)
-        return set_error(DFEA_ERR_INVALID, "FP64 vectors need FP64 moduli");
+    if (moduli_dtype != DFEA_F64 && moduli_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad moduli dtype");
+    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
     if (vec_dtype == DFEA_F32 && moduli_dtype != DFEA_F32)
         return set_error(DFEA_ERR_INVALID, "FP32 vectors need FP32 moduli");
-    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const Mesh m = kernel_mesh(*mesh);
     const int gn = grid_for(mesh->n_nodes, kThreads, 8);
     return dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
         if (vec_dtype == DFEA_F64) {
-            k_pivot_init<double><<<gn, kThreads, 0, s>>>(m, static_cast<const double*>(v), static_cast<double*>(y));
+            const double* vv = static_cast<const double*>(v);
+            double* yy = static_cast<double*>(y);
+            k_pivot_init<double><<<gn, kThreads, 0, s>>>(m, vv, yy);
             note_launches(1);
-            return launch_apply_colours<NEN, NQ, double, false>(*mesh, static_cast<const double*>(moduli), mesh->grad,
-                                                               static_cast<const double*>(v), static_cast<double*>(y),
-                                                               nullptr, nullptr, s);
+            if (moduli_dtype == DFEA_F64)
+                return launch_apply_colours<NEN, NQ, double, double, false>(*mesh, static_cast<const double*>(moduli),
+                                                                           mesh->grad, vv, yy, nullptr, nullptr, s);
+            return launch_apply_colours<NEN, NQ, float, double, false>(*mesh, static_cast<const float*>(moduli),
+                                                                      mesh->grad32, vv, yy, nullptr, nullptr, s);
         }
         k_pivot_init<float><<<gn, kThreads, 0, s>>>(m, static_cast<const float*>(v), static_cast<float*>(y));
         note_launches(1);
-        return launch_apply_colours<NEN, NQ, float, false>(*mesh, static_cast<const float*>(moduli), mesh->grad32,
-                                                          static_cast<const float*>(v), static_cast<float*>(y),
-                                                          nullptr, nullptr, s);
+        return launch_apply_colours<NEN, NQ, float, float, false>(*mesh, static_cast<const float*>(moduli), mesh->grad32,
+                                                                 static_cast<const float*>(v), static_cast<float*>(y),
+                                                                 nullptr, nullptr, s);
     });
 }
 

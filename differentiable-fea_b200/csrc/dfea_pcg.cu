@@ -255,12 +255,13 @@ struct dfea_pcg {
 
 namespace {
 
-template <typename T>
+// S: storage type of moduli and gradients, T: Krylov vector type.
+template <typename S, typename T>
 int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHandle cond, bool with_cond) {
     const dfea_mesh_view& mv = h.mesh;
     const Mesh m = kernel_mesh(mv);
-    const T* C = static_cast<const T*>(h.moduli);
-    const T* G = std::is_same<T, float>::value ? reinterpret_cast<const T*>(mv.grad32) : reinterpret_cast<const T*>(mv.grad);
+    const S* C = static_cast<const S*>(h.moduli);
+    const S* G = std::is_same<S, float>::value ? reinterpret_cast<const S*>(mv.grad32) : reinterpret_cast<const S*>(mv.grad);
     T* r = reinterpret_cast<T*>(h.work + h.layout.off_r);
     T* p = reinterpret_cast<T*>(h.work + h.layout.off_p);
     T* y = reinterpret_cast<T*>(h.work + h.layout.off_y);
@@ -271,7 +272,7 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
     for (int c = 0; c < mv.n_colours; ++c) sites[c] = h.site(c, 1);
     int rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-        return launch_apply_colours<NEN, NQ, T, true>(mv, C, G, p, y, sites, &st->done, s, !with_cond);
+        return launch_apply_colours<NEN, NQ, S, T, true>(mv, C, G, p, y, sites, &st->done, s, !with_cond);
     });
     if (rc) return rc;
     const int gn = grid_for(mv.n_nodes, kThreads, 4);
@@ -286,6 +287,12 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
     if (with_cond) k_pcg_cond<<<1, 32, 0, s>>>(st, cond);
     else note_launches(2);  // graph-captured kernels are counted when the graph's solve returns
     return launch_check("pcg iteration");
+}
+
+int launch_iteration_any(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHandle cond, bool with_cond) {
+    if (h.vec_dtype == DFEA_F64) return launch_iteration<double, double>(h, s, cond, with_cond);
+    if (h.vec_dtype == DFEA_MIXED) return launch_iteration<float, double>(h, s, cond, with_cond);
+    return launch_iteration<float, float>(h, s, cond, with_cond);
 }
 
 template <typename T>
@@ -322,8 +329,7 @@ int build_graph(dfea_pcg* h) {
                                                        cudaStreamCaptureModeThreadLocal),
                          "cudaStreamBeginCaptureToGraph")))
         return rc;
-    rc = (h->vec_dtype == DFEA_F64) ? launch_iteration<double>(*h, h->capture_stream, cond, true)
-                                    : launch_iteration<float>(*h, h->capture_stream, cond, true);
+    rc = launch_iteration_any(*h, h->capture_stream, cond, true);
     cudaGraph_t captured = body;
     const int rc_end = check_cuda(cudaStreamEndCapture(h->capture_stream, &captured), "cudaStreamEndCapture");
     if (rc) return rc;
@@ -342,17 +348,18 @@ void release(dfea_pcg* h) {
 }  // namespace
 
 extern "C" int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype) {
-    if (!mesh || (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32)) return -1;
-    return PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F64 ? 8 : 4, mesh->n_colours).total;
+    if (!mesh || (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32 && vec_dtype != DFEA_MIXED)) return -1;
+    return PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F32 ? 4 : 8, mesh->n_colours).total;
 }
 
 extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, const void* diag, const void* b,
                                void* x, int32_t vec_dtype, void* work, int32_t use_graph, dfea_pcg** out) {
     if (!out) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: out is NULL");
     *out = nullptr;
-    int rc = validate_mesh(mesh, vec_dtype == DFEA_F32);
+    int rc = validate_mesh(mesh, vec_dtype != DFEA_F64);
     if (rc) return rc;
-    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
+    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32 && vec_dtype != DFEA_MIXED)
+        return set_error(DFEA_ERR_INVALID, "bad vector dtype");
     if (!moduli || !diag || !b || !x || !work) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: NULL pointer");
     auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 255u) == 0; };
     auto al16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
@@ -370,14 +377,15 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
     h->x = x;
     h->vec_dtype = vec_dtype;
     h->work = static_cast<char*>(work);
-    h->layout = PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F64 ? 8 : 4, mesh->n_colours);
+    h->layout = PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F32 ? 4 : 8, mesh->n_colours);
     h->use_graph = use_graph ? 1 : 0;
     // device queries and kernel attributes are set up before any stream capture
     (void)device_sm_count();
     dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-        if (vec_dtype == DFEA_F64) prepare_apply<NEN, NQ, double>();
-        else prepare_apply<NEN, NQ, float>();
+        if (vec_dtype == DFEA_F64) prepare_apply<NEN, NQ, double, double>();
+        else if (vec_dtype == DFEA_MIXED) prepare_apply<NEN, NQ, float, double>();
+        else prepare_apply<NEN, NQ, float, float>();
         return DFEA_OK;
     });
     if ((rc = check_cuda(cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
@@ -407,8 +415,8 @@ extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_
     if (max_iter < 1 || max_iter > 100000000) return set_error(DFEA_ERR_INVALID, "max_iter %d out of [1, 1e8]", max_iter);
     if (!(rtol >= 0.0)) return set_error(DFEA_ERR_INVALID, "rtol must be >= 0");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc = (h->vec_dtype == DFEA_F64) ? launch_setup<double>(*h, s, rtol, max_iter)
-                                        : launch_setup<float>(*h, s, rtol, max_iter);
+    int rc = (h->vec_dtype == DFEA_F32) ? launch_setup<float>(*h, s, rtol, max_iter)
+                                        : launch_setup<double>(*h, s, rtol, max_iter);
     if (rc) return rc;
     PcgState* st = h->state();
     if (h->use_graph) {
@@ -428,8 +436,7 @@ extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_
         h->host_status[0] = DFEA_PCG_RUNNING;
         while (true) {
             for (int i = 0; i < chunk; ++i) {
-                rc = (h->vec_dtype == DFEA_F64) ? launch_iteration<double>(*h, s, 0, false)
-                                                : launch_iteration<float>(*h, s, 0, false);
+                rc = launch_iteration_any(*h, s, 0, false);
                 if (rc) return rc;
             }
             launched += chunk;
@@ -488,9 +495,10 @@ int noalloc_scratch(void** out) {
 extern "C" int dfea_pcg_solve_noalloc(const dfea_mesh_view* mesh, const void* moduli, const void* diag, const void* b,
                                       void* x, int32_t vec_dtype, double rtol, int32_t max_iter, int32_t* iters,
                                       int32_t* status, void* stream) {
-    int rc = validate_mesh(mesh, vec_dtype == DFEA_F32);
+    int rc = validate_mesh(mesh, vec_dtype != DFEA_F64);
     if (rc) return rc;
-    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
+    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32 && vec_dtype != DFEA_MIXED)
+        return set_error(DFEA_ERR_INVALID, "bad vector dtype");
     if (!moduli || !diag || !b || !x) return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve_noalloc: NULL pointer");
     auto al16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
     if (!al16(moduli) || !al16(diag) || !al16(b) || !al16(x))
@@ -504,7 +512,7 @@ extern "C" int dfea_pcg_solve_noalloc(const dfea_mesh_view* mesh, const void* mo
                          kNoallocMaxColours);
     if (max_iter < 1 || max_iter > 100000000) return set_error(DFEA_ERR_INVALID, "max_iter %d out of [1, 1e8]", max_iter);
     if (!(rtol >= 0.0)) return set_error(DFEA_ERR_INVALID, "rtol must be >= 0");
-    const PcgLayout layout(mesh->n_nodes, vec_dtype == DFEA_F64 ? 8 : 4, mesh->n_colours);
+    const PcgLayout layout(mesh->n_nodes, vec_dtype == DFEA_F32 ? 4 : 8, mesh->n_colours);
     if (layout.total > DFEA_NOALLOC_SCRATCH_BYTES)
         return set_error(DFEA_ERR_INVALID, "dfea_pcg_solve_noalloc: needs %lld scratch bytes, the fixed array has %d",
                          (long long)layout.total, DFEA_NOALLOC_SCRATCH_BYTES);
@@ -527,14 +535,14 @@ extern "C" int dfea_pcg_solve_noalloc(const dfea_mesh_view* mesh, const void* mo
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     (void)device_sm_count();
     // k_pcg_reset (first kernel of the setup) clears the tickets and state the previous call left behind
-    rc = (vec_dtype == DFEA_F64) ? launch_setup<double>(h, s, rtol, max_iter) : launch_setup<float>(h, s, rtol, max_iter);
+    rc = (vec_dtype == DFEA_F32) ? launch_setup<float>(h, s, rtol, max_iter) : launch_setup<double>(h, s, rtol, max_iter);
     if (rc) return rc;
     PcgState* st = h.state();
     const int chunk = 16;
     int launched = 0;
     while (true) {
         for (int i = 0; i < chunk; ++i) {
-            rc = (vec_dtype == DFEA_F64) ? launch_iteration<double>(h, s, 0, false) : launch_iteration<float>(h, s, 0, false);
+            rc = launch_iteration_any(h, s, 0, false);
             if (rc) return rc;
         }
         launched += chunk;

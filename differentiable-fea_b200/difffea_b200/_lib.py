@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libdifffea_b200.so")
 DFEA_OK = 0
 DFEA_F64 = 0
 DFEA_F32 = 1
+DFEA_MIXED = 2      # PCG: FP32 moduli/gradients, FP64 Krylov vectors
 MAX_COLOURS = 64
 
 PCG_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "negative_curvature", 4: "zero_rhs"}

@@ -56,7 +56,7 @@ def edge_traction_load(nodes, edges, order, node_mask, total_force, n_gauss=3):
     edges = edges[node_mask[edges].all(dim=1)]
     if edges.shape[0] == 0:
         return f
-    s, w = gauss_1d(n_gauss, dtype, device)
+    s, w = gauss_1d(n_gauss, dtype, device)   # (host leggauss values moved to the device)
     N, dN = edge_shape(order, s)                                   # (g, k)
     Xe = nodes[edges]                                              # (E, k, 2)
     tangent = torch.einsum("gk,ekd->egd", dN, Xe)                  # dX/ds at every Gauss point

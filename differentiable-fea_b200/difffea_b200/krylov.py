@@ -26,12 +26,17 @@ class DevicePCG:
 
     def __init__(self, mesh, C, diag, b, x, use_graph=True):
         use_graph = use_graph and os.environ.get("DFEA_PCG_GRAPH", "1") != "0"
-        dt = _lib.DFEA_F64 if C.dtype == torch.float64 else _lib.DFEA_F32
-        vt = torch.float64 if dt == _lib.DFEA_F64 else torch.float32
+        vt = b.dtype
+        if C.dtype == torch.float64:
+            dt = _lib.DFEA_F64
+            if vt != torch.float64:
+                raise ValueError("FP64 moduli need FP64 vectors")
+        else:
+            dt = _lib.DFEA_MIXED if vt == torch.float64 else _lib.DFEA_F32
         for name, t in (("diag", diag), ("b", b), ("x", x)):
             if t.dtype != vt or t.numel() != mesh.n_dof or not t.is_contiguous() or t.device != mesh.device:
                 raise ValueError(f"{name} must be a contiguous ({mesh.n_dof},) {vt} tensor on {mesh.device}")
-        if dt == _lib.DFEA_F32:
+        if dt != _lib.DFEA_F64:
             mesh.ensure_grad32()
         self.mesh, self.C, self.diag, self.b, self.x = mesh, C, diag, b, x
         self.vec_dtype = vt

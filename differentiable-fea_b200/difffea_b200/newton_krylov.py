@@ -16,9 +16,10 @@ are device kernels on buffers held by a ``NewtonWorkspace``; the host reads back
 and (status, iterations) per linear solve.
 
 Extra keyword arguments (not in the reference): ``pcg_max_iter``; ``precision`` = "fp64" (default) or
-"fp32" (FP32 moduli and PCG inside the FP64 Newton loop: the residual, line search, convergence test
-and state update stay FP64, so each Newton step is an iterative-refinement correction); ``workspace``
-to reuse device buffers across solves of the same problem.
+"fp32" (the PCG applies FP32 moduli and gradients -- the bytes that dominate the operator -- to FP64
+Krylov vectors; the residual, line search, convergence test and state update stay FP64, so each Newton
+step is an iterative-refinement correction of the FP64 state computed with an FP32 operator);
+``workspace`` to reuse device buffers across solves of the same problem.
 """
 import torch
 
@@ -26,7 +27,8 @@ from difffea_b200.operators import (CudaJacobiPreconditioner, CudaTangentOperato
                                     TANGENT_OPERATORS, REFERENCE_TANGENT_VARIANTS)
 from difffea_b200.workspace import NewtonWorkspace
 
-# inner-solve floor of the FP32 PCG: its recursive residual cannot certify more than this
+# inner-solve floor with the FP32 operator: the solve is of the operator rounded to FP32, so asking it
+# for more than a few digits beyond kappa * eps_32 buys nothing for the Newton step
 FP32_MIN_RTOL = 1e-5
 
 

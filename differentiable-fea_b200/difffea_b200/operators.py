@@ -81,7 +81,8 @@ class CudaTangentOperator:
         self.last_status = None
 
     def __call__(self, v):
-        if v.dtype != self.C.dtype:
+        """A(v); FP32 moduli apply to FP32 vectors, or to FP64 vectors with FP64 arithmetic."""
+        if v.dtype != self.C.dtype and not (self.C.dtype == torch.float32 and v.dtype == torch.float64):
             raise ValueError(f"this operator applies {self.C.dtype} vectors, got {v.dtype}")
         return ops.tangent_apply(self.mesh_id, self.C, v.contiguous())
 
@@ -92,8 +93,8 @@ class CudaTangentOperator:
     def pcg_solve(self, b, diag, rtol, max_iter):
         """Jacobi-PCG on the device (kernel (c)) with this operator; returns (x in b's dtype, iterations)."""
         from difffea_b200.krylov import DevicePCG
-        vt = self.C.dtype
-        if self._pcg is None or self._pcg_diag_src is not diag:
+        vt = b.dtype if self.C.dtype == torch.float32 else torch.float64   # FP32 moduli: FP64 or FP32 vectors
+        if self._pcg is None or self._pcg_diag_src is not diag or self._pcg.vec_dtype != vt:
             d = diag.detach().to(vt).contiguous()
             n = self.mesh.n_dof
             bb = torch.empty(n, dtype=vt, device=self.mesh.device)

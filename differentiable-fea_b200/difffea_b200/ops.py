@@ -66,7 +66,7 @@ def _(mesh_id, u, theta, mu0, lambda0, fp32, with_diag):
 def tangent_apply(mesh_id: int, C: torch.Tensor, v: torch.Tensor) -> torch.Tensor:
     mesh = _mesh(mesh_id)
     fp32 = v.dtype == torch.float32
-    if fp32:
+    if C.dtype == torch.float32:
         mesh.ensure_grad32()
     if v.device != mesh.device or not v.is_contiguous() or v.numel() != mesh.n_dof:
         raise ValueError("v must be a contiguous (2N,) tensor on the mesh's device")

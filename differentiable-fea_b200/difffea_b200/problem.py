@@ -59,23 +59,25 @@ def precompute_geometry(params):
 
 
 def _assemble(nodes, conn, element_type, spec, dtype):
+    """Boundary conditions, loads and material on the device of ``nodes`` (CPU or GPU)."""
     el = get_element(element_type)
-    GP, GW = element_quadrature(element_type, dtype=dtype)
+    dev = nodes.device
+    GP, GW = element_quadrature(element_type, dtype=dtype, device=dev)
     N = nodes.shape[0]
     fixed_nodes = select_boundary_nodes(nodes, spec["fixed_side"])
     comps = {"xy": (0, 1), "x": (0,), "y": (1,)}[spec.get("fixed_dofs", "xy")]
     fixed = dofs_from_node_mask(fixed_nodes, comps)
-    u_D = torch.zeros(2 * N, dtype=dtype)
+    u_D = torch.zeros(2 * N, dtype=dtype, device=dev)
     load_nodes = select_boundary_nodes(nodes, spec["load_side"])
     value = spec.get("load_value", (0.0, 0.0))
-    f = torch.zeros(N, 2, dtype=dtype)
+    f = torch.zeros(N, 2, dtype=dtype, device=dev)
     if spec.get("load_mode", "force") == "displacement":
         for c, val in enumerate(value):
             if val is None:
                 continue
             mask = dofs_from_node_mask(load_nodes, (c,))
             fixed = fixed | mask
-            u_D = torch.where(mask, torch.as_tensor(float(val), dtype=dtype), u_D)
+            u_D = torch.where(mask, torch.as_tensor(float(val), dtype=dtype, device=dev), u_D)
     else:
         edges = boundary_edges(conn, el["edges"])
         f = edge_traction_load(nodes, edges, el["order"], load_nodes, (float(value[0]), float(value[1])))
@@ -87,7 +89,7 @@ def _assemble(nodes, conn, element_type, spec, dtype):
         values = {"mu": mu0, "lmbda": lmbda0}
     mat_p, mat_scalable = material_vector(material, values, dtype=dtype)
     return {"nodes": nodes, "conn": conn, "shape_fn": make_shape_fn(element_type), "GP": GP, "GW": GW,
-            "material": material, "mat_p": mat_p, "mat_scalable": mat_scalable,
+            "material": material, "mat_p": mat_p.to(dev), "mat_scalable": mat_scalable.to(dev),
             "f": f.reshape(-1), "m": m, "fixed": fixed, "u_D": u_D, "element_type": element_type}
 
 
@@ -109,13 +111,18 @@ def build_problem(spec):
 
 def build_rectangle_problem(element_type, nx, ny, width, height, E=1.0, nu=0.3, load=(0.0, 0.0),
                             fixed_side="left", load_side="right", fixed_dofs="xy", load_mode="force",
-                            device="cpu", dtype=torch.float64):
-    """Rectangle with an exact nx x ny cell count (the spec interface derives counts from h)."""
-    nodes, conn = create_rectangle_mesh(element_type, width, height, nx, ny, dtype=dtype)
+                            device="cpu", dtype=torch.float64, build_on_device=False):
+    """
+    Rectangle with an exact nx x ny cell count (the spec interface derives counts from h).
+    ``build_on_device`` constructs mesh, loads and geometry directly on ``device`` (torch ops there)
+    instead of on the host followed by one copy.
+    """
+    where = device if build_on_device else "cpu"
+    nodes, conn = create_rectangle_mesh(element_type, width, height, nx, ny, dtype=dtype, device=where)
     spec = dict(fixed_side=fixed_side, fixed_dofs=fixed_dofs, load_side=load_side, load_mode=load_mode,
                 load_value=load, E=E, nu=nu)
     params = precompute_geometry(_assemble(nodes, conn, element_type, spec, dtype))
-    return params if str(device) == "cpu" else to_device(params, device)
+    return params if str(params["nodes"].device) == str(torch.device(device)) else to_device(params, device)
 
 
 def build_quarter_plate_problem(element_type="quad9", n_theta=256, n_radial=256, radius=1.0, half_width=10.0,

@@ -1,0 +1,245 @@
+"""
+Continuous-batching serving of Newton-Krylov solves on one GPU.
+
+A request is a structured 4:1 cantilever bar (Q4 or Q9, nx x nx/4 cells on [0, 4] x [0, 1]), clamped at
+x = 0 and pulled at x = 4 by a uniform dead traction of `load` per unit length (axial stress ~ load, strain
+~ load / E), neo-Hookean with (E, nu).  ``request_stream`` draws the seeded stream: nx uniform over the
+multiples of 4 in [16, 512], Q4/Q9 with equal probability, E log-uniform in [0.5, 2], nu uniform in
+[0.2, 0.45], load uniform in [0.01, 0.05], Poisson arrivals.
+
+``ServingEngine`` runs requests in *slots*.  Every slot is a worker with its own CUDA stream; an admitted
+request is built on the device, solved by the device-resident Newton-Krylov solver (FP32 moduli and PCG
+inside an FP64 Newton loop by default: residual, line search, convergence test and state update in
+FP64), and its displacement copied back.  Each PCG solve is one CUDA graph with a device-side loop, so a
+slot needs the host only between Newton steps, and the kernels of all slots overlap on the GPU: a
+request that arrives while others run starts as soon as a slot and enough HBM are free (admission by
+an HBM budget), its work interleaving with theirs.  Solves are deterministic and independent, so a
+request's result does not depend on what else is in flight.
+"""
+import math
+import queue
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from difffea_b200.newton_krylov import newton_krylov_solve
+from difffea_b200.problem import build_rectangle_problem
+from difffea_b200.workspace import NewtonWorkspace
+
+NEN = {"quad4": 4, "quad9": 9}
+NQ = {"quad4": 4, "quad9": 9}
+
+
+@dataclass
+class Request:
+    rid: int
+    element_type: str
+    nx: int
+    E: float
+    nu: float
+    load: float
+    arrival: float = 0.0          # seconds after the stream starts
+
+    @property
+    def ny(self):
+        return self.nx // 4
+
+    @property
+    def n_elements(self):
+        return self.nx * self.ny
+
+    @property
+    def n_nodes(self):
+        k = 2 if self.element_type == "quad9" else 1
+        return (k * self.nx + 1) * (k * self.ny + 1)
+
+
+@dataclass
+class Result:
+    rid: int
+    u: torch.Tensor = None        # host (2N,) float64
+    converged: bool = False
+    newton: int = 0
+    cg: int = 0
+    admitted: float = 0.0
+    finished: float = 0.0
+    arrival: float = 0.0
+    error: str = ""
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+def request_stream(n=2000, seed=0, rate=None):
+    """The seeded request stream; arrivals are Poisson with ``rate`` requests/s (all at t = 0 if None)."""
+    rng = np.random.default_rng(seed)
+    nxs = rng.choice(np.arange(16, 513, 4), size=n)
+    types = np.where(rng.random(n) < 0.5, "quad4", "quad9")
+    Es = np.exp(rng.uniform(np.log(0.5), np.log(2.0), size=n))
+    nus = rng.uniform(0.2, 0.45, size=n)
+    loads = rng.uniform(0.01, 0.05, size=n)
+    gaps = rng.exponential(1.0, size=n)
+    out = []
+    t = 0.0
+    for i in range(n):
+        if rate is not None:
+            t += gaps[i] / rate
+        out.append(Request(i, str(types[i]), int(nxs[i]), float(Es[i]), float(nus[i]), float(loads[i]),
+                           arrival=t if rate is not None else 0.0))
+    return out
+
+
+def with_arrivals(requests, rate, seed=1):
+    """Copies of ``requests`` with Poisson arrival times at ``rate`` requests/s."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for r in requests:
+        t += rng.exponential(1.0 / rate)
+        out.append(Request(r.rid, r.element_type, r.nx, r.E, r.nu, r.load, arrival=t))
+    return out
+
+
+def hbm_estimate(req, precision="fp32"):
+    """Bytes a request holds on the device while it runs (problem, packed mesh, moduli, vectors)."""
+    E, N = req.n_elements, req.n_nodes
+    nen, nq = NEN[req.element_type], NQ[req.element_type]
+    per_el = (8 * nen + 16 * nq * nen + 8 * nq          # problem dictionary: conn, dN_dX, w_detJ
+              + 4 * nen + 4 + 16 * nq * nen + 8 * nq + 8  # packed mesh (FP64 gradients)
+              + 8 * nq * nen                            # FP32 gradients
+              + (64 if precision == "fp32" else 128) * nq)  # moduli
+    per_node = 16 + 2 * 8 * 14 + 2 * 4 * 6 + 1          # nodes, ~14 f64 and ~6 f32 DOF vectors, fix bits
+    return int(E * per_el + N * per_node + 4 * 2 ** 20)  # + reduction scratch and PCG state
+
+
+def solve_request(req, device, precision="fp32", n_load_steps=2, tol_rel=1e-10, pcg_max_iter=5000):
+    """Build and solve one request on the current stream; returns (u on device, info)."""
+    p = build_rectangle_problem(req.element_type, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu,
+                                load=(req.load * 1.0, 0.0), device=device, build_on_device=True)
+    th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
+    tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
+    ws = NewtonWorkspace(p, precision)
+    u, info = newton_krylov_solve(p, th, n_load_steps, tol, verbose=False, workspace=ws, precision=precision,
+                                  pcg_max_iter=pcg_max_iter)
+    ws.pcg.close()
+    return u, info
+
+
+class ServingEngine:
+    """
+    Slots x worker threads, one CUDA stream each, admission by an HBM budget.  ``run(requests)`` replays
+    the requests at their arrival times (relative to the call) and returns one Result per request.
+    """
+
+    def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=2, tol_rel=1e-10,
+                 pcg_max_iter=5000):
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            hbm_budget = int(0.6 * free)
+        self.n_slots, self.hbm_budget, self.precision = n_slots, int(hbm_budget), precision
+        self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter)
+        self._cv = threading.Condition()
+        self._in_use = 0
+        self.peak_in_use = 0
+        self.peak_in_flight = 0
+        self._in_flight = 0
+
+    # admission ------------------------------------------------------------------------------------
+    def _reserve(self, nbytes):
+        with self._cv:
+            if nbytes > self.hbm_budget:
+                raise MemoryError(f"request needs {nbytes} B, the HBM budget is {self.hbm_budget} B")
+            while self._in_use + nbytes > self.hbm_budget:
+                self._cv.wait()
+            self._in_use += nbytes
+            self._in_flight += 1
+            self.peak_in_use = max(self.peak_in_use, self._in_use)
+            self.peak_in_flight = max(self.peak_in_flight, self._in_flight)
+
+    def _release(self, nbytes):
+        with self._cv:
+            self._in_use -= nbytes
+            self._in_flight -= 1
+            self._cv.notify_all()
+
+    # run --------------------------------------------------------------------------------------------
+    def run(self, requests, keep_solutions=True):
+        results = {r.rid: Result(r.rid, arrival=r.arrival) for r in requests}
+        q = queue.Queue()
+        t0 = time.perf_counter()
+        errors = []
+
+        def worker():
+            torch.cuda.set_device(self.device)
+            stream = torch.cuda.Stream(self.device)
+            while True:
+                req = q.get()
+                if req is None:
+                    return
+                res = results[req.rid]
+                nbytes = hbm_estimate(req, self.precision)
+                reserved = False
+                try:
+                    self._reserve(nbytes)
+                    reserved = True
+                    res.admitted = time.perf_counter() - t0
+                    with torch.cuda.stream(stream):
+                        u, info = solve_request(req, self.device, **self.solve_kw)
+                        res.u = u.to("cpu") if keep_solutions else None
+                        stream.synchronize()
+                    res.converged, res.newton, res.cg = info["converged"], info["total_newton"], info["total_cg"]
+                except Exception as exc:  # a failed request must not take the engine down
+                    res.error = f"{type(exc).__name__}: {exc}"
+                    errors.append(res.error)
+                finally:
+                    res.finished = time.perf_counter() - t0
+                    if reserved:
+                        self._release(nbytes)
+
+        threads = [threading.Thread(target=worker, daemon=True) for _ in range(self.n_slots)]
+        for th in threads:
+            th.start()
+        for req in sorted(requests, key=lambda r: r.arrival):
+            delay = req.arrival - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            q.put(req)
+        for _ in threads:
+            q.put(None)
+        for th in threads:
+            th.join()
+        self.wall = time.perf_counter() - t0
+        return [results[r.rid] for r in requests]
+
+
+def run_plain(requests, device, precision="fp64", **kw):
+    """The same requests one after another on one stream (the plain drop-in path); Results in order."""
+    out = []
+    t0 = time.perf_counter()
+    for req in requests:
+        res = Result(req.rid, arrival=0.0)
+        res.admitted = time.perf_counter() - t0
+        u, info = solve_request(req, device, precision=precision, **kw)
+        res.u = u.to("cpu")
+        res.converged, res.newton, res.cg = info["converged"], info["total_newton"], info["total_cg"]
+        res.finished = time.perf_counter() - t0
+        out.append(res)
+    return out
+
+
+def percentile(values, q):
+    v = sorted(values)
+    if not v:
+        return math.nan
+    k = min(len(v) - 1, max(0, int(math.ceil(q / 100.0 * len(v))) - 1))
+    return v[k]
+
+
+def shard_requests(requests, rank, world):
+    """Requests of one replica when ``world`` GPUs serve one stream independently (round robin by id)."""
+    return [r for r in requests if r.rid % world == rank]

@@ -2,8 +2,9 @@
 Per-problem device workspace of the Newton-Krylov solver.
 
 A ``NewtonWorkspace`` keeps everything a solve touches in HBM for the whole solve: the state and
-trial vectors, the residual, the Gauss-point moduli (FP64, or FP32 for the mixed-precision inner
-solver), the Jacobi diagonal, and one graph-captured ``DevicePCG`` bound to them.  The solver loop
+trial vectors, the residual, the Gauss-point moduli (FP64, or FP32 for the mixed-precision form, whose
+operator reads FP32 moduli and gradients while the Krylov vectors stay FP64), the Jacobi diagonal,
+and one graph-captured ``DevicePCG`` bound to them.  The solver loop
 calls the C ABI directly on these buffers (no allocation per Newton step), reading back only the
 scalars the algorithm branches on: ||R|| per residual evaluation and (status, iterations) per PCG.
 """
@@ -35,17 +36,14 @@ class NewtonWorkspace:
         self.diag = torch.empty(n, **f64)
         self.scal = torch.zeros(4, **f64)
         self.scal_host = torch.zeros(4, dtype=torch.float64).pin_memory()
-        vt = torch.float64 if precision == "fp64" else torch.float32
-        self.C = torch.empty(mesh.moduli_numel(), dtype=vt, device=dev)
-        if precision == "fp64":
-            # the PCG writes its solution straight into du
-            self.diag_v, self.b, self.x = self.diag, torch.empty(n, **f64), self.du
-        else:
+        # "fp32": FP32 moduli and gradients (the bytes of the operator), FP64 Krylov vectors and scalars
+        self.C = torch.empty(mesh.moduli_numel(), dtype=torch.float64 if precision == "fp64" else torch.float32,
+                             device=dev)
+        if precision == "fp32":
             mesh.ensure_grad32()
-            self.diag_v = torch.empty(n, dtype=vt, device=dev)
-            self.b = torch.empty(n, dtype=vt, device=dev)
-            self.x = torch.empty(n, dtype=vt, device=dev)
-        self.pcg = DevicePCG(mesh, self.C, self.diag_v, self.b, self.x, use_graph=use_graph)
+        # the PCG reads -R from b and writes its solution straight into du
+        self.b = torch.empty(n, **f64)
+        self.pcg = DevicePCG(mesh, self.C, self.diag, self.b, self.du, use_graph=use_graph)
         self.work = mesh.reduce_work()
         self.theta = None
         self.n_launch_groups = 0
@@ -72,19 +70,11 @@ class NewtonWorkspace:
         dt = _lib.DFEA_F64 if self.precision == "fp64" else _lib.DFEA_F32
         _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0, ptr(self.C), dt,
                   ptr(self.diag), stream_handle())
-        if self.precision == "fp32":
-            _lib.call("dfea_f64_to_f32", self.mesh.n_dof, ptr(self.diag), ptr(self.diag_v), stream_handle())
 
     def solve(self, R, rtol, max_iter):
         """du = PCG(A, -R) to relative tolerance rtol; returns (du (FP64 buffer), iterations, status)."""
-        if self.precision == "fp64":
-            torch.neg(R, out=self.b)
-        else:
-            _lib.call("dfea_f64_to_f32", self.mesh.n_dof, ptr(R), ptr(self.b), stream_handle())
-            self.b.neg_()
+        torch.neg(R, out=self.b)
         iters, status = self.pcg.solve(rtol, max_iter)
-        if self.precision == "fp32":
-            _lib.call("dfea_f32_to_f64", self.mesh.n_dof, ptr(self.x), ptr(self.du), stream_handle())
         return self.du, iters, status
 
     def trial(self, u, alpha, du, out):

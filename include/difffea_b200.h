@@ -40,6 +40,7 @@ extern "C" {
 
 #define DFEA_F64 0
 #define DFEA_F32 1
+#define DFEA_MIXED 2  /* PCG only: FP32 moduli and gradients (the operator), FP64 Krylov vectors */
 
 #define DFEA_MAX_COLOURS 64
 
@@ -128,8 +129,8 @@ int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const double* th
 /*
  * Kernel (b): y = m * J(u) (m * v) + (1 - m) * v from the stored moduli, i.e. the `qp`/`qp_ew`
  * tangent product (operators.py:345-412).  One fused gather-contract-scatter launch per colour;
- * no atomics.  vec_dtype selects f64 or f32 vectors; with f32 vectors the moduli must be f32 and
- * mesh->grad32 must be set.  y must not alias v.
+ * no atomics.  vec_dtype selects f64 or f32 vectors; f32 moduli (with mesh->grad32 set) may be applied
+ * to f64 vectors (arithmetic in f64) or f32 vectors; f32 vectors need f32 moduli.  y must not alias v.
  */
 int dfea_tangent_apply(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype,
                        const void* v, void* y, int32_t vec_dtype, void* stream);
@@ -177,7 +178,8 @@ int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
  * x0 = 0, stop when ||r|| <= rtol ||b|| or at max_iter, early exit on p.Ap <= 0 returning z at
  * k = 0 and x otherwise).  moduli/diag/b/x are device buffers that stay bound to the handle;
  * their CONTENTS may change between solves.  vec_dtype DFEA_F64 needs f64 moduli; DFEA_F32 needs
- * f32 moduli and mesh->grad32, and then diag, b and x are f32.  The graph is captured on an internal
+ * f32 moduli and mesh->grad32, and then diag, b and x are f32; DFEA_MIXED applies f32 moduli and
+ * mesh->grad32 to f64 vectors (diag, b, x f64): FP32 operator data, FP64 recurrences.  The graph is captured on an internal
  * stream; `use_graph` = 0 launches the same kernels directly (host-polled every 16 iterations).
  */
 int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, const void* diag,

@@ -145,3 +145,13 @@ def test_reference_built_dictionary_on_device_is_accepted():
     y = make_tangent_operator("cuda", u, torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV), p)(
         torch.as_tensor(d["v"], device=DEV))
     assert rel(y, d["Av_qp_ew"]) < 1e-11
+
+
+@pytest.mark.parametrize("name", ["operator_quad4_h0.1_theta", "operator_quad9_h0.25_theta"])
+def test_fp32_moduli_on_fp64_vectors(name):
+    """The mixed operator: FP32 moduli and gradients applied to FP64 vectors in FP64 arithmetic."""
+    d, p, u, v, th = golden_case(name)
+    A32 = make_A_operator_cuda(u, th, p, precision="fp32")
+    y = A32(v)
+    assert y.dtype == torch.float64
+    assert rel(y, d["Av_qp_ew"]) < 2e-6
