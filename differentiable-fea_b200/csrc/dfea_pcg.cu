@@ -337,6 +337,24 @@ int build_graph(dfea_pcg* h) {
     return check_cuda(cudaGraphInstantiate(&h->exec, h->graph, 0), "cudaGraphInstantiate");
 }
 
+// Unrolled form: kUnrolled iterations captured back to back in a plain graph (no conditional node),
+// replayed by the host until the status word reports an end.  Iterations after the end are no-ops.
+constexpr int kUnrolled = 8;
+
+int build_unrolled_graph(dfea_pcg* h) {
+    int rc;
+    if ((rc = check_cuda(cudaStreamBeginCapture(h->capture_stream, cudaStreamCaptureModeThreadLocal),
+                         "cudaStreamBeginCapture")))
+        return rc;
+    for (int i = 0; i < kUnrolled && rc == DFEA_OK; ++i) rc = launch_iteration_any(*h, h->capture_stream, 0, false);
+    cudaGraph_t g = nullptr;
+    const int rc_end = check_cuda(cudaStreamEndCapture(h->capture_stream, &g), "cudaStreamEndCapture");
+    h->graph = g;
+    if (rc) return rc;
+    if (rc_end) return rc_end;
+    return check_cuda(cudaGraphInstantiate(&h->exec, h->graph, 0), "cudaGraphInstantiate");
+}
+
 void release(dfea_pcg* h) {
     if (h->exec) cudaGraphExecDestroy(h->exec);
     if (h->graph) cudaGraphDestroy(h->graph);
@@ -378,7 +396,7 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
     h->vec_dtype = vec_dtype;
     h->work = static_cast<char*>(work);
     h->layout = PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F32 ? 4 : 8, mesh->n_colours);
-    h->use_graph = use_graph ? 1 : 0;
+    h->use_graph = (use_graph == 2) ? 2 : (use_graph ? 1 : 0);
     // device queries and kernel attributes are set up before any stream capture
     (void)device_sm_count();
     dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
@@ -401,7 +419,11 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
         release(h);
         return rc;
     }
-    if (h->use_graph && (rc = build_graph(h))) {
+    if (h->use_graph == 1 && (rc = build_graph(h))) {
+        release(h);
+        return rc;
+    }
+    if (h->use_graph == 2 && (rc = build_unrolled_graph(h))) {
         release(h);
         return rc;
     }
@@ -419,7 +441,22 @@ extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_
                                         : launch_setup<double>(*h, s, rtol, max_iter);
     if (rc) return rc;
     PcgState* st = h->state();
-    if (h->use_graph) {
+    if (h->use_graph == 2) {
+        int launched = 0;
+        h->host_status[0] = DFEA_PCG_RUNNING;
+        while (true) {
+            if ((rc = check_cuda(cudaGraphLaunch(h->exec, s), "cudaGraphLaunch"))) return rc;
+            launched += kUnrolled;
+            if ((rc = check_cuda(cudaMemcpyAsync(h->host_status, &st->done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+                                 "cudaMemcpyAsync")) ||
+                (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+                return rc;
+            if (h->host_status[0] != DFEA_PCG_RUNNING || launched > max_iter + kUnrolled) break;
+        }
+        int nonempty = 0;
+        for (int c = 0; c < h->mesh.n_colours; ++c) nonempty += h->mesh.colour_begin[c + 1] > h->mesh.colour_begin[c];
+        note_launches((long long)launched * (nonempty + 2));
+    } else if (h->use_graph) {
         if ((rc = check_cuda(cudaGraphLaunch(h->exec, s), "cudaGraphLaunch"))) return rc;
         if ((rc = check_cuda(cudaMemcpyAsync(h->host_status, &st->done, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
                              "cudaMemcpyAsync")) ||

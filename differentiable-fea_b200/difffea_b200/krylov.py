@@ -20,12 +20,14 @@ from difffea_b200.cuda_mesh import ptr, stream_handle
 
 class DevicePCG:
     """
-    use_graph=False (or DFEA_PCG_GRAPH=0 in the environment) launches the same kernels directly and
-    polls the status every 16 iterations -- for profilers that trace individual launches.
+    use_graph: True / 1 (default) the conditional while-loop graph; 2 an unrolled graph of 8 iterations
+    replayed until done (no conditional node: overlaps better with other streams, as in serving);
+    False / 0 (or DFEA_PCG_GRAPH=0 in the environment) the same kernels launched directly, polled every
+    16 iterations -- also the form for profilers that trace individual launches.
     """
 
     def __init__(self, mesh, C, diag, b, x, use_graph=True):
-        use_graph = use_graph and os.environ.get("DFEA_PCG_GRAPH", "1") != "0"
+        use_graph = int(use_graph) if os.environ.get("DFEA_PCG_GRAPH", "1") != "0" else 0
         vt = b.dtype
         if C.dtype == torch.float64:
             dt = _lib.DFEA_F64
@@ -47,7 +49,7 @@ class DevicePCG:
             # the handle zeroes its work area on an internal stream: order it after torch's stream
             torch.cuda.current_stream().synchronize()
             rc = _lib.load().dfea_pcg_create(mesh.view_ref, ptr(C), ptr(diag), ptr(b), ptr(x), dt, ptr(self.work),
-                                             1 if use_graph else 0, ctypes.byref(self._h))
+                                             use_graph, ctypes.byref(self._h))
             if rc != _lib.DFEA_OK and use_graph:
                 # the conditional-graph path could not be built on this device/driver: same kernels,
                 # launched directly (host-polled), rather than failing the solve

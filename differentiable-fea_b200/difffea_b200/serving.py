@@ -116,13 +116,17 @@ def hbm_estimate(req, precision="fp32"):
     return int(E * per_el + N * per_node + 4 * 2 ** 20)  # + reduction scratch and PCG state
 
 
-def solve_request(req, device, precision="fp32", n_load_steps=2, tol_rel=1e-10, pcg_max_iter=5000):
-    """Build and solve one request on the current stream; returns (u on device, info)."""
+def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2):
+    """
+    Build and solve one request on the current stream; returns (u on device, info).  ``pcg_graph`` is the
+    PCG launch form (2: unrolled graph, the default for concurrent slots; 1: conditional-loop graph;
+    0: direct launches).
+    """
     p = build_rectangle_problem(req.element_type, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu,
                                 load=(req.load * 1.0, 0.0), device=device, build_on_device=True)
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
-    ws = NewtonWorkspace(p, precision)
+    ws = NewtonWorkspace(p, precision, use_graph=pcg_graph)
     u, info = newton_krylov_solve(p, th, n_load_steps, tol, verbose=False, workspace=ws, precision=precision,
                                   pcg_max_iter=pcg_max_iter)
     ws.pcg.close()
@@ -135,14 +139,18 @@ class ServingEngine:
     the requests at their arrival times (relative to the call) and returns one Result per request.
     """
 
-    def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=2, tol_rel=1e-10,
-                 pcg_max_iter=5000):
+    def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
+                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = int(0.6 * free)
         self.n_slots, self.hbm_budget, self.precision = n_slots, int(hbm_budget), precision
-        self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter)
+        self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter,
+                             pcg_graph=pcg_graph)
+        # torch's caching allocator keeps one pool per stream; a slot whose pool already holds a block of
+        # the largest request never calls cudaMalloc (which synchronises the whole device) mid-run
+        self.prewarm_bytes = int(prewarm_bytes)
         self._cv = threading.Condition()
         self._in_use = 0
         self.peak_in_use = 0
@@ -167,6 +175,18 @@ class ServingEngine:
             self._in_flight -= 1
             self._cv.notify_all()
 
+    def _slot_streams(self):
+        """One stream per slot, created once; each stream's allocator pool is pre-warmed if asked."""
+        if getattr(self, "_streams", None) is None:
+            self._streams = [torch.cuda.Stream(self.device) for _ in range(self.n_slots)]
+            if self.prewarm_bytes > 0:
+                for st in self._streams:
+                    with torch.cuda.stream(st):
+                        blk = torch.empty(self.prewarm_bytes, dtype=torch.uint8, device=self.device)
+                        del blk
+                torch.cuda.synchronize(self.device)
+        return self._streams
+
     # run --------------------------------------------------------------------------------------------
     def run(self, requests, keep_solutions=True):
         results = {r.rid: Result(r.rid, arrival=r.arrival) for r in requests}
@@ -174,9 +194,8 @@ class ServingEngine:
         t0 = time.perf_counter()
         errors = []
 
-        def worker():
+        def worker(stream):
             torch.cuda.set_device(self.device)
-            stream = torch.cuda.Stream(self.device)
             while True:
                 req = q.get()
                 if req is None:
@@ -201,7 +220,8 @@ class ServingEngine:
                     if reserved:
                         self._release(nbytes)
 
-        threads = [threading.Thread(target=worker, daemon=True) for _ in range(self.n_slots)]
+        streams = self._slot_streams()
+        threads = [threading.Thread(target=worker, args=(st,), daemon=True) for st in streams]
         for th in threads:
             th.start()
         for req in sorted(requests, key=lambda r: r.arrival):
@@ -217,14 +237,17 @@ class ServingEngine:
         return [results[r.rid] for r in requests]
 
 
-def run_plain(requests, device, precision="fp64", **kw):
-    """The same requests one after another on one stream (the plain drop-in path); Results in order."""
+def run_plain(requests, device, precision="fp64", pcg_graph=1, **kw):
+    """
+    The same requests one after another on one stream -- the plain drop-in path (FP64, the
+    conditional-loop PCG graph of newton_krylov_solve's default workspace); Results in order.
+    """
     out = []
     t0 = time.perf_counter()
     for req in requests:
         res = Result(req.rid, arrival=0.0)
         res.admitted = time.perf_counter() - t0
-        u, info = solve_request(req, device, precision=precision, **kw)
+        u, info = solve_request(req, device, precision=precision, pcg_graph=pcg_graph, **kw)
         res.u = u.to("cpu")
         res.converged, res.newton, res.cg = info["converged"], info["total_newton"], info["total_cg"]
         res.finished = time.perf_counter() - t0

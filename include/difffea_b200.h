@@ -180,7 +180,9 @@ int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
  * their CONTENTS may change between solves.  vec_dtype DFEA_F64 needs f64 moduli; DFEA_F32 needs
  * f32 moduli and mesh->grad32, and then diag, b and x are f32; DFEA_MIXED applies f32 moduli and
  * mesh->grad32 to f64 vectors (diag, b, x f64): FP32 operator data, FP64 recurrences.  The graph is captured on an internal
- * stream; `use_graph` = 0 launches the same kernels directly (host-polled every 16 iterations).
+ * stream.  use_graph = 1: that graph; 2: 8 iterations captured back to back in a plain graph (no
+ * conditional node) replayed by the host until the status word ends, which overlaps better with other
+ * streams' work; 0: the same kernels launched directly, host-polled every 16 iterations.
  */
 int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, const void* diag,
                     const void* b, void* x, int32_t vec_dtype, void* work, int32_t use_graph,
