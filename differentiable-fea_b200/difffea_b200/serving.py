@@ -116,14 +116,23 @@ def hbm_estimate(req, precision="fp32"):
     return int(E * per_el + N * per_node + 4 * 2 ** 20)  # + reduction scratch and PCG state
 
 
-def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2):
+def request_problem(req, device="cpu", build_on_device=False):
+    """The problem dictionary of a request (on ``device``)."""
+    return build_rectangle_problem(req.element_type, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu,
+                                   load=(req.load * 1.0, 0.0), device=device, build_on_device=build_on_device)
+
+
+def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2,
+                  host_params=None):
     """
-    Build and solve one request on the current stream; returns (u on device, info).  ``pcg_graph`` is the
-    PCG launch form (2: unrolled graph, the default for concurrent slots; 1: conditional-loop graph;
-    0: direct launches).
+    Build (or copy from ``host_params``) and solve one request on the current stream; returns
+    (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
+    concurrent slots; 1: conditional-loop graph; 0: direct launches).
     """
-    p = build_rectangle_problem(req.element_type, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu,
-                                load=(req.load * 1.0, 0.0), device=device, build_on_device=True)
+    if host_params is not None:
+        p = {k: (v.to(device, non_blocking=True) if torch.is_tensor(v) else v) for k, v in host_params.items()}
+    else:
+        p = request_problem(req, device, build_on_device=True)
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
     ws = NewtonWorkspace(p, precision, use_graph=pcg_graph)
@@ -188,9 +197,21 @@ class ServingEngine:
         return self._streams
 
     # run --------------------------------------------------------------------------------------------
-    def run(self, requests, keep_solutions=True):
+    def run(self, requests, keep_solutions=True, host_params=None):
+        """
+        Serve ``requests``; ``host_params`` (rid -> problem dictionary in pinned host memory) makes each
+        slot copy its problem to the device instead of building it there.  After the call
+        ``self.device_ms`` is the device time from the first slot's start to the last slot's end
+        (CUDA events joined over the slot streams) and ``self.wall`` the host wall time.
+        """
         results = {r.rid: Result(r.rid, arrival=r.arrival) for r in requests}
         q = queue.Queue()
+        streams = self._slot_streams()
+        main = torch.cuda.current_stream(self.device)
+        ev_start, ev_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev_start.record(main)
+        for st in streams:
+            st.wait_event(ev_start)
         t0 = time.perf_counter()
         errors = []
 
@@ -208,7 +229,8 @@ class ServingEngine:
                     reserved = True
                     res.admitted = time.perf_counter() - t0
                     with torch.cuda.stream(stream):
-                        u, info = solve_request(req, self.device, **self.solve_kw)
+                        hp = host_params.get(req.rid) if host_params is not None else None
+                        u, info = solve_request(req, self.device, host_params=hp, **self.solve_kw)
                         res.u = u.to("cpu") if keep_solutions else None
                         stream.synchronize()
                     res.converged, res.newton, res.cg = info["converged"], info["total_newton"], info["total_cg"]
@@ -220,7 +242,6 @@ class ServingEngine:
                     if reserved:
                         self._release(nbytes)
 
-        streams = self._slot_streams()
         threads = [threading.Thread(target=worker, args=(st,), daemon=True) for st in streams]
         for th in threads:
             th.start()
@@ -233,6 +254,13 @@ class ServingEngine:
             q.put(None)
         for th in threads:
             th.join()
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+        ev_end.record(main)
+        ev_end.synchronize()
+        self.device_ms = ev_start.elapsed_time(ev_end)
         self.wall = time.perf_counter() - t0
         return [results[r.rid] for r in requests]
 
