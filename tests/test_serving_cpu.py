@@ -1,0 +1,143 @@
+"""
+Host logic of the serving path and of the benchmark's multi-process plumbing, on the CPU: the seeded
+request stream, Poisson arrivals, HBM estimates and admission, percentiles, sharding of the stream
+over replicas, and a world-size-2 ``gloo`` run of the rank helpers (barrier, max over ranks).
+"""
+import math
+import os
+import socket
+import threading
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+from difffea_b200.serving import (Request, ServingEngine, hbm_estimate, percentile, request_problem, request_stream,
+                                  shard_requests, with_arrivals)
+
+
+def test_request_stream_is_seeded_and_follows_its_distributions():
+    a, b = request_stream(2000, seed=0), request_stream(2000, seed=0)
+    assert [(r.element_type, r.nx, r.E, r.nu, r.load) for r in a] == [(r.element_type, r.nx, r.E, r.nu, r.load)
+                                                                      for r in b]
+    assert request_stream(50, seed=1)[0] != a[0]
+    nx = np.array([r.nx for r in a])
+    assert nx.min() >= 16 and nx.max() <= 512 and np.all(nx % 4 == 0)
+    assert 0.4 < np.mean([r.element_type == "quad4" for r in a]) < 0.6
+    E = np.array([r.E for r in a])
+    assert E.min() >= 0.5 and E.max() <= 2.0 and abs(np.mean(np.log(E))) < 0.05       # log-uniform, centred on 1
+    assert all(0.2 <= r.nu <= 0.45 and 0.01 <= r.load <= 0.05 for r in a)
+    assert [r.rid for r in a] == list(range(2000))
+    assert all(r.arrival == 0.0 for r in a)
+
+
+def test_poisson_arrivals_have_the_asked_rate():
+    reqs = with_arrivals(request_stream(2000, seed=0), rate=40.0, seed=3)
+    t = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(t) > 0)
+    gaps = np.diff(np.concatenate([[0.0], t]))
+    assert abs(gaps.mean() - 1 / 40.0) < 0.1 / 40.0
+    assert abs(gaps.std() / gaps.mean() - 1.0) < 0.1                                     # exponential: CV 1
+    s = request_stream(200, seed=0, rate=10.0)
+    assert s[-1].arrival > 0 and all(x.arrival < y.arrival for x, y in zip(s, s[1:]))
+
+
+def test_request_geometry_and_problem_dictionary():
+    r = Request(7, "quad9", 64, 1.3, 0.3, 0.02)
+    assert (r.ny, r.n_elements, r.n_nodes) == (16, 1024, 129 * 33)
+    p = request_problem(r, "cpu")
+    assert p["conn"].shape == (1024, 9) and p["nodes"].shape == (r.n_nodes, 2)
+    x = p["nodes"][:, 0]
+    assert float(x.min()) == 0.0 and float(x.max()) == 4.0
+    assert float(p["f"][0::2].sum()) == pytest.approx(0.02 * 1.0, rel=1e-12)   # traction x edge length 1
+    assert float(p["f"][1::2].abs().sum()) == 0.0
+
+
+def test_hbm_estimate_grows_with_size_and_precision():
+    small, large = Request(0, "quad4", 16, 1, 0.3, 0.02), Request(1, "quad4", 512, 1, 0.3, 0.02)
+    q9 = Request(2, "quad9", 512, 1, 0.3, 0.02)
+    assert hbm_estimate(small) < hbm_estimate(large) < hbm_estimate(q9)
+    assert hbm_estimate(large, "fp32") < hbm_estimate(large, "fp64")
+    assert hbm_estimate(q9) < 2 ** 30                      # the largest request of the stream fits easily
+
+
+def test_percentile_is_nearest_rank():
+    v = list(range(1, 101))
+    assert percentile(v, 50) == 50 and percentile(v, 99) == 99 and percentile(v, 100) == 100
+    assert percentile([3.0], 99) == 3.0
+    assert math.isnan(percentile([], 50))
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_shards_partition_the_stream(world):
+    reqs = request_stream(101, seed=0)
+    shards = [shard_requests(reqs, k, world) for k in range(world)]
+    ids = sorted(r.rid for s in shards for r in s)
+    assert ids == list(range(101))
+    assert max(len(s) for s in shards) - min(len(s) for s in shards) <= 1
+
+
+def test_admission_waits_for_budget_and_rejects_oversized():
+    eng = ServingEngine.__new__(ServingEngine)             # admission logic only: no device needed
+    eng.hbm_budget = 100
+    eng._cv = threading.Condition()
+    eng._in_use = eng._in_flight = eng.peak_in_use = eng.peak_in_flight = 0
+    with pytest.raises(MemoryError):
+        eng._reserve(101)
+    eng._reserve(60)
+    order = []
+
+    def second():
+        eng._reserve(60)                                   # must wait until the first 60 are released
+        order.append("second admitted")
+
+    t = threading.Thread(target=second)
+    t.start()
+    t.join(0.2)
+    assert t.is_alive() and not order
+    order.append("first released")
+    eng._release(60)
+    t.join(5)
+    assert order == ["first released", "second admitted"]
+    assert eng.peak_in_use == 60 and eng.peak_in_flight == 1
+    eng._release(60)
+    assert eng._in_use == 0
+
+
+# ------------------------------------------------------------------------------------------------
+# two gloo ranks: the benchmark's rank helpers and its stream windows
+# ------------------------------------------------------------------------------------------------
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    import bench
+    r, w, _ = bench.dist_init("gloo")
+    assert (r, w) == (rank, world)
+    bench.dist_barrier(w)
+    m = bench.dist_max(float(10 * rank + 1), w, torch.device("cpu"))
+    timed, warm, lat = bench.stream_windows(r, w, steps=2, warmup=3)
+    import torch.distributed as dist
+    ids = [None] * w
+    dist.all_gather_object(ids, [q.rid for q in timed])
+    out[rank] = (m, ids, len(warm), len(lat))
+    dist.destroy_process_group()
+
+
+def test_two_rank_bench_helpers_over_gloo():
+    world = 2
+    out = mp.get_context("spawn").Manager().dict()
+    mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
+    for rank in range(world):
+        m, ids, n_warm, n_lat = out[rank]
+        assert m == 11.0                                      # max over ranks of (1, 11)
+        assert set(ids[0]).isdisjoint(ids[1])                 # each replica serves its own requests
+        assert all(i % world == 0 for i in ids[0]) and all(i % world == 1 for i in ids[1])
+        assert len(ids[0]) == len(ids[1]) == 2 * 32
+        assert n_warm > 0 and n_lat == 48
