@@ -57,3 +57,24 @@ def test_dolfinx_known_answers():
                         ("solve_tri6_h0.5_cantilever", 0.5321248641215832)):
         d = load(name)
         assert abs(abs(d["u_star"]).max() - known) <= 1e-12 * known
+
+
+def test_oracle_on_the_plate_fixture():
+    """Quarter plate (mapped Q9): the reference's solution is an equilibrium of the oracle's residual."""
+    d = load("plate_quad9_24x24")
+    P = oracle.as_problem(params_from(d))
+    u, th = torch.as_tensor(d["u_star"]), torch.as_tensor(d["theta"])
+    assert float(torch.norm(oracle.residual(u, th, P))) < float(d["tol"])
+    assert abs(float(oracle.strain_energy(u, th, P)) - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))
+
+
+def test_oracle_on_the_gradient_fixture():
+    """Log-normal cantilever: equilibrium, the adjoint equation and -lambda^T dR/dtheta of the oracle."""
+    d = load("gradient_quad4_128x128")
+    P = oracle.as_problem(params_from(d))
+    u, th, lam = (torch.as_tensor(d[k]) for k in ("u_star", "theta", "lam"))
+    assert float(torch.norm(oracle.residual(u, th, P))) < float(d["tol"])
+    AT = oracle.make_transpose_operator(u, th, P)
+    b = P["m"] * P["f"]
+    assert float(torch.norm(AT(lam) - b)) <= 1.01e-10 * float(torch.norm(b))
+    assert rel(oracle.implicit_vjp(u, th, P, lam), d["dL_dtheta"]) < 1e-12
