@@ -147,7 +147,7 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters=64):
+def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters=64, pcg_graph=1):
     st = State(element, n_elements, precision)
     peak, peak_kind = hbm_peak()
     row = dict(kernel=kind, element=element, n_el=st.n_el, precision=precision, colours=st.mesh.n_colours)
@@ -157,14 +157,14 @@ def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters
         d = st.diag.to(vt)
         b = (st.p["m"].to(vt) * st.v).contiguous()
         x = torch.empty_like(b)
-        solver = DevicePCG(st.mesh, st.C, d, b, x, use_graph=1)
+        solver = DevicePCG(st.mesh, st.C, d, b, x, use_graph=pcg_graph)
 
         def fn():
             solver.solve(1e-30, pcg_iters)                     # exactly pcg_iters iterations
         ms, ms_min = time_launches(fn, reps=max(3, reps // 4), flush=flush)
         solver.close()
         nbytes = st.pcg_bytes_per_iteration()
-        row.update(ms_per_iteration=ms / pcg_iters, bytes_per_iteration=nbytes,
+        row.update(pcg_graph=solver.use_graph, ms_per_iteration=ms / pcg_iters, bytes_per_iteration=nbytes,
                    gbs=nbytes / (ms / pcg_iters * 1e-3) / 1e9)
     else:
         fn = getattr(st, kind)
@@ -210,10 +210,13 @@ def main(argv=None):
     ap.add_argument("--pcg-iters", type=int, default=64)
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--nx", type=int, default=256)
-    ap.add_argument("--pcg-graph", type=int, default=0, help="solve: 0 direct launches, 1 loop graph, 2 unrolled")
+    ap.add_argument("--pcg-graph", type=int, default=None,
+                    help="PCG form: 0 direct launches (solve's default), 1 loop graph (pcg's default), "
+                         "2 unrolled graph")
     a = ap.parse_args(argv)
     if a.kind == "solve":
-        print(json.dumps(solve_once(a.element, a.nx, a.precision, a.pcg_graph)), flush=True)
+        print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph)),
+              flush=True)
         return 0
     if a.kind == "sweep":
         for element in ("quad4", "quad9"):
@@ -221,7 +224,8 @@ def main(argv=None):
                 for n in SWEEP_ELEMENTS:
                     print(json.dumps(measure("apply", element, n, prec, a.reps, not a.no_flush)), flush=True)
         return 0
-    print(json.dumps(measure(a.kind, a.element, a.elements, a.precision, a.reps, not a.no_flush, a.pcg_iters)),
+    print(json.dumps(measure(a.kind, a.element, a.elements, a.precision, a.reps, not a.no_flush, a.pcg_iters,
+                             1 if a.pcg_graph is None else a.pcg_graph)),
           flush=True)
     return 0
 
