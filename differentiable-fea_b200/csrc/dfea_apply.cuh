@@ -89,18 +89,21 @@ __global__ void __launch_bounds__(kThreads) k_pivot_init(Mesh m, const T* __rest
     }
 }
 
+// The body of kernel (b) for elements [e0, e1), walked by this block in tiles of 128 (one element per
+// thread).  `start()` runs after the prologue's prefetches were issued and before any vector is read;
+// returning false abandons the walk (after draining the copies).  `scatter(e, node, fix, fx, fy)`
+// receives each element's result f_e.  With DOT the curvature contributions are added to `curv`.
 // SD: storage type of the moduli and gradients; T: type of the DOF vectors and of the arithmetic
 // (SD = float, T = double is the mixed form: FP32 operator data, FP64 Krylov vectors).
-template <int NEN, int NQ, typename SD, typename T, bool DOT>
-__global__ void __launch_bounds__(128)
-k_apply(Mesh m, int64_t e0, int64_t e1, const SD* __restrict__ C, const SD* __restrict__ G,
-        const T* __restrict__ v, T* __restrict__ y, RedSite site, const int* __restrict__ done) {
+template <int NEN, int NQ, typename SD, typename T, bool DOT, typename Start, typename Scatter>
+__device__ __forceinline__ bool apply_tiles(const Mesh& m, int64_t e0, int64_t e1, const SD* __restrict__ C,
+                                            const SD* __restrict__ G, const T* __restrict__ v, unsigned char* smem,
+                                            double& curv, Start&& start, Scatter&& scatter) {
     using Cfg = ApplyCfg<NEN, SD>;
     using CU = typename Cfg::CU;
     using GU = typename Cfg::GU;
     using T2 = v2_t<T>;
     constexpr int NT = Cfg::NT, ST = Cfg::STAGES, CR = Cfg::CROWS;
-    extern __shared__ __align__(16) unsigned char smem[];
 
     const int tid = threadIdx.x;
     const int64_t S = m.stride;
@@ -147,17 +150,12 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const SD* __restrict__ C, const SD* __re
 #pragma unroll
     for (int i = 0; i < ST - 1; ++i) issue(i);  // moduli/gradients/connectivity: no predecessor writes them
 
-    // From here on v, y and the solver state may come from the predecessor (PDL).
-    grid_dependency_wait();
-    if (DOT && done != nullptr && *done) {  // solve finished: no-op iteration of the graph
+    if (!start()) {
         cp_async_wait<0>();
-        return;
+        return false;
     }
-    grid_dependents_launch();
 
     const T2* v2 = reinterpret_cast<const T2*>(v);
-    T2* y2 = reinterpret_cast<T2*>(y);
-    double curv = 0.0;
     int node[NEN], fix[NEN];
     T vx[NEN], vy[NEN], fx[NEN], fy[NEN];
 #pragma unroll
@@ -225,7 +223,32 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const SD* __restrict__ C, const SD* __re
             fx[a] += dP[0] * gx[a] + dP[1] * gy[a];
             fy[a] += dP[2] * gx[a] + dP[3] * gy[a];
         }
-        if (q == NQ - 1) {
+        if (q == NQ - 1) scatter(e, node, fix, fx, fy);
+    }
+    cp_async_wait<0>();
+    return true;
+}
+
+// Colour form: y[dof] += f_e on the free DOFs of the element (read-modify-write; the elements of one
+// colour share no node).
+template <int NEN, int NQ, typename SD, typename T, bool DOT>
+__global__ void __launch_bounds__(128)
+k_apply(Mesh m, int64_t e0, int64_t e1, const SD* __restrict__ C, const SD* __restrict__ G,
+        const T* __restrict__ v, T* __restrict__ y, RedSite site, const int* __restrict__ done) {
+    using T2 = v2_t<T>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T2* y2 = reinterpret_cast<T2*>(y);
+    double curv = 0.0;
+    const bool ran = apply_tiles<NEN, NQ, SD, T, DOT>(
+        m, e0, e1, C, G, v, smem, curv,
+        [&]() -> bool {
+            // from here on v, y and the solver state may come from the predecessor (PDL)
+            grid_dependency_wait();
+            if (DOT && done != nullptr && *done) return false;  // solve finished: no-op iteration of the graph
+            grid_dependents_launch();
+            return true;
+        },
+        [&](int64_t, const int (&node)[NEN], const int (&fix)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
 #pragma unroll
             for (int a = 0; a < NEN; ++a) {
                 T2 t = y2[node[a]];
@@ -233,40 +256,115 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const SD* __restrict__ C, const SD* __re
                 if (!(fix[a] & 2)) t.y += fy[a];
                 y2[node[a]] = t;
             }
-        }
-    }
-    cp_async_wait<0>();
-
+        });
+    if (!ran) return;
     if (DOT) {
+        constexpr int NT = ApplyCfg<NEN, SD>::NT;
         const double vals[1] = {block_sum<NT>(curv)};
         double tot[1];
         if (last_block_sum<NT, 1>(vals, site, tot) && threadIdx.x == 0) site.result[0] = tot[0];
     }
 }
 
-// Persistent grid of k_apply for one colour: as many blocks as fit on the GPU at once (occupancy of the
-// instantiation with its shared memory), never more than there are tiles or kMaxBlocks.
+// Gather form, element pass: all elements in one launch, each element's f_e stored in its own slots,
+// fe[a][e] = (f_x, f_y) (coalesced: e runs fastest).  The node pass (k_node_gather, or the PCG's
+// update 1) sums them per node in a fixed order.  With DOT the curvature p.Ap (energy form) reduces
+// into site.result[0].
 template <int NEN, int NQ, typename SD, typename T, bool DOT>
-int apply_grid(int64_t n_elements) {
-    using Cfg = ApplyCfg<NEN, SD>;
+__global__ void __launch_bounds__(128)
+k_apply_elem(Mesh m, const SD* __restrict__ C, const SD* __restrict__ G, const T* __restrict__ v,
+             T* __restrict__ fe, RedSite site, const int* __restrict__ done) {
+    using T2 = v2_t<T>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T2* fe2 = reinterpret_cast<T2*>(fe);
+    const int64_t S = m.stride;
+    double curv = 0.0;
+    const bool ran = apply_tiles<NEN, NQ, SD, T, DOT>(
+        m, 0, m.n_el, C, G, v, smem, curv,
+        [&]() -> bool {
+            grid_dependency_wait();
+            if (DOT && done != nullptr && *done) return false;
+            grid_dependents_launch();
+            return true;
+        },
+        [&](int64_t e, const int (&)[NEN], const int (&)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) fe2[(int64_t)a * S + e] = make_v2<T>(fx[a], fy[a]);
+        });
+    if (!ran) return;
+    if (DOT) {
+        constexpr int NT = ApplyCfg<NEN, SD>::NT;
+        const double vals[1] = {block_sum<NT>(curv)};
+        double tot[1];
+        if (last_block_sum<NT, 1>(vals, site, tot) && threadIdx.x == 0) site.result[0] = tot[0];
+    }
+}
+
+// Sum of the element results at node n: f = sum over the node's (element, local node) slots, in the
+// incidence order (fixed, so the sum is reproducible).
+template <typename T>
+__device__ __forceinline__ v2_t<T> node_sum(const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc,
+                                            const v2_t<T>* __restrict__ fe2, int64_t n) {
+    T sx = T(0), sy = T(0);
+    const int j1 = inc_ptr[n + 1];
+    for (int j = inc_ptr[n]; j < j1; ++j) {
+        const v2_t<T> f = fe2[inc[j]];
+        sx += f.x;
+        sy += f.y;
+    }
+    return make_v2<T>(sx, sy);
+}
+
+// Gather form, node pass of a plain product: y = (1 - m) v + m * sum of the element results.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_node_gather(Mesh m, const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc, const T* __restrict__ fe,
+              const T* __restrict__ v, T* __restrict__ y) {
+    using T2 = v2_t<T>;
+    grid_dependency_wait();
+    grid_dependents_launch();
+    const T2* fe2 = reinterpret_cast<const T2*>(fe);
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fix = m.node_fix[n];
+        const T2 f = node_sum<T>(inc_ptr, inc, fe2, n);
+        const T2 vn = reinterpret_cast<const T2*>(v)[n];
+        reinterpret_cast<T2*>(y)[n] = make_v2<T>((fix & 1) ? vn.x : f.x, (fix & 2) ? vn.y : f.y);
+    }
+}
+
+// Persistent grid for a walk over n_elements: as many blocks as fit on the GPU at once (occupancy of
+// the kernel with its shared memory, configured once per device), never more than there are tiles or
+// kMaxBlocks.
+template <auto Kernel, int SMEM, int NT>
+int resident_grid(int64_t n_elements) {
     static unsigned long long configured = 0ull;  // one bit per device ordinal
     static int blocks_per_sm[64] = {0};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
     if (!(configured & (1ull << dev))) {
-        cudaFuncSetAttribute(k_apply<NEN, NQ, SD, T, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+        cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_apply<NEN, NQ, SD, T, DOT>, Cfg::NT, Cfg::SMEM) != cudaSuccess ||
-            b < 1)
-            b = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, Kernel, NT, SMEM) != cudaSuccess || b < 1) b = 1;
         blocks_per_sm[dev] = b;
         configured |= (1ull << dev);
     }
-    const int64_t tiles = (n_elements + Cfg::NT - 1) / Cfg::NT;
+    const int64_t tiles = (n_elements + NT - 1) / NT;
     int64_t grid = (int64_t)device_sm_count() * blocks_per_sm[dev];
     if (grid > kMaxBlocks) grid = kMaxBlocks;
     if (grid > tiles) grid = tiles;
     return (int)(grid < 1 ? 1 : grid);
+}
+
+template <int NEN, int NQ, typename SD, typename T, bool DOT>
+int apply_grid(int64_t n_elements) {
+    using Cfg = ApplyCfg<NEN, SD>;
+    return resident_grid<k_apply<NEN, NQ, SD, T, DOT>, Cfg::SMEM, Cfg::NT>(n_elements);
+}
+
+template <int NEN, int NQ, typename SD, typename T, bool DOT>
+int apply_elem_grid(int64_t n_elements) {
+    using Cfg = ApplyCfg<NEN, SD>;
+    return resident_grid<k_apply_elem<NEN, NQ, SD, T, DOT>, Cfg::SMEM, Cfg::NT>(n_elements);
 }
 
 // The byte range of the DOF vectors a product gathers (v) and scatters (y): both when they are
@@ -313,11 +411,38 @@ int launch_apply_colours(const dfea_mesh_view& mv, const SD* C, const SD* G, con
     return launch_check("k_apply");
 }
 
+// Gather form: the element pass over all elements (results into fe), launched with PDL and the L2
+// window on v.  The node pass is launched by the caller.
+template <int NEN, int NQ, typename SD, typename T, bool DOT>
+int launch_apply_elem(const dfea_mesh_view& mv, const SD* C, const SD* G, const T* v, T* fe, RedSite site,
+                      const int* done, cudaStream_t stream) {
+    using Cfg = ApplyCfg<NEN, SD>;
+    const Mesh m = kernel_mesh(mv);
+    long long max_window = 0;
+    const long long setaside = persisting_l2_bytes(&max_window);
+    size_t wb = (size_t)(2 * mv.n_nodes) * sizeof(T);
+    if ((long long)wb > max_window) wb = (size_t)max_window;
+    LaunchOpts opts;
+    opts.pdl = true;
+    if (setaside > 0 && wb > 0) {
+        opts.win_base = v;
+        opts.win_bytes = wb;
+        opts.hit_ratio = setaside >= (long long)wb ? 1.0f : (float)((double)setaside / (double)wb);
+    }
+    const int grid = apply_elem_grid<NEN, NQ, SD, T, DOT>(mv.n_el);
+    const int rc = launch_kernel(k_apply_elem<NEN, NQ, SD, T, DOT>, dim3(grid), dim3(Cfg::NT), Cfg::SMEM, stream, opts, m,
+                                 C, G, v, fe, site, done);
+    if (rc) return rc;
+    return launch_check("k_apply_elem");
+}
+
 // Configure the instantiations a solver launches (shared-memory size, occupancy) before any stream capture.
 template <int NEN, int NQ, typename SD, typename T>
 void prepare_apply() {
     (void)apply_grid<NEN, NQ, SD, T, true>(1);
     (void)apply_grid<NEN, NQ, SD, T, false>(1);
+    (void)apply_elem_grid<NEN, NQ, SD, T, true>(1);
+    (void)apply_elem_grid<NEN, NQ, SD, T, false>(1);
     (void)persisting_l2_bytes(nullptr);
 }
 

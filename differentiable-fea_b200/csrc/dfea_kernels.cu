@@ -469,6 +469,58 @@ extern "C" int dfea_tangent_apply(const dfea_mesh_view* mesh, const void* moduli
     });
 }
 
+extern "C" int64_t dfea_gather_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype) {
+    if (!mesh || (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32)) return -1;
+    return (int64_t)mesh->nen * mesh->stride * 2 * (vec_dtype == DFEA_F64 ? 8 : 4);
+}
+
+extern "C" int dfea_tangent_apply_gather(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype,
+                                         const void* v, void* y, int32_t vec_dtype, void* fe_work, void* stream) {
+    int rc = validate_mesh(mesh, moduli_dtype == DFEA_F32);
+    if (rc) return rc;
+    if (!mesh->node_elem_ptr || !mesh->node_elem)
+        return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply_gather: the mesh has no node incidence");
+    if (!moduli || !v || !y || !fe_work) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply_gather: NULL pointer");
+    if (v == y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply_gather: y must not alias v");
+    if (!aligned16(moduli) || !aligned16(v) || !aligned16(y) || !aligned16(fe_work))
+        return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply_gather: moduli, v, y and fe_work must be 16-byte aligned");
+    if (moduli_dtype != DFEA_F64 && moduli_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad moduli dtype");
+    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
+    if (vec_dtype == DFEA_F32 && moduli_dtype != DFEA_F32)
+        return set_error(DFEA_ERR_INVALID, "FP32 vectors need FP32 moduli");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const Mesh m = kernel_mesh(*mesh);
+    const int gn = grid_for(mesh->n_nodes, kThreads, 4);
+    const RedSite none{nullptr, nullptr, nullptr};
+    LaunchOpts pdl;
+    pdl.pdl = true;
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        if (vec_dtype == DFEA_F64) {
+            const double* vv = static_cast<const double*>(v);
+            double* fe = static_cast<double*>(fe_work);
+            int r = (moduli_dtype == DFEA_F64)
+                        ? launch_apply_elem<NEN, NQ, double, double, false>(*mesh, static_cast<const double*>(moduli),
+                                                                           mesh->grad, vv, fe, none, nullptr, s)
+                        : launch_apply_elem<NEN, NQ, float, double, false>(*mesh, static_cast<const float*>(moduli),
+                                                                          mesh->grad32, vv, fe, none, nullptr, s);
+            if (r) return r;
+            return launch_kernel(k_node_gather<double>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mesh->node_elem_ptr,
+                                 mesh->node_elem, (const double*)fe, vv, static_cast<double*>(y));
+        }
+        const float* vv = static_cast<const float*>(v);
+        float* fe = static_cast<float*>(fe_work);
+        int r = launch_apply_elem<NEN, NQ, float, float, false>(*mesh, static_cast<const float*>(moduli), mesh->grad32,
+                                                               vv, fe, none, nullptr, s);
+        if (r) return r;
+        return launch_kernel(k_node_gather<float>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mesh->node_elem_ptr,
+                             mesh->node_elem, (const float*)fe, vv, static_cast<float*>(y));
+    });
+    if (rc) return rc;
+    note_launches(2);
+    return launch_check("dfea_tangent_apply_gather");
+}
+
 extern "C" int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh) {
     (void)mesh;
     return ReduceWork::bytes();

@@ -45,10 +45,11 @@ struct PcgState {
     unsigned tickets[DFEA_MAX_COLOURS + 8];
 };
 
-// Work buffer: [r | p | Ap] vectors (2N each, 256-byte aligned), partials, state.
+// Work buffer: [r | p | Ap] vectors (2N each, 256-byte aligned), partials, state, and for the gather
+// form the element results fe (nen * stride pairs) at the end.
 struct PcgLayout {
-    int64_t off_r, off_p, off_y, off_part, off_state, total;
-    PcgLayout(int64_t n_nodes, int vec_bytes, int n_colours) {
+    int64_t off_r, off_p, off_y, off_part, off_state, off_fe, total;
+    PcgLayout(int64_t n_nodes, int vec_bytes, int n_colours, int64_t fe_pairs = 0) {
         auto up = [](int64_t x) { return (x + 255) / 256 * 256; };
         const int64_t vb = up(2 * n_nodes * vec_bytes);
         off_r = 0;
@@ -57,7 +58,8 @@ struct PcgLayout {
         off_part = 3 * vb;
         const int64_t n_sites = n_colours + 3;
         off_state = off_part + up(n_sites * 3 * (int64_t)kMaxBlocks * 8);
-        total = off_state + up(sizeof(PcgState));
+        off_fe = off_state + up(sizeof(PcgState));
+        total = off_fe + up(fe_pairs * 2 * vec_bytes);
     }
 };
 
@@ -109,10 +111,13 @@ k_pcg_setup(Mesh m, const T* __restrict__ b, const T* __restrict__ d, T* __restr
     }
 }
 
-template <typename T>
+// GATHER: Ap is not stored; each node sums its elements' results (fe, the element pass of the gather
+// form) in the incidence order, and takes p on its fixed DOFs (the identity rows).
+template <typename T, bool GATHER>
 __global__ void __launch_bounds__(kThreads)
 k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restrict__ y, const T* __restrict__ d,
-              T* __restrict__ x, T* __restrict__ r, PcgState* st, RedSite site) {
+              T* __restrict__ x, T* __restrict__ r, PcgState* st, RedSite site, const int32_t* __restrict__ inc_ptr,
+              const int32_t* __restrict__ inc, const T* __restrict__ fe) {
     using T2 = v2_t<T>;
     grid_dependency_wait();  // launched with PDL: everything below reads the predecessors' results
     grid_dependents_launch();
@@ -143,7 +148,14 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
     double rr = 0.0, rz = 0.0;
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
         const T2 pn = reinterpret_cast<const T2*>(p)[n];
-        const T2 yn = reinterpret_cast<const T2*>(y)[n];
+        T2 yn;
+        if constexpr (GATHER) {
+            const int fix = m.node_fix[n];
+            const T2 f = node_sum<T>(inc_ptr, inc, reinterpret_cast<const T2*>(fe), n);
+            yn = make_v2<T>((fix & 1) ? pn.x : f.x, (fix & 2) ? pn.y : f.y);
+        } else {
+            yn = reinterpret_cast<const T2*>(y)[n];
+        }
         const T2 dn = reinterpret_cast<const T2*>(d)[n];
         T2 xn = reinterpret_cast<const T2*>(x)[n];
         T2 rn = reinterpret_cast<const T2*>(r)[n];
@@ -165,7 +177,8 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
     }
 }
 
-template <typename T>
+// PIVOT: write Ap := (1 - m) p, the identity rows the colour passes then add to (the colour form).
+template <typename T, bool PIVOT>
 __global__ void __launch_bounds__(kThreads)
 k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __restrict__ p, T* __restrict__ y,
               PcgState* st, RedSite site) {
@@ -195,7 +208,7 @@ k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __res
         pn.x = rn.x / dn.x + bt * pn.x;
         pn.y = rn.y / dn.y + bt * pn.y;
         reinterpret_cast<T2*>(p)[n] = pn;
-        reinterpret_cast<T2*>(y)[n] = make_v2<T>((fix & 1) ? pn.x : T(0), (fix & 2) ? pn.y : T(0));
+        if (PIVOT) reinterpret_cast<T2*>(y)[n] = make_v2<T>((fix & 1) ? pn.x : T(0), (fix & 2) ? pn.y : T(0));
         if (fix & 1) pf += (double)pn.x * pn.x;
         if (fix & 2) pf += (double)pn.y * pn.y;
     }
@@ -236,6 +249,7 @@ struct dfea_pcg {
     char* work;
     PcgLayout layout{1, 8, 1};
     int use_graph;
+    bool gather = false;             // product in the gather form (element pass + node sums in update 1)
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -255,6 +269,15 @@ struct dfea_pcg {
 
 namespace {
 
+// Kernels of one iteration without the loop condition: the non-empty colour passes and two updates
+// (colour form), or the element pass and two updates (gather form).
+int kernels_per_iteration(const dfea_pcg& h) {
+    if (h.gather) return 3;
+    int nonempty = 0;
+    for (int c = 0; c < h.mesh.n_colours; ++c) nonempty += h.mesh.colour_begin[c + 1] > h.mesh.colour_begin[c];
+    return nonempty + 2;
+}
+
 // S: storage type of moduli and gradients, T: Krylov vector type.
 template <typename S, typename T>
 int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHandle cond, bool with_cond) {
@@ -268,24 +291,42 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
     const T* d = static_cast<const T*>(h.diag);
     T* x = static_cast<T*>(h.x);
     PcgState* st = h.state();
-    RedSite sites[DFEA_MAX_COLOURS];
-    for (int c = 0; c < mv.n_colours; ++c) sites[c] = h.site(c, 1);
-    int rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
-        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-        return launch_apply_colours<NEN, NQ, S, T, true>(mv, C, G, p, y, sites, &st->done, s, !with_cond);
-    });
-    if (rc) return rc;
     const int gn = grid_for(mv.n_nodes, kThreads, 4);
     LaunchOpts pdl;
     pdl.pdl = true;
-    if ((rc = launch_kernel(k_pcg_update1<T>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mv.n_colours, p,
-                            (const T*)y, d, x, r, st, h.site(mv.n_colours, 2))))
-        return rc;
-    if ((rc = launch_kernel(k_pcg_update2<T>, dim3(gn), dim3(kThreads), 0, s, pdl, m, (const T*)r, d, p, y, st,
-                            h.site(mv.n_colours + 1, 1))))
-        return rc;
+    int rc;
+    if (h.gather) {
+        // element pass (curvature into site 0, read as colour 0), node sums fused into update 1
+        T* fe = reinterpret_cast<T*>(h.work + h.layout.off_fe);
+        rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
+            constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+            return launch_apply_elem<NEN, NQ, S, T, true>(mv, C, G, p, fe, h.site(0, 1), &st->done, s);
+        });
+        if (rc) return rc;
+        if ((rc = launch_kernel(k_pcg_update1<T, true>, dim3(gn), dim3(kThreads), 0, s, pdl, m, 1, p, (const T*)y, d, x,
+                                r, st, h.site(mv.n_colours, 2), mv.node_elem_ptr, mv.node_elem, (const T*)fe)))
+            return rc;
+        if ((rc = launch_kernel(k_pcg_update2<T, false>, dim3(gn), dim3(kThreads), 0, s, pdl, m, (const T*)r, d, p, y,
+                                st, h.site(mv.n_colours + 1, 1))))
+            return rc;
+    } else {
+        RedSite sites[DFEA_MAX_COLOURS];
+        for (int c = 0; c < mv.n_colours; ++c) sites[c] = h.site(c, 1);
+        rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
+            constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+            return launch_apply_colours<NEN, NQ, S, T, true>(mv, C, G, p, y, sites, &st->done, s, false);
+        });
+        if (rc) return rc;
+        if ((rc = launch_kernel(k_pcg_update1<T, false>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mv.n_colours, p,
+                                (const T*)y, d, x, r, st, h.site(mv.n_colours, 2), (const int32_t*)nullptr,
+                                (const int32_t*)nullptr, (const T*)nullptr)))
+            return rc;
+        if ((rc = launch_kernel(k_pcg_update2<T, true>, dim3(gn), dim3(kThreads), 0, s, pdl, m, (const T*)r, d, p, y,
+                                st, h.site(mv.n_colours + 1, 1))))
+            return rc;
+    }
     if (with_cond) k_pcg_cond<<<1, 32, 0, s>>>(st, cond);
-    else note_launches(2);  // graph-captured kernels are counted when the graph's solve returns
+    else note_launches(kernels_per_iteration(h));  // graph-captured kernels are counted when the solve returns
     return launch_check("pcg iteration");
 }
 
@@ -365,9 +406,18 @@ void release(dfea_pcg* h) {
 
 }  // namespace
 
+namespace {
+// the layout of a handle: with room for the gather form's element results when the mesh has the
+// node incidence that form needs
+PcgLayout layout_for(const dfea_mesh_view& mv, int32_t vec_dtype) {
+    const int64_t fe_pairs = (mv.node_elem_ptr && mv.node_elem) ? (int64_t)mv.nen * mv.stride : 0;
+    return PcgLayout(mv.n_nodes, vec_dtype == DFEA_F32 ? 4 : 8, mv.n_colours, fe_pairs);
+}
+}  // namespace
+
 extern "C" int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype) {
     if (!mesh || (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32 && vec_dtype != DFEA_MIXED)) return -1;
-    return PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F32 ? 4 : 8, mesh->n_colours).total;
+    return layout_for(*mesh, vec_dtype).total;
 }
 
 extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, const void* diag, const void* b,
@@ -395,8 +445,14 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
     h->x = x;
     h->vec_dtype = vec_dtype;
     h->work = static_cast<char*>(work);
-    h->layout = PcgLayout(mesh->n_nodes, vec_dtype == DFEA_F32 ? 4 : 8, mesh->n_colours);
+    h->layout = layout_for(*mesh, vec_dtype);
+    h->gather = (use_graph & DFEA_PCG_GATHER) != 0;
+    use_graph &= ~DFEA_PCG_GATHER;
     h->use_graph = (use_graph == 2) ? 2 : (use_graph ? 1 : 0);
+    if (h->gather && h->layout.off_fe == h->layout.total) {
+        delete h;
+        return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: the gather form needs the mesh's node incidence");
+    }
     // device queries and kernel attributes are set up before any stream capture
     (void)device_sm_count();
     dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
@@ -453,19 +509,15 @@ extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_
                 return rc;
             if (h->host_status[0] != DFEA_PCG_RUNNING || launched > max_iter + kUnrolled) break;
         }
-        int nonempty = 0;
-        for (int c = 0; c < h->mesh.n_colours; ++c) nonempty += h->mesh.colour_begin[c + 1] > h->mesh.colour_begin[c];
-        note_launches((long long)launched * (nonempty + 2));
+        note_launches((long long)launched * kernels_per_iteration(*h));
     } else if (h->use_graph) {
         if ((rc = check_cuda(cudaGraphLaunch(h->exec, s), "cudaGraphLaunch"))) return rc;
         if ((rc = check_cuda(cudaMemcpyAsync(h->host_status, &st->done, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
                              "cudaMemcpyAsync")) ||
             (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
             return rc;
-        // each executed body ran the non-empty colour passes, two updates and the loop condition
-        int nonempty = 0;
-        for (int c = 0; c < h->mesh.n_colours; ++c) nonempty += h->mesh.colour_begin[c + 1] > h->mesh.colour_begin[c];
-        note_launches((long long)h->host_status[2] * (nonempty + 3));
+        // each executed body ran one iteration's kernels and the loop condition
+        note_launches((long long)h->host_status[2] * (kernels_per_iteration(*h) + 1));
     } else {
         // the same kernels launched directly; the host reads the status every 16 iterations
         const int chunk = 16;

@@ -18,6 +18,7 @@ DFEA_MIXED = 2      # PCG: FP32 moduli/gradients, FP64 Krylov vectors
 MAX_COLOURS = 64
 
 PCG_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "negative_curvature", 4: "zero_rhs"}
+DFEA_PCG_GATHER = 16  # dfea_pcg_create flag: gather form of the product
 
 c_i32, c_i64, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -29,6 +30,7 @@ class MeshView(ctypes.Structure):
         ("nen", c_i32), ("n_q", c_i32), ("n_colours", c_i32), ("reserved", c_i32),
         ("colour_begin", c_i64 * (MAX_COLOURS + 1)),
         ("conn", c_vp), ("orig", c_vp), ("grad", c_vp), ("wdet", c_vp), ("grad32", c_vp), ("node_fix", c_vp),
+        ("node_elem_ptr", c_vp), ("node_elem", c_vp),
     ]
 
 
@@ -43,6 +45,9 @@ _PROTOS = {
     "dfea_mesh_grad_to_f32": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp]),
     "dfea_qp_moduli": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp, c_vp]),
     "dfea_tangent_apply": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_i32, c_vp, c_vp, c_i32, c_vp]),
+    "dfea_gather_work_bytes": (c_i64, [ctypes.POINTER(MeshView), c_i32]),
+    "dfea_tangent_apply_gather": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_i32, c_vp, c_vp, c_i32, c_vp,
+                                                 c_vp]),
     "dfea_reduce_work_bytes": (c_i64, [ctypes.POINTER(MeshView)]),
     "dfea_residual": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_f64, c_vp, c_vp,
                                      c_vp, c_vp, c_vp]),

@@ -111,6 +111,9 @@ class CudaMesh:
                                           self.wdet.data_ptr())
         v.grad32 = None
         v.node_fix = self.node_fix.data_ptr()
+        v.node_elem_ptr = None
+        v.node_elem = None
+        self.node_elem_ptr = self.node_elem = None
         self._reduce_work = None
 
     # -------------------------------------------------------------------------------------------
@@ -131,6 +134,26 @@ class CudaMesh:
             self.view.grad32 = self.grad32.data_ptr()
         return self.grad32
 
+    def ensure_node_incidence(self):
+        """
+        Build the node -> element incidence of the gather form once: the slots of node n are the flat
+        indices a * stride + e of its (element, local node) pairs, in increasing order.
+        """
+        if self.node_elem is None:
+            S, nen, n, N, dev = self.stride, self.nen, self.n_el, self.n_nodes, self.device
+            if nen * S >= 2 ** 31:
+                raise ValueError("mesh too large for 32-bit incidence indices")
+            nodes = (self.conn.view(nen, S)[:, :n] >> 2).to(torch.int64).reshape(-1)
+            flat = (torch.arange(nen, device=dev)[:, None] * S + torch.arange(n, device=dev)[None, :]).reshape(-1)
+            order = torch.sort(nodes, stable=True).indices
+            self.node_elem = flat[order].to(torch.int32).contiguous()
+            ptr_ = torch.zeros(N + 1, dtype=torch.int64, device=dev)
+            ptr_[1:] = torch.cumsum(torch.bincount(nodes, minlength=N), 0)
+            self.node_elem_ptr = ptr_.to(torch.int32).contiguous()
+            self.view.node_elem_ptr = self.node_elem_ptr.data_ptr()
+            self.view.node_elem = self.node_elem.data_ptr()
+        return self.node_elem_ptr, self.node_elem
+
     def reduce_work(self):
         if self._reduce_work is None:
             nbytes = int(_lib.load().dfea_reduce_work_bytes(self.view_ref))
@@ -142,8 +165,9 @@ class CudaMesh:
 
     def hbm_bytes(self):
         t = [self.conn, self.orig, self.grad, self.wdet, self.node_fix, self.perm]
-        if self.grad32 is not None:
-            t.append(self.grad32)
+        for extra in (self.grad32, self.node_elem_ptr, self.node_elem):
+            if extra is not None:
+                t.append(extra)
         return sum(x.numel() * x.element_size() for x in t)
 
 

@@ -24,10 +24,19 @@ class DevicePCG:
     replayed until done (no conditional node: overlaps better with other streams, as in serving);
     False / 0 (or DFEA_PCG_GRAPH=0 in the environment) the same kernels launched directly, polled every
     16 iterations -- also the form for profilers that trace individual launches.
+    form: "colour" (one launch per colour, scatter by read-modify-write) or "gather" (one element pass,
+    per-node sums fused into the first vector update: 3 kernels per iteration; needs the mesh's node
+    incidence, built here).  Each form is reproducible; they agree to rounding.
     """
 
-    def __init__(self, mesh, C, diag, b, x, use_graph=True):
+    def __init__(self, mesh, C, diag, b, x, use_graph=True, form="colour"):
         use_graph = int(use_graph) if os.environ.get("DFEA_PCG_GRAPH", "1") != "0" else 0
+        if form not in ("colour", "gather"):
+            raise ValueError("form must be 'colour' or 'gather'")
+        flags = 0
+        if form == "gather":
+            mesh.ensure_node_incidence()
+            flags = _lib.DFEA_PCG_GATHER
         vt = b.dtype
         if C.dtype == torch.float64:
             dt = _lib.DFEA_F64
@@ -49,16 +58,17 @@ class DevicePCG:
             # the handle zeroes its work area on an internal stream: order it after torch's stream
             torch.cuda.current_stream().synchronize()
             rc = _lib.load().dfea_pcg_create(mesh.view_ref, ptr(C), ptr(diag), ptr(b), ptr(x), dt, ptr(self.work),
-                                             use_graph, ctypes.byref(self._h))
+                                             use_graph | flags, ctypes.byref(self._h))
             if rc != _lib.DFEA_OK and use_graph:
                 # the conditional-graph path could not be built on this device/driver: same kernels,
                 # launched directly (host-polled), rather than failing the solve
                 warnings.warn(f"PCG graph unavailable ({_lib.last_error()}); using direct launches")
                 use_graph = False
                 rc = _lib.load().dfea_pcg_create(mesh.view_ref, ptr(C), ptr(diag), ptr(b), ptr(x), dt,
-                                                 ptr(self.work), 0, ctypes.byref(self._h))
+                                                 ptr(self.work), flags, ctypes.byref(self._h))
             _lib.check(rc, "dfea_pcg_create")
         self.use_graph = use_graph
+        self.form = form
         self.last_status = None
 
     def solve(self, rtol, max_iter=500):

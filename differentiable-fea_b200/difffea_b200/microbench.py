@@ -8,6 +8,8 @@ launches unless ``--no-flush``).
     python -m difffea_b200.microbench solve --element quad4 --nx 256 --precision mixed
                                             one serving request (4:1 cantilever, E 1, nu 0.3, load 0.03)
                                             solved twice; the second solve is timed
+    --form gather                           the gather form of the product (element pass + node sums)
+                                            for apply, pcg, solve and sweep
 
 State: nodal displacements uniform in +-0.05 h on free DOFs (seeded), input vector N(0, 1), E = 1,
 nu = 0.3, h = 1.  Algorithmic bytes count every array a kernel must touch once:
@@ -51,8 +53,9 @@ def side_for(n_elements):
 class State:
     """A square n x n mesh of unit cells with a seeded state, its packed mesh and moduli."""
 
-    def __init__(self, element, n_elements, precision="fp64", device="cuda", seed=0):
+    def __init__(self, element, n_elements, precision="fp64", device="cuda", seed=0, form="colour"):
         n = side_for(n_elements)
+        self.form = form
         self.element, self.precision, self.device = element, precision, torch.device(device)
         self.p = build_rectangle_problem(element, n, n, float(n), float(n), E=1.0, nu=0.3, device=device,
                                          build_on_device=True)
@@ -75,9 +78,17 @@ class State:
         self.v.copy_(torch.randn(N2, dtype=torch.float64, generator=g).to(device))
         self.n_el = self.p["conn"].shape[0]
         self.nen, self.nq = self.p["conn"].shape[1], self.p["dN_dX"].shape[1]
+        self.fe = None
+        if form == "gather":
+            self.mesh.ensure_node_incidence()
+            vcode = _lib.DFEA_F32 if vt == torch.float32 else _lib.DFEA_F64
+            nbytes = int(_lib.load().dfea_gather_work_bytes(self.mesh.view_ref, vcode))
+            self.fe = torch.empty(nbytes, dtype=torch.uint8, device=device)
 
     # algorithmic bytes ----------------------------------------------------------------------------
     def apply_bytes(self):
+        """Bytes the product must move; the gather form is charged the colour form's minimum (its element
+        results and incidence are extra traffic it pays for fewer launches)."""
         sC, sG, sv = _SIZES[self.precision]
         return (self.n_el * self.nq * 16 * sC + self.n_el * self.nq * self.nen * 2 * sG
                 + self.n_el * self.nen * 4 + 3 * self.N2 * sv)
@@ -104,8 +115,12 @@ class State:
     def apply(self):
         cdt = _lib.DFEA_F64 if self.C.dtype == torch.float64 else _lib.DFEA_F32
         vdt = _lib.DFEA_F64 if self.v.dtype == torch.float64 else _lib.DFEA_F32
-        _lib.call("dfea_tangent_apply", self.mesh.view_ref, ptr(self.C), cdt, ptr(self.v), ptr(self.y), vdt,
-                  stream_handle())
+        if self.form == "gather":
+            _lib.call("dfea_tangent_apply_gather", self.mesh.view_ref, ptr(self.C), cdt, ptr(self.v), ptr(self.y), vdt,
+                      ptr(self.fe), stream_handle())
+        else:
+            _lib.call("dfea_tangent_apply", self.mesh.view_ref, ptr(self.C), cdt, ptr(self.v), ptr(self.y), vdt,
+                      stream_handle())
 
     def moduli(self):
         ops.qp_moduli(self.mid, self.u, self.theta, self.mu0, self.lam0, self.precision != "fp64", True)
@@ -147,17 +162,17 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters=64, pcg_graph=1):
-    st = State(element, n_elements, precision)
+def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters=64, pcg_graph=1, form="colour"):
+    st = State(element, n_elements, precision, form=form)
     peak, peak_kind = hbm_peak()
-    row = dict(kernel=kind, element=element, n_el=st.n_el, precision=precision, colours=st.mesh.n_colours)
+    row = dict(kernel=kind, element=element, n_el=st.n_el, precision=precision, colours=st.mesh.n_colours, form=form)
     if kind == "pcg":
         from difffea_b200.krylov import DevicePCG
         vt = st.v.dtype
         d = st.diag.to(vt)
         b = (st.p["m"].to(vt) * st.v).contiguous()
         x = torch.empty_like(b)
-        solver = DevicePCG(st.mesh, st.C, d, b, x, use_graph=pcg_graph)
+        solver = DevicePCG(st.mesh, st.C, d, b, x, use_graph=pcg_graph, form=form)
 
         def fn():
             solver.solve(1e-30, pcg_iters)                     # exactly pcg_iters iterations
@@ -177,7 +192,7 @@ def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters
     return row
 
 
-def solve_once(element, nx, precision, pcg_graph):
+def solve_once(element, nx, precision, pcg_graph, form="colour"):
     """Wall and device milliseconds of one serving-type request (the second of two identical solves)."""
     import time
     from difffea_b200.serving import Request, solve_request
@@ -190,11 +205,11 @@ def solve_once(element, nx, precision, pcg_graph):
         torch.cuda.synchronize()
         t = time.perf_counter()
         e0.record(s)
-        u, info = solve_request(req, "cuda", precision=prec, pcg_graph=pcg_graph)
+        u, info = solve_request(req, "cuda", precision=prec, pcg_graph=pcg_graph, pcg_form=form)
         e1.record(s)
         torch.cuda.synchronize()
         out = dict(kernel="solve", element=element, nx=nx, n_el=req.n_elements, precision=precision,
-                   pcg_graph=pcg_graph, newton=info["total_newton"], cg=info["total_cg"],
+                   pcg_graph=pcg_graph, form=form, newton=info["total_newton"], cg=info["total_cg"],
                    converged=info["converged"], device_ms=e0.elapsed_time(e1),
                    wall_ms=1e3 * (time.perf_counter() - t))
     return out
@@ -210,22 +225,25 @@ def main(argv=None):
     ap.add_argument("--pcg-iters", type=int, default=64)
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--form", default="colour", choices=("colour", "gather"),
+                    help="product form: one launch per colour, or element pass + node sums")
     ap.add_argument("--pcg-graph", type=int, default=None,
                     help="PCG form: 0 direct launches (solve's default), 1 loop graph (pcg's default), "
                          "2 unrolled graph")
     a = ap.parse_args(argv)
     if a.kind == "solve":
-        print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph)),
+        print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph, a.form)),
               flush=True)
         return 0
     if a.kind == "sweep":
         for element in ("quad4", "quad9"):
             for prec in ("fp64", "fp32"):
                 for n in SWEEP_ELEMENTS:
-                    print(json.dumps(measure("apply", element, n, prec, a.reps, not a.no_flush)), flush=True)
+                    print(json.dumps(measure("apply", element, n, prec, a.reps, not a.no_flush, form=a.form)),
+                          flush=True)
         return 0
     print(json.dumps(measure(a.kind, a.element, a.elements, a.precision, a.reps, not a.no_flush, a.pcg_iters,
-                             1 if a.pcg_graph is None else a.pcg_graph)),
+                             1 if a.pcg_graph is None else a.pcg_graph, a.form)),
           flush=True)
     return 0
 

@@ -111,8 +111,9 @@ def hbm_estimate(req, precision="fp32"):
     per_el = (8 * nen + 16 * nq * nen + 8 * nq          # problem dictionary: conn, dN_dX, w_detJ
               + 4 * nen + 4 + 16 * nq * nen + 8 * nq + 8  # packed mesh (FP64 gradients)
               + 8 * nq * nen                            # FP32 gradients
-              + (64 if precision == "fp32" else 128) * nq)  # moduli
-    per_node = 16 + 2 * 8 * 14 + 2 * 4 * 6 + 1          # nodes, ~14 f64 and ~6 f32 DOF vectors, fix bits
+              + (64 if precision == "fp32" else 128) * nq   # moduli
+              + 16 * nen + 4 * nen)                     # gather form: element results, node incidence
+    per_node = 16 + 2 * 8 * 14 + 2 * 4 * 6 + 1 + 4      # nodes, ~14 f64 and ~6 f32 DOF vectors, fix bits, ptr
     return int(E * per_el + N * per_node + 4 * 2 ** 20)  # + reduction scratch and PCG state
 
 
@@ -123,11 +124,12 @@ def request_problem(req, device="cpu", build_on_device=False):
 
 
 def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2,
-                  host_params=None):
+                  host_params=None, pcg_form="auto"):
     """
     Build (or copy from ``host_params``) and solve one request on the current stream; returns
     (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
-    concurrent slots; 1: conditional-loop graph; 0: direct launches).
+    concurrent slots; 1: conditional-loop graph; 0: direct launches); ``pcg_form`` the product form inside
+    it ("auto", "colour" or "gather", see DevicePCG and workspace.pcg_form_for).
     """
     if host_params is not None:
         p = {k: (v.to(device, non_blocking=True) if torch.is_tensor(v) else v) for k, v in host_params.items()}
@@ -135,7 +137,7 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
         p = request_problem(req, device, build_on_device=True)
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
-    ws = NewtonWorkspace(p, precision, use_graph=pcg_graph)
+    ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form)
     u, info = newton_krylov_solve(p, th, n_load_steps, tol, verbose=False, workspace=ws, precision=precision,
                                   pcg_max_iter=pcg_max_iter)
     ws.pcg.close()
@@ -149,14 +151,14 @@ class ServingEngine:
     """
 
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
-                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2):
+                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="auto"):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = int(0.6 * free)
         self.n_slots, self.hbm_budget, self.precision = n_slots, int(hbm_budget), precision
         self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter,
-                             pcg_graph=pcg_graph)
+                             pcg_graph=pcg_graph, pcg_form=pcg_form)
         # torch's caching allocator keeps one pool per stream; a slot whose pool already holds a block of
         # the largest request never calls cudaMalloc (which synchronises the whole device) mid-run
         self.prewarm_bytes = int(prewarm_bytes)

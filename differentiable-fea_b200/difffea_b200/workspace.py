@@ -18,8 +18,23 @@ from difffea_b200.krylov import DevicePCG
 from difffea_b200.materials import neo_hookean_parameters
 
 
+# Below this many elements the gather form of the PCG product (3 kernels per iteration) is faster than
+# the colour form (n_colours + 2); above it the colour form's lower traffic wins (measured on B200:
+# 22.6 vs 40.2 us per iteration at 16k Q4 elements, 178 vs 174 us at 640k, 610 vs 550 us at 2.56M).
+GATHER_FORM_MAX_ELEMENTS = 1_500_000
+
+
+def pcg_form_for(mesh, pcg_form="auto"):
+    """The PCG product form: "colour", "gather", or "auto" (gather below GATHER_FORM_MAX_ELEMENTS)."""
+    if pcg_form == "auto":
+        return "gather" if mesh.n_el < GATHER_FORM_MAX_ELEMENTS else "colour"
+    if pcg_form not in ("colour", "gather"):
+        raise ValueError("pcg_form must be 'auto', 'colour' or 'gather'")
+    return pcg_form
+
+
 class NewtonWorkspace:
-    def __init__(self, params, precision="fp64", use_graph=True):
+    def __init__(self, params, precision="fp64", use_graph=True, pcg_form="auto"):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")
         self.params = params
@@ -43,7 +58,8 @@ class NewtonWorkspace:
             mesh.ensure_grad32()
         # the PCG reads -R from b and writes its solution straight into du
         self.b = torch.empty(n, **f64)
-        self.pcg = DevicePCG(mesh, self.C, self.diag, self.b, self.du, use_graph=use_graph)
+        self.pcg = DevicePCG(mesh, self.C, self.diag, self.b, self.du, use_graph=use_graph,
+                             form=pcg_form_for(mesh, pcg_form))
         self.work = mesh.reduce_work()
         self.theta = None
         self.n_launch_groups = 0

@@ -51,6 +51,8 @@ extern "C" {
 #define DFEA_PCG_NEG_CURV 3    /* p.Ap <= 0: the operator is not SPD along p           */
 #define DFEA_PCG_ZERO_RHS 4    /* ||b|| == 0: x = 0 after zero iterations              */
 
+#define DFEA_PCG_GATHER 16     /* dfea_pcg_create flag: gather form of the product     */
+
 /* A mesh in device memory, colour-sorted.  Sizes are host values, pointers are device pointers. */
 typedef struct dfea_mesh_view {
     int64_t n_el;        /* number of elements                                           */
@@ -67,6 +69,11 @@ typedef struct dfea_mesh_view {
     const double* wdet;      /* [n_q][stride]                                              */
     const float* grad32;     /* optional FP32 copy of grad (NULL if not built)              */
     const uint8_t* node_fix; /* [n_nodes] fix bits of every node                           */
+    /* Optional node -> element incidence for the gather form of the product (NULL if not built):
+     * the slots of node n are node_elem[node_elem_ptr[n] .. node_elem_ptr[n+1]), each the index
+     * a * stride + e of local node a of (packed) element e, in increasing order. */
+    const int32_t* node_elem_ptr; /* [n_nodes + 1]                                           */
+    const int32_t* node_elem;     /* [n_el * nen]                                            */
 } dfea_mesh_view;
 
 /* ---------------------------------------------------------------- library --------------------- */
@@ -137,6 +144,20 @@ int dfea_tangent_apply(const dfea_mesh_view* mesh, const void* moduli, int32_t m
 
 /* ---------------------------------------------------------------- residual, energy ------------ */
 
+/* Bytes of the element-result buffer of the gather form: nen * stride pairs of vec_dtype. */
+int64_t dfea_gather_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
+
+/*
+ * The same product as dfea_tangent_apply in two passes instead of one pass per colour: every element
+ * writes its f_e into fe_work (one launch over all elements), then every node sums its elements'
+ * results in the fixed incidence order (mesh->node_elem_ptr / node_elem) and takes v on fixed DOFs.
+ * Same operator and the same arithmetic per element; the per-node sums are grouped differently from
+ * the colour order, so the two forms agree to rounding.  Two launches regardless of the colour count.
+ * Replaces the same reference interface as dfea_tangent_apply (operators.py:385-412).
+ */
+int dfea_tangent_apply_gather(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype,
+                              const void* v, void* y, int32_t vec_dtype, void* fe_work, void* stream);
+
 /* Bytes of scratch that dfea_residual and dfea_vec_norm2 need for their reductions. */
 int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh);
 
@@ -183,6 +204,11 @@ int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
  * stream.  use_graph = 1: that graph; 2: 8 iterations captured back to back in a plain graph (no
  * conditional node) replayed by the host until the status word ends, which overlaps better with other
  * streams' work; 0: the same kernels launched directly, host-polled every 16 iterations.
+ * OR-ing DFEA_PCG_GATHER into use_graph selects the gather form of the product inside each iteration
+ * (one element pass writing every element's result, the per-node sums fused into the first vector
+ * update: 3 kernels per iteration instead of n_colours + 2; needs mesh->node_elem_ptr/node_elem, and
+ * then dfea_pcg_work_bytes includes the element-result buffer).  Its iterates agree with the colour
+ * form's to rounding (the per-node sums are grouped differently); each form is reproducible.
  */
 int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, const void* diag,
                     const void* b, void* x, int32_t vec_dtype, void* work, int32_t use_graph,

@@ -155,3 +155,40 @@ def test_fp32_moduli_on_fp64_vectors(name):
     y = A32(v)
     assert y.dtype == torch.float64
     assert rel(y, d["Av_qp_ew"]) < 2e-6
+
+
+# ------------------------------------------------------------------------------------------------
+# gather form of the product: one element pass + per-node sums in the incidence order
+# ------------------------------------------------------------------------------------------------
+def _apply_gather(A, v):
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr, stream_handle
+    A.mesh.ensure_node_incidence()
+    vcode = _lib.DFEA_F32 if v.dtype == torch.float32 else _lib.DFEA_F64
+    fe = torch.empty(int(_lib.load().dfea_gather_work_bytes(A.mesh.view_ref, vcode)), dtype=torch.uint8, device=DEV)
+    y = torch.empty_like(v)
+    cdt = _lib.DFEA_F32 if A.C.dtype == torch.float32 else _lib.DFEA_F64
+    _lib.call("dfea_tangent_apply_gather", A.mesh.view_ref, ptr(A.C), cdt, ptr(v), ptr(y), vcode, ptr(fe),
+              stream_handle())
+    return y
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES)
+def test_gather_form_product_matches_qp_ew(name):
+    d, p, u, v, th = golden_case(name)
+    A = make_tangent_operator("cuda", u, th, p)
+    y = _apply_gather(A, v)
+    assert rel(y, d["Av_qp_ew"]) < 1e-11
+    assert rel(y, A(v)) < 1e-13                                     # same operator as the colour form
+    assert torch.equal(y, _apply_gather(A, v))                      # fixed summation order: bitwise
+
+
+@pytest.mark.parametrize("et,nx,ny", [("quad4", 160, 160), ("quad9", 60, 40), ("tri6", 40, 30)])
+def test_gather_form_at_size_fp64_and_fp32(et, nx, ny):
+    p = build_rectangle_problem(et, nx, ny, float(nx), float(ny), device=DEV)
+    u, v, w, th = _random_state(p, 1.0, 9)
+    A = make_tangent_operator("cuda", u, th, p)
+    assert rel(_apply_gather(A, v), A(v)) < 1e-13
+    A32 = make_A_operator_cuda(u, th, p, precision="fp32")
+    assert rel(_apply_gather(A32, v.float()).double(), A32(v.float()).double()) < 1e-5
+    assert rel(_apply_gather(A32, v), A32(v)) < 1e-13              # mixed: FP32 operator data, FP64 vectors

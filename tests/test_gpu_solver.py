@@ -8,8 +8,10 @@ import torch
 import oracle
 from difffea_b200.krylov import DevicePCG
 from difffea_b200.newton_krylov import newton_krylov_solve, pcg
-from difffea_b200.operators import make_jacobi_preconditioner, make_tangent_operator, strain_energy
+from difffea_b200.operators import (make_A_operator_cuda, make_jacobi_preconditioner, make_tangent_operator,
+                                    strain_energy)
 from difffea_b200.problem import build_rectangle_problem
+from difffea_b200.workspace import NewtonWorkspace
 from golden_utils import golden_names, load, params_from, rel
 
 pytestmark = pytest.mark.gpu
@@ -122,3 +124,69 @@ def test_load_cutbacks_recover():
     assert info["n_cutbacks"] == info_ref["n_cutbacks"]
     if info["converged"]:
         assert rel(u, u_ref) < 1e-7
+
+
+# ------------------------------------------------------------------------------------------------
+# gather form of the product inside the PCG iteration
+# ------------------------------------------------------------------------------------------------
+def _pcg_forms(A, b, rtol, max_iter, use_graph=1):
+    out = {}
+    for form in ("colour", "gather"):
+        bb, xx = b.clone(), torch.empty_like(b)
+        solver = DevicePCG(A.mesh, A.C, A.diag.to(b.dtype), bb, xx, use_graph=use_graph, form=form)
+        k, status = solver.solve(rtol, max_iter)
+        out[form] = (k, status, xx.clone())
+        solver.close()
+    return out
+
+
+@pytest.mark.parametrize("name", ["operator_quad4_h0.1_theta", "operator_quad9_h0.25_theta",
+                                  "operator_tri6_h0.25_theta", "operator_tri3_h0.25_theta",
+                                  "operator_quad8_h0.25_theta"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gather_form_pcg_matches_the_colour_form(name, precision):
+    d = load(name)
+    p = params_from(d, DEV)
+    u, th = 0.25 * _t(d, "u"), _t(d, "theta")                  # a milder state: SPD tangent for every type
+    A = make_A_operator_cuda(u, th, p, precision=precision)
+    b = p["m"] * _t(d, "v")                                     # FP64 vectors (mixed form for fp32 moduli)
+    res = _pcg_forms(A, b, 1e-9, 3000)
+    (kc, sc, xc), (kg, sg, xg) = res["colour"], res["gather"]
+    assert sc == sg == "converged" and abs(kc - kg) <= 1
+    assert rel(xg, xc) < 1e-8
+
+
+@pytest.mark.parametrize("use_graph", [0, 1, 2])
+def test_gather_form_is_reproducible_in_every_launch_form(use_graph):
+    p, A, M, A_ref, d_ref, b = _linear_system()
+    x_ref, k_ref = oracle.pcg(A_ref, b.cpu(), lambda r: r / d_ref, rtol=1e-10, max_iter=2000)
+    runs = [_pcg_forms(A, b, 1e-10, 2000, use_graph)["gather"] for _ in range(2)]
+    assert runs[0][:2] == runs[1][:2] and torch.equal(runs[0][2], runs[1][2])
+    k, status, x = runs[0]
+    assert status == "converged" and abs(k - k_ref) <= 1 and rel(x, x_ref) < 1e-9
+
+
+def test_gather_form_zero_rhs_negative_curvature_and_cap():
+    p, A, M, *_ = _linear_system()
+    z = torch.zeros(A.mesh.n_dof, dtype=torch.float64, device=DEV)
+    assert _pcg_forms(A, z, 1e-9, 100)["gather"][:2] == (0, "zero_rhs")
+    d = load("operator_quad4_h0.25_theta")
+    p = params_from(d, DEV)
+    An = make_tangent_operator("cuda", _t(d, "u"), -_t(d, "theta"), p)
+    res = _pcg_forms(An, p["m"] * _t(d, "v"), 1e-9, 100)
+    assert res["colour"][:2] == res["gather"][:2] == (0, "negative_curvature")
+    assert torch.equal(res["colour"][2], res["gather"][2])               # x = z = b / d at k = 0
+    p2, A2, *_ = _linear_system()
+    b2 = p2["m"] * torch.ones(A2.mesh.n_dof, dtype=torch.float64, device=DEV)
+    assert _pcg_forms(A2, b2, 1e-30, 7)["gather"][:2] == (7, "max_iter")
+
+
+@pytest.mark.parametrize("name", SOLVE_CASES)
+def test_newton_solve_with_the_gather_form(name):
+    d = load(name)
+    p = params_from(d, DEV)
+    th = _t(d, "theta")
+    ws = NewtonWorkspace(p, pcg_form="gather")
+    u, info = newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False, workspace=ws)
+    assert info["converged"] and rel(u, d["u_star"]) < 1e-9
+    assert info["total_newton"] == int(d["total_newton"])
