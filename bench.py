@@ -6,20 +6,22 @@ Benchmark of the matrix-free Newton-Krylov hot path on B200.
 Workload "serve" (default): the seeded 2,000-request serving stream -- 4:1 cantilever bars, nx uniform
 over the multiples of 4 in [16, 512], Q4/Q9 50/50, E log-uniform in [0.5, 2], nu uniform in [0.2, 0.45],
 axial dead traction uniform in [0.01, 0.05] (strain ~ load / E), 1 load step, Newton tol 1e-10 ||f||,
-Jacobi-PCG (Eisenstat-Walker forcing, cap 5000).  One step = one batch of 32 consecutive requests of the
-stream served by the continuous-batching engine (16 slots, FP32 operator / FP64 Newton and Krylov
-vectors); value = requests/s over all ranks (each rank serves its own shard of the stream: replicas,
-weak scaling), device-timed with CUDA events joined over the slot streams.  Beside it:
-  batched_vs_plain  the first step's requests solved one after another by the plain FP64 drop-in
-                    (newton_krylov_solve defaults), its solves/s, the ratio and the max relative
-                    difference of the solutions
+Jacobi-PCG (Eisenstat-Walker forcing, cap 5000).  One step = 32 consecutive requests of the stream; the
+K steps of the timed window are served continuously by the engine (24 slots, FP32 reference-frame
+operator / FP64 Newton and Krylov vectors, the largest waiting request first); value = requests/s over
+all ranks (each rank serves its own shard of the stream: replicas, weak scaling), device-timed with CUDA
+events joined over the slot streams.  Beside it:
+  batched_vs_plain  the first 64 requests of the window through the engine and, one after another,
+                    through the plain FP64 drop-in (newton_krylov_solve defaults): both solves/s, the
+                    ratio and the max relative difference of the solutions
+  serving_hbm       algorithmic bytes of all PCG iterations of the window / device time
   latency_ms        p50 / p99 of (finish - arrival) for 48 further requests replayed with Poisson
-                    arrivals at 80 % of the measured capacity
+                    arrivals at 80 % of the measured capacity (first come, first served)
   roofline          the tangent product (kernel (b), FP64 stored moduli) at the microbench size,
                     structured Q4 1600 x 1600 = 2.56M elements (inputs 2.2 GB >> L2), CUDA-event timed
   cpu_baseline      the oracle (CPU restatement of the reference algorithm, tangent "qp") on the first
                     requests of the window with nx <= 64, on this host's cores
-  e2e               the first step again with each problem dictionary built on the host (pinned) and
+  e2e               the 64 requests again with each problem dictionary built on the host (pinned) and
                     copied to the device inside the timed region, solutions read back to the host
 
 Workload "plain": one step = one complete FP64 solve of the 100 x 100 Q4 unit-square problem (left edge
@@ -49,7 +51,8 @@ METRIC = "solves/s + p50/p99 latency, batched vs plain, at <=1e-8 rel err; A(v) 
 PLAIN = dict(element_type="quad4", nx=100, ny=100, width=1.0, height=1.0, E=1.0, nu=0.3, load=(0.1, 0.0),
              n_load_steps=3, tol=1e-10)
 MATVEC_N = 1600
-SERVE = dict(stream=2000, seed=0, batch=32, slots=16, latency_requests=48, cpu_sample_nx=64, cpu_budget_s=20.0)
+SERVE = dict(stream=2000, seed=0, batch=32, slots=24, compare=64, latency_requests=48, cpu_sample_nx=64,
+             cpu_budget_s=20.0)
 
 
 def peaks():
@@ -291,59 +294,62 @@ def run_reference(args):
 
 def run_serve(args):
     from difffea_b200 import _lib
-    from difffea_b200.serving import (ServingEngine, hbm_estimate, percentile, request_problem, run_plain,
+    from difffea_b200.serving import (ServingEngine, pcg_iteration_bytes, percentile, request_problem, run_plain,
                                       with_arrivals)
     rank, world, local = dist_init("nccl")
     dev = torch.device("cuda", torch.cuda.current_device())
     B = SERVE["batch"]
     timed, warm, lat_reqs = stream_windows(rank, world, args.steps, args.warmup)
-    eng = ServingEngine(n_slots=SERVE["slots"], device=dev, precision="fp32")
-    for w in range(args.warmup):
-        eng.run(warm[w * B:(w + 1) * B], keep_solutions=False)
+    # the timed window is a backlog: slots take the largest waiting request first
+    eng = ServingEngine(n_slots=SERVE["slots"], device=dev, precision="fp32", order="largest_first")
+    eng.run(warm, keep_solutions=False)                        # W steps of warm-up, served continuously
     run_plain(warm[:2], dev)                                   # plain path warm-up (kernels, graphs)
     torch.cuda.synchronize()
 
     lib = _lib.load()
-    results, step_ms = [], []
     with ClockSampler(local) as clocks:
         dist_barrier(world)
         torch.cuda.synchronize()
         n0 = lib.dfea_launch_count()
-        for k in range(args.steps):
-            results += eng.run(timed[k * B:(k + 1) * B])
-            step_ms.append(eng.device_ms)
+        results = eng.run(timed)                               # K steps of B requests, served continuously
         launches = lib.dfea_launch_count() - n0
         torch.cuda.synchronize()
         dist_barrier(world)
-    total_ms = dist_max(sum(step_ms), world, dev)
+    total_ms = dist_max(eng.device_ms, world, dev)
     value = world * len(timed) / (total_ms * 1e-3)
     ok = all(r.converged and not r.error for r in results)
 
     out = None
     if rank == 0:
-        # the plain FP64 drop-in on the first step's requests, one after another
+        # the same requests through the engine and through the plain FP64 drop-in, one after another
+        C = min(SERVE["compare"], len(timed))
+        eng.run(timed[:C], keep_solutions=False)
+        batched_ms = eng.device_ms
         s = torch.cuda.current_stream()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        plain = run_plain(timed[:B], dev)
+        plain = run_plain(timed[:C], dev)
         e1.record(s)
         e1.synchronize()
         plain_ms = e0.elapsed_time(e1)
-        err = max(float((a.u - b.u).abs().max() / b.u.abs().max()) for a, b in zip(results[:B], plain))
+        err = max(float((a.u - b.u).abs().max() / b.u.abs().max()) for a, b in zip(results[:C], plain))
         # latency under Poisson arrivals at 80 % of the measured capacity of this replica
         rate = 0.8 * value / world
-        lat_res = eng.run(with_arrivals(lat_reqs, rate, seed=7), keep_solutions=False)
+        eng_fifo = ServingEngine(n_slots=SERVE["slots"], device=dev, precision="fp32", order="fifo")
+        lat_res = eng_fifo.run(with_arrivals(lat_reqs, rate, seed=7), keep_solutions=False)
         lat = [1e3 * r.latency for r in lat_res]
         # end to end: problems built on the host (pinned), copied inside the timed region
         host = {}
-        for r in timed[:B]:
+        for r in timed[:C]:
             hp = request_problem(r, "cpu")
             host[r.rid] = {k: (v.pin_memory() if torch.is_tensor(v) else v) for k, v in hp.items()}
         h2d = sum(v.numel() * v.element_size() for hp in host.values() for v in hp.values() if torch.is_tensor(v))
         torch.cuda.synchronize()
-        e2e_res = eng.run(timed[:B], host_params=host)
-        e2e = B / eng.wall                             # host wall clock: copies, solves and read-back
+        e2e_res = eng.run(timed[:C], host_params=host)
+        e2e = C / eng.wall                             # host wall clock: copies, solves and read-back
         d2h = sum(r.u.numel() * 8 for r in e2e_res)
+        # aggregate traffic of the PCG iterations in the timed window (algorithmic bytes / device time)
+        pcg_bytes = sum(r.cg * pcg_iteration_bytes(q) for r, q in zip(results, timed))
         roof = matvec_roofline(dev)
         hbm, kind = peaks()
         cpu_done, cpu_s = serve_cpu_sample(timed, SERVE["cpu_budget_s"])
@@ -353,14 +359,21 @@ def run_serve(args):
                "data": "synthetic (seeded request stream)",
                "config": {"workload": "serve: seeded 2000-request stream of 4:1 cantilever bars (nx 16..512, Q4/Q9, "
                                       "E 0.5..2, nu 0.2..0.45, axial load 0.01..0.05), 1 load step, tol 1e-10 ||f||, "
-                                      f"PCG cap 5000; {B} requests per step, {SERVE['slots']} slots",
+                                      f"PCG cap 5000; {B} requests per step ({len(timed)} served continuously, "
+                                      f"largest waiting request first), {SERVE['slots']} slots",
                           "parallelism": f"replicas x{world} (stream sharded by request id)",
                           "l2": "roofline leg inputs 2.2 GB > 126 MB L2; serving working sets stream from HBM"},
                "all_converged": ok,
-               "batched_vs_plain": {"requests": B, "batched_solves_per_s": B / (step_ms[0] * 1e-3),
-                                    "plain_fp64_solves_per_s": B / (plain_ms * 1e-3),
-                                    "ratio": (plain_ms / step_ms[0]), "max_rel_err": err,
-                                    "plain": "newton_krylov_solve defaults: FP64, conditional-loop PCG graph"},
+               "batched_vs_plain": {"requests": C, "batched_solves_per_s": C / (batched_ms * 1e-3),
+                                    "plain_fp64_solves_per_s": C / (plain_ms * 1e-3),
+                                    "ratio": (plain_ms / batched_ms), "max_rel_err": err,
+                                    "plain": "newton_krylov_solve defaults, one request after another: FP64 "
+                                             "moduli and gradients, conditional-loop PCG graph, product form "
+                                             "by mesh size"},
+               "serving_hbm": {"achieved_gbs": pcg_bytes / (total_ms * 1e-3) / 1e9,
+                               "frac": pcg_bytes / (total_ms * 1e-3) / 1e9 / hbm,
+                               "pcg_iterations": int(sum(r.cg for r in results)),
+                               "bytes": "serving.pcg_iteration_bytes x PCG iterations, over the timed window"},
                "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99), "requests": len(lat),
                               "arrival_rate_per_s": rate},
                "roofline": {"bound": "hbm", "achieved": roof["gbs"], "peak": hbm, "unit": "GB/s",
@@ -372,7 +385,8 @@ def run_serve(args):
                                 "kind": "port",
                                 "sample": f"{len(cpu_done)} requests of the timed window with nx <= "
                                           f"{SERVE['cpu_sample_nx']} ({', '.join(f'{d[1]} nx={d[2]}' for d in cpu_done)})"},
-               "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+               "e2e": {"value": e2e, "unit": "solves/s", "requests": C, "h2d_bytes_per_step": int(h2d * B / C),
+                       "d2h_bytes_per_step": int(d2h * B / C)},
                "gpu_launches": int(launches),
                "clocks": clocks.summary()}
         print(json.dumps(out))

@@ -332,6 +332,206 @@ k_node_gather(Mesh m, const int32_t* __restrict__ inc_ptr, const int32_t* __rest
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// Reference-frame form (DFEA_F32REF moduli, FP64 vectors): per Gauss point only the 10 packed FP32
+// moduli stream in (40 B); the gradients are the element type's reference gradients, a kernel
+// parameter.  With G = sum_a v_a (x) dN_a/dxi the product at a Gauss point is dPhat = Chat G and
+// f_a += dPhat . dN_a/dxi -- the same operator as C applied to the physical gradients.
+// ------------------------------------------------------------------------------------------
+template <int NEN>
+struct RefApplyCfg {
+    static constexpr int NT = 128;
+    static constexpr int STAGES = 6;
+    static constexpr int A_BYTES = 16 * NT;   // entries 00 01 02 03
+    static constexpr int B_BYTES = 16 * NT;   // entries 11 12 13 22
+    static constexpr int D_BYTES = 8 * NT;    // entries 23 33
+    static constexpr int N_BYTES = NEN * 4 * NT;
+    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES + D_BYTES + N_BYTES;
+    static constexpr int SMEM = STAGES * STAGE_BYTES;
+};
+
+template <int NEN, int NQ, typename T, bool DOT, typename Start, typename Scatter>
+__device__ __forceinline__ bool apply_tiles_ref(const Mesh& m, int64_t e0, int64_t e1, const float* __restrict__ C,
+                                                const RefGrad<NEN, NQ>& rg, const T* __restrict__ v, unsigned char* smem,
+                                                double& curv, Start&& start, Scatter&& scatter) {
+    using Cfg = RefApplyCfg<NEN>;
+    using T2 = v2_t<T>;
+    constexpr int NT = Cfg::NT, ST = Cfg::STAGES;
+
+    const int tid = threadIdx.x;
+    const int64_t S = m.stride;
+    const int64_t n_tiles = (e1 - e0 + NT - 1) / NT;
+    const int64_t my_tiles = (n_tiles > (int64_t)blockIdx.x) ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int64_t n_items = my_tiles * NQ;
+
+    auto element_of = [&](int64_t item) -> int64_t {
+        return e0 + ((int64_t)blockIdx.x + (item / NQ) * (int64_t)gridDim.x) * NT + tid;
+    };
+    auto stage = [&](int s) -> unsigned char* { return smem + s * Cfg::STAGE_BYTES; };
+    auto a_slot = [&](int s) -> float4* { return reinterpret_cast<float4*>(stage(s)) + tid; };
+    auto b_slot = [&](int s) -> float4* { return reinterpret_cast<float4*>(stage(s) + Cfg::A_BYTES) + tid; };
+    auto d_slot = [&](int s) -> float2* {
+        return reinterpret_cast<float2*>(stage(s) + Cfg::A_BYTES + Cfg::B_BYTES) + tid;
+    };
+    auto n_slot = [&](int s, int a) -> int* {
+        return reinterpret_cast<int*>(stage(s) + Cfg::A_BYTES + Cfg::B_BYTES + Cfg::D_BYTES) + a * NT + tid;
+    };
+    auto issue = [&](int64_t it) {
+        if (it < n_items) {
+            const int64_t e = element_of(it);
+            if (e < e1) {
+                const int q = (int)(it % NQ), s = (int)(it % ST);
+                const float* base = C + (int64_t)q * 10 * S;
+                cp_async16(a_slot(s), reinterpret_cast<const float4*>(base) + e);
+                cp_async16(b_slot(s), reinterpret_cast<const float4*>(base + 4 * S) + e);
+                cp_async8(d_slot(s), reinterpret_cast<const float2*>(base + 8 * S) + e);
+                if (q == 0) {
+#pragma unroll
+                    for (int a = 0; a < NEN; ++a) cp_async4(n_slot(s, a), m.conn + (int64_t)a * S + e);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+
+#pragma unroll
+    for (int i = 0; i < ST - 1; ++i) issue(i);
+
+    if (!start()) {
+        cp_async_wait<0>();
+        return false;
+    }
+
+    const T2* v2 = reinterpret_cast<const T2*>(v);
+    int node[NEN], fix[NEN];
+    T vx[NEN], vy[NEN], fx[NEN], fy[NEN];
+#pragma unroll
+    for (int a = 0; a < NEN; ++a) {
+        node[a] = 0;
+        fix[a] = 3;
+        vx[a] = vy[a] = fx[a] = fy[a] = T(0);
+    }
+
+    for (int64_t tile = 0; tile < my_tiles; ++tile) {
+        const int64_t e = element_of(tile * NQ);
+        const bool live = e < e1;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {  // unrolled: the reference gradients of point q are constants
+            const int64_t it = tile * NQ + q;
+            issue(it + ST - 1);
+            cp_async_wait<ST - 1>();
+            const int s = (int)(it % ST);
+            if (live) {
+                if (q == 0) {
+#pragma unroll
+                    for (int a = 0; a < NEN; ++a) {
+                        const int c = *n_slot(s, a);
+                        node[a] = c >> 2;
+                        fix[a] = c & 3;
+                    }
+#pragma unroll
+                    for (int a = 0; a < NEN; ++a) {
+                        const T2 t = __ldg(v2 + node[a]);
+                        vx[a] = (fix[a] & 1) ? T(0) : t.x;
+                        vy[a] = (fix[a] & 2) ? T(0) : t.y;
+                        fx[a] = T(0);
+                        fy[a] = T(0);
+                    }
+                }
+                T G[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+                for (int a = 0; a < NEN; ++a) {
+                    const T r0 = (T)rg.g[q][a][0], r1 = (T)rg.g[q][a][1];
+                    G[0] += vx[a] * r0;
+                    G[1] += vx[a] * r1;
+                    G[2] += vy[a] * r0;
+                    G[3] += vy[a] * r1;
+                }
+                const float4 A = *a_slot(s), B = *b_slot(s);
+                const float2 D = *d_slot(s);
+                const T c00 = A.x, c01 = A.y, c02 = A.z, c03 = A.w, c11 = B.x, c12 = B.y, c13 = B.z, c22 = B.w,
+                        c23 = D.x, c33 = D.y;
+                const T dP0 = c00 * G[0] + c01 * G[1] + c02 * G[2] + c03 * G[3];
+                const T dP1 = c01 * G[0] + c11 * G[1] + c12 * G[2] + c13 * G[3];
+                const T dP2 = c02 * G[0] + c12 * G[1] + c22 * G[2] + c23 * G[3];
+                const T dP3 = c03 * G[0] + c13 * G[1] + c23 * G[2] + c33 * G[3];
+                if (DOT) curv += (double)(G[0] * dP0 + G[1] * dP1 + G[2] * dP2 + G[3] * dP3);
+#pragma unroll
+                for (int a = 0; a < NEN; ++a) {
+                    const T r0 = (T)rg.g[q][a][0], r1 = (T)rg.g[q][a][1];
+                    fx[a] += dP0 * r0 + dP1 * r1;
+                    fy[a] += dP2 * r0 + dP3 * r1;
+                }
+                if (q == NQ - 1) scatter(e, node, fix, fx, fy);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    return true;
+}
+
+template <int NEN, int NQ, typename T, bool DOT>
+__global__ void __launch_bounds__(128)
+k_apply_ref(Mesh m, int64_t e0, int64_t e1, const float* __restrict__ C, const RefGrad<NEN, NQ> rg,
+            const T* __restrict__ v, T* __restrict__ y, RedSite site, const int* __restrict__ done) {
+    using T2 = v2_t<T>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T2* y2 = reinterpret_cast<T2*>(y);
+    double curv = 0.0;
+    const bool ran = apply_tiles_ref<NEN, NQ, T, DOT>(
+        m, e0, e1, C, rg, v, smem, curv,
+        [&]() -> bool {
+            grid_dependency_wait();
+            if (DOT && done != nullptr && *done) return false;
+            grid_dependents_launch();
+            return true;
+        },
+        [&](int64_t, const int (&node)[NEN], const int (&fix)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                T2 t = y2[node[a]];
+                if (!(fix[a] & 1)) t.x += fx[a];
+                if (!(fix[a] & 2)) t.y += fy[a];
+                y2[node[a]] = t;
+            }
+        });
+    if (!ran) return;
+    if (DOT) {
+        const double vals[1] = {block_sum<128>(curv)};
+        double tot[1];
+        if (last_block_sum<128, 1>(vals, site, tot) && threadIdx.x == 0) site.result[0] = tot[0];
+    }
+}
+
+template <int NEN, int NQ, typename T, bool DOT>
+__global__ void __launch_bounds__(128)
+k_apply_ref_elem(Mesh m, const float* __restrict__ C, const RefGrad<NEN, NQ> rg, const T* __restrict__ v,
+                 T* __restrict__ fe, RedSite site, const int* __restrict__ done) {
+    using T2 = v2_t<T>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T2* fe2 = reinterpret_cast<T2*>(fe);
+    const int64_t S = m.stride;
+    double curv = 0.0;
+    const bool ran = apply_tiles_ref<NEN, NQ, T, DOT>(
+        m, 0, m.n_el, C, rg, v, smem, curv,
+        [&]() -> bool {
+            grid_dependency_wait();
+            if (DOT && done != nullptr && *done) return false;
+            grid_dependents_launch();
+            return true;
+        },
+        [&](int64_t e, const int (&)[NEN], const int (&)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) fe2[(int64_t)a * S + e] = make_v2<T>(fx[a], fy[a]);
+        });
+    if (!ran) return;
+    if (DOT) {
+        const double vals[1] = {block_sum<128>(curv)};
+        double tot[1];
+        if (last_block_sum<128, 1>(vals, site, tot) && threadIdx.x == 0) site.result[0] = tot[0];
+    }
+}
+
 // Persistent grid for a walk over n_elements: as many blocks as fit on the GPU at once (occupancy of
 // the kernel with its shared memory, configured once per device), never more than there are tiles or
 // kMaxBlocks.
@@ -365,6 +565,16 @@ template <int NEN, int NQ, typename SD, typename T, bool DOT>
 int apply_elem_grid(int64_t n_elements) {
     using Cfg = ApplyCfg<NEN, SD>;
     return resident_grid<k_apply_elem<NEN, NQ, SD, T, DOT>, Cfg::SMEM, Cfg::NT>(n_elements);
+}
+
+template <int NEN, int NQ, typename T, bool DOT>
+int apply_ref_grid(int64_t n_elements) {
+    return resident_grid<k_apply_ref<NEN, NQ, T, DOT>, RefApplyCfg<NEN>::SMEM, 128>(n_elements);
+}
+
+template <int NEN, int NQ, typename T, bool DOT>
+int apply_ref_elem_grid(int64_t n_elements) {
+    return resident_grid<k_apply_ref_elem<NEN, NQ, T, DOT>, RefApplyCfg<NEN>::SMEM, 128>(n_elements);
 }
 
 // The byte range of the DOF vectors a product gathers (v) and scatters (y): both when they are
@@ -434,6 +644,66 @@ int launch_apply_elem(const dfea_mesh_view& mv, const SD* C, const SD* G, const 
                                  C, G, v, fe, site, done);
     if (rc) return rc;
     return launch_check("k_apply_elem");
+}
+
+// Reference-frame launches: colour passes (y read-modify-write) or the element pass (results into fe).
+template <int NEN, int NQ, typename T, bool DOT>
+int launch_apply_ref_colours(const dfea_mesh_view& mv, const float* C, const T* v, T* y, const RedSite* sites,
+                             const int* done, cudaStream_t stream) {
+    const Mesh m = kernel_mesh(mv);
+    const RefGrad<NEN, NQ> rg = ref_grad_of<NEN, NQ>(mv);
+    long long max_window = 0;
+    const long long setaside = persisting_l2_bytes(&max_window);
+    L2Window w = l2_window(v, y, (size_t)(2 * mv.n_nodes) * sizeof(T));
+    if ((long long)w.bytes > max_window) w.bytes = (size_t)max_window;
+    LaunchOpts opts;
+    opts.pdl = true;
+    if (setaside > 0 && w.bytes > 0) {
+        opts.win_base = w.base;
+        opts.win_bytes = w.bytes;
+        opts.hit_ratio = setaside >= (long long)w.bytes ? 1.0f : (float)((double)setaside / (double)w.bytes);
+    }
+    for (int c = 0; c < mv.n_colours; ++c) {
+        const int64_t e0 = mv.colour_begin[c], e1 = mv.colour_begin[c + 1];
+        if (e1 <= e0) continue;
+        const int grid = apply_ref_grid<NEN, NQ, T, DOT>(e1 - e0);
+        const RedSite site = DOT ? sites[c] : RedSite{nullptr, nullptr, nullptr};
+        const int rc = launch_kernel(k_apply_ref<NEN, NQ, T, DOT>, dim3(grid), dim3(128), RefApplyCfg<NEN>::SMEM, stream,
+                                     opts, m, e0, e1, C, rg, v, y, site, done);
+        if (rc) return rc;
+    }
+    return launch_check("k_apply_ref");
+}
+
+template <int NEN, int NQ, typename T, bool DOT>
+int launch_apply_ref_elem(const dfea_mesh_view& mv, const float* C, const T* v, T* fe, RedSite site, const int* done,
+                          cudaStream_t stream) {
+    const Mesh m = kernel_mesh(mv);
+    const RefGrad<NEN, NQ> rg = ref_grad_of<NEN, NQ>(mv);
+    long long max_window = 0;
+    const long long setaside = persisting_l2_bytes(&max_window);
+    size_t wb = (size_t)(2 * mv.n_nodes) * sizeof(T);
+    if ((long long)wb > max_window) wb = (size_t)max_window;
+    LaunchOpts opts;
+    opts.pdl = true;
+    if (setaside > 0 && wb > 0) {
+        opts.win_base = v;
+        opts.win_bytes = wb;
+        opts.hit_ratio = setaside >= (long long)wb ? 1.0f : (float)((double)setaside / (double)wb);
+    }
+    const int grid = apply_ref_elem_grid<NEN, NQ, T, DOT>(mv.n_el);
+    const int rc = launch_kernel(k_apply_ref_elem<NEN, NQ, T, DOT>, dim3(grid), dim3(128), RefApplyCfg<NEN>::SMEM, stream,
+                                 opts, m, C, rg, v, fe, site, done);
+    if (rc) return rc;
+    return launch_check("k_apply_ref_elem");
+}
+
+// Configure the instantiations a solver launches (shared-memory size, occupancy) before any stream capture.
+template <int NEN, int NQ, typename T>
+void prepare_apply_ref() {
+    (void)apply_ref_grid<NEN, NQ, T, true>(1);
+    (void)apply_ref_elem_grid<NEN, NQ, T, true>(1);
+    (void)persisting_l2_bytes(nullptr);
 }
 
 // Configure the instantiations a solver launches (shared-memory size, occupancy) before any stream capture.

@@ -41,6 +41,7 @@ struct Mesh {
     const double* wdet;
     const float* grad32;
     const uint8_t* node_fix;
+    const double* jinv;
 };
 
 inline Mesh kernel_mesh(const dfea_mesh_view& v) {
@@ -54,7 +55,24 @@ inline Mesh kernel_mesh(const dfea_mesh_view& v) {
     m.wdet = v.wdet;
     m.grad32 = v.grad32;
     m.node_fix = v.node_fix;
+    m.jinv = v.jinv;
     return m;
+}
+
+// The reference shape gradients of one element type at its Gauss points, passed by value (kernel
+// parameter space: read through the constant cache, broadcast to a warp since all its threads are at
+// the same Gauss point).
+template <int NEN, int NQ>
+struct RefGrad {
+    double g[NQ][NEN][2];
+};
+template <int NEN, int NQ>
+inline RefGrad<NEN, NQ> ref_grad_of(const dfea_mesh_view& v) {
+    RefGrad<NEN, NQ> r;
+    for (int q = 0; q < NQ; ++q)
+        for (int a = 0; a < NEN; ++a)
+            for (int k = 0; k < 2; ++k) r.g[q][a][k] = v.ref_grad[(q * NEN + a) * 2 + k];
+    return r;
 }
 
 // One reduction site in scratch memory: kMaxBlocks partials per value, a ticket, the result(s).
@@ -216,6 +234,36 @@ __device__ __forceinline__ void store_moduli(double* C, int64_t S, int q, int64_
 #pragma unroll
     for (int k = 0; k < 8; ++k) p[(int64_t)(q * 8 + k) * S + e] = make_double2(c[2 * k], c[2 * k + 1]);
 }
+// Moduli pulled back to the reference frame, packed symmetric (DFEA_F32REF layout):
+//   h_(ia),(kb) = sum_{J,L} Jinv_aJ C_(iJ),(kL) Jinv_bL,  ji[2a+J] = Jinv_aJ.
+__device__ __forceinline__ void store_moduli_ref(float* C, int64_t S, int q, int64_t e, const double (&c)[16],
+                                                 const double (&ji)[4]) {
+    double h[16];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            // t = B Jinv^T with B the (i, k) block of C, then h = Jinv t
+            double t[2][2];
+#pragma unroll
+            for (int J = 0; J < 2; ++J)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+                    t[J][b] = c[(2 * i + J) * 4 + 2 * k] * ji[2 * b] + c[(2 * i + J) * 4 + 2 * k + 1] * ji[2 * b + 1];
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b) h[(2 * i + a) * 4 + 2 * k + b] = ji[2 * a] * t[0][b] + ji[2 * a + 1] * t[1][b];
+        }
+    const int64_t base = (int64_t)q * 10 * S;
+    float4* A = reinterpret_cast<float4*>(C + base);
+    float4* B = reinterpret_cast<float4*>(C + base + 4 * S);
+    float2* D = reinterpret_cast<float2*>(C + base + 8 * S);
+    A[e] = make_float4((float)h[0], (float)h[1], (float)h[2], (float)h[3]);
+    B[e] = make_float4((float)h[5], (float)h[6], (float)h[7], (float)h[10]);
+    D[e] = make_float2((float)h[11], (float)h[15]);
+}
+
 __device__ __forceinline__ void store_moduli(float* C, int64_t S, int q, int64_t e, const double (&c)[16]) {
     float4* p = reinterpret_cast<float4*>(C);
 #pragma unroll

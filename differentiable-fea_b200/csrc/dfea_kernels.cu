@@ -79,7 +79,8 @@ __global__ void k_to_f64(int64_t n, const float* __restrict__ x, double* __restr
 // ------------------------------------------------------------------------------------------
 // kernel (a): moduli + element diagonals, one colour per launch
 // ------------------------------------------------------------------------------------------
-template <int NEN, int NQ, typename CT>
+// REF (with CT = float): store the moduli pulled back to the reference frame (DFEA_F32REF layout).
+template <int NEN, int NQ, typename CT, bool REF = false>
 __global__ void __launch_bounds__(128)
 k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const double* __restrict__ theta,
          double mu0, double lam0, CT* __restrict__ Cout, double* __restrict__ diag) {
@@ -116,7 +117,16 @@ k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const dou
             const NHPoint p = nh_point(F);
             double Cq[16];
             nh_moduli(p, mu, lam, m.wdet[q * S + e], Cq);
-            if (Cout != nullptr) store_moduli(Cout, S, q, e, Cq);
+            if (Cout != nullptr) {
+                if constexpr (REF) {
+                    const double2* j2 = reinterpret_cast<const double2*>(m.jinv);
+                    const double2 r0 = __ldg(j2 + (int64_t)(q * 2) * S + e), r1 = __ldg(j2 + (int64_t)(q * 2 + 1) * S + e);
+                    const double ji[4] = {r0.x, r0.y, r1.x, r1.y};
+                    store_moduli_ref(Cout, S, q, e, Cq, ji);
+                } else {
+                    store_moduli(Cout, S, q, e, Cq);
+                }
+            }
             if (diag != nullptr) {
                 // e_k^T K_e e_k for the unit DOF (a, i): sum_{J,L} C[(iJ),(iL)] dN_aJ dN_aL
 #pragma unroll
@@ -402,7 +412,10 @@ extern "C" int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const
     if (!u || !theta || (!moduli && !diag)) return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: NULL pointer");
     if (!aligned16(u) || (moduli && !aligned16(moduli)) || (diag && !aligned16(diag)))
         return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: u, moduli and diag must be 16-byte aligned");
-    if (moduli_dtype != DFEA_F64 && moduli_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad moduli dtype");
+    if (moduli_dtype != DFEA_F64 && moduli_dtype != DFEA_F32 && moduli_dtype != DFEA_F32REF)
+        return set_error(DFEA_ERR_INVALID, "bad moduli dtype");
+    if (moduli_dtype == DFEA_F32REF && moduli && !mesh->jinv)
+        return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: DFEA_F32REF moduli need mesh->jinv");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const Mesh m = kernel_mesh(*mesh);
     if (diag) {
@@ -418,6 +431,9 @@ extern "C" int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const
             if (moduli_dtype == DFEA_F64)
                 k_moduli<NEN, NQ, double><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
                                                                 static_cast<double*>(moduli), diag);
+            else if (moduli_dtype == DFEA_F32REF)
+                k_moduli<NEN, NQ, float, true><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
+                                                                     static_cast<float*>(moduli), diag);
             else
                 k_moduli<NEN, NQ, float><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
                                                                static_cast<float*>(moduli), diag);
@@ -437,6 +453,28 @@ extern "C" int dfea_tangent_apply(const dfea_mesh_view* mesh, const void* moduli
                                   void* y, int32_t vec_dtype, void* stream) {
     int rc = validate_mesh(mesh, moduli_dtype == DFEA_F32);
     if (rc) return rc;
+    if (moduli_dtype == DFEA_F32REF) {
+        if (vec_dtype != DFEA_F64) return set_error(DFEA_ERR_INVALID, "DFEA_F32REF moduli apply to f64 vectors");
+        if (!moduli || !v || !y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: NULL pointer");
+        if (v == y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: y must not alias v");
+        if (!aligned16(moduli) || !aligned16(v) || !aligned16(y))
+            return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: moduli, v and y must be 16-byte aligned");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const Mesh m = kernel_mesh(*mesh);
+        const double* vv = static_cast<const double*>(v);
+        double* yy = static_cast<double*>(y);
+        k_pivot_init<double><<<grid_for(mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(m, vv, yy);
+        rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+            constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+            return launch_apply_ref_colours<NEN, NQ, double, false>(*mesh, static_cast<const float*>(moduli), vv, yy,
+                                                                   nullptr, nullptr, s);
+        });
+        if (rc) return rc;
+        int nonempty = 0;
+        for (int c = 0; c < mesh->n_colours; ++c) nonempty += mesh->colour_begin[c + 1] > mesh->colour_begin[c];
+        note_launches(1 + nonempty);
+        return DFEA_OK;
+    }
     if (!moduli || !v || !y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: NULL pointer");
     if (v == y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply: y must not alias v");
     if (!aligned16(moduli) || !aligned16(v) || !aligned16(y))
@@ -478,13 +516,16 @@ extern "C" int dfea_tangent_apply_gather(const dfea_mesh_view* mesh, const void*
                                          const void* v, void* y, int32_t vec_dtype, void* fe_work, void* stream) {
     int rc = validate_mesh(mesh, moduli_dtype == DFEA_F32);
     if (rc) return rc;
+    if (moduli_dtype == DFEA_F32REF && vec_dtype != DFEA_F64)
+        return set_error(DFEA_ERR_INVALID, "DFEA_F32REF moduli apply to f64 vectors");
     if (!mesh->node_elem_ptr || !mesh->node_elem)
         return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply_gather: the mesh has no node incidence");
     if (!moduli || !v || !y || !fe_work) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply_gather: NULL pointer");
     if (v == y) return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply_gather: y must not alias v");
     if (!aligned16(moduli) || !aligned16(v) || !aligned16(y) || !aligned16(fe_work))
         return set_error(DFEA_ERR_INVALID, "dfea_tangent_apply_gather: moduli, v, y and fe_work must be 16-byte aligned");
-    if (moduli_dtype != DFEA_F64 && moduli_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad moduli dtype");
+    if (moduli_dtype != DFEA_F64 && moduli_dtype != DFEA_F32 && moduli_dtype != DFEA_F32REF)
+        return set_error(DFEA_ERR_INVALID, "bad moduli dtype");
     if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32) return set_error(DFEA_ERR_INVALID, "bad vector dtype");
     if (vec_dtype == DFEA_F32 && moduli_dtype != DFEA_F32)
         return set_error(DFEA_ERR_INVALID, "FP32 vectors need FP32 moduli");
@@ -496,6 +537,15 @@ extern "C" int dfea_tangent_apply_gather(const dfea_mesh_view* mesh, const void*
     pdl.pdl = true;
     rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        if (moduli_dtype == DFEA_F32REF) {
+            const double* vv = static_cast<const double*>(v);
+            double* fe = static_cast<double*>(fe_work);
+            int r = launch_apply_ref_elem<NEN, NQ, double, false>(*mesh, static_cast<const float*>(moduli), vv, fe, none,
+                                                                 nullptr, s);
+            if (r) return r;
+            return launch_kernel(k_node_gather<double>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mesh->node_elem_ptr,
+                                 mesh->node_elem, (const double*)fe, vv, static_cast<double*>(y));
+        }
         if (vec_dtype == DFEA_F64) {
             const double* vv = static_cast<const double*>(v);
             double* fe = static_cast<double*>(fe_work);

@@ -278,8 +278,9 @@ int kernels_per_iteration(const dfea_pcg& h) {
     return nonempty + 2;
 }
 
-// S: storage type of moduli and gradients, T: Krylov vector type.
-template <typename S, typename T>
+// S: storage type of moduli and gradients, T: Krylov vector type; REF: DFEA_F32REF moduli (S = float),
+// no gradients read.
+template <typename S, typename T, bool REF = false>
 int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHandle cond, bool with_cond) {
     const dfea_mesh_view& mv = h.mesh;
     const Mesh m = kernel_mesh(mv);
@@ -300,7 +301,11 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
         T* fe = reinterpret_cast<T*>(h.work + h.layout.off_fe);
         rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
             constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-            return launch_apply_elem<NEN, NQ, S, T, true>(mv, C, G, p, fe, h.site(0, 1), &st->done, s);
+            if constexpr (REF)
+                return launch_apply_ref_elem<NEN, NQ, T, true>(mv, reinterpret_cast<const float*>(C), p, fe, h.site(0, 1),
+                                                               &st->done, s);
+            else
+                return launch_apply_elem<NEN, NQ, S, T, true>(mv, C, G, p, fe, h.site(0, 1), &st->done, s);
         });
         if (rc) return rc;
         if ((rc = launch_kernel(k_pcg_update1<T, true>, dim3(gn), dim3(kThreads), 0, s, pdl, m, 1, p, (const T*)y, d, x,
@@ -314,7 +319,11 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
         for (int c = 0; c < mv.n_colours; ++c) sites[c] = h.site(c, 1);
         rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
             constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-            return launch_apply_colours<NEN, NQ, S, T, true>(mv, C, G, p, y, sites, &st->done, s, false);
+            if constexpr (REF)
+                return launch_apply_ref_colours<NEN, NQ, T, true>(mv, reinterpret_cast<const float*>(C), p, y, sites,
+                                                                  &st->done, s);
+            else
+                return launch_apply_colours<NEN, NQ, S, T, true>(mv, C, G, p, y, sites, &st->done, s, false);
         });
         if (rc) return rc;
         if ((rc = launch_kernel(k_pcg_update1<T, false>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mv.n_colours, p,
@@ -333,6 +342,7 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
 int launch_iteration_any(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHandle cond, bool with_cond) {
     if (h.vec_dtype == DFEA_F64) return launch_iteration<double, double>(h, s, cond, with_cond);
     if (h.vec_dtype == DFEA_MIXED) return launch_iteration<float, double>(h, s, cond, with_cond);
+    if (h.vec_dtype == DFEA_F32REF) return launch_iteration<float, double, true>(h, s, cond, with_cond);
     return launch_iteration<float, float>(h, s, cond, with_cond);
 }
 
@@ -416,7 +426,8 @@ PcgLayout layout_for(const dfea_mesh_view& mv, int32_t vec_dtype) {
 }  // namespace
 
 extern "C" int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype) {
-    if (!mesh || (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32 && vec_dtype != DFEA_MIXED)) return -1;
+    if (!mesh || (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32 && vec_dtype != DFEA_MIXED && vec_dtype != DFEA_F32REF))
+        return -1;
     return layout_for(*mesh, vec_dtype).total;
 }
 
@@ -424,9 +435,9 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
                                void* x, int32_t vec_dtype, void* work, int32_t use_graph, dfea_pcg** out) {
     if (!out) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: out is NULL");
     *out = nullptr;
-    int rc = validate_mesh(mesh, vec_dtype != DFEA_F64);
+    int rc = validate_mesh(mesh, vec_dtype == DFEA_F32 || vec_dtype == DFEA_MIXED);
     if (rc) return rc;
-    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32 && vec_dtype != DFEA_MIXED)
+    if (vec_dtype != DFEA_F64 && vec_dtype != DFEA_F32 && vec_dtype != DFEA_MIXED && vec_dtype != DFEA_F32REF)
         return set_error(DFEA_ERR_INVALID, "bad vector dtype");
     if (!moduli || !diag || !b || !x || !work) return set_error(DFEA_ERR_INVALID, "dfea_pcg_create: NULL pointer");
     auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 255u) == 0; };
@@ -459,6 +470,7 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
         if (vec_dtype == DFEA_F64) prepare_apply<NEN, NQ, double, double>();
         else if (vec_dtype == DFEA_MIXED) prepare_apply<NEN, NQ, float, double>();
+        else if (vec_dtype == DFEA_F32REF) prepare_apply_ref<NEN, NQ, double>();
         else prepare_apply<NEN, NQ, float, float>();
         return DFEA_OK;
     });

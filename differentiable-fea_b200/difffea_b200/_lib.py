@@ -15,6 +15,7 @@ DFEA_OK = 0
 DFEA_F64 = 0
 DFEA_F32 = 1
 DFEA_MIXED = 2      # PCG: FP32 moduli/gradients, FP64 Krylov vectors
+DFEA_F32REF = 3     # FP32 moduli in the element reference frame (10 per Gauss point), FP64 vectors
 MAX_COLOURS = 64
 
 PCG_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "negative_curvature", 4: "zero_rhs"}
@@ -31,6 +32,7 @@ class MeshView(ctypes.Structure):
         ("colour_begin", c_i64 * (MAX_COLOURS + 1)),
         ("conn", c_vp), ("orig", c_vp), ("grad", c_vp), ("wdet", c_vp), ("grad32", c_vp), ("node_fix", c_vp),
         ("node_elem_ptr", c_vp), ("node_elem", c_vp),
+        ("jinv", c_vp), ("ref_grad", ctypes.c_double * (9 * 9 * 2)),
     ]
 
 

@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from difffea_b200 import _lib
+from difffea_b200.elements import element_quadrature, shape_gradients
 
 _SUPPORTED = {(4, 4): "quad4", (9, 9): "quad9", (3, 1): "tri3", (6, 6): "tri6", (8, 9): "quad8"}
 
@@ -114,6 +115,19 @@ class CudaMesh:
         v.node_elem_ptr = None
         v.node_elem = None
         self.node_elem_ptr = self.node_elem = None
+        # reference shape gradients at the Gauss points (host values in the view) and, built on demand,
+        # the inverse element Jacobians of the reference-frame FP32 operator
+        GP = params.get("GP")
+        if GP is None:
+            GP, _ = element_quadrature(self.element_type)
+        GP = GP.detach().to("cpu", torch.float64)
+        self.ref_grad = shape_gradients(self.element_type, GP[:, 0], GP[:, 1]).to(torch.float64)  # (n_q, nen, 2)
+        flat = self.ref_grad.reshape(-1).tolist()
+        for i, x in enumerate(flat):
+            v.ref_grad[i] = x
+        v.jinv = None
+        self.jinv = None
+        self._nodes = params["nodes"]
         self._reduce_work = None
 
     # -------------------------------------------------------------------------------------------
@@ -154,6 +168,38 @@ class CudaMesh:
             self.view.node_elem = self.node_elem.data_ptr()
         return self.node_elem_ptr, self.node_elem
 
+    def ensure_ref_frame(self):
+        """
+        Inverse element Jacobians Jinv = (dX/dxi)^-1 at the Gauss points, packed [n_q][2][stride] (rows of
+        Jinv as f64 pairs), for the reference-frame FP32 operator.  The problem's dN/dX must equal
+        Jinv^T dN/dxi with this package's quadrature; a mismatch raises instead of computing a wrong
+        operator.
+        """
+        if self.jinv is None:
+            dev, S, nq, nen, n = self.device, self.stride, self.n_q, self.nen, self.n_el
+            conn = self.conn.view(nen, S)[:, :n] >> 2                                     # packed order
+            X = self._nodes.detach().to(dev, torch.float64)[conn.to(torch.int64).t()]     # (n, nen, 2)
+            dNr = self.ref_grad.to(dev)                                                   # (nq, nen, 2)
+            J = torch.einsum("eai,qaj->eqij", X, dNr)                                     # dX_i / dxi_j
+            det = J[..., 0, 0] * J[..., 1, 1] - J[..., 0, 1] * J[..., 1, 0]
+            Jinv = torch.stack([torch.stack([J[..., 1, 1], -J[..., 0, 1]], -1),
+                                torch.stack([-J[..., 1, 0], J[..., 0, 0]], -1)], -2) / det[..., None, None]
+            dN = self.grad.view(nq, nen, S, 2)[:, :, :n, :]                               # packed (nq, nen, n, 2)
+            dN_ref = torch.einsum("qaj,eqji->qaei", dNr, Jinv)
+            scale = float(dN.abs().max()) if n else 1.0
+            if n and float((dN_ref - dN).abs().max()) > 1e-9 * scale:
+                raise ValueError("dN_dX does not match this package's reference gradients and quadrature; "
+                                 "the reference-frame operator cannot be used for this problem")
+            packed = torch.zeros(nq, 2, S, 2, dtype=torch.float64, device=dev)
+            packed[:, :, :n, :] = Jinv.permute(1, 2, 0, 3)                                 # [q][row][e][col]
+            self.jinv = packed.contiguous()
+            self.view.jinv = self.jinv.data_ptr()
+        return self.jinv
+
+    def moduli_numel_ref(self):
+        """FP32 entries of the reference-frame moduli (10 per Gauss point)."""
+        return self.n_q * 10 * self.stride
+
     def reduce_work(self):
         if self._reduce_work is None:
             nbytes = int(_lib.load().dfea_reduce_work_bytes(self.view_ref))
@@ -165,7 +211,7 @@ class CudaMesh:
 
     def hbm_bytes(self):
         t = [self.conn, self.orig, self.grad, self.wdet, self.node_fix, self.perm]
-        for extra in (self.grad32, self.node_elem_ptr, self.node_elem):
+        for extra in (self.grad32, self.node_elem_ptr, self.node_elem, self.jinv):
             if extra is not None:
                 t.append(extra)
         return sum(x.numel() * x.element_size() for x in t)

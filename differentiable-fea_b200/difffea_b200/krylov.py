@@ -27,9 +27,12 @@ class DevicePCG:
     form: "colour" (one launch per colour, scatter by read-modify-write) or "gather" (one element pass,
     per-node sums fused into the first vector update: 3 kernels per iteration; needs the mesh's node
     incidence, built here).  Each form is reproducible; they agree to rounding.
+    moduli: "physical" (C with the packed dN/dX: FP64, FP32, or FP32 on FP64 vectors) or "ref" (FP32
+    moduli pulled back to the element reference frame, 10 per Gauss point, FP64 vectors; the product
+    reads no gradients).
     """
 
-    def __init__(self, mesh, C, diag, b, x, use_graph=True, form="colour"):
+    def __init__(self, mesh, C, diag, b, x, use_graph=True, form="colour", moduli="physical"):
         use_graph = int(use_graph) if os.environ.get("DFEA_PCG_GRAPH", "1") != "0" else 0
         if form not in ("colour", "gather"):
             raise ValueError("form must be 'colour' or 'gather'")
@@ -38,7 +41,14 @@ class DevicePCG:
             mesh.ensure_node_incidence()
             flags = _lib.DFEA_PCG_GATHER
         vt = b.dtype
-        if C.dtype == torch.float64:
+        if moduli == "ref":
+            # FP32 moduli in the element reference frame (10 per Gauss point): no gradients read
+            if C.dtype != torch.float32 or vt != torch.float64 or C.numel() != mesh.moduli_numel_ref():
+                raise ValueError("reference-frame moduli: FP32, 10 per Gauss point, with FP64 vectors")
+            dt = _lib.DFEA_F32REF
+        elif moduli != "physical":
+            raise ValueError("moduli must be 'physical' or 'ref'")
+        elif C.dtype == torch.float64:
             dt = _lib.DFEA_F64
             if vt != torch.float64:
                 raise ValueError("FP64 moduli need FP64 vectors")
@@ -47,7 +57,7 @@ class DevicePCG:
         for name, t in (("diag", diag), ("b", b), ("x", x)):
             if t.dtype != vt or t.numel() != mesh.n_dof or not t.is_contiguous() or t.device != mesh.device:
                 raise ValueError(f"{name} must be a contiguous ({mesh.n_dof},) {vt} tensor on {mesh.device}")
-        if dt != _lib.DFEA_F64:
+        if dt in (_lib.DFEA_MIXED, _lib.DFEA_F32):
             mesh.ensure_grad32()
         self.mesh, self.C, self.diag, self.b, self.x = mesh, C, diag, b, x
         self.vec_dtype = vt

@@ -110,11 +110,25 @@ def hbm_estimate(req, precision="fp32"):
     nen, nq = NEN[req.element_type], NQ[req.element_type]
     per_el = (8 * nen + 16 * nq * nen + 8 * nq          # problem dictionary: conn, dN_dX, w_detJ
               + 4 * nen + 4 + 16 * nq * nen + 8 * nq + 8  # packed mesh (FP64 gradients)
-              + 8 * nq * nen                            # FP32 gradients
-              + (64 if precision == "fp32" else 128) * nq   # moduli
+              + ((40 + 32) * nq if precision == "fp32"  # reference-frame FP32 moduli + inverse Jacobians
+                 else 128 * nq)                         # FP64 moduli
               + 16 * nen + 4 * nen)                     # gather form: element results, node incidence
     per_node = 16 + 2 * 8 * 14 + 2 * 4 * 6 + 1 + 4      # nodes, ~14 f64 and ~6 f32 DOF vectors, fix bits, ptr
     return int(E * per_el + N * per_node + 4 * 2 ** 20)  # + reduction scratch and PCG state
+
+
+def pcg_iteration_bytes(req):
+    """
+    Bytes one PCG iteration of a request must move in the serving configuration (reference-frame FP32
+    moduli, gather form, FP64 Krylov vectors): per element the moduli (40 B per Gauss point) and the
+    connectivity, the element results written and read back (2 x 16 B per local node) and the incidence
+    (4 B per local node); per node 11 passes over FP64 pairs (the gather of p, update 1 reading p, d, x,
+    r and writing x, r, update 2 reading r, d, p and writing p), the incidence pointer and the fix byte.
+    """
+    nen, nq = NEN[req.element_type], NQ[req.element_type]
+    per_el = 40 * nq + 4 * nen + 32 * nen + 4 * nen
+    per_node = 11 * 16 + 4 + 1
+    return req.n_elements * per_el + req.n_nodes * per_node
 
 
 def request_problem(req, device="cpu", build_on_device=False):
@@ -124,12 +138,13 @@ def request_problem(req, device="cpu", build_on_device=False):
 
 
 def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2,
-                  host_params=None, pcg_form="auto"):
+                  host_params=None, pcg_form="auto", fp32_moduli="ref"):
     """
     Build (or copy from ``host_params``) and solve one request on the current stream; returns
     (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
     concurrent slots; 1: conditional-loop graph; 0: direct launches); ``pcg_form`` the product form inside
-    it ("auto", "colour" or "gather", see DevicePCG and workspace.pcg_form_for).
+    it ("auto", "colour" or "gather", see DevicePCG and workspace.pcg_form_for); ``fp32_moduli`` the FP32
+    operator's moduli ("ref": reference frame, no gradients read; "physical").
     """
     if host_params is not None:
         p = {k: (v.to(device, non_blocking=True) if torch.is_tensor(v) else v) for k, v in host_params.items()}
@@ -137,7 +152,7 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
         p = request_problem(req, device, build_on_device=True)
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
-    ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form)
+    ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli)
     u, info = newton_krylov_solve(p, th, n_load_steps, tol, verbose=False, workspace=ws, precision=precision,
                                   pcg_max_iter=pcg_max_iter)
     ws.pcg.close()
@@ -151,17 +166,24 @@ class ServingEngine:
     """
 
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
-                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="auto"):
+                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="auto",
+                 fp32_moduli="ref", order="fifo"):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = int(0.6 * free)
         self.n_slots, self.hbm_budget, self.precision = n_slots, int(hbm_budget), precision
         self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter,
-                             pcg_graph=pcg_graph, pcg_form=pcg_form)
+                             pcg_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli)
         # torch's caching allocator keeps one pool per stream; a slot whose pool already holds a block of
         # the largest request never calls cudaMalloc (which synchronises the whole device) mid-run
         self.prewarm_bytes = int(prewarm_bytes)
+        # which waiting request a free slot takes: "fifo" (arrival order) or "largest_first" (the largest
+        # waiting request, by HBM footprint: for a backlog this is longest-processing-time-first, which
+        # keeps the slots busy until the end instead of leaving one large request running alone)
+        if order not in ("fifo", "largest_first"):
+            raise ValueError("order must be 'fifo' or 'largest_first'")
+        self.order = order
         self._cv = threading.Condition()
         self._in_use = 0
         self.peak_in_use = 0
@@ -207,7 +229,7 @@ class ServingEngine:
         (CUDA events joined over the slot streams) and ``self.wall`` the host wall time.
         """
         results = {r.rid: Result(r.rid, arrival=r.arrival) for r in requests}
-        q = queue.Queue()
+        q = queue.PriorityQueue()      # entries (priority, sequence, request); None ends a worker
         streams = self._slot_streams()
         main = torch.cuda.current_stream(self.device)
         ev_start, ev_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -220,7 +242,7 @@ class ServingEngine:
         def worker(stream):
             torch.cuda.set_device(self.device)
             while True:
-                req = q.get()
+                req = q.get()[2]
                 if req is None:
                     return
                 res = results[req.rid]
@@ -247,13 +269,17 @@ class ServingEngine:
         threads = [threading.Thread(target=worker, args=(st,), daemon=True) for st in streams]
         for th in threads:
             th.start()
+        seq = 0
         for req in sorted(requests, key=lambda r: r.arrival):
             delay = req.arrival - (time.perf_counter() - t0)
             if delay > 0:
                 time.sleep(delay)
-            q.put(req)
+            prio = -hbm_estimate(req, self.precision) if self.order == "largest_first" else 0
+            q.put((prio, seq, req))
+            seq += 1
         for _ in threads:
-            q.put(None)
+            q.put((math.inf, seq, None))
+            seq += 1
         for th in threads:
             th.join()
         for st in streams:

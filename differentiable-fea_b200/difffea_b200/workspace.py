@@ -2,8 +2,9 @@
 Per-problem device workspace of the Newton-Krylov solver.
 
 A ``NewtonWorkspace`` keeps everything a solve touches in HBM for the whole solve: the state and
-trial vectors, the residual, the Gauss-point moduli (FP64, or FP32 for the mixed-precision form, whose
-operator reads FP32 moduli and gradients while the Krylov vectors stay FP64), the Jacobi diagonal,
+trial vectors, the residual, the Gauss-point moduli (FP64, or for the mixed-precision form FP32 moduli
+pulled back to each element's reference frame, so that its operator reads 10 FP32 numbers per Gauss
+point and no gradients, while the Krylov vectors stay FP64), the Jacobi diagonal,
 and one graph-captured ``DevicePCG`` bound to them.  The solver loop
 calls the C ABI directly on these buffers (no allocation per Newton step), reading back only the
 scalars the algorithm branches on: ||R|| per residual evaluation and (status, iterations) per PCG.
@@ -34,7 +35,7 @@ def pcg_form_for(mesh, pcg_form="auto"):
 
 
 class NewtonWorkspace:
-    def __init__(self, params, precision="fp64", use_graph=True, pcg_form="auto"):
+    def __init__(self, params, precision="fp64", use_graph=True, pcg_form="auto", fp32_moduli="ref"):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")
         self.params = params
@@ -51,15 +52,26 @@ class NewtonWorkspace:
         self.diag = torch.empty(n, **f64)
         self.scal = torch.zeros(4, **f64)
         self.scal_host = torch.zeros(4, dtype=torch.float64).pin_memory()
-        # "fp32": FP32 moduli and gradients (the bytes of the operator), FP64 Krylov vectors and scalars
-        self.C = torch.empty(mesh.moduli_numel(), dtype=torch.float64 if precision == "fp64" else torch.float32,
-                             device=dev)
-        if precision == "fp32":
-            mesh.ensure_grad32()
+        # "fp32": the operator's bytes in FP32, Krylov vectors and scalars in FP64.  fp32_moduli "ref":
+        # moduli pulled back to the element reference frame, 10 per Gauss point, no gradients read
+        # (the default); "physical": the 16 moduli with FP32 gradients.
+        if fp32_moduli not in ("ref", "physical"):
+            raise ValueError("fp32_moduli must be 'ref' or 'physical'")
+        self.moduli_kind = "ref" if (precision == "fp32" and fp32_moduli == "ref") else "physical"
+        if self.moduli_kind == "ref":
+            mesh.ensure_ref_frame()
+            self.C = torch.empty(mesh.moduli_numel_ref(), dtype=torch.float32, device=dev)
+            self.moduli_code = _lib.DFEA_F32REF
+        else:
+            self.C = torch.empty(mesh.moduli_numel(), dtype=torch.float64 if precision == "fp64" else torch.float32,
+                                 device=dev)
+            self.moduli_code = _lib.DFEA_F64 if precision == "fp64" else _lib.DFEA_F32
+            if precision == "fp32":
+                mesh.ensure_grad32()
         # the PCG reads -R from b and writes its solution straight into du
         self.b = torch.empty(n, **f64)
         self.pcg = DevicePCG(mesh, self.C, self.diag, self.b, self.du, use_graph=use_graph,
-                             form=pcg_form_for(mesh, pcg_form))
+                             form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind)
         self.work = mesh.reduce_work()
         self.theta = None
         self.n_launch_groups = 0
@@ -83,9 +95,8 @@ class NewtonWorkspace:
 
     def linearize(self, u):
         """Kernel (a): moduli C and Jacobi diagonal at u (into the buffers the PCG graph is bound to)."""
-        dt = _lib.DFEA_F64 if self.precision == "fp64" else _lib.DFEA_F32
-        _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0, ptr(self.C), dt,
-                  ptr(self.diag), stream_handle())
+        _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0, ptr(self.C),
+                  self.moduli_code, ptr(self.diag), stream_handle())
 
     def solve(self, R, rtol, max_iter):
         """du = PCG(A, -R) to relative tolerance rtol; returns (du (FP64 buffer), iterations, status)."""

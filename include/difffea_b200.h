@@ -41,6 +41,15 @@ extern "C" {
 #define DFEA_F64 0
 #define DFEA_F32 1
 #define DFEA_MIXED 2  /* PCG only: FP32 moduli and gradients (the operator), FP64 Krylov vectors */
+/* Moduli in the element's reference frame, FP32, symmetric (10 entries per Gauss point):
+ * Chat_(i a),(k b) = sum_{J,L} Jinv_aJ C_(iJ),(kL) Jinv_bL with Jinv = (dX/dxi)^-1, so that the product
+ * needs the fixed reference shape gradients only (mesh->ref_grad), not the per-element dN/dX.
+ * Layout per Gauss point q: float4 [stride] (entries 00 01 02 03), float4 [stride] (11 12 13 22),
+ * float2 [stride] (23 33), i.e. 10 * stride floats per q.  As a moduli dtype (dfea_qp_moduli,
+ * dfea_tangent_apply[_gather] with f64 vectors) and as a PCG vec_dtype (FP64 Krylov vectors). */
+#define DFEA_F32REF 3
+#define DFEA_MAX_NEN 9
+#define DFEA_MAX_NQ 9
 
 #define DFEA_MAX_COLOURS 64
 
@@ -74,6 +83,11 @@ typedef struct dfea_mesh_view {
      * a * stride + e of local node a of (packed) element e, in increasing order. */
     const int32_t* node_elem_ptr; /* [n_nodes + 1]                                           */
     const int32_t* node_elem;     /* [n_el * nen]                                            */
+    /* Optional, for DFEA_F32REF moduli: inverse element Jacobians [n_q][2][stride] (rows of
+     * Jinv as f64 pairs, NULL if not built) and the reference shape gradients at the Gauss points,
+     * ref_grad[(q * nen + a) * 2 + alpha] = dN_a/dxi_alpha (host values). */
+    const double* jinv;
+    double ref_grad[DFEA_MAX_NQ * DFEA_MAX_NEN * 2];
 } dfea_mesh_view;
 
 /* ---------------------------------------------------------------- library --------------------- */
@@ -200,7 +214,8 @@ int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
  * k = 0 and x otherwise).  moduli/diag/b/x are device buffers that stay bound to the handle;
  * their CONTENTS may change between solves.  vec_dtype DFEA_F64 needs f64 moduli; DFEA_F32 needs
  * f32 moduli and mesh->grad32, and then diag, b and x are f32; DFEA_MIXED applies f32 moduli and
- * mesh->grad32 to f64 vectors (diag, b, x f64): FP32 operator data, FP64 recurrences.  The graph is captured on an internal
+ * mesh->grad32 to f64 vectors (diag, b, x f64): FP32 operator data, FP64 recurrences; DFEA_F32REF
+ * applies reference-frame FP32 moduli (no gradients read) to f64 vectors.  The graph is captured on an internal
  * stream.  use_graph = 1: that graph; 2: 8 iterations captured back to back in a plain graph (no
  * conditional node) replayed by the host until the status word ends, which overlaps better with other
  * streams' work; 0: the same kernels launched directly, host-polled every 16 iterations.

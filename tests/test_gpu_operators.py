@@ -192,3 +192,62 @@ def test_gather_form_at_size_fp64_and_fp32(et, nx, ny):
     A32 = make_A_operator_cuda(u, th, p, precision="fp32")
     assert rel(_apply_gather(A32, v.float()).double(), A32(v.float()).double()) < 1e-5
     assert rel(_apply_gather(A32, v), A32(v)) < 1e-13              # mixed: FP32 operator data, FP64 vectors
+
+
+# ------------------------------------------------------------------------------------------------
+# reference-frame FP32 moduli (DFEA_F32REF): 10 per Gauss point, no gradients read by the product
+# ------------------------------------------------------------------------------------------------
+def _ref_operator(p, u, th):
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr, stream_handle
+    mesh = cuda_mesh(p)
+    mesh.ensure_ref_frame()
+    mesh.ensure_node_incidence()
+    mu0, lam0 = neo_hookean_parameters(p)
+    C = torch.empty(mesh.moduli_numel_ref(), dtype=torch.float32, device=DEV)
+    _lib.call("dfea_qp_moduli", mesh.view_ref, ptr(u.contiguous()), ptr(th.contiguous()), mu0, lam0, ptr(C),
+              _lib.DFEA_F32REF, ptr(None), stream_handle())
+    return mesh, C
+
+
+def _ref_apply(mesh, C, v, gather):
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr, stream_handle
+    y = torch.empty_like(v)
+    if gather:
+        fe = torch.empty(int(_lib.load().dfea_gather_work_bytes(mesh.view_ref, _lib.DFEA_F64)), dtype=torch.uint8,
+                         device=DEV)
+        _lib.call("dfea_tangent_apply_gather", mesh.view_ref, ptr(C), _lib.DFEA_F32REF, ptr(v), ptr(y), _lib.DFEA_F64,
+                  ptr(fe), stream_handle())
+    else:
+        _lib.call("dfea_tangent_apply", mesh.view_ref, ptr(C), _lib.DFEA_F32REF, ptr(v), ptr(y), _lib.DFEA_F64,
+                  stream_handle())
+    return y
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES)
+def test_reference_frame_fp32_operator_matches_qp_ew(name):
+    d, p, u, v, th = golden_case(name)
+    mesh, C = _ref_operator(p, u, th)
+    y_col, y_gat = _ref_apply(mesh, C, v, False), _ref_apply(mesh, C, v, True)
+    assert rel(y_col, d["Av_qp_ew"]) < 2e-6 and rel(y_gat, d["Av_qp_ew"]) < 2e-6
+    assert rel(y_col, y_gat) < 1e-13                                  # same FP32 data, FP64 arithmetic
+    assert torch.equal(y_gat, _ref_apply(mesh, C, v, True))
+
+
+@pytest.mark.parametrize("et,nx,ny", [("quad4", 120, 60), ("quad9", 40, 20), ("tri6", 30, 20)])
+def test_reference_frame_operator_at_size_is_symmetric(et, nx, ny):
+    p = build_rectangle_problem(et, nx, ny, float(nx), float(ny), device=DEV)
+    u, v, w, th = _random_state(p, 1.0, 5)
+    mesh, C = _ref_operator(p, u, th)
+    Av, Aw = _ref_apply(mesh, C, v, True), _ref_apply(mesh, C, w, True)
+    assert abs(float(w @ Av) - float(v @ Aw)) <= 1e-10 * abs(float(v @ Aw))   # FP32 data, exact symmetry kept
+    assert rel(Av, make_tangent_operator("cuda", u, th, p)(v)) < 2e-6
+
+
+def test_reference_frame_rejects_inconsistent_geometry():
+    d, p, u, v, th = golden_case("operator_quad4_h0.5_unit")
+    q = dict(p)
+    q["dN_dX"] = p["dN_dX"].flip(1).contiguous()                        # Gauss points in another order
+    with pytest.raises(ValueError):
+        cuda_mesh(q).ensure_ref_frame()

@@ -190,3 +190,22 @@ def test_newton_solve_with_the_gather_form(name):
     u, info = newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False, workspace=ws)
     assert info["converged"] and rel(u, d["u_star"]) < 1e-9
     assert info["total_newton"] == int(d["total_newton"])
+
+
+def test_reference_frame_pcg_matches_the_fp64_solution():
+    p, A, M, A_ref, d_ref, b = _linear_system()
+    u = torch.as_tensor(load("operator_quad4_h0.1_theta")["u"], device=DEV)
+    th = torch.as_tensor(load("operator_quad4_h0.1_theta")["theta"], device=DEV)
+    ws64 = NewtonWorkspace(p, "fp64")
+    ws32 = NewtonWorkspace(p, "fp32")
+    assert ws32.moduli_kind == "ref" and ws32.C.numel() == ws32.mesh.moduli_numel_ref()
+    xs = {}
+    for ws in (ws64, ws32):
+        ws.set_theta(th)
+        ws.linearize(u)
+        ws.b.copy_(b)
+        k, status = ws.pcg.solve(1e-10, 3000)
+        assert status == "converged"
+        xs[ws.precision] = ws.du.clone()
+    assert rel(xs["fp32"], xs["fp64"]) < 1e-4                            # FP32 operator, FP64 recurrences
+    assert torch.equal(ws32.diag, ws64.diag)                            # the diagonal is FP64 in both
