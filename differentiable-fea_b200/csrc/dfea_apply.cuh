@@ -555,6 +555,10 @@ int resident_grid(int64_t n_elements) {
     return (int)(grid < 1 ? 1 : grid);
 }
 
+// A grid limited to `cap` blocks (0: no limit).  Solves that share the GPU with other streams run
+// with fewer, longer-lived blocks per launch, so that launches of different streams fit side by side.
+inline int capped(int grid, int cap) { return (cap > 0 && grid > cap) ? cap : grid; }
+
 template <int NEN, int NQ, typename SD, typename T, bool DOT>
 int apply_grid(int64_t n_elements) {
     using Cfg = ApplyCfg<NEN, SD>;
@@ -594,7 +598,8 @@ inline L2Window l2_window(const void* v, const void* y, size_t vec_bytes) {
 // With DOT, colour c reduces into sites[c] (result = curvature of that colour).
 template <int NEN, int NQ, typename SD, typename T, bool DOT>
 int launch_apply_colours(const dfea_mesh_view& mv, const SD* C, const SD* G, const T* v, T* y,
-                         const RedSite* sites, const int* done, cudaStream_t stream, bool count = true) {
+                         const RedSite* sites, const int* done, cudaStream_t stream, bool count = true,
+                         int grid_cap = 0) {
     using Cfg = ApplyCfg<NEN, SD>;
     const Mesh m = kernel_mesh(mv);
     long long max_window = 0;
@@ -611,7 +616,7 @@ int launch_apply_colours(const dfea_mesh_view& mv, const SD* C, const SD* G, con
     for (int c = 0; c < mv.n_colours; ++c) {
         const int64_t e0 = mv.colour_begin[c], e1 = mv.colour_begin[c + 1];
         if (e1 <= e0) continue;
-        const int grid = apply_grid<NEN, NQ, SD, T, DOT>(e1 - e0);
+        const int grid = capped(apply_grid<NEN, NQ, SD, T, DOT>(e1 - e0), grid_cap);
         const RedSite site = DOT ? sites[c] : RedSite{nullptr, nullptr, nullptr};
         const int rc = launch_kernel(k_apply<NEN, NQ, SD, T, DOT>, dim3(grid), dim3(Cfg::NT), Cfg::SMEM, stream, opts, m, e0,
                                      e1, C, G, v, y, site, done);
@@ -625,7 +630,7 @@ int launch_apply_colours(const dfea_mesh_view& mv, const SD* C, const SD* G, con
 // window on v.  The node pass is launched by the caller.
 template <int NEN, int NQ, typename SD, typename T, bool DOT>
 int launch_apply_elem(const dfea_mesh_view& mv, const SD* C, const SD* G, const T* v, T* fe, RedSite site,
-                      const int* done, cudaStream_t stream) {
+                      const int* done, cudaStream_t stream, int grid_cap = 0) {
     using Cfg = ApplyCfg<NEN, SD>;
     const Mesh m = kernel_mesh(mv);
     long long max_window = 0;
@@ -639,7 +644,7 @@ int launch_apply_elem(const dfea_mesh_view& mv, const SD* C, const SD* G, const 
         opts.win_bytes = wb;
         opts.hit_ratio = setaside >= (long long)wb ? 1.0f : (float)((double)setaside / (double)wb);
     }
-    const int grid = apply_elem_grid<NEN, NQ, SD, T, DOT>(mv.n_el);
+    const int grid = capped(apply_elem_grid<NEN, NQ, SD, T, DOT>(mv.n_el), grid_cap);
     const int rc = launch_kernel(k_apply_elem<NEN, NQ, SD, T, DOT>, dim3(grid), dim3(Cfg::NT), Cfg::SMEM, stream, opts, m,
                                  C, G, v, fe, site, done);
     if (rc) return rc;
@@ -649,7 +654,7 @@ int launch_apply_elem(const dfea_mesh_view& mv, const SD* C, const SD* G, const 
 // Reference-frame launches: colour passes (y read-modify-write) or the element pass (results into fe).
 template <int NEN, int NQ, typename T, bool DOT>
 int launch_apply_ref_colours(const dfea_mesh_view& mv, const float* C, const T* v, T* y, const RedSite* sites,
-                             const int* done, cudaStream_t stream) {
+                             const int* done, cudaStream_t stream, int grid_cap = 0) {
     const Mesh m = kernel_mesh(mv);
     const RefGrad<NEN, NQ> rg = ref_grad_of<NEN, NQ>(mv);
     long long max_window = 0;
@@ -666,7 +671,7 @@ int launch_apply_ref_colours(const dfea_mesh_view& mv, const float* C, const T* 
     for (int c = 0; c < mv.n_colours; ++c) {
         const int64_t e0 = mv.colour_begin[c], e1 = mv.colour_begin[c + 1];
         if (e1 <= e0) continue;
-        const int grid = apply_ref_grid<NEN, NQ, T, DOT>(e1 - e0);
+        const int grid = capped(apply_ref_grid<NEN, NQ, T, DOT>(e1 - e0), grid_cap);
         const RedSite site = DOT ? sites[c] : RedSite{nullptr, nullptr, nullptr};
         const int rc = launch_kernel(k_apply_ref<NEN, NQ, T, DOT>, dim3(grid), dim3(128), RefApplyCfg<NEN>::SMEM, stream,
                                      opts, m, e0, e1, C, rg, v, y, site, done);
@@ -677,7 +682,7 @@ int launch_apply_ref_colours(const dfea_mesh_view& mv, const float* C, const T* 
 
 template <int NEN, int NQ, typename T, bool DOT>
 int launch_apply_ref_elem(const dfea_mesh_view& mv, const float* C, const T* v, T* fe, RedSite site, const int* done,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, int grid_cap = 0) {
     const Mesh m = kernel_mesh(mv);
     const RefGrad<NEN, NQ> rg = ref_grad_of<NEN, NQ>(mv);
     long long max_window = 0;
@@ -691,7 +696,7 @@ int launch_apply_ref_elem(const dfea_mesh_view& mv, const float* C, const T* v, 
         opts.win_bytes = wb;
         opts.hit_ratio = setaside >= (long long)wb ? 1.0f : (float)((double)setaside / (double)wb);
     }
-    const int grid = apply_ref_elem_grid<NEN, NQ, T, DOT>(mv.n_el);
+    const int grid = capped(apply_ref_elem_grid<NEN, NQ, T, DOT>(mv.n_el), grid_cap);
     const int rc = launch_kernel(k_apply_ref_elem<NEN, NQ, T, DOT>, dim3(grid), dim3(128), RefApplyCfg<NEN>::SMEM, stream,
                                  opts, m, C, rg, v, fe, site, done);
     if (rc) return rc;

@@ -250,6 +250,7 @@ struct dfea_pcg {
     PcgLayout layout{1, 8, 1};
     int use_graph;
     bool gather = false;             // product in the gather form (element pass + node sums in update 1)
+    int grid_cap = 0;                // most blocks per launch (0: as many as the GPU holds)
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -292,7 +293,7 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
     const T* d = static_cast<const T*>(h.diag);
     T* x = static_cast<T*>(h.x);
     PcgState* st = h.state();
-    const int gn = grid_for(mv.n_nodes, kThreads, 4);
+    const int gn = capped(grid_for(mv.n_nodes, kThreads, 4), h.grid_cap);
     LaunchOpts pdl;
     pdl.pdl = true;
     int rc;
@@ -303,9 +304,9 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
             constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
             if constexpr (REF)
                 return launch_apply_ref_elem<NEN, NQ, T, true>(mv, reinterpret_cast<const float*>(C), p, fe, h.site(0, 1),
-                                                               &st->done, s);
+                                                               &st->done, s, h.grid_cap);
             else
-                return launch_apply_elem<NEN, NQ, S, T, true>(mv, C, G, p, fe, h.site(0, 1), &st->done, s);
+                return launch_apply_elem<NEN, NQ, S, T, true>(mv, C, G, p, fe, h.site(0, 1), &st->done, s, h.grid_cap);
         });
         if (rc) return rc;
         if ((rc = launch_kernel(k_pcg_update1<T, true>, dim3(gn), dim3(kThreads), 0, s, pdl, m, 1, p, (const T*)y, d, x,
@@ -321,9 +322,10 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
             constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
             if constexpr (REF)
                 return launch_apply_ref_colours<NEN, NQ, T, true>(mv, reinterpret_cast<const float*>(C), p, y, sites,
-                                                                  &st->done, s);
+                                                                  &st->done, s, h.grid_cap);
             else
-                return launch_apply_colours<NEN, NQ, S, T, true>(mv, C, G, p, y, sites, &st->done, s, false);
+                return launch_apply_colours<NEN, NQ, S, T, true>(mv, C, G, p, y, sites, &st->done, s, false,
+                                                                 h.grid_cap);
         });
         if (rc) return rc;
         if ((rc = launch_kernel(k_pcg_update1<T, false>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mv.n_colours, p,
@@ -458,7 +460,8 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
     h->work = static_cast<char*>(work);
     h->layout = layout_for(*mesh, vec_dtype);
     h->gather = (use_graph & DFEA_PCG_GATHER) != 0;
-    use_graph &= ~DFEA_PCG_GATHER;
+    h->grid_cap = (int)((uint32_t)use_graph >> 8);
+    use_graph &= 0xff & ~DFEA_PCG_GATHER;
     h->use_graph = (use_graph == 2) ? 2 : (use_graph ? 1 : 0);
     if (h->gather && h->layout.off_fe == h->layout.total) {
         delete h;

@@ -21,6 +21,13 @@ MAX_COLOURS = 64
 PCG_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "negative_curvature", 4: "zero_rhs"}
 DFEA_PCG_GATHER = 16  # dfea_pcg_create flag: gather form of the product
 
+
+def pcg_max_blocks(n):
+    """dfea_pcg_create option: at most n blocks per launch (0: as many as the GPU holds)."""
+    if not 0 <= n < 2 ** 23:
+        raise ValueError("max_blocks out of range")
+    return int(n) << 8
+
 c_i32, c_i64, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
 

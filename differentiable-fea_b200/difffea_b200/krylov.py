@@ -29,10 +29,11 @@ class DevicePCG:
     incidence, built here).  Each form is reproducible; they agree to rounding.
     moduli: "physical" (C with the packed dN/dX: FP64, FP32, or FP32 on FP64 vectors) or "ref" (FP32
     moduli pulled back to the element reference frame, 10 per Gauss point, FP64 vectors; the product
-    reads no gradients).
+    reads no gradients).  max_blocks: at most this many blocks per launch (0: the whole GPU), for solves
+    that share the GPU with others; results agree with the unlimited form's to rounding.
     """
 
-    def __init__(self, mesh, C, diag, b, x, use_graph=True, form="colour", moduli="physical"):
+    def __init__(self, mesh, C, diag, b, x, use_graph=True, form="colour", moduli="physical", max_blocks=0):
         use_graph = int(use_graph) if os.environ.get("DFEA_PCG_GRAPH", "1") != "0" else 0
         if form not in ("colour", "gather"):
             raise ValueError("form must be 'colour' or 'gather'")
@@ -40,6 +41,7 @@ class DevicePCG:
         if form == "gather":
             mesh.ensure_node_incidence()
             flags = _lib.DFEA_PCG_GATHER
+        flags |= _lib.pcg_max_blocks(max_blocks)
         vt = b.dtype
         if moduli == "ref":
             # FP32 moduli in the element reference frame (10 per Gauss point): no gradients read

@@ -35,7 +35,7 @@ def pcg_form_for(mesh, pcg_form="auto"):
 
 
 class NewtonWorkspace:
-    def __init__(self, params, precision="fp64", use_graph=True, pcg_form="auto", fp32_moduli="ref"):
+    def __init__(self, params, precision="fp64", use_graph=True, pcg_form="auto", fp32_moduli="ref", max_blocks=0):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")
         self.params = params
@@ -71,7 +71,7 @@ class NewtonWorkspace:
         # the PCG reads -R from b and writes its solution straight into du
         self.b = torch.empty(n, **f64)
         self.pcg = DevicePCG(mesh, self.C, self.diag, self.b, self.du, use_graph=use_graph,
-                             form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind)
+                             form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind, max_blocks=max_blocks)
         self.work = mesh.reduce_work()
         self.theta = None
         self.n_launch_groups = 0

@@ -61,6 +61,9 @@ extern "C" {
 #define DFEA_PCG_ZERO_RHS 4    /* ||b|| == 0: x = 0 after zero iterations              */
 
 #define DFEA_PCG_GATHER 16     /* dfea_pcg_create flag: gather form of the product     */
+/* dfea_pcg_create option: at most n blocks per launch (n < 2^23; 0 = as many as the GPU holds at
+ * once).  For solves that share the GPU with solves on other streams. */
+#define DFEA_PCG_MAX_BLOCKS(n) ((int32_t)(n) << 8)
 
 /* A mesh in device memory, colour-sorted.  Sizes are host values, pointers are device pointers. */
 typedef struct dfea_mesh_view {
@@ -224,6 +227,8 @@ int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
  * update: 3 kernels per iteration instead of n_colours + 2; needs mesh->node_elem_ptr/node_elem, and
  * then dfea_pcg_work_bytes includes the element-result buffer).  Its iterates agree with the colour
  * form's to rounding (the per-node sums are grouped differently); each form is reproducible.
+ * OR-ing DFEA_PCG_MAX_BLOCKS(n) limits every launch of the solve to n blocks (the results agree with
+ * the unlimited grid's to rounding: the reductions group their partial sums by block).
  */
 int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, const void* diag,
                     const void* b, void* x, int32_t vec_dtype, void* work, int32_t use_graph,

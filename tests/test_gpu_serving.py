@@ -21,8 +21,9 @@ def _requests():
 
 def test_results_are_the_same_alone_and_in_the_mix():
     reqs = _requests()
-    alone = run_plain(reqs, DEV, precision="fp32")
-    mixed = ServingEngine(n_slots=4, device=DEV).run(reqs)
+    eng = ServingEngine(n_slots=4, device=DEV)
+    alone = run_plain(reqs, DEV, precision="fp32", max_blocks=eng.max_blocks)
+    mixed = eng.run(reqs)
     for a, b in zip(alone, mixed):
         assert b.error == "" and b.converged and a.converged
         assert torch.equal(a.u, b.u)                   # deterministic: bit for bit
