@@ -23,8 +23,9 @@ nu = 0.3, h = 1.  Algorithmic bytes count every array a kernel must touch once:
     pcg          per iteration: the product with the curvature fused (apply bytes) + update 1 (7 vectors)
                  + update 2 (5 vectors + N fix bytes)
 
-``precision``: fp64 (FP64 moduli, gradients and vectors), fp32 (all FP32) or mixed (FP32 moduli and
-gradients on FP64 vectors, the serving operator).
+``precision``: fp64 (FP64 moduli, gradients and vectors), fp32 (all FP32), mixed (FP32 moduli and
+gradients on FP64 vectors) or ref (FP32 moduli in the element reference frame, 10 per Gauss point, on
+FP64 vectors: the serving operator; the product reads no gradients, its bytes count 10 moduli).
 """
 import argparse
 import json
@@ -40,7 +41,7 @@ from difffea_b200.problem import build_rectangle_problem
 NEN = {"quad4": 4, "quad9": 9}
 NQ = {"quad4": 4, "quad9": 9}
 SWEEP_ELEMENTS = (40_000, 160_000, 640_000, 2_560_000)
-_SIZES = {"fp64": (8, 8, 8), "fp32": (4, 4, 4), "mixed": (4, 4, 8)}     # (moduli, gradients, vectors)
+_SIZES = {"fp64": (8, 8, 8), "fp32": (4, 4, 4), "mixed": (4, 4, 8), "ref": (4, 0, 8)}  # (moduli, gradients, vectors)
 
 
 def side_for(n_elements):
@@ -70,7 +71,14 @@ class State:
         fp32_C = precision in ("fp32", "mixed")
         if fp32_C:
             self.mesh.ensure_grad32()
-        self.C, self.diag = ops.qp_moduli(self.mid, self.u, self.theta, self.mu0, self.lam0, fp32_C, True)
+        if precision == "ref":
+            self.mesh.ensure_ref_frame()
+            self.C = torch.empty(self.mesh.moduli_numel_ref(), dtype=torch.float32, device=device)
+            self.diag = torch.empty(N2, dtype=torch.float64, device=device)
+            _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mu0, self.lam0,
+                      ptr(self.C), _lib.DFEA_F32REF, ptr(self.diag), stream_handle())
+        else:
+            self.C, self.diag = ops.qp_moduli(self.mid, self.u, self.theta, self.mu0, self.lam0, fp32_C, True)
         vt = torch.float32 if precision == "fp32" else torch.float64
         pad = (N2 + 63) // 64 * 64
         self.buf = torch.empty(2 * pad, dtype=vt, device=device)            # [v | y], as the PCG's vectors
@@ -90,7 +98,8 @@ class State:
         """Bytes the product must move; the gather form is charged the colour form's minimum (its element
         results and incidence are extra traffic it pays for fewer launches)."""
         sC, sG, sv = _SIZES[self.precision]
-        return (self.n_el * self.nq * 16 * sC + self.n_el * self.nq * self.nen * 2 * sG
+        n_c = 10 if self.precision == "ref" else 16
+        return (self.n_el * self.nq * n_c * sC + self.n_el * self.nq * self.nen * 2 * sG
                 + self.n_el * self.nen * 4 + 3 * self.N2 * sv)
 
     def _geometry_bytes(self):
@@ -114,6 +123,8 @@ class State:
     # launches ---------------------------------------------------------------------------------------
     def apply(self):
         cdt = _lib.DFEA_F64 if self.C.dtype == torch.float64 else _lib.DFEA_F32
+        if self.precision == "ref":
+            cdt = _lib.DFEA_F32REF
         vdt = _lib.DFEA_F64 if self.v.dtype == torch.float64 else _lib.DFEA_F32
         if self.form == "gather":
             _lib.call("dfea_tangent_apply_gather", self.mesh.view_ref, ptr(self.C), cdt, ptr(self.v), ptr(self.y), vdt,
@@ -123,7 +134,11 @@ class State:
                       stream_handle())
 
     def moduli(self):
-        ops.qp_moduli(self.mid, self.u, self.theta, self.mu0, self.lam0, self.precision != "fp64", True)
+        if self.precision == "ref":
+            _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mu0, self.lam0,
+                      ptr(self.C), _lib.DFEA_F32REF, ptr(self.diag), stream_handle())
+        else:
+            ops.qp_moduli(self.mid, self.u, self.theta, self.mu0, self.lam0, self.precision != "fp64", True)
 
     def residual(self):
         ops.residual(self.mid, self.u, self.theta, self.mu0, self.lam0, self.p["f"], 1.0)
@@ -172,7 +187,8 @@ def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters
         d = st.diag.to(vt)
         b = (st.p["m"].to(vt) * st.v).contiguous()
         x = torch.empty_like(b)
-        solver = DevicePCG(st.mesh, st.C, d, b, x, use_graph=pcg_graph, form=form)
+        solver = DevicePCG(st.mesh, st.C, d, b, x, use_graph=pcg_graph, form=form,
+                           moduli="ref" if precision == "ref" else "physical")
 
         def fn():
             solver.solve(1e-30, pcg_iters)                     # exactly pcg_iters iterations
@@ -192,7 +208,7 @@ def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters
     return row
 
 
-def solve_once(element, nx, precision, pcg_graph, form="colour"):
+def solve_once(element, nx, precision, pcg_graph, form="auto"):
     """Wall and device milliseconds of one serving-type request (the second of two identical solves)."""
     import time
     from difffea_b200.serving import Request, solve_request
@@ -225,25 +241,28 @@ def main(argv=None):
     ap.add_argument("--pcg-iters", type=int, default=64)
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--nx", type=int, default=256)
-    ap.add_argument("--form", default="colour", choices=("colour", "gather"),
-                    help="product form: one launch per colour, or element pass + node sums")
+    ap.add_argument("--sweep-precisions", default="fp64,fp32", help="comma-separated precisions of the sweep")
+    ap.add_argument("--form", default=None, choices=("colour", "gather", "auto"),
+                    help="product form: one launch per colour, or element pass + node sums (default: colour; "
+                         "for solve, auto = the solver's choice by mesh size)")
     ap.add_argument("--pcg-graph", type=int, default=None,
                     help="PCG form: 0 direct launches (solve's default), 1 loop graph (pcg's default), "
                          "2 unrolled graph")
     a = ap.parse_args(argv)
     if a.kind == "solve":
-        print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph, a.form)),
+        print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph,
+                                    a.form or "auto")),
               flush=True)
         return 0
     if a.kind == "sweep":
         for element in ("quad4", "quad9"):
-            for prec in ("fp64", "fp32"):
+            for prec in a.sweep_precisions.split(","):
                 for n in SWEEP_ELEMENTS:
-                    print(json.dumps(measure("apply", element, n, prec, a.reps, not a.no_flush, form=a.form)),
+                    print(json.dumps(measure("apply", element, n, prec, a.reps, not a.no_flush, form=a.form or "colour")),
                           flush=True)
         return 0
     print(json.dumps(measure(a.kind, a.element, a.elements, a.precision, a.reps, not a.no_flush, a.pcg_iters,
-                             1 if a.pcg_graph is None else a.pcg_graph, a.form)),
+                             1 if a.pcg_graph is None else a.pcg_graph, a.form or "colour")),
           flush=True)
     return 0
 
