@@ -83,12 +83,12 @@ __global__ void k_to_f64(int64_t n, const float* __restrict__ x, double* __restr
 template <int NEN, int NQ, typename CT, bool REF = false>
 __global__ void __launch_bounds__(128)
 k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const double* __restrict__ theta,
-         double mu0, double lam0, CT* __restrict__ Cout, double* __restrict__ diag) {
+         double mu0, double lam0, CT* __restrict__ Cout, double* __restrict__ diag, double* __restrict__ blocks) {
     const int64_t S = m.stride;
     const double2* u2 = reinterpret_cast<const double2*>(u);
     for (int64_t e = e0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < e1; e += (int64_t)gridDim.x * blockDim.x) {
         int node[NEN];
-        double ux[NEN], uy[NEN], dx[NEN], dy[NEN];
+        double ux[NEN], uy[NEN], dx[NEN], dy[NEN], dxy[NEN];
 #pragma unroll
         for (int a = 0; a < NEN; ++a) {
             node[a] = m.conn[a * S + e] >> 2;
@@ -97,6 +97,7 @@ k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const dou
             uy[a] = t.y;
             dx[a] = 0.0;
             dy[a] = 0.0;
+            dxy[a] = 0.0;
         }
         const double th = theta[m.orig[e]];
         const double mu = mu0 * th, lam = lam0 * th;
@@ -134,6 +135,12 @@ k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const dou
                     dx[a] += Cq[0] * gx[a] * gx[a] + (Cq[1] + Cq[4]) * gx[a] * gy[a] + Cq[5] * gy[a] * gy[a];
                     dy[a] += Cq[10] * gx[a] * gx[a] + (Cq[11] + Cq[14]) * gx[a] * gy[a] + Cq[15] * gy[a] * gy[a];
                 }
+                if (blocks != nullptr) {
+                    // coupling term of the node's 2x2 block: sum_{J,L} C[(0J),(1L)] dN_aJ dN_aL
+#pragma unroll
+                    for (int a = 0; a < NEN; ++a)
+                        dxy[a] += Cq[2] * gx[a] * gx[a] + (Cq[3] + Cq[6]) * gx[a] * gy[a] + Cq[7] * gy[a] * gy[a];
+                }
             }
         }
         if (diag != nullptr) {
@@ -146,6 +153,28 @@ k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const dou
                 d2[node[a]] = t;
             }
         }
+        if (blocks != nullptr) {
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) blocks[4 * (int64_t)node[a] + 3] += dxy[a];  // slot 3: raw coupling
+        }
+    }
+}
+
+// Nodal block-Jacobi (operators.py:598-625): B = M B M + (I - M) + 1e-12 I from the raw diagonal (diag) and
+// coupling (blocks[4n + 3]); blocks[4n .. 4n+3] := (Binv00, Binv01, Binv11, 0).
+__global__ void k_block_finalize(Mesh m, const double* __restrict__ diag, double* __restrict__ blocks) {
+    const double2* d2 = reinterpret_cast<const double2*>(diag);
+    double2* b2 = reinterpret_cast<double2*>(blocks);
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fix = m.node_fix[n];
+        const double2 dn = d2[n];
+        const double c = b2[2 * n + 1].y;
+        const bool fx = fix & 1, fy = fix & 2;
+        const double a00 = (fx ? 1.0 : dn.x) + 1e-12, a11 = (fy ? 1.0 : dn.y) + 1e-12;
+        const double a01 = (fx || fy) ? 0.0 : c;
+        const double det = a00 * a11 - a01 * a01;
+        b2[2 * n] = make_double2(a11 / det, -a01 / det);
+        b2[2 * n + 1] = make_double2(a00 / det, 0.0);
     }
 }
 
@@ -405,8 +434,27 @@ extern "C" int dfea_mesh_grad_to_f32(const dfea_mesh_view* mesh, float* grad32_o
     return launch_check("dfea_mesh_grad_to_f32");
 }
 
+static int qp_moduli_impl(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                          double lambda0, void* moduli, int32_t moduli_dtype, double* diag, double* blocks,
+                          void* stream);
+
 extern "C" int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                               double lambda0, void* moduli, int32_t moduli_dtype, double* diag, void* stream) {
+    return qp_moduli_impl(mesh, u, theta, mu0, lambda0, moduli, moduli_dtype, diag, nullptr, stream);
+}
+
+extern "C" int dfea_qp_moduli_block(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                                    double lambda0, void* moduli, int32_t moduli_dtype, double* diag, double* blocks,
+                                    void* stream) {
+    if (!diag || !blocks) return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli_block: diag and blocks are required");
+    if (reinterpret_cast<uintptr_t>(blocks) & 15u)
+        return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli_block: blocks must be 16-byte aligned");
+    return qp_moduli_impl(mesh, u, theta, mu0, lambda0, moduli, moduli_dtype, diag, blocks, stream);
+}
+
+static int qp_moduli_impl(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                          double lambda0, void* moduli, int32_t moduli_dtype, double* diag, double* blocks,
+                          void* stream) {
     int rc = validate_mesh(mesh, false);
     if (rc) return rc;
     if (!u || !theta || (!moduli && !diag)) return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: NULL pointer");
@@ -422,6 +470,10 @@ extern "C" int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const
         k_zero<<<grid_for(2 * mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(2 * mesh->n_nodes, diag);
         note_launches(1);
     }
+    if (blocks) {
+        k_zero<<<grid_for(4 * mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(4 * mesh->n_nodes, blocks);
+        note_launches(1);
+    }
     rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
         for (int c = 0; c < mesh->n_colours; ++c) {
@@ -430,18 +482,22 @@ extern "C" int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const
             const int grid = grid_for(e1 - e0, 128, 12);
             if (moduli_dtype == DFEA_F64)
                 k_moduli<NEN, NQ, double><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
-                                                                static_cast<double*>(moduli), diag);
+                                                                static_cast<double*>(moduli), diag, blocks);
             else if (moduli_dtype == DFEA_F32REF)
                 k_moduli<NEN, NQ, float, true><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
-                                                                     static_cast<float*>(moduli), diag);
+                                                                     static_cast<float*>(moduli), diag, blocks);
             else
                 k_moduli<NEN, NQ, float><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
-                                                               static_cast<float*>(moduli), diag);
+                                                               static_cast<float*>(moduli), diag, blocks);
             note_launches(1);
         }
         return DFEA_OK;
     });
     if (rc) return rc;
+    if (blocks) {  // from the raw diagonal, before the Jacobi clamp below
+        k_block_finalize<<<grid_for(mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(m, diag, blocks);
+        note_launches(1);
+    }
     if (diag) {
         k_diag_finalize<<<grid_for(mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(m, diag);
         note_launches(1);

@@ -63,6 +63,20 @@ struct PcgLayout {
     }
 };
 
+// The preconditioner z = M^-1 r at node n.  BJ = false: point Jacobi, d = diag (2N);  BJ = true: nodal
+// block-Jacobi, d = the inverse 2x2 blocks (Binv00, Binv01, Binv11, 0) per node (4N, double vectors only).
+template <bool BJ, typename T>
+__device__ __forceinline__ v2_t<T> precond(const T* __restrict__ d, int64_t n, v2_t<T> r) {
+    if constexpr (BJ) {
+        const double2* b2 = reinterpret_cast<const double2*>(d);
+        const double2 a = b2[2 * n], b = b2[2 * n + 1];
+        return make_v2<T>((T)(a.x * r.x + a.y * r.y), (T)(a.y * r.x + b.x * r.y));
+    } else {
+        const v2_t<T> dn = reinterpret_cast<const v2_t<T>*>(d)[n];
+        return make_v2<T>(r.x / dn.x, r.y / dn.y);
+    }
+}
+
 __global__ void k_pcg_reset(PcgState* st) {
     const int i = threadIdx.x;
     if (i < DFEA_MAX_COLOURS + 8) st->tickets[i] = 0u;
@@ -76,7 +90,7 @@ __global__ void k_pcg_reset(PcgState* st) {
 }
 
 // x = 0, r = b, z = b / d, p = z, Ap := (1 - m) p;  rz = r.z, |b|, pfix.
-template <typename T>
+template <typename T, bool BJ>
 __global__ void __launch_bounds__(kThreads)
 k_pcg_setup(Mesh m, const T* __restrict__ b, const T* __restrict__ d, T* __restrict__ x, T* __restrict__ r,
             T* __restrict__ p, T* __restrict__ y, PcgState* st, RedSite site, double rtol, int max_iter) {
@@ -85,8 +99,8 @@ k_pcg_setup(Mesh m, const T* __restrict__ b, const T* __restrict__ d, T* __restr
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
         const int fix = m.node_fix[n];
         const T2 bn = reinterpret_cast<const T2*>(b)[n];
-        const T2 dn = reinterpret_cast<const T2*>(d)[n];
-        const T zx = bn.x / dn.x, zy = bn.y / dn.y;
+        const T2 zn = precond<BJ, T>(d, n, bn);
+        const T zx = zn.x, zy = zn.y;
         reinterpret_cast<T2*>(x)[n] = make_v2<T>(T(0), T(0));
         reinterpret_cast<T2*>(r)[n] = bn;
         reinterpret_cast<T2*>(p)[n] = make_v2<T>(zx, zy);
@@ -113,7 +127,7 @@ k_pcg_setup(Mesh m, const T* __restrict__ b, const T* __restrict__ d, T* __restr
 
 // GATHER: Ap is not stored; each node sums its elements' results (fe, the element pass of the gather
 // form) in the incidence order, and takes p on its fixed DOFs (the identity rows).
-template <typename T, bool GATHER>
+template <typename T, bool GATHER, bool BJ>
 __global__ void __launch_bounds__(kThreads)
 k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restrict__ y, const T* __restrict__ d,
               T* __restrict__ x, T* __restrict__ r, PcgState* st, RedSite site, const int32_t* __restrict__ inc_ptr,
@@ -130,8 +144,7 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
         if (k == 0) {
             for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
                 const T2 rn = reinterpret_cast<const T2*>(r)[n];
-                const T2 dn = reinterpret_cast<const T2*>(d)[n];
-                reinterpret_cast<T2*>(x)[n] = make_v2<T>(rn.x / dn.x, rn.y / dn.y);
+                reinterpret_cast<T2*>(x)[n] = precond<BJ, T>(d, n, rn);
             }
         }
         const double vals[1] = {0.0};
@@ -156,7 +169,6 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
         } else {
             yn = reinterpret_cast<const T2*>(y)[n];
         }
-        const T2 dn = reinterpret_cast<const T2*>(d)[n];
         T2 xn = reinterpret_cast<const T2*>(x)[n];
         T2 rn = reinterpret_cast<const T2*>(r)[n];
         xn.x += a * pn.x;
@@ -166,7 +178,8 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
         reinterpret_cast<T2*>(x)[n] = xn;
         reinterpret_cast<T2*>(r)[n] = rn;
         rr += (double)rn.x * rn.x + (double)rn.y * rn.y;
-        rz += (double)rn.x * (rn.x / dn.x) + (double)rn.y * (rn.y / dn.y);
+        const T2 zn = precond<BJ, T>(d, n, rn);
+        rz += (double)rn.x * zn.x + (double)rn.y * zn.y;
     }
     const double vals[2] = {block_sum<kThreads>(rr), block_sum<kThreads>(rz)};
     double tot[2];
@@ -178,7 +191,7 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
 }
 
 // PIVOT: write Ap := (1 - m) p, the identity rows the colour passes then add to (the colour form).
-template <typename T, bool PIVOT>
+template <typename T, bool PIVOT, bool BJ>
 __global__ void __launch_bounds__(kThreads)
 k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __restrict__ p, T* __restrict__ y,
               PcgState* st, RedSite site) {
@@ -203,10 +216,10 @@ k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __res
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
         const int fix = m.node_fix[n];
         const T2 rn = reinterpret_cast<const T2*>(r)[n];
-        const T2 dn = reinterpret_cast<const T2*>(d)[n];
+        const T2 zn = precond<BJ, T>(d, n, rn);
         T2 pn = reinterpret_cast<const T2*>(p)[n];
-        pn.x = rn.x / dn.x + bt * pn.x;
-        pn.y = rn.y / dn.y + bt * pn.y;
+        pn.x = zn.x + bt * pn.x;
+        pn.y = zn.y + bt * pn.y;
         reinterpret_cast<T2*>(p)[n] = pn;
         if (PIVOT) reinterpret_cast<T2*>(y)[n] = make_v2<T>((fix & 1) ? pn.x : T(0), (fix & 2) ? pn.y : T(0));
         if (fix & 1) pf += (double)pn.x * pn.x;
@@ -251,6 +264,7 @@ struct dfea_pcg {
     int use_graph;
     bool gather = false;             // product in the gather form (element pass + node sums in update 1)
     int grid_cap = 0;                // most blocks per launch (0: as many as the GPU holds)
+    bool block = false;              // nodal block-Jacobi: diag holds the inverse 2x2 blocks (4N doubles)
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -281,7 +295,7 @@ int kernels_per_iteration(const dfea_pcg& h) {
 
 // S: storage type of moduli and gradients, T: Krylov vector type; REF: DFEA_F32REF moduli (S = float),
 // no gradients read.
-template <typename S, typename T, bool REF = false>
+template <typename S, typename T, bool REF = false, bool BJ = false>
 int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHandle cond, bool with_cond) {
     const dfea_mesh_view& mv = h.mesh;
     const Mesh m = kernel_mesh(mv);
@@ -309,10 +323,10 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
                 return launch_apply_elem<NEN, NQ, S, T, true>(mv, C, G, p, fe, h.site(0, 1), &st->done, s, h.grid_cap);
         });
         if (rc) return rc;
-        if ((rc = launch_kernel(k_pcg_update1<T, true>, dim3(gn), dim3(kThreads), 0, s, pdl, m, 1, p, (const T*)y, d, x,
+        if ((rc = launch_kernel(k_pcg_update1<T, true, BJ>, dim3(gn), dim3(kThreads), 0, s, pdl, m, 1, p, (const T*)y, d, x,
                                 r, st, h.site(mv.n_colours, 2), mv.node_elem_ptr, mv.node_elem, (const T*)fe)))
             return rc;
-        if ((rc = launch_kernel(k_pcg_update2<T, false>, dim3(gn), dim3(kThreads), 0, s, pdl, m, (const T*)r, d, p, y,
+        if ((rc = launch_kernel(k_pcg_update2<T, false, BJ>, dim3(gn), dim3(kThreads), 0, s, pdl, m, (const T*)r, d, p, y,
                                 st, h.site(mv.n_colours + 1, 1))))
             return rc;
     } else {
@@ -328,11 +342,11 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
                                                                  h.grid_cap);
         });
         if (rc) return rc;
-        if ((rc = launch_kernel(k_pcg_update1<T, false>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mv.n_colours, p,
+        if ((rc = launch_kernel(k_pcg_update1<T, false, BJ>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mv.n_colours, p,
                                 (const T*)y, d, x, r, st, h.site(mv.n_colours, 2), (const int32_t*)nullptr,
                                 (const int32_t*)nullptr, (const T*)nullptr)))
             return rc;
-        if ((rc = launch_kernel(k_pcg_update2<T, true>, dim3(gn), dim3(kThreads), 0, s, pdl, m, (const T*)r, d, p, y,
+        if ((rc = launch_kernel(k_pcg_update2<T, true, BJ>, dim3(gn), dim3(kThreads), 0, s, pdl, m, (const T*)r, d, p, y,
                                 st, h.site(mv.n_colours + 1, 1))))
             return rc;
     }
@@ -342,13 +356,18 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
 }
 
 int launch_iteration_any(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHandle cond, bool with_cond) {
+    if (h.block) {  // block-Jacobi: double vectors only (checked at create)
+        if (h.vec_dtype == DFEA_F64) return launch_iteration<double, double, false, true>(h, s, cond, with_cond);
+        if (h.vec_dtype == DFEA_MIXED) return launch_iteration<float, double, false, true>(h, s, cond, with_cond);
+        return launch_iteration<float, double, true, true>(h, s, cond, with_cond);
+    }
     if (h.vec_dtype == DFEA_F64) return launch_iteration<double, double>(h, s, cond, with_cond);
     if (h.vec_dtype == DFEA_MIXED) return launch_iteration<float, double>(h, s, cond, with_cond);
     if (h.vec_dtype == DFEA_F32REF) return launch_iteration<float, double, true>(h, s, cond, with_cond);
     return launch_iteration<float, float>(h, s, cond, with_cond);
 }
 
-template <typename T>
+template <typename T, bool BJ = false>
 int launch_setup(const dfea_pcg& h, cudaStream_t s, double rtol, int max_iter) {
     const dfea_mesh_view& mv = h.mesh;
     const Mesh m = kernel_mesh(mv);
@@ -357,7 +376,7 @@ int launch_setup(const dfea_pcg& h, cudaStream_t s, double rtol, int max_iter) {
     T* y = reinterpret_cast<T*>(h.work + h.layout.off_y);
     PcgState* st = h.state();
     k_pcg_reset<<<1, 128, 0, s>>>(st);
-    k_pcg_setup<T><<<grid_for(mv.n_nodes, kThreads, 4), kThreads, 0, s>>>(
+    k_pcg_setup<T, BJ><<<grid_for(mv.n_nodes, kThreads, 4), kThreads, 0, s>>>(
         m, static_cast<const T*>(h.b), static_cast<const T*>(h.diag), static_cast<T*>(h.x), r, p, y, st,
         h.site(mv.n_colours + 2, 3), rtol, max_iter);
     note_launches(2);
@@ -460,8 +479,13 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
     h->work = static_cast<char*>(work);
     h->layout = layout_for(*mesh, vec_dtype);
     h->gather = (use_graph & DFEA_PCG_GATHER) != 0;
+    h->block = (use_graph & DFEA_PCG_BLOCK_JACOBI) != 0;
     h->grid_cap = (int)((uint32_t)use_graph >> 8);
-    use_graph &= 0xff & ~DFEA_PCG_GATHER;
+    use_graph &= 0xff & ~(DFEA_PCG_GATHER | DFEA_PCG_BLOCK_JACOBI);
+    if (h->block && vec_dtype == DFEA_F32) {
+        delete h;
+        return set_error(DFEA_ERR_UNSUPPORTED, "dfea_pcg_create: block-Jacobi needs f64 Krylov vectors");
+    }
     h->use_graph = (use_graph == 2) ? 2 : (use_graph ? 1 : 0);
     if (h->gather && h->layout.off_fe == h->layout.total) {
         delete h;
@@ -509,6 +533,7 @@ extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_
     if (!(rtol >= 0.0)) return set_error(DFEA_ERR_INVALID, "rtol must be >= 0");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int rc = (h->vec_dtype == DFEA_F32) ? launch_setup<float>(*h, s, rtol, max_iter)
+             : h->block                 ? launch_setup<double, true>(*h, s, rtol, max_iter)
                                         : launch_setup<double>(*h, s, rtol, max_iter);
     if (rc) return rc;
     PcgState* st = h->state();

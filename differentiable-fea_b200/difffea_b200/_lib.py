@@ -20,6 +20,7 @@ MAX_COLOURS = 64
 
 PCG_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "negative_curvature", 4: "zero_rhs"}
 DFEA_PCG_GATHER = 16  # dfea_pcg_create flag: gather form of the product
+DFEA_PCG_BLOCK_JACOBI = 32  # dfea_pcg_create flag: nodal block-Jacobi (diag = inverse 2x2 blocks, 4N)
 
 
 def pcg_max_blocks(n):
@@ -53,6 +54,8 @@ _PROTOS = {
                                       c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "dfea_mesh_grad_to_f32": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp]),
     "dfea_qp_moduli": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp, c_vp]),
+    "dfea_qp_moduli_block": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp,
+                                            c_vp, c_vp]),
     "dfea_tangent_apply": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_i32, c_vp, c_vp, c_i32, c_vp]),
     "dfea_gather_work_bytes": (c_i64, [ctypes.POINTER(MeshView), c_i32]),
     "dfea_tangent_apply_gather": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_i32, c_vp, c_vp, c_i32, c_vp,

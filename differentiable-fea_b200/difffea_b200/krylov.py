@@ -31,9 +31,12 @@ class DevicePCG:
     moduli pulled back to the element reference frame, 10 per Gauss point, FP64 vectors; the product
     reads no gradients).  max_blocks: at most this many blocks per launch (0: the whole GPU), for solves
     that share the GPU with others; results agree with the unlimited form's to rounding.
+    preconditioner: "jacobi" (diag = the (2N,) diagonal) or "block_jacobi" (diag = the (4N,) inverse 2x2
+    node blocks of dfea_qp_moduli_block; FP64 vectors).
     """
 
-    def __init__(self, mesh, C, diag, b, x, use_graph=True, form="colour", moduli="physical", max_blocks=0):
+    def __init__(self, mesh, C, diag, b, x, use_graph=True, form="colour", moduli="physical", max_blocks=0,
+                 preconditioner="jacobi"):
         use_graph = int(use_graph) if os.environ.get("DFEA_PCG_GRAPH", "1") != "0" else 0
         if form not in ("colour", "gather"):
             raise ValueError("form must be 'colour' or 'gather'")
@@ -42,6 +45,14 @@ class DevicePCG:
             mesh.ensure_node_incidence()
             flags = _lib.DFEA_PCG_GATHER
         flags |= _lib.pcg_max_blocks(max_blocks)
+        if preconditioner == "block_jacobi":
+            # diag holds the inverse 2x2 node blocks (4N doubles) of dfea_qp_moduli_block
+            if diag.dtype != torch.float64 or diag.numel() != 2 * mesh.n_dof or b.dtype != torch.float64:
+                raise ValueError("block-Jacobi: diag must be the (4N,) f64 inverse blocks, vectors f64")
+            flags |= _lib.DFEA_PCG_BLOCK_JACOBI
+        elif preconditioner != "jacobi":
+            raise ValueError("preconditioner must be 'jacobi' or 'block_jacobi'")
+        self.preconditioner = preconditioner
         vt = b.dtype
         if moduli == "ref":
             # FP32 moduli in the element reference frame (10 per Gauss point): no gradients read
@@ -56,9 +67,10 @@ class DevicePCG:
                 raise ValueError("FP64 moduli need FP64 vectors")
         else:
             dt = _lib.DFEA_MIXED if vt == torch.float64 else _lib.DFEA_F32
-        for name, t in (("diag", diag), ("b", b), ("x", x)):
-            if t.dtype != vt or t.numel() != mesh.n_dof or not t.is_contiguous() or t.device != mesh.device:
-                raise ValueError(f"{name} must be a contiguous ({mesh.n_dof},) {vt} tensor on {mesh.device}")
+        n_diag = 2 * mesh.n_dof if preconditioner == "block_jacobi" else mesh.n_dof
+        for name, t, n_t in (("diag", diag, n_diag), ("b", b, mesh.n_dof), ("x", x, mesh.n_dof)):
+            if t.dtype != vt or t.numel() != n_t or not t.is_contiguous() or t.device != mesh.device:
+                raise ValueError(f"{name} must be a contiguous ({n_t},) {vt} tensor on {mesh.device}")
         if dt in (_lib.DFEA_MIXED, _lib.DFEA_F32):
             mesh.ensure_grad32()
         self.mesh, self.C, self.diag, self.b, self.x = mesh, C, diag, b, x

@@ -15,6 +15,9 @@ What changes is where it runs: the residual (with its norm), the moduli and diag
 are device kernels on buffers held by a ``NewtonWorkspace``; the host reads back one scalar per residual
 and (status, iterations) per linear solve.
 
+``preconditioner`` is "jacobi" (the reference's default) or "block_jacobi" (nodal 2x2 blocks,
+operators.py:586-625), both applied inside the device PCG.
+
 Extra keyword arguments (not in the reference): ``pcg_max_iter``; ``precision`` = "fp64" (default) or
 "fp32" (the PCG applies FP32 moduli and gradients -- the bytes that dominate the operator -- to FP64
 Krylov vectors; the residual, line search, convergence test and state update stay FP64, so each Newton
@@ -23,8 +26,8 @@ step is an iterative-refinement correction of the FP64 state computed with an FP
 """
 import torch
 
-from difffea_b200.operators import (CudaJacobiPreconditioner, CudaTangentOperator, PRECONDITIONERS,
-                                    TANGENT_OPERATORS, REFERENCE_TANGENT_VARIANTS)
+from difffea_b200.operators import (CudaBlockJacobiPreconditioner, CudaJacobiPreconditioner, CudaTangentOperator,
+                                    PRECONDITIONERS, REFERENCE_TANGENT_VARIANTS, TANGENT_OPERATORS)
 from difffea_b200.workspace import NewtonWorkspace
 
 # inner-solve floor with the FP32 operator: the solve is of the operator rounded to FP32, so asking it
@@ -47,6 +50,9 @@ def pcg(A_fn, b, Minv_fn, rtol=1e-5, max_iter=500):
     if (isinstance(A_fn, CudaTangentOperator) and isinstance(Minv_fn, CudaJacobiPreconditioner)
             and Minv_fn.mesh is A_fn.mesh and b.is_cuda):
         return A_fn.pcg_solve(b, Minv_fn.diag, rtol, max_iter)
+    if (isinstance(A_fn, CudaTangentOperator) and isinstance(Minv_fn, CudaBlockJacobiPreconditioner)
+            and Minv_fn.mesh is A_fn.mesh and b.is_cuda):
+        return A_fn.pcg_solve(b, Minv_fn.blocks, rtol, max_iter, preconditioner="block_jacobi")
     return _pcg_steps(A_fn, b, Minv_fn, rtol, max_iter)
 
 
@@ -90,21 +96,23 @@ def _check_kinds(tangent, preconditioner):
         raise ValueError(f"Unknown preconditioner '{preconditioner}'. Choose one of {PRECONDITIONERS}.")
 
 
-def _workspace(params, theta, precision, workspace):
-    ws = workspace if workspace is not None else NewtonWorkspace(params, precision)
+def _workspace(params, theta, precision, workspace, preconditioner="jacobi"):
+    ws = workspace if workspace is not None else NewtonWorkspace(params, precision, preconditioner=preconditioner)
     if ws.precision != precision:
         raise ValueError("workspace precision does not match")
+    if ws.preconditioner != preconditioner:
+        raise ValueError(f"workspace preconditioner '{ws.preconditioner}' does not match '{preconditioner}'")
     ws.set_theta(theta)
     return ws
 
 
 def armijo_line_search(u, du, rn, theta, params, load_factor, c1=1e-4, min_alpha=2.0 ** -5, *, workspace=None,
-                       precision="fp64"):
+                       precision="fp64", preconditioner="jacobi"):
     """
     Backtrack alpha = 1, 1/2, ... >= min_alpha until ||R(u + alpha du)|| < (1 - c1 alpha) ||R(u)||.
     Returns (u_new, R_new, ||R_new||, alpha, accepted); (u, None, rn, alpha, False) if no step passes.
     """
-    ws = _workspace(params, theta, precision, workspace)
+    ws = _workspace(params, theta, precision, workspace, preconditioner)
     rn = float(rn)
     alpha = 1.0
     while alpha >= min_alpha:
@@ -121,7 +129,7 @@ def newton_at_load(u0, theta, params, load_factor, tol, max_newton, verbose, cal
                    preconditioner="jacobi", tangent="auto", *, pcg_max_iter=500, precision="fp64", workspace=None):
     """Inexact Newton-Krylov at one load factor; returns (u, converged, records)."""
     _check_kinds(tangent, preconditioner)
-    ws = _workspace(params, theta, precision, workspace)
+    ws = _workspace(params, theta, precision, workspace, preconditioner)
     u = torch.where(params["fixed"], load_factor * params["u_D"], u0).to(torch.float64).contiguous()
     rn = ws.residual(u, load_factor, ws.R)
     r0 = rn
@@ -138,7 +146,7 @@ def newton_at_load(u0, theta, params, load_factor, tol, max_newton, verbose, cal
         ws.linearize(u)
         du, cg_iters, _ = ws.solve(ws.R, rtol, pcg_max_iter)
         u, R_new, rn, alpha, accepted = armijo_line_search(u, du, rn, theta, params, load_factor, workspace=ws,
-                                                           precision=precision)
+                                                           precision=precision, preconditioner=preconditioner)
         record = dict(step=step_id, load_factor=load_factor, iteration=it, residual=float(rn),
                       cg_iters=int(cg_iters), alpha=alpha)
         records.append(record)
@@ -164,7 +172,7 @@ def newton_krylov_solve(params, theta, n_load_steps=5, tol=1e-8, max_newton=25, 
     if not nodes.is_cuda:
         raise RuntimeError("difffea_b200 solves on CUDA devices only: move the problem with "
                            "problem.to_device(params, 'cuda')")
-    ws = _workspace(params, theta, precision, workspace)
+    ws = _workspace(params, theta, precision, workspace, preconditioner)
     u = torch.zeros(2 * nodes.shape[0], dtype=torch.float64, device=nodes.device)
     info = {"converged": False, "load_factor": 0.0, "history": [], "total_newton": 0, "total_cg": 0,
             "n_cutbacks": 0, "snapshots": [(0.0, u.clone())]}

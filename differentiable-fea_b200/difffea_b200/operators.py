@@ -5,7 +5,8 @@ Residual, tangent-operator and preconditioner closures on the GPU (the reference
     make_tangent_operator(kind, u, theta, params)               operators.py:415-435, kind "cuda" / "auto"
     make_AT_operator(u, theta, params)                          operators.py:441-471
     compute_jacobi_diagonal / make_jacobi_preconditioner        operators.py:477-570
-    make_preconditioner(kind, u, theta, params)                 operators.py:702-710, kind "jacobi"
+    make_preconditioner(kind, u, theta, params)                 operators.py:702-710, "jacobi" / "block_jacobi"
+    make_block_jacobi_preconditioner(u, theta, params)          operators.py:586-625
     precompute_geometry(params)                                 operators.py:85-120
 
 Every closure has the reference's semantics -- A(v) = m * J(u)(m * v) + (1 - m) * v, symmetric, the
@@ -25,7 +26,7 @@ from difffea_b200.problem import precompute_geometry  # noqa: F401  (re-exported
 
 TANGENT_OPERATORS = ("auto", "cuda")
 REFERENCE_TANGENT_VARIANTS = ("jvp", "linearize", "qp", "qp_ew")
-PRECONDITIONERS = ("jacobi",)
+PRECONDITIONERS = ("jacobi", "block_jacobi")
 
 
 def _prepare(u, theta, params):
@@ -90,18 +91,24 @@ class CudaTangentOperator:
     def dtype(self):
         return self.C.dtype
 
-    def pcg_solve(self, b, diag, rtol, max_iter):
-        """Jacobi-PCG on the device (kernel (c)) with this operator; returns (x in b's dtype, iterations)."""
+    def pcg_solve(self, b, diag, rtol, max_iter, preconditioner="jacobi"):
+        """
+        PCG on the device (kernel (c)) with this operator; returns (x in b's dtype, iterations).  ``diag`` is
+        the Jacobi diagonal, or with preconditioner="block_jacobi" the (4N,) inverse node blocks.
+        """
         from difffea_b200.krylov import DevicePCG
         vt = b.dtype if self.C.dtype == torch.float32 else torch.float64   # FP32 moduli: FP64 or FP32 vectors
-        if self._pcg is None or self._pcg_diag_src is not diag or self._pcg.vec_dtype != vt:
+        if preconditioner == "block_jacobi":
+            vt = torch.float64
+        if (self._pcg is None or self._pcg_diag_src is not diag or self._pcg.vec_dtype != vt
+                or self._pcg.preconditioner != preconditioner):
             d = diag.detach().to(vt).contiguous()
             n = self.mesh.n_dof
             bb = torch.empty(n, dtype=vt, device=self.mesh.device)
             xx = torch.empty(n, dtype=vt, device=self.mesh.device)
             if self._pcg is not None:
                 self._pcg.close()
-            self._pcg = DevicePCG(self.mesh, self.C, d, bb, xx)
+            self._pcg = DevicePCG(self.mesh, self.C, d, bb, xx, preconditioner=preconditioner)
             self._pcg_diag_src = diag
         self._pcg.b.copy_(b)
         iters, status = self._pcg.solve(rtol, max_iter)
@@ -192,10 +199,47 @@ def make_jacobi_preconditioner(u, theta, params):
     return CudaJacobiPreconditioner(mesh, compute_jacobi_diagonal(u, theta, params))
 
 
+class CudaBlockJacobiPreconditioner:
+    """
+    r -> Binv r per node, Binv the inverse of the node's 2x2 tangent block with identity rows/columns on
+    fixed DOFs and + 1e-12 I (operators.py:598-625); ``blocks`` = (Binv00, Binv01, Binv11, 0) per node.
+    """
+
+    def __init__(self, mesh, blocks):
+        self.mesh, self.blocks = mesh, blocks
+
+    def __call__(self, r):
+        B = self.blocks.view(-1, 4).to(r.dtype)
+        rn = r.view(-1, 2)
+        return torch.stack([B[:, 0] * rn[:, 0] + B[:, 1] * rn[:, 1], B[:, 1] * rn[:, 0] + B[:, 2] * rn[:, 1]],
+                           dim=1).reshape(-1)
+
+
+def compute_block_jacobi(u, theta, params):
+    """The (4N,) inverse 2x2 node blocks of the tangent at (u, theta) (kernel (a) with the coupling term)."""
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr, stream_handle
+    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    u64, th64 = _f64c(u), _f64c(theta)
+    diag = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
+    blocks = torch.empty(2 * mesh.n_dof, dtype=torch.float64, device=mesh.device)
+    _lib.call("dfea_qp_moduli_block", mesh.view_ref, ptr(u64), ptr(th64), mu0, lam0, ptr(None), _lib.DFEA_F64,
+              ptr(diag), ptr(blocks), stream_handle())
+    return blocks
+
+
+def make_block_jacobi_preconditioner(u, theta, params):
+    mesh = cuda_mesh(params)
+    return CudaBlockJacobiPreconditioner(mesh, compute_block_jacobi(u, theta, params))
+
+
 def make_preconditioner(kind, u, theta, params):
     """Build a preconditioner by name: one of ``PRECONDITIONERS``."""
     if kind == "jacobi":
         return make_jacobi_preconditioner(u, theta, params)
-    if kind in ("block_jacobi", "ilu"):
-        raise ValueError(f"preconditioner '{kind}' is not built on the device; use 'jacobi'")
+    if kind == "block_jacobi":
+        return make_block_jacobi_preconditioner(u, theta, params)
+    if kind == "ilu":
+        raise ValueError("preconditioner 'ilu' factorises the assembled matrix on the CPU (SciPy); it is not "
+                         "built on the device: use 'jacobi' or 'block_jacobi'")
     raise ValueError(f"Unknown preconditioner '{kind}'. Choose one of {PRECONDITIONERS}.")

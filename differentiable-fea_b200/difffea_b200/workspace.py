@@ -35,9 +35,13 @@ def pcg_form_for(mesh, pcg_form="auto"):
 
 
 class NewtonWorkspace:
-    def __init__(self, params, precision="fp64", use_graph=True, pcg_form="auto", fp32_moduli="ref", max_blocks=0):
+    def __init__(self, params, precision="fp64", use_graph=True, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
+                 preconditioner="jacobi"):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")
+        if preconditioner not in ("jacobi", "block_jacobi"):
+            raise ValueError("preconditioner must be 'jacobi' or 'block_jacobi'")
+        self.preconditioner = preconditioner
         self.params = params
         self.mesh = mesh = cuda_mesh(params)
         self.mu0, self.lam0 = neo_hookean_parameters(params)
@@ -50,6 +54,8 @@ class NewtonWorkspace:
         self.uc = torch.empty(n, **f64)
         self.du = torch.empty(n, **f64)
         self.diag = torch.empty(n, **f64)
+        # block-Jacobi: the inverse 2x2 node blocks (Binv00, Binv01, Binv11, 0) per node
+        self.blocks = torch.empty(2 * n, **f64) if preconditioner == "block_jacobi" else None
         self.scal = torch.zeros(4, **f64)
         self.scal_host = torch.zeros(4, dtype=torch.float64).pin_memory()
         # "fp32": the operator's bytes in FP32, Krylov vectors and scalars in FP64.  fp32_moduli "ref":
@@ -70,8 +76,9 @@ class NewtonWorkspace:
                 mesh.ensure_grad32()
         # the PCG reads -R from b and writes its solution straight into du
         self.b = torch.empty(n, **f64)
-        self.pcg = DevicePCG(mesh, self.C, self.diag, self.b, self.du, use_graph=use_graph,
-                             form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind, max_blocks=max_blocks)
+        self.pcg = DevicePCG(mesh, self.C, self.diag if self.blocks is None else self.blocks, self.b, self.du,
+                             use_graph=use_graph, form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind,
+                             max_blocks=max_blocks, preconditioner=preconditioner)
         self.work = mesh.reduce_work()
         self.theta = None
         self.n_launch_groups = 0
@@ -94,9 +101,13 @@ class NewtonWorkspace:
         return (rn, float(self.scal_host[1])) if energy else rn
 
     def linearize(self, u):
-        """Kernel (a): moduli C and Jacobi diagonal at u (into the buffers the PCG graph is bound to)."""
-        _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0, ptr(self.C),
-                  self.moduli_code, ptr(self.diag), stream_handle())
+        """Kernel (a): moduli C and the preconditioner at u (into the buffers the PCG graph is bound to)."""
+        if self.blocks is not None:
+            _lib.call("dfea_qp_moduli_block", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0,
+                      ptr(self.C), self.moduli_code, ptr(self.diag), ptr(self.blocks), stream_handle())
+        else:
+            _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0,
+                      ptr(self.C), self.moduli_code, ptr(self.diag), stream_handle())
 
     def solve(self, R, rtol, max_iter):
         """du = PCG(A, -R) to relative tolerance rtol; returns (du (FP64 buffer), iterations, status)."""

@@ -61,6 +61,8 @@ extern "C" {
 #define DFEA_PCG_ZERO_RHS 4    /* ||b|| == 0: x = 0 after zero iterations              */
 
 #define DFEA_PCG_GATHER 16     /* dfea_pcg_create flag: gather form of the product     */
+#define DFEA_PCG_BLOCK_JACOBI 32 /* dfea_pcg_create flag: nodal block-Jacobi; diag = the
+                                  * inverse 2x2 blocks of dfea_qp_moduli_block (4N f64) */
 /* dfea_pcg_create option: at most n blocks per launch (n < 2^23; 0 = as many as the GPU holds at
  * once).  For solves that share the GPU with solves on other streams. */
 #define DFEA_PCG_MAX_BLOCKS(n) ((int32_t)(n) << 8)
@@ -163,6 +165,16 @@ int dfea_tangent_apply(const dfea_mesh_view* mesh, const void* moduli, int32_t m
 
 /* Bytes of the element-result buffer of the gather form: nen * stride pairs of vec_dtype. */
 int64_t dfea_gather_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
+
+/*
+ * dfea_qp_moduli plus the nodal block-Jacobi preconditioner (operators.py:586-625,
+ * make_block_jacobi_preconditioner): blocks (4N f64, 16-byte aligned) receives per node the inverse of
+ * B = M B_K M + (I - M) + 1e-12 I, B_K the 2x2 diagonal block of the tangent, as (Binv00, Binv01, Binv11,
+ * 0); diag (2N) receives the Jacobi diagonal as in dfea_qp_moduli.  Both are required.
+ */
+int dfea_qp_moduli_block(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                         double lambda0, void* moduli, int32_t moduli_dtype, double* diag, double* blocks,
+                         void* stream);
 
 /*
  * The same product as dfea_tangent_apply in two passes instead of one pass per colour: every element

@@ -170,6 +170,49 @@ def jacobi_diagonal(u, theta, P):
     return torch.where(P["m"] > 0.0, torch.clamp(diag, min=1e-6), torch.ones_like(diag))
 
 
+def block_jacobi(u, theta, P):
+    """
+    Nodal block-Jacobi M^-1 (operators.py:586-625): the 2x2 diagonal block of every element tangent from
+    one jvp of the element force per local unit vector (its node's rows), scattered to the nodes, identity
+    rows/columns on fixed DOFs, + 1e-12 I, inverted.  Returns the closure r -> Binv r.
+    """
+    conn, dN, wd = P["conn"], P["dN_dX"], P["w_detJ"]
+    n_el, nen = conn.shape
+    N = P["nodes"].shape[0]
+    ue = gather_nodes(u, conn)
+    pe = element_parameters(theta, P)
+    basis = torch.eye(2 * nen, dtype=F64).reshape(2 * nen, nen, 2)
+    node_of = torch.arange(2 * nen) // 2
+
+    def force(w, dN_e, wd_e, p_e):
+        F = torch.eye(2, dtype=F64) + torch.einsum("ai,qaj->qij", w, dN_e)
+        st = vmap(grad(psi), in_dims=(0, None))(F, p_e)
+        return torch.einsum("q,qij,qaj->ai", wd_e, st, dN_e)
+
+    def column(u_e, dN_e, wd_e, p_e, e_vec, a):
+        _, t = jvp(lambda w: force(w, dN_e, wd_e, p_e), (u_e,), (e_vec,))
+        return t[a]                                             # rows of node a: column j of its block
+
+    cols = vmap(lambda a, b, c, d: vmap(column, in_dims=(None, None, None, None, 0, 0))(a, b, c, d, basis, node_of))(
+        ue, dN, wd, pe)                                         # (n_el, 2 nen, 2): [e, (a, j), i]
+    blocks = cols.reshape(n_el, nen, 2, 2).transpose(2, 3)      # [e, a, i, j]
+    B = torch.zeros(N, 2, 2, dtype=F64).index_add_(0, conn.reshape(-1), blocks.reshape(-1, 2, 2))
+    mn = P["m"].reshape(N, 2)
+    B = B * (mn[:, :, None] * mn[:, None, :]) + torch.diag_embed(1.0 - mn) + 1e-12 * torch.eye(2, dtype=F64)
+    Binv = torch.linalg.inv(B)
+    return lambda r: torch.einsum("nij,nj->ni", Binv, r.reshape(N, 2)).reshape(-1)
+
+
+def preconditioner(kind, u, theta, P):
+    """M^-1 as a closure: "jacobi" (r / diag) or "block_jacobi"."""
+    if kind == "jacobi":
+        d = jacobi_diagonal(u, theta, P)
+        return lambda r: r / d
+    if kind == "block_jacobi":
+        return block_jacobi(u, theta, P)
+    raise ValueError(kind)
+
+
 # ---------------------------------------------------------------------------------------------
 # PCG, line search, Newton, continuation (newton_krylov.py:28-274)
 # ---------------------------------------------------------------------------------------------
@@ -213,7 +256,7 @@ def line_search(u, du, rn, theta, P, lf, c1=1e-4, min_alpha=2.0 ** -5):
     return u, None, rn, alpha, False
 
 
-def newton_at_load(u0, theta, P, lf, tol, max_newton, tangent="qp", pcg_max_iter=500):
+def newton_at_load(u0, theta, P, lf, tol, max_newton, tangent="qp", pcg_max_iter=500, precond="jacobi"):
     """Inexact Newton with the Eisenstat-Walker forcing term (newton_krylov.py:126-179)."""
     u = torch.where(P["fixed"], lf * P["u_D"], u0)
     R = residual(u, theta, P, lf)
@@ -226,8 +269,7 @@ def newton_at_load(u0, theta, P, lf, tol, max_newton, tangent="qp", pcg_max_iter
             break
         eta = min(0.5, float((rn / (r0 + 1e-14)) ** 0.5))
         A = make_operator(tangent, u, theta, P)
-        d = jacobi_diagonal(u, theta, P)
-        du, iters = pcg(A, -R, lambda r: r / d, rtol=eta, max_iter=pcg_max_iter)
+        du, iters = pcg(A, -R, preconditioner(precond, u, theta, P), rtol=eta, max_iter=pcg_max_iter)
         u, R_new, rn, alpha, ok = line_search(u, du, rn, theta, P, lf)
         records.append(dict(iteration=it, residual=float(rn), cg_iters=int(iters), alpha=alpha, load_factor=lf))
         if not ok:
@@ -238,7 +280,7 @@ def newton_at_load(u0, theta, P, lf, tol, max_newton, tangent="qp", pcg_max_iter
 
 @torch.no_grad()
 def newton_krylov_solve(P, theta, n_load_steps=5, tol=1e-8, max_newton=25, max_cutbacks=8, tangent="qp",
-                        pcg_max_iter=500):
+                        pcg_max_iter=500, precond="jacobi"):
     """Load continuation with cut-backs (newton_krylov.py:185-264); returns (u, info)."""
     u = torch.zeros(2 * P["nodes"].shape[0], dtype=F64)
     info = dict(converged=False, load_factor=0.0, history=[], total_newton=0, total_cg=0, n_cutbacks=0)
@@ -246,7 +288,7 @@ def newton_krylov_solve(P, theta, n_load_steps=5, tol=1e-8, max_newton=25, max_c
     d_lf, lf, streak = d_nom, 0.0, 0
     while lf < 1.0 - 1e-12:
         lf_try = min(1.0, lf + d_lf)
-        u_try, ok, rec = newton_at_load(u, theta, P, lf_try, tol, max_newton, tangent, pcg_max_iter)
+        u_try, ok, rec = newton_at_load(u, theta, P, lf_try, tol, max_newton, tangent, pcg_max_iter, precond)
         info["history"] += rec
         info["total_newton"] += len(rec)
         info["total_cg"] += sum(r["cg_iters"] for r in rec)

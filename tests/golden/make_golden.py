@@ -28,7 +28,7 @@ sys.path.insert(0, REF_SRC)
 
 from difffea.newton_krylov import newton_krylov_solve  # noqa: E402
 from difffea.operators import (_qp_setup, compute_jacobi_diagonal, global_residual,  # noqa: E402
-                               make_tangent_operator)
+                               make_block_jacobi_preconditioner, make_tangent_operator)
 from difffea.postprocess import compute_fields  # noqa: E402
 from difffea.problem import build_problem, default_spec  # noqa: E402
 from difffea.sensitivity import compute_sensitivity  # noqa: E402
@@ -83,22 +83,24 @@ def operator_case(element_type, h, seed, nonuniform_theta):
                R=global_residual(u, theta, p).numpy(),
                R_half=global_residual(u, theta, p, load_factor=0.5).numpy(),
                diag=compute_jacobi_diagonal(u, theta, p).numpy(),
+               Minv_block_v=make_block_jacobi_preconditioner(u, theta, p)(v).numpy(),
                energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])))
     tag = "theta" if nonuniform_theta else "unit"
     save(f"operator_{element_type}_h{h}_{tag}", **out)
 
 
-def solve_case(element_type, h, load, n_steps, tol_rel, name):
+def solve_case(element_type, h, load, n_steps, tol_rel, name, preconditioner="jacobi"):
     p = problem(element_type, h, load=load)
     theta = torch.ones(p["conn"].shape[0], dtype=DT)
     tol = tol_rel * float(torch.norm(p["f"]))
-    u, info = newton_krylov_solve(p, theta, n_steps, tol, verbose=False, preconditioner="jacobi", tangent="qp")
+    u, info = newton_krylov_solve(p, theta, n_steps, tol, verbose=False, preconditioner=preconditioner, tangent="qp")
     assert info["converged"]
     hist = info["history"]
     save(name, **arrays(p), theta=theta.numpy(), u_star=u.numpy(), tol=np.array(tol),
          n_load_steps=np.array(n_steps), total_newton=np.array(info["total_newton"]),
          total_cg=np.array(info["total_cg"]), residuals=np.array([r["residual"] for r in hist]),
          cg_iters=np.array([r["cg_iters"] for r in hist]), alphas=np.array([r["alpha"] for r in hist]),
+         preconditioner=np.array(preconditioner),
          energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])))
 
 
@@ -191,6 +193,11 @@ EXTRA = {
     "plate": lambda: plate_case(24, 5, 1e-11, "plate_quad9_24x24"),
     # the differentiation study's torch.func parity case (128 x 128 cells)
     "gradient": lambda: gradient_case(128, 0.0072, "gradient_quad4_128x128"),
+    # nodal block-Jacobi (operators.py:586-625) inside the reference's own Newton-Krylov solve
+    "block_jacobi": lambda: (solve_case("quad4", 0.2, (60.0, 0.0), 2, 1e-10, "solve_quad4_h0.2_tension_bj",
+                                        preconditioner="block_jacobi"),
+                             solve_case("quad9", 0.5, (0.0, -40.0), 3, 1e-9, "solve_quad9_h0.5_cantilever_bj",
+                                        preconditioner="block_jacobi")),
 }
 
 

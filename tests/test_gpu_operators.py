@@ -251,3 +251,11 @@ def test_reference_frame_rejects_inconsistent_geometry():
     q["dN_dX"] = p["dN_dX"].flip(1).contiguous()                        # Gauss points in another order
     with pytest.raises(ValueError):
         cuda_mesh(q).ensure_ref_frame()
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES)
+def test_block_jacobi_matches_reference(name):
+    from difffea_b200.operators import make_preconditioner
+    d, p, u, v, th = golden_case(name)
+    M = make_preconditioner("block_jacobi", u, th, p)
+    assert rel(M(v), d["Minv_block_v"]) < 1e-12

@@ -27,7 +27,9 @@ def _t(d, k):
 def test_complete_solve_matches_reference(name):
     d = load(name)
     p = params_from(d, DEV)
-    u, info = newton_krylov_solve(p, _t(d, "theta"), int(d["n_load_steps"]), float(d["tol"]), verbose=False)
+    pre = str(d["preconditioner"]) if "preconditioner" in d else "jacobi"
+    u, info = newton_krylov_solve(p, _t(d, "theta"), int(d["n_load_steps"]), float(d["tol"]), verbose=False,
+                                  preconditioner=pre)
     assert info["converged"] and info["load_factor"] == 1.0
     assert rel(u, d["u_star"]) < 1e-9                      # complete solutions: the north star's bar
     assert info["total_newton"] == int(d["total_newton"])
@@ -186,8 +188,10 @@ def test_newton_solve_with_the_gather_form(name):
     d = load(name)
     p = params_from(d, DEV)
     th = _t(d, "theta")
-    ws = NewtonWorkspace(p, pcg_form="gather")
-    u, info = newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False, workspace=ws)
+    pre = str(d["preconditioner"]) if "preconditioner" in d else "jacobi"
+    ws = NewtonWorkspace(p, pcg_form="gather", preconditioner=pre)
+    u, info = newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False, workspace=ws,
+                                  preconditioner=pre)
     assert info["converged"] and rel(u, d["u_star"]) < 1e-9
     assert info["total_newton"] == int(d["total_newton"])
 
@@ -209,3 +213,35 @@ def test_reference_frame_pcg_matches_the_fp64_solution():
         xs[ws.precision] = ws.du.clone()
     assert rel(xs["fp32"], xs["fp64"]) < 1e-4                            # FP32 operator, FP64 recurrences
     assert torch.equal(ws32.diag, ws64.diag)                            # the diagonal is FP64 in both
+
+
+# ------------------------------------------------------------------------------------------------
+# nodal block-Jacobi (operators.py:586-625) inside the device PCG
+# ------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("form", ["colour", "gather"])
+def test_block_jacobi_pcg_follows_the_reference_recurrences(form):
+    from difffea_b200.operators import compute_block_jacobi
+    d = load("operator_quad4_h0.1_theta")
+    p = params_from(d, DEV)
+    u, th = _t(d, "u"), _t(d, "theta")
+    A = make_tangent_operator("cuda", u, th, p)
+    blocks = compute_block_jacobi(u, th, p)
+    b = p["m"] * _t(d, "v")
+    bb, xx = b.clone(), torch.empty_like(b)
+    solver = DevicePCG(A.mesh, A.C, blocks, bb, xx, form=form, preconditioner="block_jacobi")
+    k, status = solver.solve(1e-10, 2000)
+    solver.close()
+    P = oracle.as_problem(p)
+    x_ref, k_ref = oracle.pcg(oracle.make_operator("qp_ew", u.cpu(), th.cpu(), P), b.cpu(),
+                              oracle.block_jacobi(u.cpu(), th.cpu(), P), rtol=1e-10, max_iter=2000)
+    assert status == "converged" and abs(k - k_ref) <= 1 and rel(xx, x_ref) < 1e-9
+
+
+def test_block_jacobi_mixed_precision_solve():
+    p = build_rectangle_problem("quad9", 24, 12, 2.0, 1.0, E=1.0, nu=0.44, load=(0.0, -2e-3), device=DEV)
+    th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV)
+    tol = 1e-11 * float(torch.norm(p["f"]))
+    u_j, i_j = newton_krylov_solve(p, th, 2, tol, verbose=False, pcg_max_iter=5000)
+    u_b, i_b = newton_krylov_solve(p, th, 2, tol, verbose=False, pcg_max_iter=5000, precision="fp32",
+                                   preconditioner="block_jacobi")
+    assert i_j["converged"] and i_b["converged"] and rel(u_b, u_j) < 1e-8

@@ -26,6 +26,7 @@ def test_oracle_operator_quantities_match_reference(name):
     assert rel(oracle.residual(u, th, P), d["R"]) < 1e-13
     assert rel(oracle.residual(u, th, P, 0.5), d["R_half"]) < 1e-13
     assert rel(oracle.jacobi_diagonal(u, th, P), d["diag"]) < 1e-13
+    assert rel(oracle.block_jacobi(u, th, P)(v), d["Minv_block_v"]) < 1e-12
     assert abs(float(oracle.strain_energy(u, th, P)) - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))
 
 
@@ -34,7 +35,8 @@ def test_oracle_solve_matches_reference(name):
     d = load(name)
     P = oracle.as_problem(params_from(d))
     th = torch.as_tensor(d["theta"])
-    u, info = oracle.newton_krylov_solve(P, th, int(d["n_load_steps"]), float(d["tol"]), tangent="qp")
+    pre = str(d["preconditioner"]) if "preconditioner" in d else "jacobi"
+    u, info = oracle.newton_krylov_solve(P, th, int(d["n_load_steps"]), float(d["tol"]), tangent="qp", precond=pre)
     assert info["converged"]
     assert rel(u, d["u_star"]) < 1e-9
     assert info["total_newton"] == int(d["total_newton"])
