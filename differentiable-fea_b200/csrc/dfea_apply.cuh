@@ -95,10 +95,10 @@ __global__ void __launch_bounds__(kThreads) k_pivot_init(Mesh m, const T* __rest
 // receives each element's result f_e.  With DOT the curvature contributions are added to `curv`.
 // SD: storage type of the moduli and gradients; T: type of the DOF vectors and of the arithmetic
 // (SD = float, T = double is the mixed form: FP32 operator data, FP64 Krylov vectors).
-template <int NEN, int NQ, typename SD, typename T, bool DOT, typename Start, typename Scatter>
+template <int NEN, int NQ, typename SD, typename T, bool DOT, typename Start, typename Gather, typename Scatter>
 __device__ __forceinline__ bool apply_tiles(const Mesh& m, int64_t e0, int64_t e1, const SD* __restrict__ C,
-                                            const SD* __restrict__ G, const T* __restrict__ v, unsigned char* smem,
-                                            double& curv, Start&& start, Scatter&& scatter) {
+                                            const SD* __restrict__ G, unsigned char* smem, double& curv, Start&& start,
+                                            Gather&& gather, Scatter&& scatter) {
     using Cfg = ApplyCfg<NEN, SD>;
     using CU = typename Cfg::CU;
     using GU = typename Cfg::GU;
@@ -155,7 +155,6 @@ __device__ __forceinline__ bool apply_tiles(const Mesh& m, int64_t e0, int64_t e
         return false;
     }
 
-    const T2* v2 = reinterpret_cast<const T2*>(v);
     int node[NEN], fix[NEN];
     T vx[NEN], vy[NEN], fx[NEN], fy[NEN];
 #pragma unroll
@@ -180,7 +179,7 @@ __device__ __forceinline__ bool apply_tiles(const Mesh& m, int64_t e0, int64_t e
             }
 #pragma unroll
             for (int a = 0; a < NEN; ++a) {
-                const T2 t = __ldg(v2 + node[a]);
+                const T2 t = gather(node[a]);
                 vx[a] = (fix[a] & 1) ? T(0) : t.x;
                 vy[a] = (fix[a] & 2) ? T(0) : t.y;
                 fx[a] = T(0);
@@ -239,8 +238,9 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const SD* __restrict__ C, const SD* __re
     extern __shared__ __align__(16) unsigned char smem[];
     T2* y2 = reinterpret_cast<T2*>(y);
     double curv = 0.0;
+    const T2* v2 = reinterpret_cast<const T2*>(v);
     const bool ran = apply_tiles<NEN, NQ, SD, T, DOT>(
-        m, e0, e1, C, G, v, smem, curv,
+        m, e0, e1, C, G, smem, curv,
         [&]() -> bool {
             // from here on v, y and the solver state may come from the predecessor (PDL)
             grid_dependency_wait();
@@ -248,6 +248,7 @@ k_apply(Mesh m, int64_t e0, int64_t e1, const SD* __restrict__ C, const SD* __re
             grid_dependents_launch();
             return true;
         },
+        [&](int n) { return __ldg(v2 + n); },
         [&](int64_t, const int (&node)[NEN], const int (&fix)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
 #pragma unroll
             for (int a = 0; a < NEN; ++a) {
@@ -279,14 +280,16 @@ k_apply_elem(Mesh m, const SD* __restrict__ C, const SD* __restrict__ G, const T
     T2* fe2 = reinterpret_cast<T2*>(fe);
     const int64_t S = m.stride;
     double curv = 0.0;
+    const T2* v2 = reinterpret_cast<const T2*>(v);
     const bool ran = apply_tiles<NEN, NQ, SD, T, DOT>(
-        m, 0, m.n_el, C, G, v, smem, curv,
+        m, 0, m.n_el, C, G, smem, curv,
         [&]() -> bool {
             grid_dependency_wait();
             if (DOT && done != nullptr && *done) return false;
             grid_dependents_launch();
             return true;
         },
+        [&](int n) { return __ldg(v2 + n); },
         [&](int64_t e, const int (&)[NEN], const int (&)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
 #pragma unroll
             for (int a = 0; a < NEN; ++a) fe2[(int64_t)a * S + e] = make_v2<T>(fx[a], fy[a]);
@@ -350,10 +353,10 @@ struct RefApplyCfg {
     static constexpr int SMEM = STAGES * STAGE_BYTES;
 };
 
-template <int NEN, int NQ, typename T, bool DOT, typename Start, typename Scatter>
+template <int NEN, int NQ, typename T, bool DOT, typename Start, typename Gather, typename Scatter>
 __device__ __forceinline__ bool apply_tiles_ref(const Mesh& m, int64_t e0, int64_t e1, const float* __restrict__ C,
-                                                const RefGrad<NEN, NQ>& rg, const T* __restrict__ v, unsigned char* smem,
-                                                double& curv, Start&& start, Scatter&& scatter) {
+                                                const RefGrad<NEN, NQ>& rg, unsigned char* smem, double& curv,
+                                                Start&& start, Gather&& gather, Scatter&& scatter) {
     using Cfg = RefApplyCfg<NEN>;
     using T2 = v2_t<T>;
     constexpr int NT = Cfg::NT, ST = Cfg::STAGES;
@@ -402,7 +405,6 @@ __device__ __forceinline__ bool apply_tiles_ref(const Mesh& m, int64_t e0, int64
         return false;
     }
 
-    const T2* v2 = reinterpret_cast<const T2*>(v);
     int node[NEN], fix[NEN];
     T vx[NEN], vy[NEN], fx[NEN], fy[NEN];
 #pragma unroll
@@ -431,7 +433,7 @@ __device__ __forceinline__ bool apply_tiles_ref(const Mesh& m, int64_t e0, int64
                     }
 #pragma unroll
                     for (int a = 0; a < NEN; ++a) {
-                        const T2 t = __ldg(v2 + node[a]);
+                        const T2 t = gather(node[a]);
                         vx[a] = (fix[a] & 1) ? T(0) : t.x;
                         vy[a] = (fix[a] & 2) ? T(0) : t.y;
                         fx[a] = T(0);
@@ -478,14 +480,16 @@ k_apply_ref(Mesh m, int64_t e0, int64_t e1, const float* __restrict__ C, const R
     extern __shared__ __align__(16) unsigned char smem[];
     T2* y2 = reinterpret_cast<T2*>(y);
     double curv = 0.0;
+    const T2* v2 = reinterpret_cast<const T2*>(v);
     const bool ran = apply_tiles_ref<NEN, NQ, T, DOT>(
-        m, e0, e1, C, rg, v, smem, curv,
+        m, e0, e1, C, rg, smem, curv,
         [&]() -> bool {
             grid_dependency_wait();
             if (DOT && done != nullptr && *done) return false;
             grid_dependents_launch();
             return true;
         },
+        [&](int n) { return __ldg(v2 + n); },
         [&](int64_t, const int (&node)[NEN], const int (&fix)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
 #pragma unroll
             for (int a = 0; a < NEN; ++a) {
@@ -512,14 +516,16 @@ k_apply_ref_elem(Mesh m, const float* __restrict__ C, const RefGrad<NEN, NQ> rg,
     T2* fe2 = reinterpret_cast<T2*>(fe);
     const int64_t S = m.stride;
     double curv = 0.0;
+    const T2* v2 = reinterpret_cast<const T2*>(v);
     const bool ran = apply_tiles_ref<NEN, NQ, T, DOT>(
-        m, 0, m.n_el, C, rg, v, smem, curv,
+        m, 0, m.n_el, C, rg, smem, curv,
         [&]() -> bool {
             grid_dependency_wait();
             if (DOT && done != nullptr && *done) return false;
             grid_dependents_launch();
             return true;
         },
+        [&](int n) { return __ldg(v2 + n); },
         [&](int64_t e, const int (&)[NEN], const int (&)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
 #pragma unroll
             for (int a = 0; a < NEN; ++a) fe2[(int64_t)a * S + e] = make_v2<T>(fx[a], fy[a]);

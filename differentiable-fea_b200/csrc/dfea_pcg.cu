@@ -34,7 +34,7 @@ struct PcgState {
     double rtol;
     double pfix;    // sum of p^2 over fixed DOFs (identity rows of A)
     double curv;    // last p.Ap
-    double spare;
+    double beta;    // fused form: beta of the last update (0 before the first iteration)
     double curv_c[DFEA_MAX_COLOURS];
     int32_t k;
     int32_t max_iter;
@@ -116,6 +116,7 @@ k_pcg_setup(Mesh m, const T* __restrict__ b, const T* __restrict__ d, T* __restr
         st->rz = tot[0];
         st->norm_b = sqrt(tot[1]);
         st->pfix = tot[2];
+        st->beta = 0.0;
         st->rtol = rtol;
         st->max_iter = max_iter;
         st->k = 0;
@@ -238,6 +239,168 @@ k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __res
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Fused gather form: 2 kernels per iteration.  The direction update p_k = M^-1 r_k + beta_{k-1} p_{k-1}
+// moves out of the second vector kernel: the element pass computes p_k at the nodes it gathers, and the
+// node pass computes it again (same expression, same bits) and stores it.  The node pass also sums the
+// element results (Ap), updates x and r, reduces |r|^2 and r.z, and its last block does the scalar step
+// (convergence test, beta, k).  The identity rows' part of p.Ap (fixed DOFs) is added by the element
+// pass, counted once per node by the node's first incidence slot.
+// ------------------------------------------------------------------------------------------------
+template <bool BJ, typename T>
+__device__ __forceinline__ v2_t<T> next_direction(const T* __restrict__ d, int64_t n, v2_t<T> r, v2_t<T> p, T beta) {
+    const v2_t<T> z = precond<BJ, T>(d, n, r);
+    return make_v2<T>(z.x + beta * p.x, z.y + beta * p.y);
+}
+
+template <typename T, bool BJ, int NEN>
+__device__ __forceinline__ void fused_scatter(int64_t e, int64_t S, const int (&node)[NEN], const int (&fix)[NEN],
+                                              const T (&fx)[NEN], const T (&fy)[NEN], v2_t<T>* __restrict__ fe2,
+                                              const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc,
+                                              const T* __restrict__ d, const v2_t<T>* __restrict__ r2,
+                                              const v2_t<T>* __restrict__ p2, T beta, double& pfix) {
+#pragma unroll
+    for (int a = 0; a < NEN; ++a) fe2[(int64_t)a * S + e] = make_v2<T>(fx[a], fy[a]);
+#pragma unroll
+    for (int a = 0; a < NEN; ++a) {
+        if (fix[a] && inc[inc_ptr[node[a]]] == (int32_t)((int64_t)a * S + e)) {
+            const v2_t<T> pn = next_direction<BJ, T>(d, node[a], __ldg(r2 + node[a]), __ldg(p2 + node[a]), beta);
+            if (fix[a] & 1) pfix += (double)pn.x * pn.x;
+            if (fix[a] & 2) pfix += (double)pn.y * pn.y;
+        }
+    }
+}
+
+template <int NEN, int NQ, typename SD, typename T, bool BJ>
+__global__ void __launch_bounds__(128)
+k_pcg_elem_fused(Mesh m, const SD* __restrict__ C, const SD* __restrict__ G, const T* __restrict__ r,
+                 const T* __restrict__ d, const T* __restrict__ p, T* __restrict__ fe, const int32_t* __restrict__ inc_ptr,
+                 const int32_t* __restrict__ inc, PcgState* st, RedSite site) {
+    using T2 = v2_t<T>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const T2* r2 = reinterpret_cast<const T2*>(r);
+    const T2* p2 = reinterpret_cast<const T2*>(p);
+    T2* fe2 = reinterpret_cast<T2*>(fe);
+    double curv = 0.0, pfix = 0.0;
+    T beta = T(0);
+    const bool ran = apply_tiles<NEN, NQ, SD, T, true>(
+        m, 0, m.n_el, C, G, smem, curv,
+        [&]() -> bool {
+            grid_dependency_wait();
+            if (st->done) return false;
+            beta = (T)st->beta;
+            grid_dependents_launch();
+            return true;
+        },
+        [&](int n) { return next_direction<BJ, T>(d, n, __ldg(r2 + n), __ldg(p2 + n), beta); },
+        [&](int64_t e, const int (&node)[NEN], const int (&fix)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
+            fused_scatter<T, BJ, NEN>(e, m.stride, node, fix, fx, fy, fe2, inc_ptr, inc, d, r2, p2, beta, pfix);
+        });
+    if (!ran) return;
+    const double vals[1] = {block_sum<128>(curv + pfix)};
+    double tot[1];
+    if (last_block_sum<128, 1>(vals, site, tot) && threadIdx.x == 0) site.result[0] = tot[0];
+}
+
+template <int NEN, int NQ, typename T, bool BJ>
+__global__ void __launch_bounds__(128)
+k_pcg_elem_fused_ref(Mesh m, const float* __restrict__ C, const RefGrad<NEN, NQ> rg, const T* __restrict__ r,
+                     const T* __restrict__ d, const T* __restrict__ p, T* __restrict__ fe,
+                     const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc, PcgState* st, RedSite site) {
+    using T2 = v2_t<T>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const T2* r2 = reinterpret_cast<const T2*>(r);
+    const T2* p2 = reinterpret_cast<const T2*>(p);
+    T2* fe2 = reinterpret_cast<T2*>(fe);
+    double curv = 0.0, pfix = 0.0;
+    T beta = T(0);
+    const bool ran = apply_tiles_ref<NEN, NQ, T, true>(
+        m, 0, m.n_el, C, rg, smem, curv,
+        [&]() -> bool {
+            grid_dependency_wait();
+            if (st->done) return false;
+            beta = (T)st->beta;
+            grid_dependents_launch();
+            return true;
+        },
+        [&](int n) { return next_direction<BJ, T>(d, n, __ldg(r2 + n), __ldg(p2 + n), beta); },
+        [&](int64_t e, const int (&node)[NEN], const int (&fix)[NEN], const T (&fx)[NEN], const T (&fy)[NEN]) {
+            fused_scatter<T, BJ, NEN>(e, m.stride, node, fix, fx, fy, fe2, inc_ptr, inc, d, r2, p2, beta, pfix);
+        });
+    if (!ran) return;
+    const double vals[1] = {block_sum<128>(curv + pfix)};
+    double tot[1];
+    if (last_block_sum<128, 1>(vals, site, tot) && threadIdx.x == 0) site.result[0] = tot[0];
+}
+
+template <typename T, bool BJ>
+__global__ void __launch_bounds__(kThreads)
+k_pcg_node_fused(Mesh m, const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc, const T* __restrict__ fe,
+                 const T* __restrict__ d, T* __restrict__ x, T* __restrict__ r, T* __restrict__ p, PcgState* st,
+                 RedSite site) {
+    using T2 = v2_t<T>;
+    grid_dependency_wait();
+    grid_dependents_launch();
+    if (st->done) return;
+    const double curv = st->curv_c[0];
+    const int k = st->k;
+    if (curv <= 0.0) {
+        // not SPD along p: return z at k = 0 and x otherwise (newton_krylov.py:69-70)
+        if (k == 0) {
+            for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x)
+                reinterpret_cast<T2*>(x)[n] = precond<BJ, T>(d, n, reinterpret_cast<const T2*>(r)[n]);
+        }
+        const double vals[1] = {0.0};
+        double tot[1];
+        if (last_block_sum<kThreads, 1>(vals, site, tot) && threadIdx.x == 0) {
+            st->curv = curv;
+            st->iters = k;
+            st->done = DFEA_PCG_NEG_CURV;
+        }
+        return;
+    }
+    const T a = (T)(st->rz / curv);
+    const T beta = (T)st->beta;
+    const T2* fe2 = reinterpret_cast<const T2*>(fe);
+    double rr = 0.0, rz = 0.0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fix = m.node_fix[n];
+        T2 rn = reinterpret_cast<const T2*>(r)[n];
+        const T2 pn = next_direction<BJ, T>(d, n, rn, reinterpret_cast<const T2*>(p)[n], beta);
+        reinterpret_cast<T2*>(p)[n] = pn;
+        const T2 f = node_sum<T>(inc_ptr, inc, fe2, n);
+        const T2 yn = make_v2<T>((fix & 1) ? pn.x : f.x, (fix & 2) ? pn.y : f.y);
+        T2 xn = reinterpret_cast<const T2*>(x)[n];
+        xn.x += a * pn.x;
+        xn.y += a * pn.y;
+        rn.x -= a * yn.x;
+        rn.y -= a * yn.y;
+        reinterpret_cast<T2*>(x)[n] = xn;
+        reinterpret_cast<T2*>(r)[n] = rn;
+        const T2 zn = precond<BJ, T>(d, n, rn);
+        rr += (double)rn.x * rn.x + (double)rn.y * rn.y;
+        rz += (double)rn.x * zn.x + (double)rn.y * zn.y;
+    }
+    const double vals[2] = {block_sum<kThreads>(rr), block_sum<kThreads>(rz)};
+    double tot[2];
+    if (last_block_sum<kThreads, 2>(vals, site, tot) && threadIdx.x == 0) {
+        st->rr = tot[0];
+        st->curv = curv;
+        if (sqrt(tot[0]) <= st->rtol * st->norm_b) {  // newton_krylov.py:77-79
+            st->iters = k + 1;
+            st->done = DFEA_PCG_CONVERGED;
+        } else {
+            st->beta = tot[1] / st->rz;
+            st->rz = tot[1];
+            st->k = k + 1;
+            if (k + 1 >= st->max_iter) {
+                st->iters = st->max_iter;
+                st->done = DFEA_PCG_MAX_ITER;
+            }
+        }
+    }
+}
+
 __global__ void k_pcg_cond(PcgState* st, cudaGraphConditionalHandle h) {
     if (threadIdx.x != 0) return;
     const int g = ++st->guard;
@@ -265,6 +428,7 @@ struct dfea_pcg {
     bool gather = false;             // product in the gather form (element pass + node sums in update 1)
     int grid_cap = 0;                // most blocks per launch (0: as many as the GPU holds)
     bool block = false;              // nodal block-Jacobi: diag holds the inverse 2x2 blocks (4N doubles)
+    bool fused = false;              // fused gather form: 2 kernels per iteration
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -287,6 +451,7 @@ namespace {
 // Kernels of one iteration without the loop condition: the non-empty colour passes and two updates
 // (colour form), or the element pass and two updates (gather form).
 int kernels_per_iteration(const dfea_pcg& h) {
+    if (h.fused) return 2;
     if (h.gather) return 3;
     int nonempty = 0;
     for (int c = 0; c < h.mesh.n_colours; ++c) nonempty += h.mesh.colour_begin[c + 1] > h.mesh.colour_begin[c];
@@ -311,7 +476,42 @@ int launch_iteration(const dfea_pcg& h, cudaStream_t s, cudaGraphConditionalHand
     LaunchOpts pdl;
     pdl.pdl = true;
     int rc;
-    if (h.gather) {
+    if (h.fused) {
+        T* fe = reinterpret_cast<T*>(h.work + h.layout.off_fe);
+        rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
+            constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+            long long max_window = 0;
+            const long long setaside = persisting_l2_bytes(&max_window);
+            LaunchOpts opts;
+            opts.pdl = true;
+            // r and p (adjacent in the work buffer) are gathered by every element: keep them in L2
+            L2Window w = l2_window(r, p, (size_t)(2 * mv.n_nodes) * sizeof(T));
+            if ((long long)w.bytes > max_window) w.bytes = (size_t)max_window;
+            if (setaside > 0 && w.bytes > 0) {
+                opts.win_base = w.base;
+                opts.win_bytes = w.bytes;
+                opts.hit_ratio = setaside >= (long long)w.bytes ? 1.0f : (float)((double)setaside / (double)w.bytes);
+            }
+            if constexpr (REF) {
+                const int grid = capped(resident_grid<k_pcg_elem_fused_ref<NEN, NQ, T, BJ>, RefApplyCfg<NEN>::SMEM, 128>(mv.n_el),
+                                        h.grid_cap);
+                return launch_kernel(k_pcg_elem_fused_ref<NEN, NQ, T, BJ>, dim3(grid), dim3(128), RefApplyCfg<NEN>::SMEM,
+                                     s, opts, m, reinterpret_cast<const float*>(C), ref_grad_of<NEN, NQ>(mv), (const T*)r,
+                                     d, (const T*)p, fe, mv.node_elem_ptr, mv.node_elem, st, h.site(0, 1));
+            } else {
+                using Cfg = ApplyCfg<NEN, S>;
+                const int grid = capped(resident_grid<k_pcg_elem_fused<NEN, NQ, S, T, BJ>, Cfg::SMEM, Cfg::NT>(mv.n_el),
+                                        h.grid_cap);
+                return launch_kernel(k_pcg_elem_fused<NEN, NQ, S, T, BJ>, dim3(grid), dim3(Cfg::NT), Cfg::SMEM, s, opts,
+                                     m, C, G, (const T*)r, d, (const T*)p, fe, mv.node_elem_ptr, mv.node_elem, st,
+                                     h.site(0, 1));
+            }
+        });
+        if (rc) return rc;
+        if ((rc = launch_kernel(k_pcg_node_fused<T, BJ>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mv.node_elem_ptr,
+                                mv.node_elem, (const T*)fe, d, x, r, p, st, h.site(mv.n_colours, 2))))
+            return rc;
+    } else if (h.gather) {
         // element pass (curvature into site 0, read as colour 0), node sums fused into update 1
         T* fe = reinterpret_cast<T*>(h.work + h.layout.off_fe);
         rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
@@ -480,8 +680,10 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
     h->layout = layout_for(*mesh, vec_dtype);
     h->gather = (use_graph & DFEA_PCG_GATHER) != 0;
     h->block = (use_graph & DFEA_PCG_BLOCK_JACOBI) != 0;
+    h->fused = (use_graph & DFEA_PCG_FUSED) != 0;
+    if (h->fused) h->gather = true;
     h->grid_cap = (int)((uint32_t)use_graph >> 8);
-    use_graph &= 0xff & ~(DFEA_PCG_GATHER | DFEA_PCG_BLOCK_JACOBI);
+    use_graph &= 0xff & ~(DFEA_PCG_GATHER | DFEA_PCG_BLOCK_JACOBI | DFEA_PCG_FUSED);
     if (h->block && vec_dtype == DFEA_F32) {
         delete h;
         return set_error(DFEA_ERR_UNSUPPORTED, "dfea_pcg_create: block-Jacobi needs f64 Krylov vectors");
@@ -499,6 +701,23 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
         else if (vec_dtype == DFEA_MIXED) prepare_apply<NEN, NQ, float, double>();
         else if (vec_dtype == DFEA_F32REF) prepare_apply_ref<NEN, NQ, double>();
         else prepare_apply<NEN, NQ, float, float>();
+        if (h->fused) {  // the fused element pass of this handle's types
+            if (vec_dtype == DFEA_F32REF) {
+                if (h->block) (void)resident_grid<k_pcg_elem_fused_ref<NEN, NQ, double, true>, RefApplyCfg<NEN>::SMEM, 128>(1);
+                else (void)resident_grid<k_pcg_elem_fused_ref<NEN, NQ, double, false>, RefApplyCfg<NEN>::SMEM, 128>(1);
+            } else if (vec_dtype == DFEA_F64) {
+                using Cfg = ApplyCfg<NEN, double>;
+                if (h->block) (void)resident_grid<k_pcg_elem_fused<NEN, NQ, double, double, true>, Cfg::SMEM, Cfg::NT>(1);
+                else (void)resident_grid<k_pcg_elem_fused<NEN, NQ, double, double, false>, Cfg::SMEM, Cfg::NT>(1);
+            } else if (vec_dtype == DFEA_MIXED) {
+                using Cfg = ApplyCfg<NEN, float>;
+                if (h->block) (void)resident_grid<k_pcg_elem_fused<NEN, NQ, float, double, true>, Cfg::SMEM, Cfg::NT>(1);
+                else (void)resident_grid<k_pcg_elem_fused<NEN, NQ, float, double, false>, Cfg::SMEM, Cfg::NT>(1);
+            } else {
+                using Cfg = ApplyCfg<NEN, float>;
+                (void)resident_grid<k_pcg_elem_fused<NEN, NQ, float, float, false>, Cfg::SMEM, Cfg::NT>(1);
+            }
+        }
         return DFEA_OK;
     });
     if ((rc = check_cuda(cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||

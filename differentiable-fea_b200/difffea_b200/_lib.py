@@ -21,6 +21,7 @@ MAX_COLOURS = 64
 PCG_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "negative_curvature", 4: "zero_rhs"}
 DFEA_PCG_GATHER = 16  # dfea_pcg_create flag: gather form of the product
 DFEA_PCG_BLOCK_JACOBI = 32  # dfea_pcg_create flag: nodal block-Jacobi (diag = inverse 2x2 blocks, 4N)
+DFEA_PCG_FUSED = 64  # dfea_pcg_create flag: fused gather form (2 kernels per iteration)
 
 
 def pcg_max_blocks(n):

@@ -26,7 +26,8 @@ class DevicePCG:
     16 iterations -- also the form for profilers that trace individual launches.
     form: "colour" (one launch per colour, scatter by read-modify-write) or "gather" (one element pass,
     per-node sums fused into the first vector update: 3 kernels per iteration; needs the mesh's node
-    incidence, built here).  Each form is reproducible; they agree to rounding.
+    incidence, built here) or "fused" (the gather form with the direction update moved into the next
+    element pass: 2 kernels per iteration).  Each form is reproducible; they agree to rounding.
     moduli: "physical" (C with the packed dN/dX: FP64, FP32, or FP32 on FP64 vectors) or "ref" (FP32
     moduli pulled back to the element reference frame, 10 per Gauss point, FP64 vectors; the product
     reads no gradients).  max_blocks: at most this many blocks per launch (0: the whole GPU), for solves
@@ -38,12 +39,12 @@ class DevicePCG:
     def __init__(self, mesh, C, diag, b, x, use_graph=True, form="colour", moduli="physical", max_blocks=0,
                  preconditioner="jacobi"):
         use_graph = int(use_graph) if os.environ.get("DFEA_PCG_GRAPH", "1") != "0" else 0
-        if form not in ("colour", "gather"):
-            raise ValueError("form must be 'colour' or 'gather'")
+        if form not in ("colour", "gather", "fused"):
+            raise ValueError("form must be 'colour', 'gather' or 'fused'")
         flags = 0
-        if form == "gather":
+        if form in ("gather", "fused"):
             mesh.ensure_node_incidence()
-            flags = _lib.DFEA_PCG_GATHER
+            flags = _lib.DFEA_PCG_GATHER | (_lib.DFEA_PCG_FUSED if form == "fused" else 0)
         flags |= _lib.pcg_max_blocks(max_blocks)
         if preconditioner == "block_jacobi":
             # diag holds the inverse 2x2 node blocks (4N doubles) of dfea_qp_moduli_block

@@ -87,7 +87,7 @@ class State:
         self.n_el = self.p["conn"].shape[0]
         self.nen, self.nq = self.p["conn"].shape[1], self.p["dN_dX"].shape[1]
         self.fe = None
-        if form == "gather":
+        if form in ("gather", "fused"):
             self.mesh.ensure_node_incidence()
             vcode = _lib.DFEA_F32 if vt == torch.float32 else _lib.DFEA_F64
             nbytes = int(_lib.load().dfea_gather_work_bytes(self.mesh.view_ref, vcode))
@@ -126,7 +126,7 @@ class State:
         if self.precision == "ref":
             cdt = _lib.DFEA_F32REF
         vdt = _lib.DFEA_F64 if self.v.dtype == torch.float64 else _lib.DFEA_F32
-        if self.form == "gather":
+        if self.form in ("gather", "fused"):
             _lib.call("dfea_tangent_apply_gather", self.mesh.view_ref, ptr(self.C), cdt, ptr(self.v), ptr(self.y), vdt,
                       ptr(self.fe), stream_handle())
         else:
@@ -242,7 +242,7 @@ def main(argv=None):
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--nx", type=int, default=256)
     ap.add_argument("--sweep-precisions", default="fp64,fp32", help="comma-separated precisions of the sweep")
-    ap.add_argument("--form", default=None, choices=("colour", "gather", "auto"),
+    ap.add_argument("--form", default=None, choices=("colour", "gather", "fused", "auto"),
                     help="product form: one launch per colour, or element pass + node sums (default: colour; "
                          "for solve, auto = the solver's choice by mesh size)")
     ap.add_argument("--pcg-graph", type=int, default=None,

@@ -301,10 +301,10 @@ class ServingEngine:
         return [results[r.rid] for r in requests]
 
 
-def run_plain(requests, device, precision="fp64", pcg_graph=1, **kw):
+def run_plain(requests, device, precision="fp64", pcg_graph=2, **kw):
     """
-    The same requests one after another on one stream -- the plain drop-in path (FP64, the
-    conditional-loop PCG graph of newton_krylov_solve's default workspace); Results in order.
+    The same requests one after another on one stream -- the plain drop-in path (FP64, the PCG form of
+    newton_krylov_solve's default workspace); Results in order.
     """
     out = []
     t0 = time.perf_counter()

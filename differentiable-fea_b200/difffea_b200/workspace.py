@@ -5,7 +5,8 @@ A ``NewtonWorkspace`` keeps everything a solve touches in HBM for the whole solv
 trial vectors, the residual, the Gauss-point moduli (FP64, or for the mixed-precision form FP32 moduli
 pulled back to each element's reference frame, so that its operator reads 10 FP32 numbers per Gauss
 point and no gradients, while the Krylov vectors stay FP64), the Jacobi diagonal,
-and one graph-captured ``DevicePCG`` bound to them.  The solver loop
+and one graph-captured ``DevicePCG`` bound to them (eight iterations per graph launch, replayed until
+the solve ends: faster than the conditional-loop graph, 23 vs 28 us per iteration at 16k elements).  The solver loop
 calls the C ABI directly on these buffers (no allocation per Newton step), reading back only the
 scalars the algorithm branches on: ||R|| per residual evaluation and (status, iterations) per PCG.
 """
@@ -19,23 +20,24 @@ from difffea_b200.krylov import DevicePCG
 from difffea_b200.materials import neo_hookean_parameters
 
 
-# Below this many elements the gather form of the PCG product (3 kernels per iteration) is faster than
-# the colour form (n_colours + 2); above it the colour form's lower traffic wins (measured on B200:
-# 22.6 vs 40.2 us per iteration at 16k Q4 elements, 178 vs 174 us at 640k, 610 vs 550 us at 2.56M).
+# Below this many elements the fused gather form of the PCG iteration (2 kernels) is faster than the
+# colour form (n_colours + 2 kernels); above it the colour form's lower traffic wins (measured on B200,
+# FP64, per iteration: 23.0 vs 40.2 us at 16k Q4 elements, 27.5 vs 46.5 at 40k, 171 vs 174 at 640k,
+# 608 vs 550 at 2.56M).
 GATHER_FORM_MAX_ELEMENTS = 1_500_000
 
 
 def pcg_form_for(mesh, pcg_form="auto"):
-    """The PCG product form: "colour", "gather", or "auto" (gather below GATHER_FORM_MAX_ELEMENTS)."""
+    """The PCG product form: "colour", "gather", "fused", or "auto" (fused below GATHER_FORM_MAX_ELEMENTS)."""
     if pcg_form == "auto":
-        return "gather" if mesh.n_el < GATHER_FORM_MAX_ELEMENTS else "colour"
-    if pcg_form not in ("colour", "gather"):
-        raise ValueError("pcg_form must be 'auto', 'colour' or 'gather'")
+        return "fused" if mesh.n_el < GATHER_FORM_MAX_ELEMENTS else "colour"
+    if pcg_form not in ("colour", "gather", "fused"):
+        raise ValueError("pcg_form must be 'auto', 'colour', 'gather' or 'fused'")
     return pcg_form
 
 
 class NewtonWorkspace:
-    def __init__(self, params, precision="fp64", use_graph=True, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
+    def __init__(self, params, precision="fp64", use_graph=2, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
                  preconditioner="jacobi"):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")

@@ -63,6 +63,8 @@ extern "C" {
 #define DFEA_PCG_GATHER 16     /* dfea_pcg_create flag: gather form of the product     */
 #define DFEA_PCG_BLOCK_JACOBI 32 /* dfea_pcg_create flag: nodal block-Jacobi; diag = the
                                   * inverse 2x2 blocks of dfea_qp_moduli_block (4N f64) */
+#define DFEA_PCG_FUSED 64      /* dfea_pcg_create flag: fused gather form, 2 kernels per iteration
+                                * (implies DFEA_PCG_GATHER) */
 /* dfea_pcg_create option: at most n blocks per launch (n < 2^23; 0 = as many as the GPU holds at
  * once).  For solves that share the GPU with solves on other streams. */
 #define DFEA_PCG_MAX_BLOCKS(n) ((int32_t)(n) << 8)
@@ -239,6 +241,9 @@ int64_t dfea_pcg_work_bytes(const dfea_mesh_view* mesh, int32_t vec_dtype);
  * update: 3 kernels per iteration instead of n_colours + 2; needs mesh->node_elem_ptr/node_elem, and
  * then dfea_pcg_work_bytes includes the element-result buffer).  Its iterates agree with the colour
  * form's to rounding (the per-node sums are grouped differently); each form is reproducible.
+ * DFEA_PCG_FUSED moves the direction update into the next element pass (each element computes
+ * p = M^-1 r + beta p at the nodes it gathers; the node pass recomputes and stores it): 2 kernels per
+ * iteration, the same recurrences, sums grouped differently.
  * OR-ing DFEA_PCG_MAX_BLOCKS(n) limits every launch of the solve to n blocks (the results agree with
  * the unlimited grid's to rounding: the reductions group their partial sums by block).
  */

@@ -133,7 +133,7 @@ def test_load_cutbacks_recover():
 # ------------------------------------------------------------------------------------------------
 def _pcg_forms(A, b, rtol, max_iter, use_graph=1):
     out = {}
-    for form in ("colour", "gather"):
+    for form in ("colour", "gather", "fused"):
         bb, xx = b.clone(), torch.empty_like(b)
         solver = DevicePCG(A.mesh, A.C, A.diag.to(b.dtype), bb, xx, use_graph=use_graph, form=form)
         k, status = solver.solve(rtol, max_iter)
@@ -153,16 +153,19 @@ def test_gather_form_pcg_matches_the_colour_form(name, precision):
     A = make_A_operator_cuda(u, th, p, precision=precision)
     b = p["m"] * _t(d, "v")                                     # FP64 vectors (mixed form for fp32 moduli)
     res = _pcg_forms(A, b, 1e-9, 3000)
-    (kc, sc, xc), (kg, sg, xg) = res["colour"], res["gather"]
-    assert sc == sg == "converged" and abs(kc - kg) <= 1
-    assert rel(xg, xc) < 1e-8
+    kc, sc, xc = res["colour"]
+    for form in ("gather", "fused"):
+        kg, sg, xg = res[form]
+        assert sc == sg == "converged" and abs(kc - kg) <= 1
+        assert rel(xg, xc) < 1e-8
 
 
 @pytest.mark.parametrize("use_graph", [0, 1, 2])
-def test_gather_form_is_reproducible_in_every_launch_form(use_graph):
+@pytest.mark.parametrize("form", ["gather", "fused"])
+def test_gather_form_is_reproducible_in_every_launch_form(use_graph, form):
     p, A, M, A_ref, d_ref, b = _linear_system()
     x_ref, k_ref = oracle.pcg(A_ref, b.cpu(), lambda r: r / d_ref, rtol=1e-10, max_iter=2000)
-    runs = [_pcg_forms(A, b, 1e-10, 2000, use_graph)["gather"] for _ in range(2)]
+    runs = [_pcg_forms(A, b, 1e-10, 2000, use_graph)[form] for _ in range(2)]
     assert runs[0][:2] == runs[1][:2] and torch.equal(runs[0][2], runs[1][2])
     k, status, x = runs[0]
     assert status == "converged" and abs(k - k_ref) <= 1 and rel(x, x_ref) < 1e-9
@@ -171,25 +174,30 @@ def test_gather_form_is_reproducible_in_every_launch_form(use_graph):
 def test_gather_form_zero_rhs_negative_curvature_and_cap():
     p, A, M, *_ = _linear_system()
     z = torch.zeros(A.mesh.n_dof, dtype=torch.float64, device=DEV)
-    assert _pcg_forms(A, z, 1e-9, 100)["gather"][:2] == (0, "zero_rhs")
+    zr = _pcg_forms(A, z, 1e-9, 100)
+    assert zr["gather"][:2] == zr["fused"][:2] == (0, "zero_rhs")
     d = load("operator_quad4_h0.25_theta")
     p = params_from(d, DEV)
     An = make_tangent_operator("cuda", _t(d, "u"), -_t(d, "theta"), p)
     res = _pcg_forms(An, p["m"] * _t(d, "v"), 1e-9, 100)
-    assert res["colour"][:2] == res["gather"][:2] == (0, "negative_curvature")
+    assert res["colour"][:2] == res["gather"][:2] == res["fused"][:2] == (0, "negative_curvature")
     assert torch.equal(res["colour"][2], res["gather"][2])               # x = z = b / d at k = 0
+    assert torch.equal(res["colour"][2], res["fused"][2])
     p2, A2, *_ = _linear_system()
     b2 = p2["m"] * torch.ones(A2.mesh.n_dof, dtype=torch.float64, device=DEV)
-    assert _pcg_forms(A2, b2, 1e-30, 7)["gather"][:2] == (7, "max_iter")
+    cap = _pcg_forms(A2, b2, 1e-30, 7)
+    assert cap["gather"][:2] == cap["fused"][:2] == (7, "max_iter")
+    assert rel(cap["fused"][2], cap["colour"][2]) < 1e-10
 
 
 @pytest.mark.parametrize("name", SOLVE_CASES)
-def test_newton_solve_with_the_gather_form(name):
+@pytest.mark.parametrize("form", ["gather", "fused"])
+def test_newton_solve_with_the_gather_form(name, form):
     d = load(name)
     p = params_from(d, DEV)
     th = _t(d, "theta")
     pre = str(d["preconditioner"]) if "preconditioner" in d else "jacobi"
-    ws = NewtonWorkspace(p, pcg_form="gather", preconditioner=pre)
+    ws = NewtonWorkspace(p, pcg_form=form, preconditioner=pre)
     u, info = newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False, workspace=ws,
                                   preconditioner=pre)
     assert info["converged"] and rel(u, d["u_star"]) < 1e-9
@@ -218,7 +226,7 @@ def test_reference_frame_pcg_matches_the_fp64_solution():
 # ------------------------------------------------------------------------------------------------
 # nodal block-Jacobi (operators.py:586-625) inside the device PCG
 # ------------------------------------------------------------------------------------------------
-@pytest.mark.parametrize("form", ["colour", "gather"])
+@pytest.mark.parametrize("form", ["colour", "gather", "fused"])
 def test_block_jacobi_pcg_follows_the_reference_recurrences(form):
     from difffea_b200.operators import compute_block_jacobi
     d = load("operator_quad4_h0.1_theta")
