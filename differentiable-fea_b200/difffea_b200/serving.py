@@ -169,7 +169,7 @@ class ServingEngine:
     """
 
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
-                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="auto",
+                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
                  fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="jacobi"):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if hbm_budget is None:
@@ -192,6 +192,9 @@ class ServingEngine:
         # launches of several slots run side by side instead of each spreading thinly over the whole GPU
         # (measured: 23.6 solves/s at 64 blocks vs 19.7 unlimited, 24 slots, 128 requests of the stream)
         self.max_blocks = int(max_blocks)
+        # pcg_form "gather" (3 kernels per iteration) rather than the fused form (2): with many solves in
+        # flight the fused form's extra gathers (r, M^-1, p at every element node) cost more than the
+        # launch it saves (measured: 24.0 vs 20.7 solves/s, 24 slots, 128 requests of the stream)
         self._cv = threading.Condition()
         self._in_use = 0
         self.peak_in_use = 0
