@@ -356,7 +356,12 @@ struct RefApplyCfg {
 template <int NEN, int NQ, typename T, bool DOT, typename Start, typename Gather, typename Scatter>
 __device__ __forceinline__ bool apply_tiles_ref(const Mesh& m, int64_t e0, int64_t e1, const float* __restrict__ C,
                                                 const RefGrad<NEN, NQ>& rg, unsigned char* smem, double& curv,
-                                                Start&& start, Gather&& gather, Scatter&& scatter) {
+                                                Start&& start, Gather&& gather, Scatter&& scatter,
+                                                int64_t blk = -1, int64_t nblk = -1) {
+    if (blk < 0) {  // the whole launch walks [e0, e1)
+        blk = blockIdx.x;
+        nblk = gridDim.x;
+    }
     using Cfg = RefApplyCfg<NEN>;
     using T2 = v2_t<T>;
     constexpr int NT = Cfg::NT, ST = Cfg::STAGES;
@@ -364,11 +369,11 @@ __device__ __forceinline__ bool apply_tiles_ref(const Mesh& m, int64_t e0, int64
     const int tid = threadIdx.x;
     const int64_t S = m.stride;
     const int64_t n_tiles = (e1 - e0 + NT - 1) / NT;
-    const int64_t my_tiles = (n_tiles > (int64_t)blockIdx.x) ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int64_t my_tiles = (n_tiles > blk) ? (n_tiles - 1 - blk) / nblk + 1 : 0;
     const int64_t n_items = my_tiles * NQ;
 
     auto element_of = [&](int64_t item) -> int64_t {
-        return e0 + ((int64_t)blockIdx.x + (item / NQ) * (int64_t)gridDim.x) * NT + tid;
+        return e0 + (blk + (item / NQ) * nblk) * NT + tid;
     };
     auto stage = [&](int s) -> unsigned char* { return smem + s * Cfg::STAGE_BYTES; };
     auto a_slot = [&](int s) -> float4* { return reinterpret_cast<float4*>(stage(s)) + tid; };

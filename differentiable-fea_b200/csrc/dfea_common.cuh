@@ -170,15 +170,17 @@ __device__ __forceinline__ double block_sum(double v) {
 // to arrive adds all partials in block order and returns true (in all its threads) with the totals
 // in tot[] (valid in thread 0).  It resets the ticket for the next launch.  Every thread of every
 // block must call this with the same K.
+// The same over a group of blocks [0, nblk) of which this block is number blk (several groups, each
+// with its own site, can share one launch).
 template <int NT, int K>
-__device__ bool last_block_sum(const double (&vals)[K], const RedSite& site, double (&tot)[K]) {
+__device__ bool last_block_sum_in(const double (&vals)[K], const RedSite& site, double (&tot)[K], int blk, int nblk) {
     __shared__ int am_last;
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < K; ++k) site.partials[k * kMaxBlocks + blockIdx.x] = vals[k];
+        for (int k = 0; k < K; ++k) site.partials[k * kMaxBlocks + blk] = vals[k];
         __threadfence();
         const unsigned t = atomicAdd(site.ticket, 1u);
-        am_last = (t == gridDim.x - 1) ? 1 : 0;
+        am_last = (t == (unsigned)nblk - 1) ? 1 : 0;
     }
     __syncthreads();
     if (!am_last) return false;
@@ -186,11 +188,16 @@ __device__ bool last_block_sum(const double (&vals)[K], const RedSite& site, dou
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         double s = 0.0;
-        for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) s += __ldcg(site.partials + k * kMaxBlocks + i);
+        for (int i = threadIdx.x; i < nblk; i += NT) s += __ldcg(site.partials + k * kMaxBlocks + i);
         tot[k] = block_sum<NT>(s);
     }
     if (threadIdx.x == 0) *site.ticket = 0u;
     return true;
+}
+
+template <int NT, int K>
+__device__ bool last_block_sum(const double (&vals)[K], const RedSite& site, double (&tot)[K]) {
+    return last_block_sum_in<NT, K>(vals, site, tot, (int)blockIdx.x, (int)gridDim.x);
 }
 
 // ------------------------------------------------------------------------------------------

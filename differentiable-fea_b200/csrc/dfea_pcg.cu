@@ -128,14 +128,14 @@ k_pcg_setup(Mesh m, const T* __restrict__ b, const T* __restrict__ d, T* __restr
 
 // GATHER: Ap is not stored; each node sums its elements' results (fe, the element pass of the gather
 // form) in the incidence order, and takes p on its fixed DOFs (the identity rows).
+// The body of update 1 for block blk of nblk (one launch, or one solve's share of a batched launch).
 template <typename T, bool GATHER, bool BJ>
-__global__ void __launch_bounds__(kThreads)
-k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restrict__ y, const T* __restrict__ d,
-              T* __restrict__ x, T* __restrict__ r, PcgState* st, RedSite site, const int32_t* __restrict__ inc_ptr,
-              const int32_t* __restrict__ inc, const T* __restrict__ fe) {
+__device__ __forceinline__ void pcg_update1_body(const Mesh& m, int n_colours, const T* __restrict__ p,
+                                                 const T* __restrict__ y, const T* __restrict__ d, T* __restrict__ x,
+                                                 T* __restrict__ r, PcgState* st, const RedSite& site,
+                                                 const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc,
+                                                 const T* __restrict__ fe, int64_t blk, int64_t nblk) {
     using T2 = v2_t<T>;
-    grid_dependency_wait();  // launched with PDL: everything below reads the predecessors' results
-    grid_dependents_launch();
     if (st->done) return;
     double curv = st->pfix;
     for (int c = 0; c < n_colours; ++c) curv += st->curv_c[c];
@@ -143,14 +143,14 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
     if (curv <= 0.0) {
         // not SPD along p: return z at k = 0 and x otherwise (newton_krylov.py:69-70)
         if (k == 0) {
-            for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+            for (int64_t n = blk * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)nblk * blockDim.x) {
                 const T2 rn = reinterpret_cast<const T2*>(r)[n];
                 reinterpret_cast<T2*>(x)[n] = precond<BJ, T>(d, n, rn);
             }
         }
         const double vals[1] = {0.0};
         double tot[1];
-        if (last_block_sum<kThreads, 1>(vals, site, tot) && threadIdx.x == 0) {
+        if (last_block_sum_in<kThreads, 1>(vals, site, tot, blk, nblk) && threadIdx.x == 0) {
             st->curv = curv;
             st->iters = k;
             st->done = DFEA_PCG_NEG_CURV;
@@ -160,7 +160,7 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
     const double alpha = st->rz / curv;
     const T a = (T)alpha;
     double rr = 0.0, rz = 0.0;
-    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t n = blk * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)nblk * blockDim.x) {
         const T2 pn = reinterpret_cast<const T2*>(p)[n];
         T2 yn;
         if constexpr (GATHER) {
@@ -184,28 +184,36 @@ k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restric
     }
     const double vals[2] = {block_sum<kThreads>(rr), block_sum<kThreads>(rz)};
     double tot[2];
-    if (last_block_sum<kThreads, 2>(vals, site, tot) && threadIdx.x == 0) {
+    if (last_block_sum_in<kThreads, 2>(vals, site, tot, blk, nblk) && threadIdx.x == 0) {
         st->rr = tot[0];
         st->rz_new = tot[1];
         st->curv = curv;
     }
 }
 
+template <typename T, bool GATHER, bool BJ>
+__global__ void __launch_bounds__(kThreads)
+k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restrict__ y, const T* __restrict__ d,
+              T* __restrict__ x, T* __restrict__ r, PcgState* st, RedSite site, const int32_t* __restrict__ inc_ptr,
+              const int32_t* __restrict__ inc, const T* __restrict__ fe) {
+    grid_dependency_wait();  // launched with PDL: everything below reads the predecessors' results
+    grid_dependents_launch();
+    pcg_update1_body<T, GATHER, BJ>(m, n_colours, p, y, d, x, r, st, site, inc_ptr, inc, fe, blockIdx.x, gridDim.x);
+}
+
 // PIVOT: write Ap := (1 - m) p, the identity rows the colour passes then add to (the colour form).
 template <typename T, bool PIVOT, bool BJ>
-__global__ void __launch_bounds__(kThreads)
-k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __restrict__ p, T* __restrict__ y,
-              PcgState* st, RedSite site) {
+__device__ __forceinline__ void pcg_update2_body(const Mesh& m, const T* __restrict__ r, const T* __restrict__ d,
+                                                 T* __restrict__ p, T* __restrict__ y, PcgState* st,
+                                                 const RedSite& site, int64_t blk, int64_t nblk) {
     using T2 = v2_t<T>;
-    grid_dependency_wait();
-    grid_dependents_launch();
     if (st->done) return;
     const int k = st->k;
     if (sqrt(st->rr) <= st->rtol * st->norm_b) {
         // converged: ||r|| <= rtol ||b||  (newton_krylov.py:77-79)
         const double vals[1] = {0.0};
         double tot[1];
-        if (last_block_sum<kThreads, 1>(vals, site, tot) && threadIdx.x == 0) {
+        if (last_block_sum_in<kThreads, 1>(vals, site, tot, blk, nblk) && threadIdx.x == 0) {
             st->iters = k + 1;
             st->done = DFEA_PCG_CONVERGED;
         }
@@ -214,7 +222,7 @@ k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __res
     const double beta = st->rz_new / st->rz;
     const T bt = (T)beta;
     double pf = 0.0;
-    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t n = blk * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)nblk * blockDim.x) {
         const int fix = m.node_fix[n];
         const T2 rn = reinterpret_cast<const T2*>(r)[n];
         const T2 zn = precond<BJ, T>(d, n, rn);
@@ -228,7 +236,7 @@ k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __res
     }
     const double vals[1] = {block_sum<kThreads>(pf)};
     double tot[1];
-    if (last_block_sum<kThreads, 1>(vals, site, tot) && threadIdx.x == 0) {
+    if (last_block_sum_in<kThreads, 1>(vals, site, tot, blk, nblk) && threadIdx.x == 0) {
         st->rz = st->rz_new;
         st->pfix = tot[0];
         st->k = k + 1;
@@ -237,6 +245,15 @@ k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __res
             st->done = DFEA_PCG_MAX_ITER;
         }
     }
+}
+
+template <typename T, bool PIVOT, bool BJ>
+__global__ void __launch_bounds__(kThreads)
+k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __restrict__ p, T* __restrict__ y,
+              PcgState* st, RedSite site) {
+    grid_dependency_wait();
+    grid_dependents_launch();
+    pcg_update2_body<T, PIVOT, BJ>(m, r, d, p, y, st, site, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -903,5 +920,286 @@ extern "C" int dfea_pcg_solve_noalloc(const dfea_mesh_view* mesh, const void* mo
     if (host_status[0] == DFEA_PCG_RUNNING) return set_error(DFEA_ERR_INVALID, "PCG ended without a status (internal error)");
     if (status) *status = host_status[0];
     if (iters) *iters = host_status[1];
+    return DFEA_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Batched PCG: the solves of several handles advance together, one set of launches per iteration for
+// all of them (an element pass per element type, one launch of each vector update).  Every block works
+// for one solve (a block map gives the solve and the block's number within it); each solve keeps its
+// own state, partial sums and tickets.  A solve's blocks are as many, and split its work the same way,
+// as when it runs alone with the same block cap, so its iterates are bitwise those of its own handle.
+// Supported handles: gather form (not fused), Jacobi, DFEA_F32REF moduli on f64 vectors (the serving
+// configuration).
+// ------------------------------------------------------------------------------------------------
+namespace dfea {
+
+struct BatchSolve {
+    Mesh m;
+    const int32_t* inc_ptr;
+    const int32_t* inc;
+    const float* C;
+    const double* d;
+    double* x;
+    double* r;
+    double* p;
+    double* fe;
+    PcgState* st;
+    RedSite site_elem, site_u1, site_u2;
+    int elem_blocks;
+    int node_blocks;
+};
+
+template <int NEN, int NQ>
+__global__ void __launch_bounds__(128)
+k_batch_elem(const BatchSolve* __restrict__ solves, const int2* __restrict__ block_map, const RefGrad<NEN, NQ> rg) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int2 bm = block_map[blockIdx.x];
+    const BatchSolve* S = solves + bm.x;
+    const Mesh m = S->m;
+    PcgState* st = S->st;
+    const double2* p2 = reinterpret_cast<const double2*>(S->p);
+    double2* fe2 = reinterpret_cast<double2*>(S->fe);
+    const int64_t Sd = m.stride;
+    double curv = 0.0;
+    const bool ran = apply_tiles_ref<NEN, NQ, double, true>(
+        m, 0, m.n_el, S->C, rg, smem, curv,
+        [&]() -> bool {
+            grid_dependency_wait();
+            if (st->done) return false;
+            grid_dependents_launch();
+            return true;
+        },
+        [&](int n) { return __ldg(p2 + n); },
+        [&](int64_t e, const int (&)[NEN], const int (&)[NEN], const double (&fx)[NEN], const double (&fy)[NEN]) {
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) fe2[(int64_t)a * Sd + e] = make_double2(fx[a], fy[a]);
+        },
+        bm.y, S->elem_blocks);
+    if (!ran) return;
+    const double vals[1] = {block_sum<128>(curv)};
+    double tot[1];
+    if (last_block_sum_in<128, 1>(vals, S->site_elem, tot, bm.y, S->elem_blocks) && threadIdx.x == 0)
+        S->site_elem.result[0] = tot[0];
+}
+
+__global__ void __launch_bounds__(kThreads) k_batch_update1(const BatchSolve* __restrict__ solves,
+                                                           const int2* __restrict__ block_map) {
+    grid_dependency_wait();
+    grid_dependents_launch();
+    const int2 bm = block_map[blockIdx.x];
+    const BatchSolve* S = solves + bm.x;
+    pcg_update1_body<double, true, false>(S->m, 1, S->p, S->p, S->d, S->x, S->r, S->st, S->site_u1, S->inc_ptr, S->inc,
+                                          S->fe, bm.y, S->node_blocks);
+}
+
+__global__ void __launch_bounds__(kThreads) k_batch_update2(const BatchSolve* __restrict__ solves,
+                                                           const int2* __restrict__ block_map) {
+    grid_dependency_wait();
+    grid_dependents_launch();
+    const int2 bm = block_map[blockIdx.x];
+    const BatchSolve* S = solves + bm.x;
+    pcg_update2_body<double, false, false>(S->m, S->r, S->d, S->p, S->p, S->st, S->site_u2, bm.y, S->node_blocks);
+}
+
+__global__ void k_batch_status(const BatchSolve* __restrict__ solves, int n, int32_t* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        out[2 * i] = solves[i].st->done;
+        out[2 * i + 1] = solves[i].st->iters;
+    }
+}
+
+}  // namespace dfea
+
+struct dfea_batch {
+    int capacity = 0;
+    int max_blocks = 0;
+    int n = 0;
+    BatchSolve* d_solves = nullptr;
+    BatchSolve* h_solves = nullptr;  // pinned
+    int2* d_map = nullptr;
+    int2* h_map = nullptr;           // pinned: element maps by type, then the node map
+    int32_t* d_status = nullptr;
+    int32_t* h_status = nullptr;     // pinned
+    int map_entries = 0;
+    struct TypeRange {
+        int nen, nq, first, count;   // element-map entries [first, first + count)
+        dfea_mesh_view view;         // a view of this type (for its reference gradients)
+    } types[8];
+    int n_types = 0;
+    int node_first = 0, node_count = 0;
+};
+
+namespace {
+
+void batch_release(dfea_batch* b) {
+    if (b->d_solves) cudaFree(b->d_solves);
+    if (b->d_map) cudaFree(b->d_map);
+    if (b->d_status) cudaFree(b->d_status);
+    if (b->h_solves) cudaFreeHost(b->h_solves);
+    if (b->h_map) cudaFreeHost(b->h_map);
+    if (b->h_status) cudaFreeHost(b->h_status);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" int dfea_batch_create(int32_t capacity, int32_t max_blocks, dfea_batch** out) {
+    if (!out) return set_error(DFEA_ERR_INVALID, "dfea_batch_create: out is NULL");
+    *out = nullptr;
+    if (capacity < 1 || capacity > 4096) return set_error(DFEA_ERR_INVALID, "dfea_batch_create: capacity out of [1, 4096]");
+    if (max_blocks < 1 || max_blocks > kMaxBlocks)
+        return set_error(DFEA_ERR_INVALID, "dfea_batch_create: max_blocks out of [1, %d]", kMaxBlocks);
+    dfea_batch* b = new (std::nothrow) dfea_batch;
+    if (!b) return set_error(DFEA_ERR_INVALID, "dfea_batch_create: out of host memory");
+    b->capacity = capacity;
+    b->max_blocks = max_blocks;
+    b->map_entries = 2 * capacity * max_blocks;  // element blocks + node blocks, at most max_blocks each
+    int rc;
+    if ((rc = check_cuda(cudaMalloc(&b->d_solves, sizeof(BatchSolve) * capacity), "cudaMalloc")) ||
+        (rc = check_cuda(cudaMalloc(&b->d_map, sizeof(int2) * b->map_entries), "cudaMalloc")) ||
+        (rc = check_cuda(cudaMalloc(&b->d_status, sizeof(int32_t) * 2 * capacity), "cudaMalloc")) ||
+        (rc = check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&b->h_solves), sizeof(BatchSolve) * capacity,
+                                       cudaHostAllocDefault), "cudaHostAlloc")) ||
+        (rc = check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&b->h_map), sizeof(int2) * b->map_entries,
+                                       cudaHostAllocDefault), "cudaHostAlloc")) ||
+        (rc = check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&b->h_status), sizeof(int32_t) * 2 * capacity,
+                                       cudaHostAllocDefault), "cudaHostAlloc"))) {
+        batch_release(b);
+        return rc;
+    }
+    *out = b;
+    return DFEA_OK;
+}
+
+extern "C" int dfea_batch_destroy(dfea_batch* b) {
+    if (b) batch_release(b);
+    return DFEA_OK;
+}
+
+extern "C" int dfea_batch_start(dfea_batch* b, dfea_pcg* h, double rtol, int32_t max_iter, void* stream) {
+    if (!b || !h) return set_error(DFEA_ERR_INVALID, "dfea_batch_start: NULL pointer");
+    if (!h->gather || h->fused || h->block || h->vec_dtype != DFEA_F32REF)
+        return set_error(DFEA_ERR_UNSUPPORTED,
+                         "dfea_batch_start: batched solves need the gather form, Jacobi and DFEA_F32REF moduli");
+    if (max_iter < 1 || max_iter > 100000000) return set_error(DFEA_ERR_INVALID, "max_iter %d out of [1, 1e8]", max_iter);
+    if (!(rtol >= 0.0)) return set_error(DFEA_ERR_INVALID, "rtol must be >= 0");
+    return launch_setup<double>(*h, static_cast<cudaStream_t>(stream), rtol, max_iter);
+}
+
+extern "C" int dfea_batch_set(dfea_batch* b, dfea_pcg* const* solves, int32_t n, void* stream) {
+    if (!b || (n > 0 && !solves)) return set_error(DFEA_ERR_INVALID, "dfea_batch_set: NULL pointer");
+    if (n < 0 || n > b->capacity) return set_error(DFEA_ERR_INVALID, "dfea_batch_set: %d solves, capacity %d", n, b->capacity);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the previous table may still be read by launched kernels: wait for them before rewriting it
+    int rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (rc) return rc;
+    b->n = n;
+    b->n_types = 0;
+    int entries = 0;
+    for (int i = 0; i < n; ++i) {
+        const dfea_pcg& h = *solves[i];
+        if (!h.gather || h.fused || h.block || h.vec_dtype != DFEA_F32REF)
+            return set_error(DFEA_ERR_UNSUPPORTED, "dfea_batch_set: solve %d is not in the batched configuration", i);
+        const dfea_mesh_view& mv = h.mesh;
+        BatchSolve& S = b->h_solves[i];
+        S.m = kernel_mesh(mv);
+        S.inc_ptr = mv.node_elem_ptr;
+        S.inc = mv.node_elem;
+        S.C = static_cast<const float*>(h.moduli);
+        S.d = static_cast<const double*>(h.diag);
+        S.x = static_cast<double*>(h.x);
+        S.r = reinterpret_cast<double*>(h.work + h.layout.off_r);
+        S.p = reinterpret_cast<double*>(h.work + h.layout.off_p);
+        S.fe = reinterpret_cast<double*>(h.work + h.layout.off_fe);
+        S.st = h.state();
+        S.site_elem = h.site(0, 1);
+        S.site_u1 = h.site(mv.n_colours, 2);
+        S.site_u2 = h.site(mv.n_colours + 1, 1);
+        const int cap = h.grid_cap > 0 ? h.grid_cap : b->max_blocks;
+        rc = dispatch_element(mv.nen, mv.n_q, [&](auto nen_c, auto nq_c) -> int {
+            constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+            S.elem_blocks = capped(apply_ref_elem_grid<NEN, NQ, double, true>(mv.n_el), cap);
+            (void)resident_grid<k_batch_elem<NEN, NQ>, RefApplyCfg<NEN>::SMEM, 128>(1);  // shared-memory attribute
+            return DFEA_OK;
+        });
+        if (rc) return rc;
+        S.node_blocks = capped(grid_for(mv.n_nodes, kThreads, 4), cap);
+        if (S.elem_blocks > b->max_blocks || S.node_blocks > b->max_blocks)
+            return set_error(DFEA_ERR_INVALID, "dfea_batch_set: solve %d needs more blocks than the batch's cap", i);
+    }
+    // element maps grouped by element type, then the node map
+    for (int i = 0; i < n; ++i) {
+        const dfea_mesh_view& mv = solves[i]->mesh;
+        int t = 0;
+        while (t < b->n_types && !(b->types[t].nen == mv.nen && b->types[t].nq == mv.n_q)) ++t;
+        if (t == b->n_types) {
+            if (b->n_types == 8) return set_error(DFEA_ERR_UNSUPPORTED, "dfea_batch_set: too many element types");
+            b->types[t] = {mv.nen, mv.n_q, 0, 0, mv};
+            ++b->n_types;
+        } else if (std::memcmp(b->types[t].view.ref_grad, mv.ref_grad, sizeof(double) * mv.nen * mv.n_q * 2) != 0) {
+            // one launch per element type passes one table of reference gradients
+            return set_error(DFEA_ERR_INVALID, "dfea_batch_set: solves of one element type differ in ref_grad");
+        }
+    }
+    for (int t = 0; t < b->n_types; ++t) {
+        b->types[t].first = entries;
+        for (int i = 0; i < n; ++i) {
+            const dfea_mesh_view& mv = solves[i]->mesh;
+            if (mv.nen != b->types[t].nen || mv.n_q != b->types[t].nq) continue;
+            for (int k = 0; k < b->h_solves[i].elem_blocks; ++k) b->h_map[entries++] = make_int2(i, k);
+        }
+        b->types[t].count = entries - b->types[t].first;
+    }
+    b->node_first = entries;
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < b->h_solves[i].node_blocks; ++k) b->h_map[entries++] = make_int2(i, k);
+    b->node_count = entries - b->node_first;
+    if (n == 0) return DFEA_OK;
+    if ((rc = check_cuda(cudaMemcpyAsync(b->d_solves, b->h_solves, sizeof(BatchSolve) * n, cudaMemcpyHostToDevice, s),
+                         "cudaMemcpyAsync")) ||
+        (rc = check_cuda(cudaMemcpyAsync(b->d_map, b->h_map, sizeof(int2) * entries, cudaMemcpyHostToDevice, s),
+                         "cudaMemcpyAsync")))
+        return rc;
+    return DFEA_OK;
+}
+
+extern "C" int dfea_batch_iterate(dfea_batch* b, int32_t n_iterations, int32_t* status, int32_t* iters, void* stream) {
+    if (!b) return set_error(DFEA_ERR_INVALID, "dfea_batch_iterate: NULL batch");
+    if (n_iterations < 0 || n_iterations > 1000000) return set_error(DFEA_ERR_INVALID, "n_iterations out of range");
+    if (b->n == 0) return DFEA_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    LaunchOpts pdl;
+    pdl.pdl = true;
+    int rc = DFEA_OK;
+    for (int it = 0; it < n_iterations && rc == DFEA_OK; ++it) {
+        for (int t = 0; t < b->n_types && rc == DFEA_OK; ++t) {
+            const auto& ty = b->types[t];
+            rc = dispatch_element(ty.nen, ty.nq, [&](auto nen_c, auto nq_c) -> int {
+                constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+                return launch_kernel(k_batch_elem<NEN, NQ>, dim3(ty.count), dim3(128), RefApplyCfg<NEN>::SMEM, s, pdl,
+                                     (const BatchSolve*)b->d_solves, (const int2*)(b->d_map + ty.first),
+                                     ref_grad_of<NEN, NQ>(ty.view));
+            });
+        }
+        if (rc) break;
+        if ((rc = launch_kernel(k_batch_update1, dim3(b->node_count), dim3(kThreads), 0, s, pdl,
+                                (const BatchSolve*)b->d_solves, (const int2*)(b->d_map + b->node_first))))
+            break;
+        rc = launch_kernel(k_batch_update2, dim3(b->node_count), dim3(kThreads), 0, s, pdl, (const BatchSolve*)b->d_solves,
+                           (const int2*)(b->d_map + b->node_first));
+    }
+    if (rc) return rc;
+    note_launches((long long)n_iterations * (b->n_types + 2));
+    k_batch_status<<<1, 128, 0, s>>>(b->d_solves, b->n, b->d_status);
+    if ((rc = launch_check("k_batch_status")) ||
+        (rc = check_cuda(cudaMemcpyAsync(b->h_status, b->d_status, sizeof(int32_t) * 2 * b->n, cudaMemcpyDeviceToHost, s),
+                         "cudaMemcpyAsync")) ||
+        (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+        return rc;
+    for (int i = 0; i < b->n; ++i) {
+        if (status) status[i] = b->h_status[2 * i];
+        if (iters) iters[i] = b->h_status[2 * i + 1];
+    }
     return DFEA_OK;
 }

@@ -10,6 +10,8 @@ contents may change between solves.
 """
 import ctypes
 import os
+import queue
+import threading
 import warnings
 
 import torch
@@ -108,6 +110,135 @@ class DevicePCG:
     def close(self):
         if self._h and self._h.value:
             _lib.load().dfea_pcg_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Ticket:
+    __slots__ = ("pcg", "rtol", "max_iter", "event", "done", "iters", "status", "error", "rounds")
+
+    def __init__(self, pcg, rtol, max_iter, event):
+        self.pcg, self.rtol, self.max_iter, self.event = pcg, rtol, max_iter, event
+        self.done = threading.Event()
+        self.iters, self.status, self.error, self.rounds = 0, None, "", 0
+
+
+class BatchExecutor:
+    """
+    Runs the PCG solves of many threads together on one stream: every round advances all solves in
+    flight by ``iterations_per_check`` iterations with one element-pass launch per element type and one
+    launch of each vector update for all of them (``dfea_batch_*``), then reads their statuses.  A
+    thread calls ``solve(pcg, rtol, max_iter)`` after queueing the right-hand side on its current
+    stream; the call returns when that solve has ended (its ``x`` is then final).  New solves join at
+    the next round.  Each solve's iterates are bitwise those of ``pcg.solve`` alone (same block cap).
+    Handles must be in the serving configuration: gather form, Jacobi, reference-frame FP32 moduli.
+    """
+
+    def __init__(self, device, capacity=64, max_blocks=64, iterations_per_check=8):
+        device = torch.device(device)
+        if device.index is None:
+            device = torch.device("cuda", torch.cuda.current_device())
+        self.device = device
+        self.capacity, self.max_blocks, self.iterations_per_check = int(capacity), int(max_blocks), int(iterations_per_check)
+        self._h = ctypes.c_void_p(0)
+        with torch.cuda.device(self.device):
+            _lib.call("dfea_batch_create", self.capacity, self.max_blocks, ctypes.byref(self._h))
+            self.stream = torch.cuda.Stream(self.device)
+        self._q = queue.Queue()
+        self._failure = ""
+        self.rounds = 0
+        self.peak_batch = 0
+        self._thread = threading.Thread(target=self._loop, daemon=True)
+        self._thread.start()
+
+    def solve(self, pcg, rtol, max_iter):
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.device))
+        t = _Ticket(pcg, float(rtol), int(max_iter), ev)
+        self._q.put(t)
+        while not t.done.wait(1.0):
+            if not self._thread.is_alive():   # the executor ended: this solve will never be served
+                raise RuntimeError(f"batch executor stopped: {self._failure or 'closed'}")
+        if t.error:
+            raise RuntimeError(t.error)
+        pcg.last_status = t.status
+        return t.iters, t.status
+
+    def _set(self, active):
+        arr = (ctypes.c_void_p * max(1, len(active)))(*[t.pcg._h.value for t in active])
+        _lib.call("dfea_batch_set", self._h, arr, len(active), ctypes.c_void_p(self.stream.cuda_stream))
+
+    def _loop(self):
+        try:
+            self._serve()
+        except BaseException as exc:  # anything outside a round: record it, solve() reports it
+            self._failure = f"{type(exc).__name__}: {exc}"
+
+    def _serve(self):
+        torch.cuda.set_device(self.device)
+        status = (ctypes.c_int32 * self.capacity)()
+        iters = (ctypes.c_int32 * self.capacity)()
+        s = ctypes.c_void_p(self.stream.cuda_stream)
+        active, stop = [], False
+        while not (stop and not active):
+            new = []
+            if not active:
+                t = self._q.get()
+                if t is None:
+                    break
+                new.append(t)
+            while len(active) + len(new) < self.capacity:
+                try:
+                    t = self._q.get_nowait()
+                except queue.Empty:
+                    break
+                if t is None:
+                    stop = True
+                    break
+                new.append(t)
+            try:
+                for t in new:
+                    self.stream.wait_event(t.event)          # the right-hand side is ready on the caller's stream
+                    _lib.call("dfea_batch_start", self._h, t.pcg._h, t.rtol, t.max_iter, s)
+                if new:
+                    active += new
+                    self._set(active)
+                self.peak_batch = max(self.peak_batch, len(active))
+                _lib.call("dfea_batch_iterate", self._h, self.iterations_per_check, status, iters, s)
+                self.rounds += 1
+                keep = []
+                for i, t in enumerate(active):
+                    t.rounds += 1
+                    if status[i] != 0:
+                        t.iters, t.status = int(iters[i]), _lib.PCG_STATUS.get(status[i], str(status[i]))
+                        t.done.set()
+                    elif t.rounds * self.iterations_per_check > t.max_iter + 2 * self.iterations_per_check + 8:
+                        # the device stops every solve at max_iter; a solve still running is a fault
+                        t.error = "batched PCG solve did not end after max_iter iterations"
+                        t.done.set()
+                    else:
+                        keep.append(t)
+                if len(keep) != len(active):
+                    active = keep
+                    self._set(active)
+            except Exception as exc:  # a failed round fails its solves, not the executor
+                for t in active + new:
+                    if not t.done.is_set():
+                        t.error = f"{type(exc).__name__}: {exc}"
+                        t.done.set()
+                active = []
+
+    def close(self):
+        if self._thread.is_alive():
+            self._q.put(None)
+            self._thread.join()
+        if self._h and self._h.value:
+            _lib.load().dfea_batch_destroy(self._h)
             self._h = ctypes.c_void_p(0)
 
     def __del__(self):

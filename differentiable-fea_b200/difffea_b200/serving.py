@@ -139,14 +139,15 @@ def request_problem(req, device="cpu", build_on_device=False):
 
 def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2,
                   host_params=None, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
-                  preconditioner="jacobi"):
+                  preconditioner="jacobi", batch=None):
     """
     Build (or copy from ``host_params``) and solve one request on the current stream; returns
     (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
     concurrent slots; 1: conditional-loop graph; 0: direct launches); ``pcg_form`` the product form inside
     it ("auto", "colour" or "gather", see DevicePCG and workspace.pcg_form_for); ``fp32_moduli`` the FP32
     operator's moduli ("ref": reference frame, no gradients read; "physical"); ``max_blocks`` the most blocks
-    per PCG launch (0: the whole GPU); ``preconditioner`` "jacobi" or "block_jacobi".
+    per PCG launch (0: the whole GPU); ``preconditioner`` "jacobi" or "block_jacobi"; ``batch`` a
+    ``BatchExecutor`` that runs the PCG solves of all slots together.
     """
     if host_params is not None:
         p = {k: (v.to(device, non_blocking=True) if torch.is_tensor(v) else v) for k, v in host_params.items()}
@@ -155,7 +156,7 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
     ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli,
-                         max_blocks=max_blocks, preconditioner=preconditioner)
+                         max_blocks=max_blocks, preconditioner=preconditioner, batch=batch)
     u, info = newton_krylov_solve(p, th, n_load_steps, tol, verbose=False, workspace=ws, precision=precision,
                                   pcg_max_iter=pcg_max_iter, preconditioner=preconditioner)
     ws.pcg.close()
@@ -170,15 +171,21 @@ class ServingEngine:
 
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
                  pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
-                 fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="jacobi"):
+                 fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="jacobi", batched=False):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = int(0.6 * free)
         self.n_slots, self.hbm_budget, self.precision = n_slots, int(hbm_budget), precision
+        # batched: the PCG solves of all slots advance together on one stream (BatchExecutor), one set of
+        # launches per iteration for all of them
+        self.batch = None
+        if batched:
+            from difffea_b200.krylov import BatchExecutor
+            self.batch = BatchExecutor(self.device, capacity=n_slots, max_blocks=max_blocks)
         self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter,
                              pcg_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli, max_blocks=max_blocks,
-                             preconditioner=preconditioner)
+                             preconditioner=preconditioner, batch=self.batch)
         # torch's caching allocator keeps one pool per stream; a slot whose pool already holds a block of
         # the largest request never calls cudaMalloc (which synchronises the whole device) mid-run
         self.prewarm_bytes = int(prewarm_bytes)

@@ -38,7 +38,7 @@ def pcg_form_for(mesh, pcg_form="auto"):
 
 class NewtonWorkspace:
     def __init__(self, params, precision="fp64", use_graph=2, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
-                 preconditioner="jacobi"):
+                 preconditioner="jacobi", batch=None):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")
         if preconditioner not in ("jacobi", "block_jacobi"):
@@ -78,6 +78,11 @@ class NewtonWorkspace:
                 mesh.ensure_grad32()
         # the PCG reads -R from b and writes its solution straight into du
         self.b = torch.empty(n, **f64)
+        # batch: a BatchExecutor that runs this workspace's PCG solves together with other threads' (the
+        # handle then needs no graph of its own and takes the executor's block cap)
+        self.batch = batch
+        if batch is not None:
+            use_graph, pcg_form, max_blocks = 0, "gather", batch.max_blocks
         self.pcg = DevicePCG(mesh, self.C, self.diag if self.blocks is None else self.blocks, self.b, self.du,
                              use_graph=use_graph, form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind,
                              max_blocks=max_blocks, preconditioner=preconditioner)
@@ -114,7 +119,10 @@ class NewtonWorkspace:
     def solve(self, R, rtol, max_iter):
         """du = PCG(A, -R) to relative tolerance rtol; returns (du (FP64 buffer), iterations, status)."""
         torch.neg(R, out=self.b)
-        iters, status = self.pcg.solve(rtol, max_iter)
+        if self.batch is not None:
+            iters, status = self.batch.solve(self.pcg, rtol, max_iter)
+        else:
+            iters, status = self.pcg.solve(rtol, max_iter)
         return self.du, iters, status
 
     def trial(self, u, alpha, du, out):

@@ -262,6 +262,28 @@ int dfea_pcg_solve(dfea_pcg* pcg, double rtol, int32_t max_iter, int32_t* iters,
 int dfea_pcg_destroy(dfea_pcg* pcg);
 
 /*
+ * Batched PCG (no reference counterpart beyond newton_krylov.py:28-88: it runs several of its solves
+ * at once).  The solves of several handles advance together: each iteration is one element-pass launch
+ * per element type present plus one launch of each vector update for all of them.  A solve's blocks
+ * split its work exactly as its own handle does (same block cap), so its iterates are bitwise those
+ * of dfea_pcg_solve.  Handles must be in the serving configuration: gather form (not fused), Jacobi,
+ * vec_dtype DFEA_F32REF.  Typical use from one host thread: dfea_batch_start for each new solve (after
+ * its right-hand side is ready on `stream`), dfea_batch_set with the solves in flight, then
+ * dfea_batch_iterate repeatedly; finished solves (status != DFEA_PCG_RUNNING) are dropped with the
+ * next dfea_batch_set and their x is final.
+ */
+typedef struct dfea_batch dfea_batch;
+int dfea_batch_create(int32_t capacity, int32_t max_blocks, dfea_batch** out);
+int dfea_batch_destroy(dfea_batch* batch);
+/* Reset and set up one handle's solve (x = 0, r = b, ...) on `stream`. */
+int dfea_batch_start(dfea_batch* batch, dfea_pcg* pcg, double rtol, int32_t max_iter, void* stream);
+/* The solves in flight (at most `capacity`); waits for the stream before replacing the table. */
+int dfea_batch_set(dfea_batch* batch, dfea_pcg* const* pcgs, int32_t n, void* stream);
+/* n_iterations iterations of every solve in the table (finished ones idle), then status[i], iters[i]
+ * of each solve (host arrays of n entries); blocks until they are known. */
+int dfea_batch_iterate(dfea_batch* batch, int32_t n_iterations, int32_t* status, int32_t* iters, void* stream);
+
+/*
  * Jacobi-PCG without any device allocation.  This entry point has no counterpart in the reference.
  *
  * It is for callers that cannot allocate GPU memory themselves: a solver embedded in a host

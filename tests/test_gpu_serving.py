@@ -48,3 +48,14 @@ def test_hbm_budget_admission():
     assert eng.peak_in_flight == 1 and eng.peak_in_use <= biggest
     small = ServingEngine(n_slots=2, hbm_budget=1000, device=DEV).run(reqs[:1])
     assert "MemoryError" in small[0].error
+
+
+def test_batched_engine_gives_the_slot_results_bit_for_bit():
+    reqs = _requests()
+    slots = ServingEngine(n_slots=4, device=DEV).run(reqs)
+    eng = ServingEngine(n_slots=4, device=DEV, batched=True)
+    batched = eng.run(reqs)
+    assert eng.batch.peak_batch >= 2                       # solves really advanced together
+    for a, b in zip(slots, batched):
+        assert b.error == "" and b.converged
+        assert torch.equal(a.u, b.u) and (a.newton, a.cg) == (b.newton, b.cg)

@@ -253,3 +253,54 @@ def test_block_jacobi_mixed_precision_solve():
     u_b, i_b = newton_krylov_solve(p, th, 2, tol, verbose=False, pcg_max_iter=5000, precision="fp32",
                                    preconditioner="block_jacobi")
     assert i_j["converged"] and i_b["converged"] and rel(u_b, u_j) < 1e-8
+
+
+# ------------------------------------------------------------------------------------------------
+# batched PCG: several solves advance together, bitwise as when each runs alone
+# ------------------------------------------------------------------------------------------------
+def _serving_system(et, nx, seed):
+    from difffea_b200.serving import Request, request_problem
+    p = request_problem(Request(seed, et, nx, 1.0 + 0.1 * seed, 0.3, 0.02), DEV, build_on_device=True)
+    th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV)
+    ws = NewtonWorkspace(p, "fp32", use_graph=0, pcg_form="gather", max_blocks=64)
+    ws.set_theta(th)
+    g = torch.Generator().manual_seed(seed)
+    u = (((torch.rand(p["f"].shape[0], dtype=torch.float64, generator=g) * 2 - 1) * 1e-3).to(DEV)) * p["m"]
+    ws.linearize(u)
+    b = p["m"] * torch.randn(p["f"].shape[0], dtype=torch.float64, generator=g).to(DEV)
+    return ws, b
+
+
+def test_batched_pcg_is_bitwise_the_solo_solve():
+    import threading
+    from difffea_b200.krylov import BatchExecutor
+    cases = [("quad4", 64, 1, 1e-10, 5000), ("quad9", 32, 2, 1e-10, 5000), ("quad4", 128, 3, 1e-8, 60),
+             ("quad9", 16, 4, 1e-12, 5000)]
+    systems = [_serving_system(et, nx, seed) for et, nx, seed, _, _ in cases]
+    solo = []
+    for (ws, b), (_, _, _, rtol, cap) in zip(systems, cases):
+        ws.b.copy_(b)
+        k, status = ws.pcg.solve(rtol, cap)
+        solo.append((k, status, ws.du.clone()))
+    ex = BatchExecutor(DEV, capacity=4, max_blocks=64)
+    out = [None] * len(cases)
+
+    def run(i):
+        ws, b = systems[i]
+        torch.cuda.set_device(0)
+        with torch.cuda.stream(torch.cuda.Stream()):
+            ws.b.copy_(b)
+            k, status = ex.solve(ws.pcg, cases[i][3], cases[i][4])
+            out[i] = (k, status, ws.du.clone())
+
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(len(cases))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    ex.close()
+    assert ex.peak_batch >= 2
+    for (k0, s0, x0), (k1, s1, x1) in zip(solo, out):
+        assert (k0, s0) == (k1, s1)
+        assert torch.equal(x0, x1)
+    assert solo[2][:2] == (60, "max_iter")
