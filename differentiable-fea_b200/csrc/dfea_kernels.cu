@@ -208,7 +208,8 @@ __global__ void k_residual_init(Mesh m, const double* __restrict__ f, double lf,
     }
 }
 
-template <int NEN, int NQ, bool ENERGY>
+// MASK = false: the internal force at every DOF (constrained ones included), for support reactions.
+template <int NEN, int NQ, bool ENERGY, bool MASK = true>
 __global__ void __launch_bounds__(128)
 k_residual(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const double* __restrict__ theta,
            double mu0, double lam0, double* __restrict__ R, RedSite site) {
@@ -260,8 +261,8 @@ k_residual(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const d
 #pragma unroll
         for (int a = 0; a < NEN; ++a) {
             double2 t = R2[node[a]];
-            if (!(fix[a] & 1)) t.x += fx[a];
-            if (!(fix[a] & 2)) t.y += fy[a];
+            if (!MASK || !(fix[a] & 1)) t.x += fx[a];
+            if (!MASK || !(fix[a] & 2)) t.y += fy[a];
             R2[node[a]] = t;
         }
     }
@@ -269,6 +270,91 @@ k_residual(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const d
         const double vals[1] = {block_sum<128>(energy)};
         double tot[1];
         if (last_block_sum<128, 1>(vals, site, tot) && threadIdx.x == 0) site.result[0] = tot[0];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Post-processing (postprocess.py:24-118): per element the quadrature-weighted averages of the
+// Gauss-point state [J, sigma_xx, sigma_yy, sigma_xy, sigma_zz, psi] (weights w detJ), the area, and von
+// Mises from the averaged components; per node the plain average over the incident elements.  Cauchy
+// stress of the plane-strain neo-Hookean energy: sigma = (mu (F F^T - I) + lambda lnJ I) / J in 3D with
+// F33 = 1, so sigma_zz = lambda lnJ / J.
+// ------------------------------------------------------------------------------------------
+constexpr int kNodeFields = 6;  // J, sxx, syy, sxy, mises, psi   ([field][n_nodes])
+
+template <int NEN, int NQ>
+__global__ void __launch_bounds__(128)
+k_element_fields(Mesh m, const double* __restrict__ u, const double* __restrict__ theta, double mu0, double lam0,
+                 double* __restrict__ out) {
+    const int64_t S = m.stride, n_el = m.n_el;
+    const double2* u2 = reinterpret_cast<const double2*>(u);
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_el; e += (int64_t)gridDim.x * blockDim.x) {
+        double ux[NEN], uy[NEN];
+#pragma unroll
+        for (int a = 0; a < NEN; ++a) {
+            const double2 t = __ldg(u2 + (m.conn[a * S + e] >> 2));
+            ux[a] = t.x;
+            uy[a] = t.y;
+        }
+        const int64_t oe = m.orig[e];
+        const double th = theta ? theta[oe] : 1.0;
+        const double mu = mu0 * th, lam = lam0 * th;
+        double area = 0.0, acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double F[4] = {1.0, 0.0, 0.0, 1.0};
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                const double2 g = load_grad(m.grad, (int64_t)(q * NEN + a) * S + e);
+                F[0] += ux[a] * g.x;
+                F[1] += ux[a] * g.y;
+                F[2] += uy[a] * g.x;
+                F[3] += uy[a] * g.y;
+            }
+            const NHPoint pt = nh_point(F);
+            const double iJ = 1.0 / pt.J, c = lam * pt.lnJ;
+            const double b00 = F[0] * F[0] + F[1] * F[1], b11 = F[2] * F[2] + F[3] * F[3], b01 = F[0] * F[2] + F[1] * F[3];
+            const double w = m.wdet[q * S + e];
+            area += w;
+            acc[0] += w * pt.J;
+            acc[1] += w * (mu * (b00 - 1.0) + c) * iJ;
+            acc[2] += w * (mu * (b11 - 1.0) + c) * iJ;
+            acc[3] += w * (mu * b01) * iJ;
+            acc[4] += w * c * iJ;
+            acc[5] += w * nh_energy(F, pt, mu, lam);
+        }
+        double mean[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) mean[k] = acc[k] / area;
+        const double sxx = mean[1], syy = mean[2], sxy = mean[3], szz = mean[4];
+        const double mises = sqrt(0.5 * ((sxx - syy) * (sxx - syy) + (syy - szz) * (syy - szz) + (szz - sxx) * (szz - sxx)) +
+                                  3.0 * sxy * sxy);
+        out[0 * n_el + oe] = area;
+        out[1 * n_el + oe] = mean[0];
+        out[2 * n_el + oe] = sxx;
+        out[3 * n_el + oe] = syy;
+        out[4 * n_el + oe] = sxy;
+        out[5 * n_el + oe] = mises;
+        out[6 * n_el + oe] = mean[5];
+    }
+}
+
+// node value = sum over the node's incident elements (incidence order) / their number
+__global__ void __launch_bounds__(kThreads)
+k_node_fields(Mesh m, const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc,
+              const double* __restrict__ elem, double* __restrict__ out) {
+    const int64_t S = m.stride, n_el = m.n_el, N = m.n_nodes;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+        double acc[kNodeFields] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        const int j0 = inc_ptr[n], j1 = inc_ptr[n + 1];
+        for (int j = j0; j < j1; ++j) {
+            const int64_t oe = m.orig[inc[j] % S];
+#pragma unroll
+            for (int k = 0; k < kNodeFields; ++k) acc[k] += elem[(k + 1) * n_el + oe];
+        }
+        const double cnt = (j1 > j0) ? (double)(j1 - j0) : 1.0;
+#pragma unroll
+        for (int k = 0; k < kNodeFields; ++k) out[k * N + n] = acc[k] / cnt;
     }
 }
 
@@ -737,4 +823,61 @@ extern "C" int dfea_f32_to_f64(int64_t n, const float* x, double* y, void* strea
     k_to_f64<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, x, y);
     note_launches(1);
     return launch_check("dfea_f32_to_f64");
+}
+
+extern "C" int dfea_element_fields(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                                   double lambda0, double* elem_out, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!u || !elem_out) return set_error(DFEA_ERR_INVALID, "dfea_element_fields: NULL pointer");
+    if (!aligned16(u)) return set_error(DFEA_ERR_INVALID, "dfea_element_fields: u must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const Mesh m = kernel_mesh(*mesh);
+    const int grid = grid_for(mesh->n_el, 128, 12);
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        k_element_fields<NEN, NQ><<<grid, 128, 0, s>>>(m, u, theta, mu0, lambda0, elem_out);
+        return DFEA_OK;
+    });
+    if (rc) return rc;
+    note_launches(1);
+    return launch_check("dfea_element_fields");
+}
+
+extern "C" int dfea_node_fields(const dfea_mesh_view* mesh, const double* elem, double* node_out, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!elem || !node_out) return set_error(DFEA_ERR_INVALID, "dfea_node_fields: NULL pointer");
+    if (!mesh->node_elem_ptr || !mesh->node_elem)
+        return set_error(DFEA_ERR_INVALID, "dfea_node_fields: the mesh has no node incidence");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_node_fields<<<grid_for(mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(kernel_mesh(*mesh), mesh->node_elem_ptr,
+                                                                           mesh->node_elem, elem, node_out);
+    note_launches(1);
+    return launch_check("dfea_node_fields");
+}
+
+extern "C" int dfea_internal_force(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                                   double lambda0, double* R_int, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!u || !R_int) return set_error(DFEA_ERR_INVALID, "dfea_internal_force: NULL pointer");
+    if (!aligned16(u) || !aligned16(R_int)) return set_error(DFEA_ERR_INVALID, "dfea_internal_force: alignment");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const Mesh m = kernel_mesh(*mesh);
+    k_zero<<<grid_for(2 * mesh->n_nodes, kThreads, 8), kThreads, 0, s>>>(2 * mesh->n_nodes, R_int);
+    note_launches(1);
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        for (int c = 0; c < mesh->n_colours; ++c) {
+            const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
+            if (e1 <= e0) continue;
+            k_residual<NEN, NQ, false, false><<<grid_for(e1 - e0, 128, 12), 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
+                                                                                        R_int, RedSite{});
+            note_launches(1);
+        }
+        return DFEA_OK;
+    });
+    if (rc) return rc;
+    return launch_check("dfea_internal_force");
 }

@@ -66,6 +66,9 @@ _PROTOS = {
                                      c_vp, c_vp, c_vp]),
     "dfea_vec_norm2": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp]),
     "dfea_element_sensitivity": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_vp]),
+    "dfea_element_fields": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_vp]),
+    "dfea_node_fields": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp]),
+    "dfea_internal_force": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_vp]),
     "dfea_batch_create": (ctypes.c_int, [c_i32, c_i32, c_vp]),
     "dfea_batch_destroy": (ctypes.c_int, [c_vp]),
     "dfea_batch_start": (ctypes.c_int, [c_vp, c_vp, c_f64, c_i32, c_vp]),

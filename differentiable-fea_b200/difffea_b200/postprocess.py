@@ -1,0 +1,69 @@
+"""
+Post-processing of a converged displacement on the GPU (the reference's postprocess.py API).
+
+    compute_fields(u, theta, params) -> dict         postprocess.py:70-118
+    support_reactions(u, theta, params) -> (2,)      postprocess.py:121-137
+
+Per element, one kernel evaluates the Gauss-point state [J, sigma_xx, sigma_yy, sigma_xy, sigma_zz, psi] of
+the plane-strain neo-Hookean energy (sigma = P F^T / J with F33 = 1, postprocess.py:24-47), averages it
+with the physical weights w detJ and writes the element area and von Mises of the averaged components
+(postprocess.py:50-67, 96-98).  A second kernel averages the element fields over each node's incident
+elements through the node -> element incidence (postprocess.py:109-117); it sums in incidence order
+instead of conn order, so nodal values differ from a sequential scatter-add by rounding only.  The
+support reactions are the internal force with no mask (every DOF) summed over the fixed DOFs.
+"""
+import torch
+
+from difffea_b200 import _lib
+from difffea_b200.cuda_mesh import ptr, stream_handle
+from difffea_b200.operators import _f64c, _prepare
+
+ELEMENT_FIELDS = ("J", "sxx", "syy", "sxy", "mises", "energy_density")
+
+
+def element_fields(u, theta, params):
+    """(7, n_el) per original element: area, then the weighted means J, sxx, syy, sxy, mises, psi."""
+    mesh, _, mu0, lam0 = _prepare(u, theta, params)
+    u, theta = _f64c(u), _f64c(theta)
+    out = torch.empty(7, mesh.n_el, dtype=torch.float64, device=mesh.device)
+    _lib.call("dfea_element_fields", mesh.view_ref, ptr(u), ptr(theta), mu0, lam0, ptr(out), stream_handle())
+    return out
+
+
+def compute_fields(u, theta, params) -> dict:
+    """
+    All post-processing fields of a converged solution, keys as the reference's:
+        per element (n_el,):  J, sxx, syy, sxy, mises, energy_density
+        per node (N,):        ux, uy, u_mag (and ux_n, uy_n, u_mag_n), and J_n ... energy_density_n
+        scalars (0-d):        strain_energy, min_J
+    """
+    mesh, _, _, _ = _prepare(u, theta, params)
+    el = element_fields(u, theta, params)
+    mesh.ensure_node_incidence()
+    nodal = torch.empty(6, mesh.n_nodes, dtype=torch.float64, device=mesh.device)
+    _lib.call("dfea_node_fields", mesh.view_ref, ptr(el), ptr(nodal), stream_handle())
+    un = _f64c(u).view(mesh.n_nodes, 2)
+    out = {name: el[k + 1] for k, name in enumerate(ELEMENT_FIELDS)}
+    out.update(ux=un[:, 0], uy=un[:, 1], u_mag=torch.linalg.norm(un, dim=1),
+               strain_energy=torch.sum(el[6] * el[0]), min_J=el[1].min())
+    for name in ("ux", "uy", "u_mag"):
+        out[name + "_n"] = out[name]
+    for k, name in enumerate(ELEMENT_FIELDS):
+        out[name + "_n"] = nodal[k]
+    return out
+
+
+def internal_force(u, theta, params):
+    """R_int(u) at every DOF, the constrained ones included (no mask, no external load)."""
+    mesh, _, mu0, lam0 = _prepare(u, theta, params)
+    u, theta = _f64c(u), _f64c(theta)
+    R = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
+    _lib.call("dfea_internal_force", mesh.view_ref, ptr(u), ptr(theta), mu0, lam0, ptr(R), stream_handle())
+    return R
+
+
+def support_reactions(u, theta, params) -> torch.Tensor:
+    """Total reaction (Rx, Ry) at the constrained DOFs; sum(reactions) + sum(applied loads) = 0 at equilibrium."""
+    R = internal_force(u, theta, params).view(-1, 2)
+    fixed = params["fixed"].to(R.device).reshape(-1, 2).bool()
+    return torch.sum(torch.where(fixed, R, torch.zeros_like(R)), dim=0)

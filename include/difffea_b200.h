@@ -189,6 +189,22 @@ int dfea_qp_moduli_block(const dfea_mesh_view* mesh, const double* u, const doub
 int dfea_tangent_apply_gather(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype,
                               const void* v, void* y, int32_t vec_dtype, void* fe_work, void* stream);
 
+/*
+ * Post-processing (postprocess.py:70-118, compute_fields).  dfea_element_fields writes per element, in
+ * ORIGINAL element order, 7 rows of n_el doubles: area (sum w detJ), and the w detJ-weighted averages of
+ * J, sigma_xx, sigma_yy, sigma_xy, then von Mises from the averaged components (sigma_zz included),
+ * then psi.  dfea_node_fields averages rows 1..6 of that output over each node's incident elements
+ * (needs node_elem_ptr/node_elem): 6 rows of n_nodes doubles.
+ */
+int dfea_element_fields(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                        double lambda0, double* elem_out, void* stream);
+int dfea_node_fields(const dfea_mesh_view* mesh, const double* elem, double* node_out, void* stream);
+
+/* Internal force at every DOF, constrained ones included (the support_reactions evaluation,
+ * postprocess.py:121-137): R_int (2N) = sum_e f_e(u, theta). */
+int dfea_internal_force(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
+                        double lambda0, double* R_int, void* stream);
+
 /* Bytes of scratch that dfea_residual and dfea_vec_norm2 need for their reductions. */
 int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh);
 

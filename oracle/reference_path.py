@@ -330,3 +330,54 @@ def compute_sensitivity(P, theta, loss_fn, n_load_steps=5, tol=1e-8, max_newton=
     dL_du = grad(loss_fn)(u)
     lam, _ = solve_adjoint(u, theta, P, dL_du, rtol=adjoint_rtol, max_iter=adjoint_max_iter)
     return u, implicit_vjp(u, theta, P, lam)
+
+
+# ---------------------------------------------------------------------------------------------
+# post-processing (postprocess.py:24-137)
+# ---------------------------------------------------------------------------------------------
+def psi3(F3, p):
+    """The 3D neo-Hookean energy mu/2 (I1 - 3) - mu lnJ + lambda/2 lnJ^2 (materials.py:181-217)."""
+    J = torch.linalg.det(F3)
+    lnJ = torch.log(J)
+    return 0.5 * p[0] * ((F3 * F3).sum() - 3.0) - p[0] * lnJ + 0.5 * p[1] * lnJ ** 2
+
+
+def gauss_point_state(F, p):
+    """[J, sxx, syy, sxy, szz, psi] at one Gauss point: P3 = d psi3 / d F3, sigma = P3 F3^T / J (postprocess.py:24-47)."""
+    F3 = torch.cat([torch.cat([F, torch.zeros(2, 1, dtype=F.dtype)], 1),
+                    torch.tensor([[0.0, 0.0, 1.0]], dtype=F.dtype)], 0)
+    P3 = grad(psi3)(F3, p)
+    J = F[0, 0] * F[1, 1] - F[0, 1] * F[1, 0]
+    sigma = P3 @ F3.T / J
+    return torch.stack([J, sigma[0, 0], sigma[1, 1], sigma[0, 1], sigma[2, 2], psi3(F3, p)])
+
+
+def compute_fields(u, theta, P):
+    """compute_fields (postprocess.py:70-118): w detJ-weighted element means, von Mises, nodal averages."""
+    conn, N = P["conn"], P["nodes"].shape[0]
+    F = deformation_gradient(gather_nodes(u, conn), P["dN_dX"])
+    pe = element_parameters(theta, P)
+    S = vmap(vmap(gauss_point_state, in_dims=(0, None)), in_dims=(0, 0))(F, pe)        # (n_el, n_q, 6)
+    w = P["w_detJ"]
+    area = w.sum(1)
+    mean = torch.einsum("eq,eqk->ek", w, S) / area[:, None]
+    J, sxx, syy, sxy, szz, dens = mean.unbind(1)
+    mises = torch.sqrt(0.5 * ((sxx - syy) ** 2 + (syy - szz) ** 2 + (szz - sxx) ** 2) + 3.0 * sxy ** 2)
+    un = u.reshape(N, 2)
+    out = {"J": J, "sxx": sxx, "syy": syy, "sxy": sxy, "mises": mises, "energy_density": dens,
+           "ux": un[:, 0], "uy": un[:, 1], "u_mag": torch.linalg.norm(un, dim=1),
+           "strain_energy": torch.sum(dens * area), "min_J": J.min()}
+    for name in ("ux", "uy", "u_mag"):
+        out[name + "_n"] = out[name]
+    count = torch.zeros(N, dtype=F64).index_add_(0, conn.reshape(-1), torch.ones(conn.numel(), dtype=F64))
+    for name in ("J", "sxx", "syy", "sxy", "mises", "energy_density"):
+        s = torch.zeros(N, dtype=F64).index_add_(0, conn.reshape(-1), out[name][:, None].expand(-1, conn.shape[1]).reshape(-1))
+        out[name + "_n"] = s / count.clamp(min=1.0)
+    return out
+
+
+def support_reactions(u, theta, P):
+    """Total (Rx, Ry) of the unmasked internal force over the fixed DOFs (postprocess.py:121-137)."""
+    R = scatter_nodes(element_forces(u, theta, P), P["conn"], P["nodes"].shape[0]).reshape(-1, 2)
+    fixed = P["fixed"].reshape(-1, 2)
+    return torch.sum(torch.where(fixed, R, torch.zeros_like(R)), dim=0)

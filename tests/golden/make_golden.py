@@ -8,7 +8,8 @@ Every fixture is produced by calling the reference's own public functions on sma
 problem dictionaries from build_problem (structured rectangle meshes, as in the reference's
 tests/helpers.py small_problem), moduli from _qp_setup, products from the qp / qp_ew / jvp tangent
 variants, residuals, Jacobi diagonals, strain energies, complete Newton-Krylov solves and adjoint
-sensitivities.  File names say what each fixture holds.
+sensitivities, and the post-processing fields and support reactions of the operator states and of the
+solutions.  File names say what each fixture holds.
 
 Two fixtures feed the reference hand-built problem dictionaries, since its build_problem meshes only
 rectangles with one clamped side (problem.py:144-146): the quarter plate with a hole (the mapped Q9 mesh
@@ -29,7 +30,7 @@ sys.path.insert(0, REF_SRC)
 from difffea.newton_krylov import newton_krylov_solve  # noqa: E402
 from difffea.operators import (_qp_setup, compute_jacobi_diagonal, global_residual,  # noqa: E402
                                make_block_jacobi_preconditioner, make_tangent_operator)
-from difffea.postprocess import compute_fields  # noqa: E402
+from difffea.postprocess import compute_fields, support_reactions  # noqa: E402
 from difffea.problem import build_problem, default_spec  # noqa: E402
 from difffea.sensitivity import compute_sensitivity  # noqa: E402
 from difffea.adjoint import compute_implicit_vjp, solve_adjoint  # noqa: E402
@@ -59,6 +60,13 @@ def arrays(params):
     return {k: params[k].numpy() for k in KEYS}
 
 
+def fields(u, theta, p):
+    """compute_fields (postprocess.py:70-118) as fields_<name> arrays, and support_reactions (121-137)."""
+    out = {"fields_" + k: v.numpy() for k, v in compute_fields(u, theta, p).items()}
+    out["reactions"] = support_reactions(u, theta, p).numpy()
+    return out
+
+
 def save(name, **arrs):
     path = os.path.join(HERE, name + ".npz")
     np.savez_compressed(path, **{k: np.asarray(v) for k, v in arrs.items()})
@@ -84,7 +92,7 @@ def operator_case(element_type, h, seed, nonuniform_theta):
                R_half=global_residual(u, theta, p, load_factor=0.5).numpy(),
                diag=compute_jacobi_diagonal(u, theta, p).numpy(),
                Minv_block_v=make_block_jacobi_preconditioner(u, theta, p)(v).numpy(),
-               energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])))
+               energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])), **fields(u, theta, p))
     tag = "theta" if nonuniform_theta else "unit"
     save(f"operator_{element_type}_h{h}_{tag}", **out)
 
@@ -101,7 +109,7 @@ def solve_case(element_type, h, load, n_steps, tol_rel, name, preconditioner="ja
          total_cg=np.array(info["total_cg"]), residuals=np.array([r["residual"] for r in hist]),
          cg_iters=np.array([r["cg_iters"] for r in hist]), alphas=np.array([r["alpha"] for r in hist]),
          preconditioner=np.array(preconditioner),
-         energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])))
+         energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])), **fields(u, theta, p))
 
 
 def sensitivity_case(element_type, h, name):

@@ -30,6 +30,28 @@ def test_oracle_operator_quantities_match_reference(name):
     assert abs(float(oracle.strain_energy(u, th, P)) - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))
 
 
+FIELD_KEYS = ("J", "sxx", "syy", "sxy", "mises", "energy_density", "ux", "uy", "u_mag", "strain_energy", "min_J",
+              "ux_n", "uy_n", "u_mag_n", "J_n", "sxx_n", "syy_n", "sxy_n", "mises_n", "energy_density_n")
+
+
+@pytest.mark.parametrize("name", OPERATOR_CASES + SOLVE_CASES)
+def test_oracle_fields_and_reactions_match_reference(name):
+    """compute_fields and support_reactions (postprocess.py:70-137) at the operator states and solutions."""
+    d = load(name)
+    P = oracle.as_problem(params_from(d))
+    u = torch.as_tensor(d["u"] if "u" in d else d["u_star"])
+    th = torch.as_tensor(d["theta"])
+    out = oracle.compute_fields(u, th, P)
+    assert sorted(out) == sorted(FIELD_KEYS)
+    for k in FIELD_KEYS:
+        assert rel(out[k], d["fields_" + k]) < 1e-12, k
+    R = oracle.support_reactions(u, th, P)
+    assert rel(R, d["reactions"]) < 1e-12
+    if "u_star" in d:                 # equilibrium: reactions balance the applied load
+        f = torch.as_tensor(d["f"]).reshape(-1, 2).sum(0)
+        assert float((R + f).abs().max()) < 1e-6 * float(f.abs().max())
+
+
 @pytest.mark.parametrize("name", SOLVE_CASES)
 def test_oracle_solve_matches_reference(name):
     d = load(name)
