@@ -4,7 +4,7 @@ launches unless ``--no-flush``).
 
     python -m difffea_b200.microbench sweep                       tangent product: Q4/Q9 x 40k..2.56M x fp64/fp32
     python -m difffea_b200.microbench apply --element quad4 --elements 640000 --precision fp64
-    python -m difffea_b200.microbench moduli|residual|sensitivity|pcg --element quad4 --elements 640000
+    python -m difffea_b200.microbench moduli|residual|sensitivity|fields|pcg --element quad4 --elements 640000
     python -m difffea_b200.microbench solve --element quad4 --nx 256 --precision mixed
                                             one serving request (4:1 cantilever, E 1, nu 0.3, load 0.03)
                                             solved twice; the second solve is timed
@@ -20,6 +20,7 @@ nu = 0.3, h = 1.  Algorithmic bytes count every array a kernel must touch once:
                  + moduli written n_el n_q 16 s_C + diagonal 2 x 2N 8
     residual     connectivity + gradients + w detJ + theta + u, f read + R written (3 x 2N 8)
     sensitivity  connectivity + gradients + w detJ + u, lambda read (2 x 2N 8) + g written n_el 8
+    fields       connectivity + gradients + w detJ + theta + u + 7 element rows written (n_el 56)
     pcg          per iteration: the product with the curvature fused (apply bytes) + update 1 (7 vectors)
                  + update 2 (5 vectors + N fix bytes)
 
@@ -116,6 +117,9 @@ class State:
     def sensitivity_bytes(self):
         return self._geometry_bytes() + 2 * self.N2 * 8 + self.n_el * 8
 
+    def fields_bytes(self):
+        return self._geometry_bytes() + self.n_el * 8 + self.N2 * 8 + 7 * self.n_el * 8
+
     def pcg_bytes_per_iteration(self):
         sv = _SIZES[self.precision][2]
         return self.apply_bytes() + 12 * self.N2 * sv + self.N2 // 2
@@ -145,6 +149,12 @@ class State:
 
     def sensitivity(self):
         ops.element_sensitivity(self.mid, self.u, self.v.double(), self.mu0, self.lam0)
+
+    def fields(self):
+        if getattr(self, "el_fields", None) is None:
+            self.el_fields = torch.empty(7, self.n_el, dtype=torch.float64, device=self.device)
+        _lib.call("dfea_element_fields", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mu0, self.lam0,
+                  ptr(self.el_fields), stream_handle())
 
 
 def time_launches(fn, reps=20, warmup=3, flush=True, device="cuda"):
@@ -233,7 +243,7 @@ def solve_once(element, nx, precision, pcg_graph, form="auto"):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m difffea_b200.microbench")
-    ap.add_argument("kind", choices=("sweep", "apply", "moduli", "residual", "sensitivity", "pcg", "solve"))
+    ap.add_argument("kind", choices=("sweep", "apply", "moduli", "residual", "sensitivity", "fields", "pcg", "solve"))
     ap.add_argument("--element", default="quad4", choices=tuple(NEN))
     ap.add_argument("--elements", type=int, default=640_000)
     ap.add_argument("--precision", default="fp64", choices=tuple(_SIZES))
