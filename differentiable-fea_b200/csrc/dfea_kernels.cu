@@ -3,8 +3,11 @@
 // and small vector helpers.  All entry points are `extern "C"` (include/difffea_b200.h).
 #include <cstdio>
 
+#include <type_traits>
+
 #include "dfea_apply.cuh"
 #include "dfea_common.cuh"
+#include "dfea_material.cuh"
 
 namespace dfea {
 
@@ -34,6 +37,33 @@ int validate_mesh(const dfea_mesh_view* mv, bool need_grad32) {
 }
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int validate_material(const dfea_material* mat) {
+    if (mat == nullptr) return set_error(DFEA_ERR_INVALID, "material is NULL");
+    const int n = material_n_params(mat->model);
+    if (n == 0) return set_error(DFEA_ERR_UNSUPPORTED, "material model %d is not built", mat->model);
+    if (mat->scalable >> n) return set_error(DFEA_ERR_INVALID, "scalable mask 0x%x names parameters beyond the %d of model %d",
+                                             mat->scalable, n, mat->model);
+    return DFEA_OK;
+}
+
+// The neo-Hookean material with theta scaling both parameters: the legacy (mu0, lambda0) entry points.
+static dfea_material neo_hookean(double mu0, double lambda0) {
+    dfea_material mt{};
+    mt.model = DFEA_MAT_NEO_HOOKEAN;
+    mt.scalable = 0x3u;
+    mt.p[0] = mu0;
+    mt.p[1] = lambda0;
+    return mt;
+}
+
+// fn(std::bool_constant<GEN>): GEN = the model is evaluated by forward-mode differentiation of its
+// energy; neo-Hookean keeps the closed form.
+template <typename Fn>
+int dispatch_material(const dfea_material& mat, Fn&& fn) {
+    if (mat.model == DFEA_MAT_NEO_HOOKEAN) return fn(std::false_type{});
+    return fn(std::true_type{});
+}
 
 // ------------------------------------------------------------------------------------------
 // mesh packing
@@ -80,10 +110,12 @@ __global__ void k_to_f64(int64_t n, const float* __restrict__ x, double* __restr
 // kernel (a): moduli + element diagonals, one colour per launch
 // ------------------------------------------------------------------------------------------
 // REF (with CT = float): store the moduli pulled back to the reference frame (DFEA_F32REF layout).
-template <int NEN, int NQ, typename CT, bool REF = false>
+// GEN: moduli of the material's energy by forward-mode differentiation (dfea_material.cuh), else closed-form
+// neo-Hookean.
+template <int NEN, int NQ, typename CT, bool REF = false, bool GEN = false>
 __global__ void __launch_bounds__(128)
 k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const double* __restrict__ theta,
-         double mu0, double lam0, CT* __restrict__ Cout, double* __restrict__ diag, double* __restrict__ blocks) {
+         dfea_material mat, CT* __restrict__ Cout, double* __restrict__ diag, double* __restrict__ blocks) {
     const int64_t S = m.stride;
     const double2* u2 = reinterpret_cast<const double2*>(u);
     for (int64_t e = e0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < e1; e += (int64_t)gridDim.x * blockDim.x) {
@@ -99,9 +131,9 @@ k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const dou
             dy[a] = 0.0;
             dxy[a] = 0.0;
         }
-        const double th = theta[m.orig[e]];
-        const double mu = mu0 * th, lam = lam0 * th;
-#pragma unroll
+        double pe[DFEA_MAX_MAT_PARAMS];
+        element_params(mat, theta[m.orig[e]], pe);
+#pragma unroll(GEN ? 1 : NQ)
         for (int q = 0; q < NQ; ++q) {
             double gx[NEN], gy[NEN];
             double F[4] = {1.0, 0.0, 0.0, 1.0};
@@ -115,9 +147,13 @@ k_moduli(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const dou
                 F[2] += uy[a] * g.x;
                 F[3] += uy[a] * g.y;
             }
-            const NHPoint p = nh_point(F);
             double Cq[16];
-            nh_moduli(p, mu, lam, m.wdet[q * S + e], Cq);
+            if constexpr (GEN) {
+                gen_moduli(mat.model, F, pe, m.wdet[q * S + e], Cq);
+            } else {
+                const NHPoint p = nh_point(F);
+                nh_moduli(p, pe[0], pe[1], m.wdet[q * S + e], Cq);
+            }
             if (Cout != nullptr) {
                 if constexpr (REF) {
                     const double2* j2 = reinterpret_cast<const double2*>(m.jinv);
@@ -209,10 +245,10 @@ __global__ void k_residual_init(Mesh m, const double* __restrict__ f, double lf,
 }
 
 // MASK = false: the internal force at every DOF (constrained ones included), for support reactions.
-template <int NEN, int NQ, bool ENERGY, bool MASK = true>
+template <int NEN, int NQ, bool ENERGY, bool MASK = true, bool GEN = false>
 __global__ void __launch_bounds__(128)
 k_residual(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const double* __restrict__ theta,
-           double mu0, double lam0, double* __restrict__ R, RedSite site) {
+           dfea_material mat, double* __restrict__ R, RedSite site) {
     const int64_t S = m.stride;
     const double2* u2 = reinterpret_cast<const double2*>(u);
     double2* R2 = reinterpret_cast<double2*>(R);
@@ -231,9 +267,9 @@ k_residual(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const d
             fx[a] = 0.0;
             fy[a] = 0.0;
         }
-        const double th = theta ? theta[m.orig[e]] : 1.0;
-        const double mu = mu0 * th, lam = lam0 * th;
-#pragma unroll
+        double pe[DFEA_MAX_MAT_PARAMS];
+        element_params(mat, theta ? theta[m.orig[e]] : 1.0, pe);
+#pragma unroll(GEN ? 1 : NQ)
         for (int q = 0; q < NQ; ++q) {
             double gx[NEN], gy[NEN];
             double F[4] = {1.0, 0.0, 0.0, 1.0};
@@ -247,11 +283,16 @@ k_residual(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const d
                 F[2] += uy[a] * g.x;
                 F[3] += uy[a] * g.y;
             }
-            const NHPoint p = nh_point(F);
             double P[4];
-            nh_stress(F, p, mu, lam, P);
             const double w = m.wdet[q * S + e];
-            if (ENERGY) energy += w * nh_energy(F, p, mu, lam);
+            if constexpr (GEN) {
+                const double psi = gen_stress(mat.model, F, pe, P);
+                if (ENERGY) energy += w * psi;
+            } else {
+                const NHPoint p = nh_point(F);
+                nh_stress(F, p, pe[0], pe[1], P);
+                if (ENERGY) energy += w * nh_energy(F, p, pe[0], pe[1]);
+            }
 #pragma unroll
             for (int a = 0; a < NEN; ++a) {
                 fx[a] += w * (P[0] * gx[a] + P[1] * gy[a]);
@@ -282,9 +323,9 @@ k_residual(Mesh m, int64_t e0, int64_t e1, const double* __restrict__ u, const d
 // ------------------------------------------------------------------------------------------
 constexpr int kNodeFields = 6;  // J, sxx, syy, sxy, mises, psi   ([field][n_nodes])
 
-template <int NEN, int NQ>
+template <int NEN, int NQ, bool GEN = false>
 __global__ void __launch_bounds__(128)
-k_element_fields(Mesh m, const double* __restrict__ u, const double* __restrict__ theta, double mu0, double lam0,
+k_element_fields(Mesh m, const double* __restrict__ u, const double* __restrict__ theta, dfea_material mat,
                  double* __restrict__ out) {
     const int64_t S = m.stride, n_el = m.n_el;
     const double2* u2 = reinterpret_cast<const double2*>(u);
@@ -297,10 +338,10 @@ k_element_fields(Mesh m, const double* __restrict__ u, const double* __restrict_
             uy[a] = t.y;
         }
         const int64_t oe = m.orig[e];
-        const double th = theta ? theta[oe] : 1.0;
-        const double mu = mu0 * th, lam = lam0 * th;
+        double pe[DFEA_MAX_MAT_PARAMS];
+        element_params(mat, theta ? theta[oe] : 1.0, pe);
         double area = 0.0, acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
+#pragma unroll(GEN ? 1 : NQ)
         for (int q = 0; q < NQ; ++q) {
             double F[4] = {1.0, 0.0, 0.0, 1.0};
 #pragma unroll
@@ -311,17 +352,37 @@ k_element_fields(Mesh m, const double* __restrict__ u, const double* __restrict_
                 F[2] += uy[a] * g.x;
                 F[3] += uy[a] * g.y;
             }
-            const NHPoint pt = nh_point(F);
-            const double iJ = 1.0 / pt.J, c = lam * pt.lnJ;
-            const double b00 = F[0] * F[0] + F[1] * F[1], b11 = F[2] * F[2] + F[3] * F[3], b01 = F[0] * F[2] + F[1] * F[3];
+            double J, sxx, syy, sxy, szz, psi;
+            if constexpr (GEN) {
+                // sigma = P3 F3^T / J (postprocess.py:40-44); P3 is zero in the (i, 3) and (3, i) slots
+                double P[5];
+                psi = gen_stress3(mat.model, F, pe, P);
+                J = F[0] * F[3] - F[1] * F[2];
+                const double iJ = 1.0 / J;
+                sxx = (P[0] * F[0] + P[1] * F[1]) * iJ;
+                syy = (P[2] * F[2] + P[3] * F[3]) * iJ;
+                sxy = (P[0] * F[2] + P[1] * F[3]) * iJ;
+                szz = P[4] * iJ;
+            } else {
+                const double mu = pe[0], lam = pe[1];
+                const NHPoint pt = nh_point(F);
+                const double iJ = 1.0 / pt.J, c = lam * pt.lnJ;
+                const double b00 = F[0] * F[0] + F[1] * F[1], b11 = F[2] * F[2] + F[3] * F[3], b01 = F[0] * F[2] + F[1] * F[3];
+                J = pt.J;
+                sxx = (mu * (b00 - 1.0) + c) * iJ;
+                syy = (mu * (b11 - 1.0) + c) * iJ;
+                sxy = (mu * b01) * iJ;
+                szz = c * iJ;
+                psi = nh_energy(F, pt, mu, lam);
+            }
             const double w = m.wdet[q * S + e];
             area += w;
-            acc[0] += w * pt.J;
-            acc[1] += w * (mu * (b00 - 1.0) + c) * iJ;
-            acc[2] += w * (mu * (b11 - 1.0) + c) * iJ;
-            acc[3] += w * (mu * b01) * iJ;
-            acc[4] += w * c * iJ;
-            acc[5] += w * nh_energy(F, pt, mu, lam);
+            acc[0] += w * J;
+            acc[1] += w * sxx;
+            acc[2] += w * syy;
+            acc[3] += w * sxy;
+            acc[4] += w * szz;
+            acc[5] += w * psi;
         }
         double mean[6];
 #pragma unroll
@@ -382,9 +443,11 @@ k_norm2(int64_t n, const double* __restrict__ x, RedSite site, double* __restric
 // ------------------------------------------------------------------------------------------
 // kernel (d): per-element sensitivity g_e = -lambda_e . f_e(u; p0)
 // ------------------------------------------------------------------------------------------
-template <int NEN, int NQ>
+// mat.p holds d p_e / d theta_e: the nominal value of every scalable parameter, 0 for the others (all of
+// them prefactors of terms of the energy, so f_e is linear in theta_e with slope f_e(u; mat.p)).
+template <int NEN, int NQ, bool GEN = false>
 __global__ void __launch_bounds__(128)
-k_sensitivity(Mesh m, const double* __restrict__ u, const double* __restrict__ lam_adj, double mu0, double lam0,
+k_sensitivity(Mesh m, const double* __restrict__ u, const double* __restrict__ lam_adj, dfea_material mat,
               double* __restrict__ g) {
     const int64_t S = m.stride;
     const double2* u2 = reinterpret_cast<const double2*>(u);
@@ -403,7 +466,7 @@ k_sensitivity(Mesh m, const double* __restrict__ u, const double* __restrict__ l
             ly[a] = (fix & 2) ? 0.0 : l.y;
         }
         double ge = 0.0;
-#pragma unroll
+#pragma unroll(GEN ? 1 : NQ)
         for (int q = 0; q < NQ; ++q) {
             double gx[NEN], gy[NEN];
             double F[4] = {1.0, 0.0, 0.0, 1.0};
@@ -417,9 +480,13 @@ k_sensitivity(Mesh m, const double* __restrict__ u, const double* __restrict__ l
                 F[2] += uy[a] * gg.x;
                 F[3] += uy[a] * gg.y;
             }
-            const NHPoint p = nh_point(F);
             double P[4];
-            nh_stress(F, p, mu0, lam0, P);
+            if constexpr (GEN) {
+                gen_stress(mat.model, F, mat.p, P);
+            } else {
+                const NHPoint p = nh_point(F);
+                nh_stress(F, p, mat.p[0], mat.p[1], P);
+            }
             const double w = m.wdet[q * S + e];
             // lambda_e : (P dN^T) integrated, i.e. sum_a lambda_a . f_a
             double lgx = 0.0, lgy = 0.0, lgx2 = 0.0, lgy2 = 0.0;
@@ -520,29 +587,29 @@ extern "C" int dfea_mesh_grad_to_f32(const dfea_mesh_view* mesh, float* grad32_o
     return launch_check("dfea_mesh_grad_to_f32");
 }
 
-static int qp_moduli_impl(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
-                          double lambda0, void* moduli, int32_t moduli_dtype, double* diag, double* blocks,
-                          void* stream);
-
 extern "C" int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                               double lambda0, void* moduli, int32_t moduli_dtype, double* diag, void* stream) {
-    return qp_moduli_impl(mesh, u, theta, mu0, lambda0, moduli, moduli_dtype, diag, nullptr, stream);
+    const dfea_material mat = neo_hookean(mu0, lambda0);
+    return dfea_qp_moduli_mat(mesh, u, theta, &mat, moduli, moduli_dtype, diag, nullptr, stream);
 }
 
 extern "C" int dfea_qp_moduli_block(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                                     double lambda0, void* moduli, int32_t moduli_dtype, double* diag, double* blocks,
                                     void* stream) {
     if (!diag || !blocks) return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli_block: diag and blocks are required");
-    if (reinterpret_cast<uintptr_t>(blocks) & 15u)
-        return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli_block: blocks must be 16-byte aligned");
-    return qp_moduli_impl(mesh, u, theta, mu0, lambda0, moduli, moduli_dtype, diag, blocks, stream);
+    const dfea_material mat = neo_hookean(mu0, lambda0);
+    return dfea_qp_moduli_mat(mesh, u, theta, &mat, moduli, moduli_dtype, diag, blocks, stream);
 }
 
-static int qp_moduli_impl(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
-                          double lambda0, void* moduli, int32_t moduli_dtype, double* diag, double* blocks,
-                          void* stream) {
+extern "C" int dfea_qp_moduli_mat(const dfea_mesh_view* mesh, const double* u, const double* theta,
+                                  const dfea_material* material, void* moduli, int32_t moduli_dtype, double* diag,
+                                  double* blocks, void* stream) {
     int rc = validate_mesh(mesh, false);
     if (rc) return rc;
+    if ((rc = validate_material(material))) return rc;
+    const dfea_material mat = *material;
+    if (blocks && !diag) return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: blocks need diag");
+    if (blocks && !aligned16(blocks)) return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: blocks must be 16-byte aligned");
     if (!u || !theta || (!moduli && !diag)) return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: NULL pointer");
     if (!aligned16(u) || (moduli && !aligned16(moduli)) || (diag && !aligned16(diag)))
         return set_error(DFEA_ERR_INVALID, "dfea_qp_moduli: u, moduli and diag must be 16-byte aligned");
@@ -562,22 +629,25 @@ static int qp_moduli_impl(const dfea_mesh_view* mesh, const double* u, const dou
     }
     rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-        for (int c = 0; c < mesh->n_colours; ++c) {
-            const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
-            if (e1 <= e0) continue;
-            const int grid = grid_for(e1 - e0, 128, 12);
-            if (moduli_dtype == DFEA_F64)
-                k_moduli<NEN, NQ, double><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
-                                                                static_cast<double*>(moduli), diag, blocks);
-            else if (moduli_dtype == DFEA_F32REF)
-                k_moduli<NEN, NQ, float, true><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
-                                                                     static_cast<float*>(moduli), diag, blocks);
-            else
-                k_moduli<NEN, NQ, float><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
-                                                               static_cast<float*>(moduli), diag, blocks);
-            note_launches(1);
-        }
-        return DFEA_OK;
+        return dispatch_material(mat, [&](auto gen_c) -> int {
+            constexpr bool GEN = decltype(gen_c)::value;
+            for (int c = 0; c < mesh->n_colours; ++c) {
+                const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
+                if (e1 <= e0) continue;
+                const int grid = grid_for(e1 - e0, 128, 12);
+                if (moduli_dtype == DFEA_F64)
+                    k_moduli<NEN, NQ, double, false, GEN><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mat,
+                                                                               static_cast<double*>(moduli), diag, blocks);
+                else if (moduli_dtype == DFEA_F32REF)
+                    k_moduli<NEN, NQ, float, true, GEN><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mat,
+                                                                             static_cast<float*>(moduli), diag, blocks);
+                else
+                    k_moduli<NEN, NQ, float, false, GEN><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mat,
+                                                                              static_cast<float*>(moduli), diag, blocks);
+                note_launches(1);
+            }
+            return DFEA_OK;
+        });
     });
     if (rc) return rc;
     if (blocks) {  // from the raw diagonal, before the Jacobi clamp below
@@ -721,8 +791,17 @@ extern "C" int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh) {
 extern "C" int dfea_residual(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                              double lambda0, const double* f, double load_factor, double* R, double* out_norm2,
                              double* out_energy, void* work, void* stream) {
+    const dfea_material mat = neo_hookean(mu0, lambda0);
+    return dfea_residual_mat(mesh, u, theta, &mat, f, load_factor, R, out_norm2, out_energy, work, stream);
+}
+
+extern "C" int dfea_residual_mat(const dfea_mesh_view* mesh, const double* u, const double* theta,
+                                 const dfea_material* material, const double* f, double load_factor, double* R,
+                                 double* out_norm2, double* out_energy, void* work, void* stream) {
     int rc = validate_mesh(mesh, false);
     if (rc) return rc;
+    if ((rc = validate_material(material))) return rc;
+    const dfea_material mat = *material;
     if (!u || !R) return set_error(DFEA_ERR_INVALID, "dfea_residual: NULL pointer");
     if ((out_norm2 || out_energy) && !work) return set_error(DFEA_ERR_INVALID, "dfea_residual: reductions need work");
     if (!aligned16(u) || !aligned16(R) || (f && !aligned16(f)) || (work && !aligned16(work)))
@@ -738,17 +817,20 @@ extern "C" int dfea_residual(const dfea_mesh_view* mesh, const double* u, const 
     note_launches(1);
     rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-        for (int c = 0; c < mesh->n_colours; ++c) {
-            const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
-            if (e1 <= e0) continue;
-            const int grid = grid_for(e1 - e0, 128, 12);
-            if (out_energy)
-                k_residual<NEN, NQ, true><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0, R, w.site(1 + c));
-            else
-                k_residual<NEN, NQ, false><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0, R, RedSite{});
-            note_launches(1);
-        }
-        return DFEA_OK;
+        return dispatch_material(mat, [&](auto gen_c) -> int {
+            constexpr bool GEN = decltype(gen_c)::value;
+            for (int c = 0; c < mesh->n_colours; ++c) {
+                const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
+                if (e1 <= e0) continue;
+                const int grid = grid_for(e1 - e0, 128, 12);
+                if (out_energy)
+                    k_residual<NEN, NQ, true, true, GEN><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mat, R, w.site(1 + c));
+                else
+                    k_residual<NEN, NQ, false, true, GEN><<<grid, 128, 0, s>>>(m, e0, e1, u, theta, mat, R, RedSite{});
+                note_launches(1);
+            }
+            return DFEA_OK;
+        });
     });
     if (rc) return rc;
     if (out_norm2 || out_energy) {
@@ -776,8 +858,22 @@ extern "C" int dfea_vec_norm2(const dfea_mesh_view* mesh, const double* x, doubl
 
 extern "C" int dfea_element_sensitivity(const dfea_mesh_view* mesh, const double* u, const double* lam, double mu0,
                                         double lambda0, double* g, void* stream) {
+    const dfea_material mat = neo_hookean(mu0, lambda0);
+    return dfea_element_sensitivity_mat(mesh, u, lam, &mat, g, stream);
+}
+
+extern "C" int dfea_element_sensitivity_mat(const dfea_mesh_view* mesh, const double* u, const double* lam,
+                                            const dfea_material* material, double* g, void* stream) {
     int rc = validate_mesh(mesh, false);
     if (rc) return rc;
+    if ((rc = validate_material(material))) return rc;
+    const unsigned linear = material_linear_mask(material->model);
+    if (material->scalable & ~linear)
+        return set_error(DFEA_ERR_UNSUPPORTED, "dfea_element_sensitivity: theta scales a parameter that enters the "
+                                               "energy nonlinearly (scalable 0x%x, linear 0x%x)", material->scalable, linear);
+    dfea_material slope = *material;  // d p_e / d theta_e
+    for (int k = 0; k < DFEA_MAX_MAT_PARAMS; ++k)
+        if (((linear >> k) & 1u) && !((material->scalable >> k) & 1u)) slope.p[k] = 0.0;
     if (!u || !lam || !g) return set_error(DFEA_ERR_INVALID, "dfea_element_sensitivity: NULL pointer");
     if (!aligned16(u) || !aligned16(lam)) return set_error(DFEA_ERR_INVALID, "u and lambda must be 16-byte aligned");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -785,9 +881,12 @@ extern "C" int dfea_element_sensitivity(const dfea_mesh_view* mesh, const double
     if (mesh->n_el == 0) return DFEA_OK;
     rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-        k_sensitivity<NEN, NQ><<<grid_for(mesh->n_el, 128, 12), 128, 0, s>>>(m, u, lam, mu0, lambda0, g);
-        note_launches(1);
-        return DFEA_OK;
+        return dispatch_material(slope, [&](auto gen_c) -> int {
+            constexpr bool GEN = decltype(gen_c)::value;
+            k_sensitivity<NEN, NQ, GEN><<<grid_for(mesh->n_el, 128, 12), 128, 0, s>>>(m, u, lam, slope, g);
+            note_launches(1);
+            return DFEA_OK;
+        });
     });
     if (rc) return rc;
     return launch_check("dfea_element_sensitivity");
@@ -827,8 +926,16 @@ extern "C" int dfea_f32_to_f64(int64_t n, const float* x, double* y, void* strea
 
 extern "C" int dfea_element_fields(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                                    double lambda0, double* elem_out, void* stream) {
+    const dfea_material mat = neo_hookean(mu0, lambda0);
+    return dfea_element_fields_mat(mesh, u, theta, &mat, elem_out, stream);
+}
+
+extern "C" int dfea_element_fields_mat(const dfea_mesh_view* mesh, const double* u, const double* theta,
+                                       const dfea_material* material, double* elem_out, void* stream) {
     int rc = validate_mesh(mesh, false);
     if (rc) return rc;
+    if ((rc = validate_material(material))) return rc;
+    const dfea_material mat = *material;
     if (!u || !elem_out) return set_error(DFEA_ERR_INVALID, "dfea_element_fields: NULL pointer");
     if (!aligned16(u)) return set_error(DFEA_ERR_INVALID, "dfea_element_fields: u must be 16-byte aligned");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -836,8 +943,11 @@ extern "C" int dfea_element_fields(const dfea_mesh_view* mesh, const double* u, 
     const int grid = grid_for(mesh->n_el, 128, 12);
     rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-        k_element_fields<NEN, NQ><<<grid, 128, 0, s>>>(m, u, theta, mu0, lambda0, elem_out);
-        return DFEA_OK;
+        return dispatch_material(mat, [&](auto gen_c) -> int {
+            constexpr bool GEN = decltype(gen_c)::value;
+            k_element_fields<NEN, NQ, GEN><<<grid, 128, 0, s>>>(m, u, theta, mat, elem_out);
+            return DFEA_OK;
+        });
     });
     if (rc) return rc;
     note_launches(1);
@@ -859,8 +969,16 @@ extern "C" int dfea_node_fields(const dfea_mesh_view* mesh, const double* elem, 
 
 extern "C" int dfea_internal_force(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                                    double lambda0, double* R_int, void* stream) {
+    const dfea_material mat = neo_hookean(mu0, lambda0);
+    return dfea_internal_force_mat(mesh, u, theta, &mat, R_int, stream);
+}
+
+extern "C" int dfea_internal_force_mat(const dfea_mesh_view* mesh, const double* u, const double* theta,
+                                       const dfea_material* material, double* R_int, void* stream) {
     int rc = validate_mesh(mesh, false);
     if (rc) return rc;
+    if ((rc = validate_material(material))) return rc;
+    const dfea_material mat = *material;
     if (!u || !R_int) return set_error(DFEA_ERR_INVALID, "dfea_internal_force: NULL pointer");
     if (!aligned16(u) || !aligned16(R_int)) return set_error(DFEA_ERR_INVALID, "dfea_internal_force: alignment");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -869,14 +987,17 @@ extern "C" int dfea_internal_force(const dfea_mesh_view* mesh, const double* u, 
     note_launches(1);
     rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
-        for (int c = 0; c < mesh->n_colours; ++c) {
-            const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
-            if (e1 <= e0) continue;
-            k_residual<NEN, NQ, false, false><<<grid_for(e1 - e0, 128, 12), 128, 0, s>>>(m, e0, e1, u, theta, mu0, lambda0,
-                                                                                        R_int, RedSite{});
-            note_launches(1);
-        }
-        return DFEA_OK;
+        return dispatch_material(mat, [&](auto gen_c) -> int {
+            constexpr bool GEN = decltype(gen_c)::value;
+            for (int c = 0; c < mesh->n_colours; ++c) {
+                const int64_t e0 = mesh->colour_begin[c], e1 = mesh->colour_begin[c + 1];
+                if (e1 <= e0) continue;
+                k_residual<NEN, NQ, false, false, GEN><<<grid_for(e1 - e0, 128, 12), 128, 0, s>>>(m, e0, e1, u, theta, mat,
+                                                                                                 R_int, RedSite{});
+                note_launches(1);
+            }
+            return DFEA_OK;
+        });
     });
     if (rc) return rc;
     return launch_check("dfea_internal_force");

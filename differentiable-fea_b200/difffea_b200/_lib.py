@@ -33,6 +33,15 @@ def pcg_max_blocks(n):
 c_i32, c_i64, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
 
+MAX_MAT_PARAMS = 8
+DFEA_MAT = {"neo_hookean": 0, "mooney_rivlin": 1, "saint_venant": 2, "demiray": 3, "fiber_reinforced": 4}
+
+
+class Material(ctypes.Structure):
+    """Mirror of ``dfea_material``: model id, theta-scaled parameter bits, nominal parameters."""
+    _fields_ = [("model", c_i32), ("scalable", ctypes.c_uint32), ("p", ctypes.c_double * MAX_MAT_PARAMS)]
+
+
 class MeshView(ctypes.Structure):
     """Mirror of ``dfea_mesh_view``."""
     _fields_ = [
@@ -57,6 +66,16 @@ _PROTOS = {
     "dfea_qp_moduli": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp, c_vp]),
     "dfea_qp_moduli_block": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp,
                                             c_vp, c_vp]),
+    "dfea_qp_moduli_mat": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, ctypes.POINTER(Material), c_vp, c_i32,
+                                          c_vp, c_vp, c_vp]),
+    "dfea_residual_mat": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, ctypes.POINTER(Material), c_vp, c_f64,
+                                         c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "dfea_element_sensitivity_mat": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, ctypes.POINTER(Material),
+                                                    c_vp, c_vp]),
+    "dfea_element_fields_mat": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, ctypes.POINTER(Material), c_vp,
+                                               c_vp]),
+    "dfea_internal_force_mat": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, ctypes.POINTER(Material), c_vp,
+                                               c_vp]),
     "dfea_tangent_apply": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_i32, c_vp, c_vp, c_i32, c_vp]),
     "dfea_gather_work_bytes": (c_i64, [ctypes.POINTER(MeshView), c_i32]),
     "dfea_tangent_apply_gather": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_i32, c_vp, c_vp, c_i32, c_vp,

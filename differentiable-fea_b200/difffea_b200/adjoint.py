@@ -6,8 +6,9 @@ Adjoint sensitivities on the GPU (the reference's adjoint.py API).
 
 The adjoint system A^T lambda = m * dL/du is solved by the device PCG with the stored-moduli operator
 (the hyperelastic tangent is symmetric, so A^T = A).  The implicit VJP  dL/dtheta = -lambda^T dR/dtheta
-is kernel (d): one thread per element evaluates f_e(u*; mu0, lambda0) and contracts it with the masked
-adjoint, which is exact because R_int is linear in theta_e.
+is kernel (d): one thread per element evaluates f_e(u*; dp/dtheta) and contracts it with the masked
+adjoint, which is exact because every energy of the library is linear in its theta-scaled parameters, so
+R_int is linear in theta_e.
 """
 import torch
 
@@ -26,5 +27,5 @@ def solve_adjoint(u_star, theta, params, dL_du, rtol=1e-6, max_iter=500):
 
 def compute_implicit_vjp(u_star, theta, params, lambda_adj):
     """dL/dtheta (n_el,) = -lambda^T dR/dtheta (theta enters linearly, so no theta dependence remains)."""
-    mesh, mid, mu0, lam0 = _prepare(u_star, theta, params)
-    return ops.element_sensitivity(mid, _f64c(u_star), _f64c(lambda_adj), mu0, lam0)
+    mesh, mid, mat = _prepare(u_star, theta, params)
+    return ops.element_sensitivity(mid, _f64c(u_star), _f64c(lambda_adj), *ops.material_args(mat))

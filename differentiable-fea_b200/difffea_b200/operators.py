@@ -21,7 +21,7 @@ import torch
 
 from difffea_b200 import ops
 from difffea_b200.cuda_mesh import _require_cuda, cuda_mesh
-from difffea_b200.materials import neo_hookean_parameters
+from difffea_b200.materials import device_material
 from difffea_b200.problem import precompute_geometry  # noqa: F401  (re-exported, as in the reference)
 
 TANGENT_OPERATORS = ("auto", "cuda")
@@ -34,8 +34,7 @@ def _prepare(u, theta, params):
     mesh = cuda_mesh(params)
     if u.device != mesh.device:
         raise RuntimeError("u and params must be on the same device")
-    mu0, lam0 = neo_hookean_parameters(params)
-    return mesh, ops.register_mesh(mesh), mu0, lam0
+    return mesh, ops.register_mesh(mesh), device_material(params)
 
 
 def _f64c(t):
@@ -47,22 +46,23 @@ def _f64c(t):
 # ---------------------------------------------------------------------------------------------
 def global_residual(u, theta, params, load_factor=1.0):
     """R(u) = m * (R_int(u, theta) - load_factor * f), shape (2N,)."""
-    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
-    R, _, _ = ops.residual(mid, _f64c(u), _f64c(theta), mu0, lam0, _f64c(params["f"]), float(load_factor))
+    mesh, mid, mat = _prepare(u, theta, params)
+    R, _, _ = ops.residual(mid, _f64c(u), _f64c(theta), *ops.material_args(mat), _f64c(params["f"]), float(load_factor))
     return R
 
 
 def residual_and_norm(u, theta, params, load_factor=1.0):
     """(R, ||R||) with the norm reduced on the device in fixed order (one scalar read-back)."""
-    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
-    R, n2, _ = ops.residual(mid, _f64c(u), _f64c(theta), mu0, lam0, _f64c(params["f"]), float(load_factor))
+    mesh, mid, mat = _prepare(u, theta, params)
+    R, n2, _ = ops.residual(mid, _f64c(u), _f64c(theta), *ops.material_args(mat), _f64c(params["f"]),
+                            float(load_factor))
     return R, float(n2) ** 0.5
 
 
 def strain_energy(u, theta, params):
     """Total strain energy sum_e sum_q w detJ psi(F), the ``strain_energy`` of compute_fields."""
-    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
-    _, _, W = ops.residual(mid, _f64c(u), _f64c(theta), mu0, lam0, _f64c(params["f"]), 0.0)
+    mesh, mid, mat = _prepare(u, theta, params)
+    _, _, W = ops.residual(mid, _f64c(u), _f64c(theta), *ops.material_args(mat), _f64c(params["f"]), 0.0)
     return W
 
 
@@ -129,10 +129,10 @@ def make_A_operator_cuda(u, theta, params, precision="fp64"):
     """The stored-moduli tangent operator at (u, theta); precision "fp64" or "fp32" (moduli and vectors)."""
     if precision not in ("fp64", "fp32"):
         raise ValueError("precision must be 'fp64' or 'fp32'")
-    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    mesh, mid, mat = _prepare(u, theta, params)
     if precision == "fp32":
         mesh.ensure_grad32()
-    C, diag = ops.qp_moduli(mid, _f64c(u), _f64c(theta), mu0, lam0, precision == "fp32", True)
+    C, diag = ops.qp_moduli(mid, _f64c(u), _f64c(theta), *ops.material_args(mat), precision == "fp32", True)
     _LAST_DIAG.clear()
     _LAST_DIAG[_diag_key(u, theta, mesh)] = (weakref.ref(u), weakref.ref(theta), diag)
     return CudaTangentOperator(mesh, mid, C, diag, precision)
@@ -177,20 +177,20 @@ class CudaJacobiPreconditioner:
 
 def compute_jacobi_diagonal(u, theta, params):
     """diag(K) without forming K (kernel (a)'s element diagonals, scattered by colour), shape (2N,)."""
-    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    mesh, mid, mat = _prepare(u, theta, params)
     hit = _LAST_DIAG.get(_diag_key(u, theta, mesh))
     if hit is not None and hit[0]() is u and hit[1]() is theta:
         return hit[2]
-    return _diag_only(mesh, u, theta, mu0, lam0)
+    return _diag_only(mesh, u, theta, mat)
 
 
-def _diag_only(mesh, u, theta, mu0, lam0):
+def _diag_only(mesh, u, theta, mat):
     from difffea_b200 import _lib
     from difffea_b200.cuda_mesh import ptr, stream_handle
     u64, th64 = _f64c(u), _f64c(theta)
     diag = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_qp_moduli", mesh.view_ref, ptr(u64), ptr(th64), mu0, lam0, ptr(None), _lib.DFEA_F64, ptr(diag),
-              stream_handle())
+    _lib.call("dfea_qp_moduli_mat", mesh.view_ref, ptr(u64), ptr(th64), mat, ptr(None), _lib.DFEA_F64, ptr(diag),
+              ptr(None), stream_handle())
     return diag
 
 
@@ -219,11 +219,11 @@ def compute_block_jacobi(u, theta, params):
     """The (4N,) inverse 2x2 node blocks of the tangent at (u, theta) (kernel (a) with the coupling term)."""
     from difffea_b200 import _lib
     from difffea_b200.cuda_mesh import ptr, stream_handle
-    mesh, mid, mu0, lam0 = _prepare(u, theta, params)
+    mesh, mid, mat = _prepare(u, theta, params)
     u64, th64 = _f64c(u), _f64c(theta)
     diag = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
     blocks = torch.empty(2 * mesh.n_dof, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_qp_moduli_block", mesh.view_ref, ptr(u64), ptr(th64), mu0, lam0, ptr(None), _lib.DFEA_F64,
+    _lib.call("dfea_qp_moduli_mat", mesh.view_ref, ptr(u64), ptr(th64), mat, ptr(None), _lib.DFEA_F64,
               ptr(diag), ptr(blocks), stream_handle())
     return blocks
 

@@ -5,7 +5,7 @@ Post-processing of a converged displacement on the GPU (the reference's postproc
     support_reactions(u, theta, params) -> (2,)      postprocess.py:121-137
 
 Per element, one kernel evaluates the Gauss-point state [J, sigma_xx, sigma_yy, sigma_xy, sigma_zz, psi] of
-the plane-strain neo-Hookean energy (sigma = P F^T / J with F33 = 1, postprocess.py:24-47), averages it
+the problem's material (sigma = P3 F3^T / J with F33 = 1, postprocess.py:24-47), averages it
 with the physical weights w detJ and writes the element area and von Mises of the averaged components
 (postprocess.py:50-67, 96-98).  A second kernel averages the element fields over each node's incident
 elements through the node -> element incidence (postprocess.py:109-117); it sums in incidence order
@@ -23,10 +23,10 @@ ELEMENT_FIELDS = ("J", "sxx", "syy", "sxy", "mises", "energy_density")
 
 def element_fields(u, theta, params):
     """(7, n_el) per original element: area, then the weighted means J, sxx, syy, sxy, mises, psi."""
-    mesh, _, mu0, lam0 = _prepare(u, theta, params)
+    mesh, _, mat = _prepare(u, theta, params)
     u, theta = _f64c(u), _f64c(theta)
     out = torch.empty(7, mesh.n_el, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_element_fields", mesh.view_ref, ptr(u), ptr(theta), mu0, lam0, ptr(out), stream_handle())
+    _lib.call("dfea_element_fields_mat", mesh.view_ref, ptr(u), ptr(theta), mat, ptr(out), stream_handle())
     return out
 
 
@@ -37,7 +37,7 @@ def compute_fields(u, theta, params) -> dict:
         per node (N,):        ux, uy, u_mag (and ux_n, uy_n, u_mag_n), and J_n ... energy_density_n
         scalars (0-d):        strain_energy, min_J
     """
-    mesh, _, _, _ = _prepare(u, theta, params)
+    mesh, _, _ = _prepare(u, theta, params)
     el = element_fields(u, theta, params)
     mesh.ensure_node_incidence()
     nodal = torch.empty(6, mesh.n_nodes, dtype=torch.float64, device=mesh.device)
@@ -55,10 +55,10 @@ def compute_fields(u, theta, params) -> dict:
 
 def internal_force(u, theta, params):
     """R_int(u) at every DOF, the constrained ones included (no mask, no external load)."""
-    mesh, _, mu0, lam0 = _prepare(u, theta, params)
+    mesh, _, mat = _prepare(u, theta, params)
     u, theta = _f64c(u), _f64c(theta)
     R = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_internal_force", mesh.view_ref, ptr(u), ptr(theta), mu0, lam0, ptr(R), stream_handle())
+    _lib.call("dfea_internal_force_mat", mesh.view_ref, ptr(u), ptr(theta), mat, ptr(R), stream_handle())
     return R
 
 

@@ -111,16 +111,18 @@ def build_problem(spec):
 
 def build_rectangle_problem(element_type, nx, ny, width, height, E=1.0, nu=0.3, load=(0.0, 0.0),
                             fixed_side="left", load_side="right", fixed_dofs="xy", load_mode="force",
-                            device="cpu", dtype=torch.float64, build_on_device=False):
+                            device="cpu", dtype=torch.float64, build_on_device=False, material="neo_hookean",
+                            material_params=None):
     """
     Rectangle with an exact nx x ny cell count (the spec interface derives counts from h).
     ``build_on_device`` constructs mesh, loads and geometry directly on ``device`` (torch ops there)
-    instead of on the host followed by one copy.
+    instead of on the host followed by one copy.  ``material`` / ``material_params`` as in the spec
+    (neo-Hookean from E and nu when no parameters are given).
     """
     where = device if build_on_device else "cpu"
     nodes, conn = create_rectangle_mesh(element_type, width, height, nx, ny, dtype=dtype, device=where)
     spec = dict(fixed_side=fixed_side, fixed_dofs=fixed_dofs, load_side=load_side, load_mode=load_mode,
-                load_value=load, E=E, nu=nu)
+                load_value=load, E=E, nu=nu, material=material, material_params=material_params)
     params = precompute_geometry(_assemble(nodes, conn, element_type, spec, dtype))
     return params if str(params["nodes"].device) == str(torch.device(device)) else to_device(params, device)
 

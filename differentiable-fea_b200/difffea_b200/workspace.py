@@ -17,7 +17,7 @@ import torch
 from difffea_b200 import _lib
 from difffea_b200.cuda_mesh import _require_cuda, cuda_mesh, ptr, stream_handle
 from difffea_b200.krylov import DevicePCG
-from difffea_b200.materials import neo_hookean_parameters
+from difffea_b200.materials import device_material
 
 
 # Below this many elements the fused gather form of the PCG iteration (2 kernels) is faster than the
@@ -46,7 +46,7 @@ class NewtonWorkspace:
         self.preconditioner = preconditioner
         self.params = params
         self.mesh = mesh = cuda_mesh(params)
-        self.mu0, self.lam0 = neo_hookean_parameters(params)
+        self.material = device_material(params)
         self.precision = precision
         dev, n = mesh.device, mesh.n_dof
         f64 = dict(dtype=torch.float64, device=dev)
@@ -99,7 +99,7 @@ class NewtonWorkspace:
 
     def residual(self, u, load_factor, out, energy=False):
         """out = R(u) (FP64); returns ||R|| (and the strain energy if asked) as Python floats."""
-        _lib.call("dfea_residual", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0, ptr(self.f),
+        _lib.call("dfea_residual_mat", self.mesh.view_ref, ptr(u), ptr(self.theta), self.material, ptr(self.f),
                   float(load_factor), ptr(out), ptr(self.scal), ptr(self.scal[1:]) if energy else ptr(None),
                   ptr(self.work), stream_handle())
         self.scal_host.copy_(self.scal, non_blocking=True)
@@ -109,12 +109,8 @@ class NewtonWorkspace:
 
     def linearize(self, u):
         """Kernel (a): moduli C and the preconditioner at u (into the buffers the PCG graph is bound to)."""
-        if self.blocks is not None:
-            _lib.call("dfea_qp_moduli_block", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0,
-                      ptr(self.C), self.moduli_code, ptr(self.diag), ptr(self.blocks), stream_handle())
-        else:
-            _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(u), ptr(self.theta), self.mu0, self.lam0,
-                      ptr(self.C), self.moduli_code, ptr(self.diag), stream_handle())
+        _lib.call("dfea_qp_moduli_mat", self.mesh.view_ref, ptr(u), ptr(self.theta), self.material, ptr(self.C),
+                  self.moduli_code, ptr(self.diag), ptr(self.blocks), stream_handle())
 
     def solve(self, R, rtol, max_iter):
         """du = PCG(A, -R) to relative tolerance rtol; returns (du (FP64 buffer), iterations, status)."""

@@ -69,6 +69,26 @@ extern "C" {
  * once).  For solves that share the GPU with solves on other streams. */
 #define DFEA_PCG_MAX_BLOCKS(n) ((int32_t)(n) << 8)
 
+/*
+ * Material models of the reference's library (materials.py:65-186, MATERIAL_LIBRARY at :164-186), with
+ * the parameter order of its param_names.  Every model is an energy psi3(F3, p) of the plane-strain
+ * embedding F3 = [[F, 0], [0, 1]]; neo-Hookean is evaluated in closed form, the others by forward-mode
+ * differentiation of their energy on the device.
+ */
+#define DFEA_MAT_NEO_HOOKEAN 0      /* p = (mu, lambda)                                      */
+#define DFEA_MAT_MOONEY_RIVLIN 1    /* p = (c10, c01, kappa)                                 */
+#define DFEA_MAT_SAINT_VENANT 2     /* p = (mu, lambda)                                      */
+#define DFEA_MAT_DEMIRAY 3          /* p = (mu, gamma, lambda)                               */
+#define DFEA_MAT_FIBER_REINFORCED 4 /* p = (mu, lambda, k1, k2, beta_deg, d, second_family)  */
+#define DFEA_MAX_MAT_PARAMS 8
+
+/* A material (host struct, passed by pointer): the problem's material, mat_p and mat_scalable. */
+typedef struct dfea_material {
+    int32_t model;                 /* DFEA_MAT_*                                                  */
+    uint32_t scalable;             /* bit k set: the design field theta_e scales p[k] per element */
+    double p[DFEA_MAX_MAT_PARAMS]; /* nominal parameters p0; entries past the model's count unused */
+} dfea_material;
+
 /* A mesh in device memory, colour-sorted.  Sizes are host values, pointers are device pointers. */
 typedef struct dfea_mesh_view {
     int64_t n_el;        /* number of elements                                           */
@@ -155,6 +175,16 @@ int dfea_qp_moduli(const dfea_mesh_view* mesh, const double* u, const double* th
                    double lambda0, void* moduli, int32_t moduli_dtype, double* diag, void* stream);
 
 /*
+ * dfea_qp_moduli (and, with blocks != NULL, dfea_qp_moduli_block) for any material of the library:
+ * p_e = p0 with the scalable entries times theta_e (materials.py:239-246), C = w detJ d2psi/dF2 of that
+ * material's energy.  The (mu0, lambda0) entry points are these with the neo-Hookean material and
+ * scalable = 0x3.
+ */
+int dfea_qp_moduli_mat(const dfea_mesh_view* mesh, const double* u, const double* theta,
+                       const dfea_material* material, void* moduli, int32_t moduli_dtype, double* diag,
+                       double* blocks, void* stream);
+
+/*
  * Kernel (b): y = m * J(u) (m * v) + (1 - m) * v from the stored moduli, i.e. the `qp`/`qp_ew`
  * tangent product (operators.py:345-412).  One fused gather-contract-scatter launch per colour;
  * no atomics.  vec_dtype selects f64 or f32 vectors; f32 moduli (with mesh->grad32 set) may be applied
@@ -198,12 +228,16 @@ int dfea_tangent_apply_gather(const dfea_mesh_view* mesh, const void* moduli, in
  */
 int dfea_element_fields(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                         double lambda0, double* elem_out, void* stream);
+int dfea_element_fields_mat(const dfea_mesh_view* mesh, const double* u, const double* theta,
+                            const dfea_material* material, double* elem_out, void* stream);
 int dfea_node_fields(const dfea_mesh_view* mesh, const double* elem, double* node_out, void* stream);
 
 /* Internal force at every DOF, constrained ones included (the support_reactions evaluation,
  * postprocess.py:121-137): R_int (2N) = sum_e f_e(u, theta). */
 int dfea_internal_force(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                         double lambda0, double* R_int, void* stream);
+int dfea_internal_force_mat(const dfea_mesh_view* mesh, const double* u, const double* theta,
+                            const dfea_material* material, double* R_int, void* stream);
 
 /* Bytes of scratch that dfea_residual and dfea_vec_norm2 need for their reductions. */
 int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh);
@@ -218,6 +252,9 @@ int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh);
 int dfea_residual(const dfea_mesh_view* mesh, const double* u, const double* theta, double mu0,
                   double lambda0, const double* f, double load_factor, double* R, double* out_norm2,
                   double* out_energy, void* work, void* stream);
+int dfea_residual_mat(const dfea_mesh_view* mesh, const double* u, const double* theta,
+                      const dfea_material* material, const double* f, double load_factor, double* R,
+                      double* out_norm2, double* out_energy, void* work, void* stream);
 
 /* *out (device) = sum_i x_i^2 over 2N entries, fixed-order reduction.  work as for dfea_residual. */
 int dfea_vec_norm2(const dfea_mesh_view* mesh, const double* x, double* out, void* work, void* stream);
@@ -232,6 +269,15 @@ int dfea_vec_norm2(const dfea_mesh_view* mesh, const double* x, double* out, voi
  */
 int dfea_element_sensitivity(const dfea_mesh_view* mesh, const double* u, const double* lam,
                              double mu0, double lambda0, double* g, void* stream);
+
+/*
+ * The same for any material: every energy of the library is linear in each parameter that may be
+ * scaled (mu, lambda, c10, c01, kappa, k1: prefactors of its terms), so f_e is linear in theta_e with
+ * slope f_e(u; p0 restricted to the scalable entries).  DFEA_ERR_UNSUPPORTED if theta scales a
+ * parameter that enters nonlinearly (gamma, k2, beta_deg, d, second_family).
+ */
+int dfea_element_sensitivity_mat(const dfea_mesh_view* mesh, const double* u, const double* lam,
+                                 const dfea_material* material, double* g, void* stream);
 
 /* ---------------------------------------------------------------- kernel (c): PCG ------------- */
 

@@ -3,7 +3,7 @@ CPU restatement of the reference's Newton-Krylov path (test infrastructure; see 
 
 Inputs are "problem" dictionaries with the reference's keys (operators.py:19-34): nodes (N,2),
 conn (n_el,nen) int64, dN_dX (n_el,n_q,nen,2), w_detJ (n_el,n_q), f, m, u_D (2N,) float64,
-fixed (2N,) bool, mat_p (2,) = [mu0, lambda0].  Everything runs in float64 on the CPU with PyTorch's
+fixed (2N,) bool, material (name), mat_p (n_p,), mat_scalable (n_p,) bool.  Everything runs in float64 on the CPU with PyTorch's
 CPU kernels and torch.func autodiff, i.e. the same arithmetic the reference performs -- which is also
 why this module doubles as the reference CPU baseline for timing.
 """
@@ -20,6 +20,10 @@ def as_problem(p):
         out[k] = torch.as_tensor(p[k]).detach().to("cpu", F64).contiguous()
     out["conn"] = torch.as_tensor(p["conn"]).detach().to("cpu", torch.int64).contiguous()
     out["fixed"] = torch.as_tensor(p["fixed"]).detach().to("cpu", torch.bool)
+    out["material"] = p.get("material", "neo_hookean")
+    sc = p.get("mat_scalable")
+    out["mat_scalable"] = (torch.ones(out["mat_p"].numel(), dtype=torch.bool) if sc is None
+                           else torch.as_tensor(sc).detach().to("cpu", torch.bool))
     return out
 
 
@@ -35,8 +39,71 @@ def psi(F, p):
 
 
 def element_parameters(theta, P):
-    """p_e = p0 * theta_e on both (scalable) neo-Hookean parameters (materials.py:383-390)."""
-    return P["mat_p"][None, :] * theta[:, None]
+    """p_e = p0 * theta_e on the scalable parameters, p0 on the others (materials.py:239-246)."""
+    factor = torch.where(P["mat_scalable"][None, :], theta[:, None], torch.ones_like(theta)[:, None])
+    return P["mat_p"][None, :] * factor
+
+
+# the other energies of the library (materials.py:65-161), as functions of the 3x3 embedding
+def _det3(F3):
+    return (F3[0, 0] * F3[1, 1] - F3[0, 1] * F3[1, 0]) * F3[2, 2]       # materials.py:51-54
+
+
+def _psi3_neo_hookean(F3, p):
+    lnJ = torch.log(_det3(F3))
+    return 0.5 * p[0] * ((F3 * F3).sum() - 3.0 - 2.0 * lnJ) + 0.5 * p[1] * lnJ ** 2
+
+
+def _psi3_mooney_rivlin(F3, p):
+    C = F3.T @ F3
+    I1 = torch.trace(C)
+    I2 = 0.5 * (I1 ** 2 - torch.trace(C @ C))
+    J = _det3(F3)
+    return p[0] * (J ** (-2.0 / 3.0) * I1 - 3.0) + p[1] * (J ** (-4.0 / 3.0) * I2 - 3.0) + 0.5 * p[2] * torch.log(J) ** 2
+
+
+def _psi3_saint_venant(F3, p):
+    E = 0.5 * (F3.T @ F3 - torch.eye(3, dtype=F3.dtype))
+    return 0.5 * p[1] * torch.trace(E) ** 2 + p[0] * (E * E).sum()
+
+
+def _psi3_demiray(F3, p):
+    lnJ = torch.log(_det3(F3))
+    return p[0] / (2.0 * p[1]) * (torch.exp(p[1] * ((F3 * F3).sum() - 3.0)) - 1.0) - p[0] * lnJ + 0.5 * p[2] * lnJ ** 2
+
+
+def _psi3_fiber_reinforced(F3, p):
+    C = F3.T @ F3
+    I1 = torch.trace(C)
+    beta = torch.deg2rad(p[4])
+    zero = torch.zeros_like(beta)
+    total = _psi3_neo_hookean(F3, p[:2])
+    for k, sign in enumerate((1.0, -1.0)):
+        a = torch.stack([torch.cos(beta), sign * torch.sin(beta), zero])
+        E = p[5] * I1 + (1.0 - 3.0 * p[5]) * (a @ C @ a) - 1.0
+        fib = p[2] / (2.0 * p[3]) * (torch.exp(p[3] * torch.relu(E) ** 2) - 1.0)
+        total = total + (fib if k == 0 else p[6] * fib)
+    return total
+
+
+PSI3 = {"neo_hookean": _psi3_neo_hookean, "mooney_rivlin": _psi3_mooney_rivlin, "saint_venant": _psi3_saint_venant,
+        "demiray": _psi3_demiray, "fiber_reinforced": _psi3_fiber_reinforced}
+
+
+def embed(F):
+    """F3 = [[F, 0], [0, 1]] built with stack, so that every autodiff transform sees through it."""
+    z, o = torch.zeros_like(F[0, 0]), torch.ones_like(F[0, 0])
+    return torch.stack([torch.stack([F[0, 0], F[0, 1], z]), torch.stack([F[1, 0], F[1, 1], z]),
+                        torch.stack([z, z, o])])
+
+
+def energy(P):
+    """psi(F2, p) of the problem's material: the closed neo-Hookean form above, else psi3 of the embedding."""
+    name = P.get("material", "neo_hookean")
+    if name == "neo_hookean":
+        return psi
+    psi3_fn = PSI3[name]
+    return lambda F, p: psi3_fn(embed(F), p)
 
 
 def gather_nodes(u, conn):
@@ -64,7 +131,7 @@ def element_forces(u, theta, P):
     ue = gather_nodes(u, P["conn"])
     F = deformation_gradient(ue, P["dN_dX"])
     pe = element_parameters(theta, P)
-    stress = vmap(vmap(grad(psi), in_dims=(0, None)), in_dims=(0, 0))(F, pe)
+    stress = vmap(vmap(grad(energy(P)), in_dims=(0, None)), in_dims=(0, 0))(F, pe)
     return torch.einsum("eq,eqij,eqaj->eai", P["w_detJ"], stress, P["dN_dX"])
 
 
@@ -78,7 +145,7 @@ def strain_energy(u, theta, P):
     """sum_e sum_q w detJ psi(F_q) (compute_fields' "strain_energy")."""
     F = deformation_gradient(gather_nodes(u, P["conn"]), P["dN_dX"])
     pe = element_parameters(theta, P)
-    dens = vmap(vmap(psi, in_dims=(0, None)), in_dims=(0, 0))(F, pe)
+    dens = vmap(vmap(energy(P), in_dims=(0, None)), in_dims=(0, 0))(F, pe)
     return (dens * P["w_detJ"]).sum()
 
 
@@ -89,7 +156,7 @@ def moduli(u, theta, P):
     """C[e, q] = w detJ * hessian(psi)(F) flattened (ij),(kl) -> 4x4 (_qp_setup, operators.py:316-342)."""
     F = deformation_gradient(gather_nodes(u, P["conn"]), P["dN_dX"])
     pe = element_parameters(theta, P)
-    H = vmap(vmap(hessian(psi), in_dims=(0, None)), in_dims=(0, 0))(F, pe)      # (n_el, n_q, 2, 2, 2, 2)
+    H = vmap(vmap(hessian(energy(P)), in_dims=(0, None)), in_dims=(0, 0))(F, pe)      # (n_el, n_q, 2, 2, 2, 2)
     n_el, n_q = F.shape[:2]
     return (H * P["w_detJ"][:, :, None, None, None, None]).reshape(n_el, n_q, 4, 4)
 
@@ -153,11 +220,12 @@ def jacobi_diagonal(u, theta, P):
     n_el, nen = conn.shape
     ue = gather_nodes(u, conn)
     pe = element_parameters(theta, P)
+    psi_e = energy(P)
     basis = torch.eye(2 * nen, dtype=F64).reshape(2 * nen, nen, 2)
 
     def force(w, dN_e, wd_e, p_e):
         F = torch.eye(2, dtype=F64) + torch.einsum("ai,qaj->qij", w, dN_e)
-        st = vmap(grad(psi), in_dims=(0, None))(F, p_e)
+        st = vmap(grad(psi_e), in_dims=(0, None))(F, p_e)
         return torch.einsum("q,qij,qaj->ai", wd_e, st, dN_e)
 
     def entry(u_e, dN_e, wd_e, p_e, e_vec):
@@ -181,12 +249,13 @@ def block_jacobi(u, theta, P):
     N = P["nodes"].shape[0]
     ue = gather_nodes(u, conn)
     pe = element_parameters(theta, P)
+    psi_e = energy(P)
     basis = torch.eye(2 * nen, dtype=F64).reshape(2 * nen, nen, 2)
     node_of = torch.arange(2 * nen) // 2
 
     def force(w, dN_e, wd_e, p_e):
         F = torch.eye(2, dtype=F64) + torch.einsum("ai,qaj->qij", w, dN_e)
-        st = vmap(grad(psi), in_dims=(0, None))(F, p_e)
+        st = vmap(grad(psi_e), in_dims=(0, None))(F, p_e)
         return torch.einsum("q,qij,qaj->ai", wd_e, st, dN_e)
 
     def column(u_e, dN_e, wd_e, p_e, e_vec, a):
@@ -335,14 +404,7 @@ def compute_sensitivity(P, theta, loss_fn, n_load_steps=5, tol=1e-8, max_newton=
 # ---------------------------------------------------------------------------------------------
 # post-processing (postprocess.py:24-137)
 # ---------------------------------------------------------------------------------------------
-def psi3(F3, p):
-    """The 3D neo-Hookean energy mu/2 (I1 - 3) - mu lnJ + lambda/2 lnJ^2 (materials.py:181-217)."""
-    J = torch.linalg.det(F3)
-    lnJ = torch.log(J)
-    return 0.5 * p[0] * ((F3 * F3).sum() - 3.0) - p[0] * lnJ + 0.5 * p[1] * lnJ ** 2
-
-
-def gauss_point_state(F, p):
+def gauss_point_state(F, p, psi3):
     """[J, sxx, syy, sxy, szz, psi] at one Gauss point: P3 = d psi3 / d F3, sigma = P3 F3^T / J (postprocess.py:24-47)."""
     F3 = torch.cat([torch.cat([F, torch.zeros(2, 1, dtype=F.dtype)], 1),
                     torch.tensor([[0.0, 0.0, 1.0]], dtype=F.dtype)], 0)
@@ -357,7 +419,8 @@ def compute_fields(u, theta, P):
     conn, N = P["conn"], P["nodes"].shape[0]
     F = deformation_gradient(gather_nodes(u, conn), P["dN_dX"])
     pe = element_parameters(theta, P)
-    S = vmap(vmap(gauss_point_state, in_dims=(0, None)), in_dims=(0, 0))(F, pe)        # (n_el, n_q, 6)
+    psi3 = PSI3[P.get("material", "neo_hookean")]
+    S = vmap(vmap(lambda F_, p_: gauss_point_state(F_, p_, psi3), in_dims=(0, None)), in_dims=(0, 0))(F, pe)
     w = P["w_detJ"]
     area = w.sum(1)
     mean = torch.einsum("eq,eqk->ek", w, S) / area[:, None]

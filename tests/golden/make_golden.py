@@ -153,6 +153,72 @@ def plate_case(n, n_steps, tol_rel, name):
          energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])))
 
 
+def material_arrays(p):
+    return dict(arrays(p), material=np.array(p["material"]), mat_scalable=p["mat_scalable"].numpy())
+
+
+def material_operator_case(material, element_type, h, seed, scalable=None):
+    """operator_case's quantities for another material of the library (materials.py:65-186)."""
+    p = problem(element_type, h, material=material)
+    if scalable is not None:
+        p = dict(p, mat_scalable=torch.tensor(scalable))
+    n_el, n = p["conn"].shape[0], p["f"].shape[0]
+    g = torch.Generator().manual_seed(seed)
+    u = 0.04 * h * torch.randn(n, dtype=DT, generator=g) * p["m"]
+    v = torch.randn(n, dtype=DT, generator=g)
+    theta = 0.5 + torch.rand(n_el, dtype=DT, generator=g)
+    C, _ = _qp_setup(u, theta, p)
+    tag = "" if scalable is None else "_partial"
+    save(f"material_{material}{tag}_{element_type}_h{h}", **material_arrays(p), u=u.numpy(), v=v.numpy(),
+         theta=theta.numpy(), C=C.numpy(), Av_qp_ew=make_tangent_operator("qp_ew", u, theta, p)(v).numpy(),
+         R=global_residual(u, theta, p).numpy(), R_half=global_residual(u, theta, p, load_factor=0.5).numpy(),
+         diag=compute_jacobi_diagonal(u, theta, p).numpy(),
+         Minv_block_v=make_block_jacobi_preconditioner(u, theta, p)(v).numpy(),
+         energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])), **fields(u, theta, p))
+
+
+def material_solve_case(material, element_type, h, load, n_steps, tol):
+    """The reference's test_materials.py:67-78 problem: a complete solve with the material, tangent qp."""
+    p = problem(element_type, h, load=load, material=material)
+    theta = torch.ones(p["conn"].shape[0], dtype=DT)
+    u, info = newton_krylov_solve(p, theta, n_steps, tol, verbose=False, tangent="qp")
+    assert info["converged"]
+    save(f"material_solve_{material}_{element_type}_h{h}", **material_arrays(p), theta=theta.numpy(),
+         u_star=u.numpy(), tol=np.array(tol), n_load_steps=np.array(n_steps),
+         total_newton=np.array(info["total_newton"]), total_cg=np.array(info["total_cg"]),
+         energy=np.array(float(compute_fields(u, theta, p)["strain_energy"])), **fields(u, theta, p))
+
+
+def material_sensitivity_case(material, scalable=None):
+    """The reference's test_materials.py:101-114 problem (quad4, h = 1, load (60, 0)) for a material."""
+    p = problem("quad4", 1.0, load=(60.0, 0.0), material=material)
+    if scalable is not None:
+        p = dict(p, mat_scalable=torch.tensor(scalable))
+    n_el = p["conn"].shape[0]
+    theta = 1.0 + 0.2 * torch.sin(torch.arange(n_el, dtype=DT))
+    loss_fn = lambda u: torch.dot(p["f"], u)  # noqa: E731  compliance
+    u, g = compute_sensitivity(p, theta, loss_fn, n_load_steps=2, tol=1e-12)
+    tag = "" if scalable is None else "_partial"
+    save(f"material_sensitivity_{material}{tag}_quad4_h1", **material_arrays(p), theta=theta.numpy(),
+         u_star=u.numpy(), dL_dtheta=g.numpy())
+
+
+OTHER_MATERIALS = ("mooney_rivlin", "saint_venant", "demiray", "fiber_reinforced")
+
+
+def material_cases():
+    for i, mat in enumerate(OTHER_MATERIALS):
+        material_operator_case(mat, "quad4", 0.25, seed=10 + i)
+        material_operator_case(mat, "quad9", 0.5, seed=20 + i)
+        material_operator_case(mat, "tri6", 0.5, seed=30 + i)
+        material_solve_case(mat, "quad4", 0.5, (0.0, -15.0), 3, 1e-9)
+        material_sensitivity_case(mat)
+    # theta scaling only some of the parameters: mu alone (neo-Hookean), mu and k1 (fibre-reinforced)
+    material_operator_case("neo_hookean", "quad4", 0.25, seed=40, scalable=[True, False])
+    material_sensitivity_case("neo_hookean", scalable=[True, False])
+    material_sensitivity_case("fiber_reinforced", scalable=[True, False, True, False, False, False, False])
+
+
 def gradient_case(n, shear, name, adjoint_max_iter=20000):
     """Unit-square cantilever, n x n Q4, theta = exp(0.3 z) seeded, dead tip shear; compliance gradient."""
     spec = default_spec("rectangle", "quad4", 1.0 / n)
@@ -206,6 +272,8 @@ EXTRA = {
                                         preconditioner="block_jacobi"),
                              solve_case("quad9", 0.5, (0.0, -40.0), 3, 1e-9, "solve_quad9_h0.5_cantilever_bj",
                                         preconditioner="block_jacobi")),
+    # the other materials of the library: operators, solves and sensitivities
+    "materials": material_cases,
 }
 
 

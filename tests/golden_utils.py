@@ -22,9 +22,11 @@ def params_from(d, device="cpu"):
     t = lambda k, dt=torch.float64: torch.as_tensor(d[k]).to(dtype=dt, device=device)  # noqa: E731
     conn = t("conn", torch.int64)
     dN = t("dN_dX")
+    scalable = (t("mat_scalable", torch.bool) if "mat_scalable" in d
+                else torch.ones(d["mat_p"].size, dtype=torch.bool, device=device))
     return {"nodes": t("nodes"), "conn": conn, "dN_dX": dN, "w_detJ": t("w_detJ"), "f": t("f"), "m": t("m"),
-            "fixed": t("fixed", torch.bool), "u_D": t("u_D"), "mat_p": t("mat_p"),
-            "mat_scalable": torch.ones(2, dtype=torch.bool, device=device), "material": "neo_hookean",
+            "fixed": t("fixed", torch.bool), "u_D": t("u_D"), "mat_p": t("mat_p"), "mat_scalable": scalable,
+            "material": str(d["material"]) if "material" in d else "neo_hookean",
             "element_type": TYPES[(conn.shape[1], dN.shape[1])]}
 
 

@@ -8,7 +8,7 @@ import torch
 import oracle
 from difffea_b200 import ops
 from difffea_b200.cuda_mesh import cuda_mesh
-from difffea_b200.materials import neo_hookean_parameters
+from difffea_b200.materials import device_material, neo_hookean_parameters
 from difffea_b200.operators import global_residual, make_A_operator_cuda, make_tangent_operator, strain_energy
 from difffea_b200.problem import build_rectangle_problem, to_device
 from golden_utils import golden_names, load, params_from, rel
@@ -132,8 +132,7 @@ def test_custom_ops_are_registered():
     d, p, u, v, th = golden_case("operator_quad4_h0.5_unit")
     mesh = cuda_mesh(p)
     mid = ops.register_mesh(mesh)
-    mu0, lam0 = neo_hookean_parameters(p)
-    C, _ = torch.ops.difffea_b200.qp_moduli(mid, u, th, mu0, lam0, False, False)
+    C, _ = torch.ops.difffea_b200.qp_moduli(mid, u, th, *ops.material_args(device_material(p)), False, False)
     assert rel(torch.ops.difffea_b200.tangent_apply(mid, C, v), d["Av_qp_ew"]) < 1e-11
 
 

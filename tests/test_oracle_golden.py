@@ -11,6 +11,9 @@ from golden_utils import golden_names, load, params_from, rel
 OPERATOR_CASES = golden_names("operator_")
 SOLVE_CASES = golden_names("solve_")
 SENS_CASES = golden_names("sensitivity_")
+MAT_OPERATOR_CASES = [n for n in golden_names("material_") if not n.startswith(("material_solve", "material_sens"))]
+MAT_SOLVE_CASES = golden_names("material_solve_")
+MAT_SENS_CASES = golden_names("material_sensitivity_")
 
 
 @pytest.mark.parametrize("name", OPERATOR_CASES)
@@ -102,3 +105,47 @@ def test_oracle_on_the_gradient_fixture():
     b = P["m"] * P["f"]
     assert float(torch.norm(AT(lam) - b)) <= 1.01e-10 * float(torch.norm(b))
     assert rel(oracle.implicit_vjp(u, th, P, lam), d["dL_dtheta"]) < 1e-12
+
+
+# ---------------------------------------------------------------------------------------------
+# the other materials of the library (materials.py:65-186)
+# ---------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("name", MAT_OPERATOR_CASES)
+def test_oracle_material_operator_quantities_match_reference(name):
+    d = load(name)
+    P = oracle.as_problem(params_from(d))
+    u, v, th = (torch.as_tensor(d[k]) for k in ("u", "v", "theta"))
+    C = oracle.moduli(u, th, P)
+    assert rel(C, d["C"]) < 1e-12
+    assert rel(oracle.apply_qp_ew(C, v, P), d["Av_qp_ew"]) < 1e-12
+    assert rel(oracle.residual(u, th, P), d["R"]) < 1e-12
+    assert rel(oracle.residual(u, th, P, 0.5), d["R_half"]) < 1e-12
+    assert rel(oracle.jacobi_diagonal(u, th, P), d["diag"]) < 1e-12
+    assert rel(oracle.block_jacobi(u, th, P)(v), d["Minv_block_v"]) < 1e-12
+    assert abs(float(oracle.strain_energy(u, th, P)) - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))
+    out = oracle.compute_fields(u, th, P)
+    for k in FIELD_KEYS:
+        assert rel(out[k], d["fields_" + k]) < 1e-12, k
+    assert rel(oracle.support_reactions(u, th, P), d["reactions"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", MAT_SOLVE_CASES)
+def test_oracle_material_solve_matches_reference(name):
+    d = load(name)
+    P = oracle.as_problem(params_from(d))
+    th = torch.as_tensor(d["theta"])
+    u, info = oracle.newton_krylov_solve(P, th, int(d["n_load_steps"]), float(d["tol"]), tangent="qp")
+    assert info["converged"]
+    assert rel(u, d["u_star"]) < 1e-9
+    assert info["total_newton"] == int(d["total_newton"])
+
+
+@pytest.mark.parametrize("name", MAT_SENS_CASES)
+def test_oracle_material_sensitivity_matches_reference(name):
+    d = load(name)
+    P = oracle.as_problem(params_from(d))
+    th = torch.as_tensor(d["theta"])
+    f = P["f"]
+    u, g = oracle.compute_sensitivity(P, th, lambda w: torch.dot(f, w), n_load_steps=2, tol=1e-12)
+    assert rel(u, d["u_star"]) < 1e-9
+    assert rel(g, d["dL_dtheta"]) < 1e-8
