@@ -5,6 +5,7 @@ launches unless ``--no-flush``).
     python -m difffea_b200.microbench sweep                       tangent product: Q4/Q9 x 40k..2.56M x fp64/fp32
     python -m difffea_b200.microbench apply --element quad4 --elements 640000 --precision fp64
     python -m difffea_b200.microbench moduli|residual|sensitivity|fields|pcg --element quad4 --elements 640000
+                                            [--material mooney_rivlin|...|all]
     python -m difffea_b200.microbench solve --element quad4 --nx 256 --precision mixed
                                             one serving request (4:1 cantilever, E 1, nu 0.3, load 0.03)
                                             solved twice; the second solve is timed
@@ -36,7 +37,7 @@ import torch
 
 from difffea_b200 import _lib, ops
 from difffea_b200.cuda_mesh import cuda_mesh, ptr, stream_handle
-from difffea_b200.materials import neo_hookean_parameters
+from difffea_b200.materials import MATERIAL_LIBRARY, device_material
 from difffea_b200.problem import build_rectangle_problem
 
 NEN = {"quad4": 4, "quad9": 9}
@@ -55,12 +56,13 @@ def side_for(n_elements):
 class State:
     """A square n x n mesh of unit cells with a seeded state, its packed mesh and moduli."""
 
-    def __init__(self, element, n_elements, precision="fp64", device="cuda", seed=0, form="colour"):
+    def __init__(self, element, n_elements, precision="fp64", device="cuda", seed=0, form="colour",
+                 material="neo_hookean"):
         n = side_for(n_elements)
         self.form = form
         self.element, self.precision, self.device = element, precision, torch.device(device)
         self.p = build_rectangle_problem(element, n, n, float(n), float(n), E=1.0, nu=0.3, device=device,
-                                         build_on_device=True)
+                                         build_on_device=True, material=material)
         g = torch.Generator().manual_seed(seed)
         N2 = self.p["f"].shape[0]
         self.N2 = N2
@@ -68,7 +70,7 @@ class State:
         self.theta = torch.ones(self.p["conn"].shape[0], dtype=torch.float64, device=device)
         self.mesh = cuda_mesh(self.p)
         self.mid = ops.register_mesh(self.mesh)
-        self.mu0, self.lam0 = neo_hookean_parameters(self.p)
+        self.mat = device_material(self.p)
         fp32_C = precision in ("fp32", "mixed")
         if fp32_C:
             self.mesh.ensure_grad32()
@@ -76,10 +78,11 @@ class State:
             self.mesh.ensure_ref_frame()
             self.C = torch.empty(self.mesh.moduli_numel_ref(), dtype=torch.float32, device=device)
             self.diag = torch.empty(N2, dtype=torch.float64, device=device)
-            _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mu0, self.lam0,
-                      ptr(self.C), _lib.DFEA_F32REF, ptr(self.diag), stream_handle())
+            _lib.call("dfea_qp_moduli_mat", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mat,
+                      ptr(self.C), _lib.DFEA_F32REF, ptr(self.diag), ptr(None), stream_handle())
         else:
-            self.C, self.diag = ops.qp_moduli(self.mid, self.u, self.theta, self.mu0, self.lam0, fp32_C, True)
+            self.C, self.diag = ops.qp_moduli(self.mid, self.u, self.theta, *ops.material_args(self.mat), fp32_C,
+                                              True)
         vt = torch.float32 if precision == "fp32" else torch.float64
         pad = (N2 + 63) // 64 * 64
         self.buf = torch.empty(2 * pad, dtype=vt, device=device)            # [v | y], as the PCG's vectors
@@ -139,21 +142,21 @@ class State:
 
     def moduli(self):
         if self.precision == "ref":
-            _lib.call("dfea_qp_moduli", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mu0, self.lam0,
-                      ptr(self.C), _lib.DFEA_F32REF, ptr(self.diag), stream_handle())
+            _lib.call("dfea_qp_moduli_mat", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mat,
+                      ptr(self.C), _lib.DFEA_F32REF, ptr(self.diag), ptr(None), stream_handle())
         else:
-            ops.qp_moduli(self.mid, self.u, self.theta, self.mu0, self.lam0, self.precision != "fp64", True)
+            ops.qp_moduli(self.mid, self.u, self.theta, *ops.material_args(self.mat), self.precision != "fp64", True)
 
     def residual(self):
-        ops.residual(self.mid, self.u, self.theta, self.mu0, self.lam0, self.p["f"], 1.0)
+        ops.residual(self.mid, self.u, self.theta, *ops.material_args(self.mat), self.p["f"], 1.0)
 
     def sensitivity(self):
-        ops.element_sensitivity(self.mid, self.u, self.v.double(), self.mu0, self.lam0)
+        ops.element_sensitivity(self.mid, self.u, self.v.double(), *ops.material_args(self.mat))
 
     def fields(self):
         if getattr(self, "el_fields", None) is None:
             self.el_fields = torch.empty(7, self.n_el, dtype=torch.float64, device=self.device)
-        _lib.call("dfea_element_fields", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mu0, self.lam0,
+        _lib.call("dfea_element_fields_mat", self.mesh.view_ref, ptr(self.u), ptr(self.theta), self.mat,
                   ptr(self.el_fields), stream_handle())
 
 
@@ -187,10 +190,12 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters=64, pcg_graph=1, form="colour"):
-    st = State(element, n_elements, precision, form=form)
+def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters=64, pcg_graph=1, form="colour",
+            material="neo_hookean"):
+    st = State(element, n_elements, precision, form=form, material=material)
     peak, peak_kind = hbm_peak()
-    row = dict(kernel=kind, element=element, n_el=st.n_el, precision=precision, colours=st.mesh.n_colours, form=form)
+    row = dict(kernel=kind, element=element, n_el=st.n_el, precision=precision, colours=st.mesh.n_colours, form=form,
+               material=material)
     if kind == "pcg":
         from difffea_b200.krylov import DevicePCG
         vt = st.v.dtype
@@ -255,6 +260,9 @@ def main(argv=None):
     ap.add_argument("--form", default=None, choices=("colour", "gather", "fused", "auto"),
                     help="product form: one launch per colour, or element pass + node sums (default: colour; "
                          "for solve, auto = the solver's choice by mesh size)")
+    ap.add_argument("--material", default="neo_hookean", choices=tuple(MATERIAL_LIBRARY) + ("all",),
+                    help="material of the moduli / residual / sensitivity / fields kernels (library defaults); "
+                         "all = every material in turn")
     ap.add_argument("--pcg-graph", type=int, default=None,
                     help="PCG form: 0 direct launches (solve's default), 1 loop graph (pcg's default), "
                          "2 unrolled graph")
@@ -271,9 +279,10 @@ def main(argv=None):
                     print(json.dumps(measure("apply", element, n, prec, a.reps, not a.no_flush, form=a.form or "colour")),
                           flush=True)
         return 0
-    print(json.dumps(measure(a.kind, a.element, a.elements, a.precision, a.reps, not a.no_flush, a.pcg_iters,
-                             1 if a.pcg_graph is None else a.pcg_graph, a.form or "colour")),
-          flush=True)
+    for material in (MATERIAL_LIBRARY if a.material == "all" else (a.material,)):
+        print(json.dumps(measure(a.kind, a.element, a.elements, a.precision, a.reps, not a.no_flush, a.pcg_iters,
+                                 1 if a.pcg_graph is None else a.pcg_graph, a.form or "colour", material)),
+              flush=True)
     return 0
 
 
