@@ -1,0 +1,647 @@
+// dfea_mg.cu -- geometric multigrid on structured quadrilateral grids: the kernels of a V-cycle
+// preconditioner for the PCG of the Newton-Krylov solve.
+//
+// Levels.  Level 0 is the finite-element mesh (Q4, or Q9 whose nodes form a grid refined twice); every
+// coarser level l >= 1 is a Q4 grid of gx x gy cells with bilinear interpolation between levels, each
+// level halving the cell count of the one above it in both directions (a last cell one line wide when
+// the count is odd).  Coarse operators are Galerkin products built element by element: level 1 from
+// the stored Gauss-point moduli of the fine mesh, K_C = sum_{e in C} sum_q (B_q P~)^T C_q (B_q P~), and
+// level l + 1 from level l's 8 x 8 element matrices, K_C = sum P^T K_c P.  P~ zeroes fixed fine DOFs, so
+// a coarse DOF whose whole support is fixed has a zero row and becomes an identity row; the coarse
+// operator equals P~^T A P~ of A = M K M + (I - M) on the free DOFs.
+//
+// Everything here is deterministic: node-centric gathers in a fixed order, single-block reductions.
+#include <cstdio>
+
+#include "dfea_common.cuh"
+
+namespace dfea {
+
+int validate_mesh(const dfea_mesh_view* mv, bool need_grad32);
+
+struct MgGrid {
+    int gx, gy;
+    const int32_t* line_x;
+    const int32_t* line_y;
+    const int32_t* cell_x;
+    const int32_t* cell_y;
+    double* K;
+    uint8_t* fix;
+};
+
+static MgGrid mg_grid(const dfea_mg_grid& g) {
+    return MgGrid{g.gx, g.gy, g.line_x, g.line_y, g.cell_x, g.cell_y, g.K, g.fix};
+}
+
+static int validate_grid(const dfea_mg_grid* g, bool coarse, const char* what) {
+    if (!g || g->gx < 1 || g->gy < 1) return set_error(DFEA_ERR_INVALID, "%s: bad grid", what);
+    if ((int64_t)(g->gx + 1) * (g->gy + 1) >= (int64_t(1) << 30)) return set_error(DFEA_ERR_INVALID, "%s: grid too large", what);
+    if (coarse && (!g->line_x || !g->line_y || !g->cell_x || !g->cell_y))
+        return set_error(DFEA_ERR_INVALID, "%s: a coarse grid needs its line and cell maps", what);
+    return DFEA_OK;
+}
+
+// weight of coarse line c (lines X) at finer line i, for i in [X[c-1], X[c+1]]
+__device__ __forceinline__ double hat(const int32_t* X, int n_lines, int c, int i) {
+    const int xc = X[c];
+    if (i == xc) return 1.0;
+    if (i < xc) {
+        if (c == 0) return 0.0;
+        const int xl = X[c - 1];
+        return i <= xl ? 0.0 : (double)(i - xl) / (double)(xc - xl);
+    }
+    if (c == n_lines - 1) return 0.0;
+    const int xr = X[c + 1];
+    return i >= xr ? 0.0 : (double)(xr - i) / (double)(xr - xc);
+}
+
+// ------------------------------------------------------------------------------------------
+// level 1 from the finite-element mesh: K_C = sum_e sum_q (B_q P~)^T C_q (B_q P~)
+// ------------------------------------------------------------------------------------------
+// MOD 0: FP64 physical moduli (16 per Gauss point) with the mesh gradients; 1: FP32 physical moduli; 2: FP32
+// reference-frame moduli (10 per Gauss point, DFEA_F32REF) with the reference gradients.
+template <int NEN, int NQ, int MOD>
+__global__ void __launch_bounds__(128)
+k_mg_galerkin_fe(Mesh m, const void* __restrict__ moduli, RefGrad<NEN, NQ> rg, const int32_t* __restrict__ node_ij,
+                 const int32_t* __restrict__ cell_slot, int span, int ncy, MgGrid cg) {
+    const int n_cells = cg.gx * cg.gy;
+    const int64_t S = m.stride;
+    for (int C = blockIdx.x * blockDim.x + threadIdx.x; C < n_cells; C += gridDim.x * blockDim.x) {
+        const int CX = C / cg.gy, CY = C % cg.gy;
+        const int x0 = cg.line_x[CX], x1 = cg.line_x[CX + 1], y0 = cg.line_y[CY], y1 = cg.line_y[CY + 1];
+        double K[64];
+#pragma unroll
+        for (int k = 0; k < 64; ++k) K[k] = 0.0;
+#pragma unroll 1
+        for (int fcx = x0 / span; fcx < x1 / span; ++fcx) {
+#pragma unroll 1
+            for (int fcy = y0 / span; fcy < y1 / span; ++fcy) {
+                const int64_t s = cell_slot[(int64_t)fcx * ncy + fcy];
+                double P[NEN][4];
+                int fix[NEN];
+#pragma unroll
+                for (int a = 0; a < NEN; ++a) {
+                    const int c = m.conn[a * S + s];
+                    const int n = c >> 2;
+                    fix[a] = c & 3;
+                    const double wx1 = (double)(node_ij[2 * n] - x0) / (double)(x1 - x0);
+                    const double wy1 = (double)(node_ij[2 * n + 1] - y0) / (double)(y1 - y0);
+                    const double wx0 = 1.0 - wx1, wy0 = 1.0 - wy1;
+                    P[a][0] = wx0 * wy0;
+                    P[a][1] = wx1 * wy0;
+                    P[a][2] = wx1 * wy1;
+                    P[a][3] = wx0 * wy1;
+                }
+#pragma unroll 1
+                for (int q = 0; q < NQ; ++q) {
+                    double g[NEN][2], M[16];
+                    if constexpr (MOD == 2) {
+                        const float* Cf = static_cast<const float*>(moduli);
+                        const int64_t base = (int64_t)q * 10 * S;
+                        const float4 A = reinterpret_cast<const float4*>(Cf + base)[s];
+                        const float4 B = reinterpret_cast<const float4*>(Cf + base + 4 * S)[s];
+                        const float2 D = reinterpret_cast<const float2*>(Cf + base + 8 * S)[s];
+                        const double h[10] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w, D.x, D.y};
+                        // packed upper triangle: (0,0..3) (1,1..3) (2,2..3) (3,3)
+                        M[0] = h[0]; M[1] = h[1]; M[2] = h[2]; M[3] = h[3];
+                        M[5] = h[4]; M[6] = h[5]; M[7] = h[6];
+                        M[10] = h[7]; M[11] = h[8];
+                        M[15] = h[9];
+                        M[4] = M[1]; M[8] = M[2]; M[12] = M[3]; M[9] = M[6]; M[13] = M[7]; M[14] = M[11];
+#pragma unroll
+                        for (int a = 0; a < NEN; ++a) {
+                            g[a][0] = rg.g[q][a][0];
+                            g[a][1] = rg.g[q][a][1];
+                        }
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            if constexpr (MOD == 0) {
+                                double row[4];
+                                load_moduli_row(static_cast<const double*>(moduli), S, q, r, s, row);
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) M[4 * r + c] = row[c];
+                            } else {
+                                float row[4];
+                                load_moduli_row(static_cast<const float*>(moduli), S, q, r, s, row);
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) M[4 * r + c] = row[c];
+                            }
+                        }
+#pragma unroll
+                        for (int a = 0; a < NEN; ++a) {
+                            const double2 t = load_grad(m.grad, (int64_t)(q * NEN + a) * S + s);
+                            g[a][0] = t.x;
+                            g[a][1] = t.y;
+                        }
+                    }
+                    // coarse gradients per component: G[i][b][J] = sum_a P~_(a,i),b dN_a,J
+                    double G[2][4][2];
+#pragma unroll
+                    for (int i = 0; i < 2; ++i)
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                            for (int a = 0; a < NEN; ++a) {
+                                const double w = (fix[a] >> i) & 1 ? 0.0 : P[a][b];
+                                s0 += w * g[a][0];
+                                s1 += w * g[a][1];
+                            }
+                            G[i][b][0] = s0;
+                            G[i][b][1] = s1;
+                        }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+#pragma unroll
+                        for (int k = 0; k < 2; ++k) {
+                            double t[4];
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) t[r] = M[4 * r + 2 * k] * G[k][c][0] + M[4 * r + 2 * k + 1] * G[k][c][1];
+#pragma unroll
+                            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                                for (int i = 0; i < 2; ++i)
+                                    K[(2 * b + i) * 8 + 2 * c + k] += G[i][b][0] * t[2 * i] + G[i][b][1] * t[2 * i + 1];
+                        }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 64; ++k) cg.K[(int64_t)k * n_cells + C] = K[k];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// level l + 1 from level l: K_C = sum_{fine cells c in C} P_c^T K_c P_c
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_mg_galerkin(MgGrid fg, MgGrid cg) {
+    const int n_cells = cg.gx * cg.gy, nf_cells = fg.gx * fg.gy;
+    for (int C = blockIdx.x * blockDim.x + threadIdx.x; C < n_cells; C += gridDim.x * blockDim.x) {
+        const int CX = C / cg.gy, CY = C % cg.gy;
+        const int x0 = cg.line_x[CX], x1 = cg.line_x[CX + 1], y0 = cg.line_y[CY], y1 = cg.line_y[CY + 1];
+        double K[64];
+#pragma unroll
+        for (int k = 0; k < 64; ++k) K[k] = 0.0;
+#pragma unroll 1
+        for (int fx = x0; fx < x1; ++fx) {
+#pragma unroll 1
+            for (int fy = y0; fy < y1; ++fy) {
+                const int fc = fx * fg.gy + fy;
+                // P[a][b]: weight of coarse corner b at fine corner a (corners (0,0) (1,0) (1,1) (0,1))
+                double P[4][4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const int i = fx + ((a == 1 || a == 2) ? 1 : 0), j = fy + ((a >= 2) ? 1 : 0);
+                    const double wx1 = (double)(i - x0) / (double)(x1 - x0), wy1 = (double)(j - y0) / (double)(y1 - y0);
+                    const double wx0 = 1.0 - wx1, wy0 = 1.0 - wy1;
+                    P[a][0] = wx0 * wy0;
+                    P[a][1] = wx1 * wy0;
+                    P[a][2] = wx1 * wy1;
+                    P[a][3] = wx0 * wy1;
+                }
+                // T = K_c P (8 x 8), then K += P^T T; P acts on both components alike
+#pragma unroll 1
+                for (int col = 0; col < 8; ++col) {
+                    const int b = col >> 1, k = col & 1;
+                    double t[8];
+#pragma unroll
+                    for (int row = 0; row < 8; ++row) {
+                        double acc = 0.0;
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) acc += fg.K[(int64_t)(row * 8 + 2 * a + k) * nf_cells + fc] * P[a][b];
+                        t[row] = acc;
+                    }
+#pragma unroll
+                    for (int bb = 0; bb < 4; ++bb)
+#pragma unroll
+                        for (int i = 0; i < 2; ++i) {
+                            double acc = 0.0;
+#pragma unroll
+                            for (int a = 0; a < 4; ++a) acc += P[a][bb] * t[2 * a + i];
+                            K[(2 * bb + i) * 8 + col] += acc;
+                        }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 64; ++k) cg.K[(int64_t)k * n_cells + C] = K[k];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// transfers; gnode maps a grid node of the finer level to its DOF node (level 0: the FE node id, -1 where
+// the grid has no node), NULL for the lexicographic numbering of the coarse levels
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ int fine_node(const int32_t* gnode, int fgy, int i, int j) {
+    const int id = i * (fgy + 1) + j;
+    return gnode ? gnode[id] : id;
+}
+
+// rc = P~^T r (masked at fixed fine DOFs); with fix_out, also the coarse fix bits (a coarse DOF is fixed
+// when every fine DOF it interpolates to is fixed)
+__global__ void k_mg_restrict(MgGrid fg, MgGrid cg, const int32_t* __restrict__ gnode, const uint8_t* __restrict__ ffix,
+                              const double* __restrict__ r, double* __restrict__ rc, uint8_t* __restrict__ fix_out) {
+    const int nx = cg.gx + 1, ny = cg.gy + 1;
+    const double2* r2 = reinterpret_cast<const double2*>(r);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nx * ny; n += gridDim.x * blockDim.x) {
+        const int I = n / ny, J = n % ny;
+        const int ilo = I > 0 ? cg.line_x[I - 1] + 1 : cg.line_x[I], ihi = I < cg.gx ? cg.line_x[I + 1] - 1 : cg.line_x[I];
+        const int jlo = J > 0 ? cg.line_y[J - 1] + 1 : cg.line_y[J], jhi = J < cg.gy ? cg.line_y[J + 1] - 1 : cg.line_y[J];
+        double ax = 0.0, ay = 0.0;
+        int free_bits = 0;
+        for (int i = ilo; i <= ihi; ++i) {
+            const double wx = hat(cg.line_x, nx, I, i);
+            for (int j = jlo; j <= jhi; ++j) {
+                const int id = fine_node(gnode, fg.gy, i, j);
+                if (id < 0) continue;
+                const double w = wx * hat(cg.line_y, ny, J, j);
+                const int f = ffix[id];
+                if (r) {
+                    const double2 t = r2[id];
+                    if (!(f & 1)) ax += w * t.x;
+                    if (!(f & 2)) ay += w * t.y;
+                }
+                if (w > 0.0) free_bits |= (~f) & 3;
+            }
+        }
+        if (rc) reinterpret_cast<double2*>(rc)[n] = make_double2(ax, ay);
+        if (fix_out) fix_out[n] = (uint8_t)((~free_bits) & 3);
+    }
+}
+
+// x += P~ ec (x untouched at fixed fine DOFs)
+__global__ void k_mg_prolong_add(MgGrid fg, MgGrid cg, const int32_t* __restrict__ gnode, const uint8_t* __restrict__ ffix,
+                                 const double* __restrict__ ec, double* __restrict__ x) {
+    const int fnx = fg.gx + 1, fny = fg.gy + 1, cny = cg.gy + 1;
+    const double2* e2 = reinterpret_cast<const double2*>(ec);
+    double2* x2 = reinterpret_cast<double2*>(x);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < fnx * fny; n += gridDim.x * blockDim.x) {
+        const int i = n / fny, j = n % fny;
+        const int id = gnode ? gnode[n] : n;
+        if (id < 0) continue;
+        const int f = ffix[id];
+        if ((f & 3) == 3) continue;
+        const int CX = cg.cell_x[i], CY = cg.cell_y[j];
+        const int x0 = cg.line_x[CX], x1 = cg.line_x[CX + 1], y0 = cg.line_y[CY], y1 = cg.line_y[CY + 1];
+        const double wx1 = (double)(i - x0) / (double)(x1 - x0), wy1 = (double)(j - y0) / (double)(y1 - y0);
+        const double wx0 = 1.0 - wx1, wy0 = 1.0 - wy1;
+        const double2 e00 = e2[CX * cny + CY], e10 = e2[(CX + 1) * cny + CY];
+        const double2 e11 = e2[(CX + 1) * cny + CY + 1], e01 = e2[CX * cny + CY + 1];
+        double2 t = x2[id];
+        if (!(f & 1)) t.x += wx0 * wy0 * e00.x + wx1 * wy0 * e10.x + wx1 * wy1 * e11.x + wx0 * wy1 * e01.x;
+        if (!(f & 2)) t.y += wx0 * wy0 * e00.y + wx1 * wy0 * e10.y + wx1 * wy1 * e11.y + wx0 * wy1 * e01.y;
+        x2[id] = t;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// coarse-level operator: y = K v + (I - M) v (K has zero rows and columns at fixed DOFs); DIAG: diag(A)
+// ------------------------------------------------------------------------------------------
+template <bool DIAG>
+__global__ void __launch_bounds__(256) k_mg_apply(MgGrid g, const double* __restrict__ v, double* __restrict__ y) {
+    const int nx = g.gx + 1, ny = g.gy + 1, n_cells = g.gx * g.gy;
+    const double2* v2 = reinterpret_cast<const double2*>(v);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nx * ny; n += gridDim.x * blockDim.x) {
+        const int I = n / ny, J = n % ny;
+        double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            // cells around the node and the node's corner in each: (I-1,J-1):2 (I,J-1):3 (I,J):0 (I-1,J):1
+            const int CX = (k == 0 || k == 3) ? I - 1 : I, CY = (k <= 1) ? J - 1 : J;
+            const int b = k == 0 ? 2 : k == 1 ? 3 : k == 2 ? 0 : 1;
+            if (CX < 0 || CY < 0 || CX >= g.gx || CY >= g.gy) continue;
+            const int c = CX * g.gy + CY;
+            if (DIAG) {
+                y0 += g.K[(int64_t)((2 * b) * 8 + 2 * b) * n_cells + c];
+                y1 += g.K[(int64_t)((2 * b + 1) * 8 + 2 * b + 1) * n_cells + c];
+            } else {
+                const int cn[4] = {CX * ny + CY, (CX + 1) * ny + CY, (CX + 1) * ny + CY + 1, CX * ny + CY + 1};
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const double2 t = v2[cn[a]];
+                    y0 += g.K[(int64_t)((2 * b) * 8 + 2 * a) * n_cells + c] * t.x +
+                          g.K[(int64_t)((2 * b) * 8 + 2 * a + 1) * n_cells + c] * t.y;
+                    y1 += g.K[(int64_t)((2 * b + 1) * 8 + 2 * a) * n_cells + c] * t.x +
+                          g.K[(int64_t)((2 * b + 1) * 8 + 2 * a + 1) * n_cells + c] * t.y;
+                }
+            }
+        }
+        const int f = g.fix[n];
+        if (DIAG) {
+            y0 = (f & 1) ? 1.0 : y0;
+            y1 = (f & 2) ? 1.0 : y1;
+        } else {
+            const double2 t = v2[n];
+            if (f & 1) y0 += t.x;
+            if (f & 2) y1 += t.y;
+        }
+        reinterpret_cast<double2*>(y)[n] = make_double2(y0, y1);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Chebyshev smoothing steps (the Chebyshev iteration, e.g. Saad, Iterative Methods, Alg. 12.1, with the
+// Jacobi diagonal as preconditioner)
+// ------------------------------------------------------------------------------------------
+__global__ void k_mg_cheb_start(int64_t n, const double* __restrict__ r, const double* __restrict__ diag, double s,
+                                double* __restrict__ d) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = s * r[i] / diag[i];
+}
+
+__global__ void k_mg_cheb_step(int64_t n, double* __restrict__ x, double* __restrict__ r, double* __restrict__ d,
+                               const double* __restrict__ q, const double* __restrict__ diag, double c1, double c2,
+                               int last) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double di = d[i];
+        x[i] += di;
+        const double ri = r[i] - q[i];
+        r[i] = ri;
+        if (!last) d[i] = c1 * di + c2 * ri / diag[i];
+    }
+}
+
+// out[0] = x . y, out[1] = sum x^2 diag (one block, fixed order)
+__global__ void __launch_bounds__(1024) k_mg_dots(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                                  const double* __restrict__ diag, double* __restrict__ out) {
+    double a = 0.0, b = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        a += x[i] * y[i];
+        b += x[i] * x[i] * diag[i];
+    }
+    a = block_sum<1024>(a);
+    b = block_sum<1024>(b);
+    if (threadIdx.x == 0) {
+        out[0] = a;
+        out[1] = b;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Lanczos by Jacobi-preconditioned CG (the extreme eigenvalue of D^-1 A from the CG coefficients): the
+// scalars stay on the device, s = [p.Ap, r.z, -, beta], hist = (alpha_k, beta_k) per step
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_mg_dot(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                                 double* __restrict__ out) {
+    double a = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) a += x[i] * y[i];
+    a = block_sum<1024>(a);
+    if (threadIdx.x == 0) *out = a;
+}
+
+__global__ void k_mg_lanczos_step(int64_t n, const double* __restrict__ q, double* __restrict__ r, double* __restrict__ z,
+                                  const double* __restrict__ diag, const double* __restrict__ s) {
+    const double alpha = s[1] / s[0];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        z[i] = ri / diag[i];
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_mg_lanczos_dot(int64_t n, const double* __restrict__ r, const double* __restrict__ z,
+                                                         double* __restrict__ s, double* __restrict__ hist, int k) {
+    double a = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) a += r[i] * z[i];
+    a = block_sum<1024>(a);
+    if (threadIdx.x == 0) {
+        const double alpha = s[1] / s[0], beta = a / s[1];
+        hist[2 * k] = alpha;
+        hist[2 * k + 1] = beta;
+        s[1] = a;
+        s[3] = beta;
+    }
+}
+
+__global__ void k_mg_lanczos_p(int64_t n, double* __restrict__ p, const double* __restrict__ z, const double* __restrict__ s) {
+    const double beta = s[3];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+// ------------------------------------------------------------------------------------------
+// coarsest level: dense A (assembled in cell order), inverted by Gauss-Jordan (A is SPD: no pivoting)
+// ------------------------------------------------------------------------------------------
+constexpr int kMgDenseMax = 256;  // DOFs
+
+__global__ void __launch_bounds__(1024) k_mg_dense_inverse(MgGrid g, double* __restrict__ A, double* __restrict__ Ainv) {
+    const int ny = g.gy + 1, nn = (g.gx + 1) * ny, n = 2 * nn, n_cells = g.gx * g.gy;
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        A[k] = 0.0;
+        Ainv[k] = (k / n == k % n) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int c = 0; c < n_cells; ++c) {
+        const int CX = c / g.gy, CY = c % g.gy;
+        if (threadIdx.x < 64) {
+            const int row = threadIdx.x >> 3, col = threadIdx.x & 7;
+            const int cn[4] = {CX * ny + CY, (CX + 1) * ny + CY, (CX + 1) * ny + CY + 1, CX * ny + CY + 1};
+            const int R = 2 * cn[row >> 1] + (row & 1), Cc = 2 * cn[col >> 1] + (col & 1);
+            A[R * n + Cc] += g.K[(int64_t)threadIdx.x * n_cells + c];
+        }
+        __syncthreads();
+    }
+    for (int d = threadIdx.x; d < n; d += blockDim.x)
+        if ((g.fix[d >> 1] >> (d & 1)) & 1) A[d * n + d] += 1.0;
+    __syncthreads();
+    __shared__ double fcol[2 * kMgDenseMax];
+    for (int k = 0; k < n; ++k) {
+        const double p = 1.0 / A[k * n + k];
+        __syncthreads();
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            A[k * n + j] *= p;
+            Ainv[k * n + j] *= p;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < n; r += blockDim.x) fcol[r] = A[r * n + k];
+        __syncthreads();
+        for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+            const int r = t / n, j = t % n;
+            if (r == k) continue;
+            const double f = fcol[r];
+            A[r * n + j] -= f * A[k * n + j];
+            Ainv[r * n + j] -= f * Ainv[k * n + j];
+        }
+        __syncthreads();
+    }
+}
+
+// x = Ainv b, one warp per row
+__global__ void k_mg_dense_solve(int n, const double* __restrict__ Ainv, const double* __restrict__ b, double* __restrict__ x) {
+    const int lane = threadIdx.x & 31;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
+        double s = 0.0;
+        for (int j = lane; j < n; j += 32) s += Ainv[(int64_t)r * n + j] * b[j];
+        s = warp_sum(s);
+        if (lane == 0) x[r] = s;
+    }
+}
+
+}  // namespace dfea
+
+using namespace dfea;
+
+extern "C" int dfea_mg_galerkin_fe(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype,
+                                   const int32_t* node_ij, const int32_t* cell_slot, int32_t span,
+                                   const dfea_mg_grid* fine, const dfea_mg_grid* coarse, void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if ((rc = validate_grid(fine, false, "dfea_mg_galerkin_fe")) || (rc = validate_grid(coarse, true, "dfea_mg_galerkin_fe")))
+        return rc;
+    if (!moduli || !node_ij || !cell_slot || !coarse->K) return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin_fe: NULL pointer");
+    if (span != 1 && span != 2) return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin_fe: span must be 1 or 2");
+    if (fine->gx % span || fine->gy % span || (int64_t)(fine->gx / span) * (fine->gy / span) != mesh->n_el)
+        return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin_fe: the grid does not match the mesh's element count");
+    if (moduli_dtype == DFEA_F32REF && !(mesh->nen == 4 || mesh->nen == 9))
+        return set_error(DFEA_ERR_UNSUPPORTED, "dfea_mg_galerkin_fe: quadrilateral grids only");
+    const Mesh m = kernel_mesh(*mesh);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int n_cells = coarse->gx * coarse->gy;
+    const int grid = grid_for(n_cells, 128, 8);
+    const MgGrid cg = mg_grid(*coarse);
+    auto launch = [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        const RefGrad<NEN, NQ> rg = ref_grad_of<NEN, NQ>(*mesh);
+        if (moduli_dtype == DFEA_F64)
+            k_mg_galerkin_fe<NEN, NQ, 0><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, fine->gy / span, cg);
+        else if (moduli_dtype == DFEA_F32)
+            k_mg_galerkin_fe<NEN, NQ, 1><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, fine->gy / span, cg);
+        else if (moduli_dtype == DFEA_F32REF)
+            k_mg_galerkin_fe<NEN, NQ, 2><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, fine->gy / span, cg);
+        else
+            return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin_fe: bad moduli dtype");
+        return DFEA_OK;
+    };
+    if (mesh->nen == 4 && mesh->n_q == 4) rc = launch(IntC<4>{}, IntC<4>{});
+    else if (mesh->nen == 9 && mesh->n_q == 9) rc = launch(IntC<9>{}, IntC<9>{});
+    else return set_error(DFEA_ERR_UNSUPPORTED, "dfea_mg_galerkin_fe: Q4 and Q9 meshes only");
+    if (rc) return rc;
+    note_launches(1);
+    return launch_check("dfea_mg_galerkin_fe");
+}
+
+extern "C" int dfea_mg_galerkin(const dfea_mg_grid* fine, const dfea_mg_grid* coarse, void* stream) {
+    int rc;
+    if ((rc = validate_grid(fine, true, "dfea_mg_galerkin")) || (rc = validate_grid(coarse, true, "dfea_mg_galerkin")))
+        return rc;
+    if (!fine->K || !coarse->K) return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin: NULL element matrices");
+    const int n_cells = coarse->gx * coarse->gy;
+    k_mg_galerkin<<<grid_for(n_cells, 128, 8), 128, 0, static_cast<cudaStream_t>(stream)>>>(mg_grid(*fine), mg_grid(*coarse));
+    note_launches(1);
+    return launch_check("dfea_mg_galerkin");
+}
+
+extern "C" int dfea_mg_restrict(const dfea_mg_grid* fine, const dfea_mg_grid* coarse, const int32_t* gnode,
+                                const uint8_t* fine_fix, const double* r, double* rc_out, uint8_t* coarse_fix_out,
+                                void* stream) {
+    int rc;
+    if ((rc = validate_grid(fine, false, "dfea_mg_restrict")) || (rc = validate_grid(coarse, true, "dfea_mg_restrict")))
+        return rc;
+    if (!fine_fix || (!rc_out && !coarse_fix_out) || (rc_out && !r))
+        return set_error(DFEA_ERR_INVALID, "dfea_mg_restrict: NULL pointer");
+    const int n = (coarse->gx + 1) * (coarse->gy + 1);
+    k_mg_restrict<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+        mg_grid(*fine), mg_grid(*coarse), gnode, fine_fix, r, rc_out, coarse_fix_out);
+    note_launches(1);
+    return launch_check("dfea_mg_restrict");
+}
+
+extern "C" int dfea_mg_prolong_add(const dfea_mg_grid* fine, const dfea_mg_grid* coarse, const int32_t* gnode,
+                                   const uint8_t* fine_fix, const double* ec, double* x, void* stream) {
+    int rc;
+    if ((rc = validate_grid(fine, false, "dfea_mg_prolong_add")) || (rc = validate_grid(coarse, true, "dfea_mg_prolong_add")))
+        return rc;
+    if (!fine_fix || !ec || !x) return set_error(DFEA_ERR_INVALID, "dfea_mg_prolong_add: NULL pointer");
+    const int n = (fine->gx + 1) * (fine->gy + 1);
+    k_mg_prolong_add<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+        mg_grid(*fine), mg_grid(*coarse), gnode, fine_fix, ec, x);
+    note_launches(1);
+    return launch_check("dfea_mg_prolong_add");
+}
+
+extern "C" int dfea_mg_apply(const dfea_mg_grid* grid, const double* v, double* y, void* stream) {
+    int rc = validate_grid(grid, false, "dfea_mg_apply");
+    if (rc) return rc;
+    if (!grid->K || !grid->fix || !y || (v == nullptr)) return set_error(DFEA_ERR_INVALID, "dfea_mg_apply: NULL pointer");
+    const int n = (grid->gx + 1) * (grid->gy + 1);
+    k_mg_apply<false><<<grid_for(n, 256, 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(mg_grid(*grid), v, y);
+    note_launches(1);
+    return launch_check("dfea_mg_apply");
+}
+
+extern "C" int dfea_mg_diag(const dfea_mg_grid* grid, double* diag, void* stream) {
+    int rc = validate_grid(grid, false, "dfea_mg_diag");
+    if (rc) return rc;
+    if (!grid->K || !grid->fix || !diag) return set_error(DFEA_ERR_INVALID, "dfea_mg_diag: NULL pointer");
+    const int n = (grid->gx + 1) * (grid->gy + 1);
+    k_mg_apply<true><<<grid_for(n, 256, 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(mg_grid(*grid), nullptr, diag);
+    note_launches(1);
+    return launch_check("dfea_mg_diag");
+}
+
+extern "C" int dfea_mg_cheb_start(int64_t n, const double* r, const double* diag, double scale, double* d, void* stream) {
+    if (n < 0 || (n > 0 && (!r || !diag || !d))) return set_error(DFEA_ERR_INVALID, "dfea_mg_cheb_start: bad arguments");
+    if (n == 0) return DFEA_OK;
+    k_mg_cheb_start<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, r, diag, scale, d);
+    note_launches(1);
+    return launch_check("dfea_mg_cheb_start");
+}
+
+extern "C" int dfea_mg_cheb_step(int64_t n, double* x, double* r, double* d, const double* q, const double* diag,
+                                 double c1, double c2, int32_t last, void* stream) {
+    if (n < 0 || (n > 0 && (!x || !r || !d || !q || !diag)))
+        return set_error(DFEA_ERR_INVALID, "dfea_mg_cheb_step: bad arguments");
+    if (n == 0) return DFEA_OK;
+    k_mg_cheb_step<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, x, r, d, q, diag, c1,
+                                                                                                    c2, last);
+    note_launches(1);
+    return launch_check("dfea_mg_cheb_step");
+}
+
+extern "C" int dfea_mg_dots(int64_t n, const double* x, const double* y, const double* diag, double* out, void* stream) {
+    if (n < 0 || !x || !y || !diag || !out) return set_error(DFEA_ERR_INVALID, "dfea_mg_dots: bad arguments");
+    k_mg_dots<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(n, x, y, diag, out);
+    note_launches(1);
+    return launch_check("dfea_mg_dots");
+}
+
+extern "C" int64_t dfea_mg_dense_max(void) { return kMgDenseMax; }
+
+extern "C" int dfea_mg_dense_inverse(const dfea_mg_grid* grid, double* work, double* Ainv, void* stream) {
+    int rc = validate_grid(grid, false, "dfea_mg_dense_inverse");
+    if (rc) return rc;
+    const int n = 2 * (grid->gx + 1) * (grid->gy + 1);
+    if (n > kMgDenseMax) return set_error(DFEA_ERR_INVALID, "dfea_mg_dense_inverse: %d DOFs exceed %d", n, kMgDenseMax);
+    if (!grid->K || !grid->fix || !work || !Ainv) return set_error(DFEA_ERR_INVALID, "dfea_mg_dense_inverse: NULL pointer");
+    k_mg_dense_inverse<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(mg_grid(*grid), work, Ainv);
+    note_launches(1);
+    return launch_check("dfea_mg_dense_inverse");
+}
+
+extern "C" int dfea_mg_dense_solve(int32_t n, const double* Ainv, const double* b, double* x, void* stream) {
+    if (n < 1 || n > kMgDenseMax || !Ainv || !b || !x) return set_error(DFEA_ERR_INVALID, "dfea_mg_dense_solve: bad arguments");
+    k_mg_dense_solve<<<(n + 7) / 8, 256, 0, static_cast<cudaStream_t>(stream)>>>(n, Ainv, b, x);
+    note_launches(1);
+    return launch_check("dfea_mg_dense_solve");
+}
+
+extern "C" int dfea_mg_dot(int64_t n, const double* x, const double* y, double* out, void* stream) {
+    if (n < 0 || !x || !y || !out) return set_error(DFEA_ERR_INVALID, "dfea_mg_dot: bad arguments");
+    k_mg_dot<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(n, x, y, out);
+    note_launches(1);
+    return launch_check("dfea_mg_dot");
+}
+
+extern "C" int dfea_mg_lanczos_step(int64_t n, double* p, const double* q, double* r, double* z, const double* diag,
+                                    double* s, double* hist, int32_t k, void* stream) {
+    if (n < 1 || !p || !q || !r || !z || !diag || !s || !hist || k < 0)
+        return set_error(DFEA_ERR_INVALID, "dfea_mg_lanczos_step: bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_mg_dot<<<1, 1024, 0, st>>>(n, p, q, s);
+    k_mg_lanczos_step<<<grid_for(n, kThreads, 8), kThreads, 0, st>>>(n, q, r, z, diag, s);
+    k_mg_lanczos_dot<<<1, 1024, 0, st>>>(n, r, z, s, hist, k);
+    k_mg_lanczos_p<<<grid_for(n, kThreads, 8), kThreads, 0, st>>>(n, p, z, s);
+    note_launches(4);
+    return launch_check("dfea_mg_lanczos_step");
+}

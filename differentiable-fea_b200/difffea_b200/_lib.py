@@ -54,6 +54,14 @@ class MeshView(ctypes.Structure):
     ]
 
 
+class MgGrid(ctypes.Structure):
+    """Mirror of ``dfea_mg_grid``."""
+    _fields_ = [("gx", c_i32), ("gy", c_i32), ("line_x", c_vp), ("line_y", c_vp), ("cell_x", c_vp),
+                ("cell_y", c_vp), ("K", c_vp), ("fix", c_vp)]
+
+
+_MGP = ctypes.POINTER(MgGrid)
+
 _PROTOS = {
     "dfea_last_error": (ctypes.c_char_p, []),
     "dfea_version": (ctypes.c_int, []),
@@ -88,6 +96,21 @@ _PROTOS = {
     "dfea_element_fields": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_vp]),
     "dfea_node_fields": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp]),
     "dfea_internal_force": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_vp]),
+    "dfea_mg_galerkin_fe": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_i32, c_vp, c_vp, c_i32, _MGP, _MGP,
+                                           c_vp]),
+    "dfea_mg_galerkin": (ctypes.c_int, [_MGP, _MGP, c_vp]),
+    "dfea_mg_restrict": (ctypes.c_int, [_MGP, _MGP, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "dfea_mg_prolong_add": (ctypes.c_int, [_MGP, _MGP, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "dfea_mg_apply": (ctypes.c_int, [_MGP, c_vp, c_vp, c_vp]),
+    "dfea_mg_diag": (ctypes.c_int, [_MGP, c_vp, c_vp]),
+    "dfea_mg_cheb_start": (ctypes.c_int, [c_i64, c_vp, c_vp, c_f64, c_vp, c_vp]),
+    "dfea_mg_cheb_step": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_f64, c_f64, c_i32, c_vp]),
+    "dfea_mg_dots": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "dfea_mg_dot": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp]),
+    "dfea_mg_lanczos_step": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp]),
+    "dfea_mg_dense_max": (c_i64, []),
+    "dfea_mg_dense_inverse": (ctypes.c_int, [_MGP, c_vp, c_vp, c_vp]),
+    "dfea_mg_dense_solve": (ctypes.c_int, [c_i32, c_vp, c_vp, c_vp, c_vp]),
     "dfea_batch_create": (ctypes.c_int, [c_i32, c_i32, c_vp]),
     "dfea_batch_destroy": (ctypes.c_int, [c_vp]),
     "dfea_batch_start": (ctypes.c_int, [c_vp, c_vp, c_f64, c_i32, c_vp]),

@@ -223,7 +223,7 @@ def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters
     return row
 
 
-def solve_once(element, nx, precision, pcg_graph, form="auto"):
+def solve_once(element, nx, precision, pcg_graph, form="auto", preconditioner="jacobi"):
     """Wall and device milliseconds of one serving-type request (the second of two identical solves)."""
     import time
     from difffea_b200.serving import Request, solve_request
@@ -236,11 +236,13 @@ def solve_once(element, nx, precision, pcg_graph, form="auto"):
         torch.cuda.synchronize()
         t = time.perf_counter()
         e0.record(s)
-        u, info = solve_request(req, "cuda", precision=prec, pcg_graph=pcg_graph, pcg_form=form)
+        u, info = solve_request(req, "cuda", precision=prec, pcg_graph=pcg_graph, pcg_form=form,
+                                preconditioner=preconditioner)
         e1.record(s)
         torch.cuda.synchronize()
         out = dict(kernel="solve", element=element, nx=nx, n_el=req.n_elements, precision=precision,
-                   pcg_graph=pcg_graph, form=form, newton=info["total_newton"], cg=info["total_cg"],
+                   pcg_graph=pcg_graph, form=form, preconditioner=preconditioner, newton=info["total_newton"],
+                   cg=info["total_cg"],
                    converged=info["converged"], device_ms=e0.elapsed_time(e1),
                    wall_ms=1e3 * (time.perf_counter() - t))
     return out
@@ -263,13 +265,15 @@ def main(argv=None):
     ap.add_argument("--material", default="neo_hookean", choices=tuple(MATERIAL_LIBRARY) + ("all",),
                     help="material of the moduli / residual / sensitivity / fields kernels (library defaults); "
                          "all = every material in turn")
+    ap.add_argument("--preconditioner", default="jacobi", choices=("jacobi", "block_jacobi", "multigrid"),
+                    help="preconditioner of the solve kind")
     ap.add_argument("--pcg-graph", type=int, default=None,
                     help="PCG form: 0 direct launches (solve's default), 1 loop graph (pcg's default), "
                          "2 unrolled graph")
     a = ap.parse_args(argv)
     if a.kind == "solve":
         print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph,
-                                    a.form or "auto")),
+                                    a.form or "auto", a.preconditioner)),
               flush=True)
         return 0
     if a.kind == "sweep":

@@ -5,7 +5,8 @@ Residual, tangent-operator and preconditioner closures on the GPU (the reference
     make_tangent_operator(kind, u, theta, params)               operators.py:415-435, kind "cuda" / "auto"
     make_AT_operator(u, theta, params)                          operators.py:441-471
     compute_jacobi_diagonal / make_jacobi_preconditioner        operators.py:477-570
-    make_preconditioner(kind, u, theta, params)                 operators.py:702-710, "jacobi" / "block_jacobi"
+    make_preconditioner(kind, u, theta, params)                 operators.py:702-710, "jacobi" / "block_jacobi" /
+                                                                "multigrid" (structured quad meshes, multigrid.py)
     make_block_jacobi_preconditioner(u, theta, params)          operators.py:586-625
     precompute_geometry(params)                                 operators.py:85-120
 
@@ -26,7 +27,7 @@ from difffea_b200.problem import precompute_geometry  # noqa: F401  (re-exported
 
 TANGENT_OPERATORS = ("auto", "cuda")
 REFERENCE_TANGENT_VARIANTS = ("jvp", "linearize", "qp", "qp_ew")
-PRECONDITIONERS = ("jacobi", "block_jacobi")
+PRECONDITIONERS = ("jacobi", "block_jacobi", "multigrid")
 
 
 def _prepare(u, theta, params):
@@ -233,10 +234,46 @@ def make_block_jacobi_preconditioner(u, theta, params):
     return CudaBlockJacobiPreconditioner(mesh, compute_block_jacobi(u, theta, params))
 
 
+class CudaMultigridPreconditioner:
+    """r -> one V-cycle of the geometric multigrid of a structured mesh (multigrid.py), set up at (u, theta)."""
+
+    def __init__(self, mg):
+        self.mg = mg
+        self.mesh = mg.mesh
+
+    def __call__(self, r):
+        return self.mg(r.to(torch.float64))
+
+
+_MG = {}
+
+
+def multigrid_for(mesh, params):
+    """The (cached) Multigrid hierarchy of a mesh."""
+    from difffea_b200.multigrid import Multigrid
+    key = id(mesh)
+    hit = _MG.get(key)
+    if hit is None or hit[0]() is not mesh:
+        hit = (weakref.ref(mesh), Multigrid(mesh, params))
+        _MG.clear()
+        _MG[key] = hit
+    return hit[1]
+
+
+def make_multigrid_preconditioner(u, theta, params):
+    A = make_A_operator_cuda(u, theta, params)
+    mg = multigrid_for(A.mesh, params)
+    from difffea_b200 import _lib
+    mg.setup(A.C, _lib.DFEA_F64, A.diag)
+    return CudaMultigridPreconditioner(mg)
+
+
 def make_preconditioner(kind, u, theta, params):
     """Build a preconditioner by name: one of ``PRECONDITIONERS``."""
     if kind == "jacobi":
         return make_jacobi_preconditioner(u, theta, params)
+    if kind == "multigrid":
+        return make_multigrid_preconditioner(u, theta, params)
     if kind == "block_jacobi":
         return make_block_jacobi_preconditioner(u, theta, params)
     if kind == "ilu":

@@ -159,7 +159,8 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
                          max_blocks=max_blocks, preconditioner=preconditioner, batch=batch)
     u, info = newton_krylov_solve(p, th, n_load_steps, tol, verbose=False, workspace=ws, precision=precision,
                                   pcg_max_iter=pcg_max_iter, preconditioner=preconditioner)
-    ws.pcg.close()
+    if ws.pcg is not None:
+        ws.pcg.close()
     return u, info
 
 

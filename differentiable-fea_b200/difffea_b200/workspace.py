@@ -41,8 +41,8 @@ class NewtonWorkspace:
                  preconditioner="jacobi", batch=None):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")
-        if preconditioner not in ("jacobi", "block_jacobi"):
-            raise ValueError("preconditioner must be 'jacobi' or 'block_jacobi'")
+        if preconditioner not in ("jacobi", "block_jacobi", "multigrid"):
+            raise ValueError("preconditioner must be 'jacobi', 'block_jacobi' or 'multigrid'")
         self.preconditioner = preconditioner
         self.params = params
         self.mesh = mesh = cuda_mesh(params)
@@ -83,9 +83,17 @@ class NewtonWorkspace:
         self.batch = batch
         if batch is not None:
             use_graph, pcg_form, max_blocks = 0, "gather", batch.max_blocks
-        self.pcg = DevicePCG(mesh, self.C, self.diag if self.blocks is None else self.blocks, self.b, self.du,
-                             use_graph=use_graph, form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind,
-                             max_blocks=max_blocks, preconditioner=preconditioner)
+        self.mg = None
+        if preconditioner == "multigrid":
+            # geometric multigrid V-cycle (structured meshes) inside a PCG driven from the host
+            from difffea_b200.multigrid import Multigrid
+            self.mg = Multigrid(mesh, params)
+            self.mg_work = torch.empty(4, n, **f64)
+            self.pcg = None
+        else:
+            self.pcg = DevicePCG(mesh, self.C, self.diag if self.blocks is None else self.blocks, self.b, self.du,
+                                 use_graph=use_graph, form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind,
+                                 max_blocks=max_blocks, preconditioner=preconditioner)
         self.work = mesh.reduce_work()
         self.theta = None
         self.n_launch_groups = 0
@@ -111,15 +119,24 @@ class NewtonWorkspace:
         """Kernel (a): moduli C and the preconditioner at u (into the buffers the PCG graph is bound to)."""
         _lib.call("dfea_qp_moduli_mat", self.mesh.view_ref, ptr(u), ptr(self.theta), self.material, ptr(self.C),
                   self.moduli_code, ptr(self.diag), ptr(self.blocks), stream_handle())
+        if self.mg is not None:
+            self.mg.setup(self.C, self.moduli_code, self.diag)
 
     def solve(self, R, rtol, max_iter):
         """du = PCG(A, -R) to relative tolerance rtol; returns (du (FP64 buffer), iterations, status)."""
         torch.neg(R, out=self.b)
-        if self.batch is not None:
+        if self.mg is not None:
+            from difffea_b200.multigrid import mg_pcg
+            iters, status = mg_pcg(self._apply, self.mg, self.b, self.du, rtol, max_iter, self.mg_work)
+        elif self.batch is not None:
             iters, status = self.batch.solve(self.pcg, rtol, max_iter)
         else:
             iters, status = self.pcg.solve(rtol, max_iter)
         return self.du, iters, status
+
+    def _apply(self, v, y):
+        _lib.call("dfea_tangent_apply", self.mesh.view_ref, ptr(self.C), self.moduli_code, ptr(v), ptr(y),
+                  _lib.DFEA_F64, stream_handle())
 
     def trial(self, u, alpha, du, out):
         _lib.call("dfea_add_scaled", self.mesh.n_dof, ptr(u), float(alpha), ptr(du), ptr(out), stream_handle())

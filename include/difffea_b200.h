@@ -279,6 +279,69 @@ int dfea_element_sensitivity(const dfea_mesh_view* mesh, const double* u, const 
 int dfea_element_sensitivity_mat(const dfea_mesh_view* mesh, const double* u, const double* lam,
                                  const dfea_material* material, double* g, void* stream);
 
+/* ---------------------------------------------------------------- multigrid ------------------- */
+/*
+ * Geometric multigrid on structured quadrilateral grids: the kernels of a V-cycle preconditioner
+ * (preconditioner="multigrid"; the reference lists a scalable preconditioner as its main open item,
+ * docs/ROADMAP.md:11).  Level 0 is the finite-element mesh, described as a grid of gx x gy node-grid
+ * cells (Q4: the element grid; Q9: the element grid refined twice) with node_ij (2N int32, the grid
+ * position of every FE node), gnode ((gx+1)(gy+1) int32, the FE node at every grid node) and
+ * cell_slot (one int32 per element cell, the element's packed slot; element cell (cx, cy) spans grid
+ * nodes [span cx, span cx + span] x [span cy, span cy + span]).  Every coarser level is a Q4 grid whose
+ * grid lines sit on lines of the level above (line_x / line_y) with bilinear interpolation between them;
+ * its nodes are numbered i * (gy + 1) + j and its cells cx * gy + cy; its operator is stored as one
+ * 8 x 8 Galerkin element matrix per cell (K: [64][gx gy], DOF order 2 corner + component, corners
+ * (0,0) (1,0) (1,1) (0,1)) plus fix bits per node (identity rows).  All device pointers.
+ */
+typedef struct dfea_mg_grid {
+    int32_t gx, gy;         /* cells; nodes (gx + 1) x (gy + 1)                                     */
+    const int32_t* line_x;  /* [gx + 1]: the grid line of the finer level under each line (coarse)  */
+    const int32_t* line_y;  /* [gy + 1]                                                              */
+    const int32_t* cell_x;  /* [finer gx + 1]: the cell of this level holding each finer line        */
+    const int32_t* cell_y;  /* [finer gy + 1]                                                        */
+    double* K;              /* [64][gx * gy] element matrices (coarse levels)                        */
+    uint8_t* fix;           /* [(gx + 1) (gy + 1)] fix bits (coarse levels)                          */
+} dfea_mg_grid;
+
+/* Level 1 from the stored moduli (DFEA_F64, DFEA_F32 or DFEA_F32REF) of a Q4 or Q9 mesh: coarse->K. */
+int dfea_mg_galerkin_fe(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype,
+                        const int32_t* node_ij, const int32_t* cell_slot, int32_t span,
+                        const dfea_mg_grid* fine, const dfea_mg_grid* coarse, void* stream);
+/* Level l + 1 from level l (l >= 1): coarse->K = sum over fine cells of P^T K P. */
+int dfea_mg_galerkin(const dfea_mg_grid* fine, const dfea_mg_grid* coarse, void* stream);
+/* rc = P~^T r, P~ the interpolation with fixed fine DOFs zeroed (r, rc may be NULL); coarse_fix_out
+ * (optional) receives the coarse fix bits.  gnode: level 0's grid-to-FE-node map, NULL on coarse levels;
+ * fine_fix: the fine level's fix bits per DOF node (level 0: the mesh's node_fix). */
+int dfea_mg_restrict(const dfea_mg_grid* fine, const dfea_mg_grid* coarse, const int32_t* gnode,
+                     const uint8_t* fine_fix, const double* r, double* rc, uint8_t* coarse_fix_out,
+                     void* stream);
+/* x += P~ ec. */
+int dfea_mg_prolong_add(const dfea_mg_grid* fine, const dfea_mg_grid* coarse, const int32_t* gnode,
+                        const uint8_t* fine_fix, const double* ec, double* x, void* stream);
+/* y = K v + (I - M) v on a coarse level; dfea_mg_diag: its diagonal. */
+int dfea_mg_apply(const dfea_mg_grid* grid, const double* v, double* y, void* stream);
+int dfea_mg_diag(const dfea_mg_grid* grid, double* diag, void* stream);
+/* Chebyshev smoothing (Jacobi-preconditioned Chebyshev iteration): d = scale r / diag; and one step
+ * x += d, r -= q (q = A d), then unless last d = c1 d + c2 r / diag. */
+int dfea_mg_cheb_start(int64_t n, const double* r, const double* diag, double scale, double* d, void* stream);
+int dfea_mg_cheb_step(int64_t n, double* x, double* r, double* d, const double* q, const double* diag,
+                      double c1, double c2, int32_t last, void* stream);
+/* out[0] = x . y, out[1] = sum x_i^2 diag_i (device, fixed order). */
+int dfea_mg_dots(int64_t n, const double* x, const double* y, const double* diag, double* out, void* stream);
+/* Lanczos for lambda_max(D^-1 A) by Jacobi-preconditioned CG, scalars on the device: *out = x . y; and
+ * after q = A p, one CG step: s[0] = p.q, alpha = s[1] / s[0], r -= alpha q, z = r / diag,
+ * beta = r.z / s[1], p = z + beta p, s[1] = r.z, s[3] = beta, (alpha, beta) into hist[2k], hist[2k+1].
+ * Start: r = b, z = r / diag, p = z, s[1] = r.z.  The eigenvalues of the tridiagonal matrix of the
+ * coefficients approximate those of D^-1 A (Saad, Iterative Methods, section 6.7). */
+int dfea_mg_dot(int64_t n, const double* x, const double* y, double* out, void* stream);
+int dfea_mg_lanczos_step(int64_t n, double* p, const double* q, double* r, double* z, const double* diag,
+                         double* s, double* hist, int32_t k, void* stream);
+/* Coarsest level: the dense inverse of its operator (at most dfea_mg_dense_max() DOFs; work and Ainv
+ * hold n x n doubles each), and x = Ainv b. */
+int64_t dfea_mg_dense_max(void);
+int dfea_mg_dense_inverse(const dfea_mg_grid* grid, double* work, double* Ainv, void* stream);
+int dfea_mg_dense_solve(int32_t n, const double* Ainv, const double* b, double* x, void* stream);
+
 /* ---------------------------------------------------------------- kernel (c): PCG ------------- */
 
 typedef struct dfea_pcg dfea_pcg; /* opaque: a captured CUDA graph of one PCG iteration */
