@@ -6,7 +6,8 @@ Benchmark of the matrix-free Newton-Krylov hot path on B200.
 Workload "serve" (default): the seeded 2,000-request serving stream -- 4:1 cantilever bars, nx uniform
 over the multiples of 4 in [16, 512], Q4/Q9 50/50, E log-uniform in [0.5, 2], nu uniform in [0.2, 0.45],
 axial dead traction uniform in [0.01, 0.05] (strain ~ load / E), 1 load step, Newton tol 1e-10 ||f||,
-Jacobi-PCG (Eisenstat-Walker forcing, cap 5000).  One step = 32 consecutive requests of the stream; the
+PCG with Eisenstat-Walker forcing (cap 5000), preconditioned by geometric multigrid for requests of at
+least 2,500 nodes and by Jacobi below (serving.preconditioner_for).  One step = 32 consecutive requests of the stream; the
 K steps of the timed window are served continuously by the engine (24 slots, FP32 reference-frame
 operator / FP64 Newton and Krylov vectors, the largest waiting request first); value = requests/s over
 all ranks (each rank serves its own shard of the stream: replicas, weak scaling), device-timed with CUDA
@@ -364,7 +365,8 @@ def run_serve(args):
                "data": "synthetic (seeded request stream)",
                "config": {"workload": "serve: seeded 2000-request stream of 4:1 cantilever bars (nx 16..512, Q4/Q9, "
                                       "E 0.5..2, nu 0.2..0.45, axial load 0.01..0.05), 1 load step, tol 1e-10 ||f||, "
-                                      f"PCG cap 5000; {B} requests per step ({len(timed)} served continuously, "
+                                      "PCG cap 5000, multigrid-preconditioned from 2500 nodes, Jacobi below; "
+                                      f"{B} requests per step ({len(timed)} served continuously, "
                                       f"largest waiting request first), {SERVE['slots']} slots",
                           "parallelism": f"replicas x{world} (stream sharded by request id)",
                           "l2": "roofline leg inputs 2.2 GB > 126 MB L2; serving working sets stream from HBM"},
@@ -378,7 +380,9 @@ def run_serve(args):
                "serving_hbm": {"achieved_gbs": pcg_bytes / (total_ms * 1e-3) / 1e9,
                                "frac": pcg_bytes / (total_ms * 1e-3) / 1e9 / hbm,
                                "pcg_iterations": int(sum(r.cg for r in results)),
-                               "bytes": "serving.pcg_iteration_bytes x PCG iterations, over the timed window"},
+                               "bytes": "serving.pcg_iteration_bytes x PCG iterations, over the timed window (the "
+                                        "operator's bytes per iteration; a multigrid iteration moves more: its "
+                                        "cycle's products and transfers are not counted)"},
                "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99), "requests": len(lat),
                               "arrival_rate_per_s": rate},
                "roofline": {"bound": "hbm", "achieved": roof["gbs"], "peak": hbm, "unit": "GB/s",

@@ -11,6 +11,7 @@
 // operator equals P~^T A P~ of A = M K M + (I - M) on the free DOFs.
 //
 // Everything here is deterministic: node-centric gathers in a fixed order, single-block reductions.
+#include <cmath>
 #include <cstdio>
 
 #include "dfea_common.cuh"
@@ -344,15 +345,19 @@ __global__ void __launch_bounds__(256) k_mg_apply(MgGrid g, const double* __rest
 // Chebyshev smoothing steps (the Chebyshev iteration, e.g. Saad, Iterative Methods, Alg. 12.1, with the
 // Jacobi diagonal as preconditioner)
 // ------------------------------------------------------------------------------------------
-__global__ void k_mg_cheb_start(int64_t n, const double* __restrict__ r, const double* __restrict__ diag, double s,
-                                double* __restrict__ d) {
+// the coefficients are read from device memory, so a captured cycle follows them from one linearisation
+// to the next
+__global__ void k_mg_cheb_start(int64_t n, const double* __restrict__ r, const double* __restrict__ diag,
+                                const double* __restrict__ scale, double* __restrict__ d) {
+    const double s = *scale;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         d[i] = s * r[i] / diag[i];
 }
 
 __global__ void k_mg_cheb_step(int64_t n, double* __restrict__ x, double* __restrict__ r, double* __restrict__ d,
-                               const double* __restrict__ q, const double* __restrict__ diag, double c1, double c2,
-                               int last) {
+                               const double* __restrict__ q, const double* __restrict__ diag,
+                               const double* __restrict__ c, int last) {
+    const double c1 = last ? 0.0 : c[0], c2 = last ? 0.0 : c[1];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double di = d[i];
         x[i] += di;
@@ -362,32 +367,47 @@ __global__ void k_mg_cheb_step(int64_t n, double* __restrict__ x, double* __rest
     }
 }
 
-// out[0] = x . y, out[1] = sum x^2 diag (one block, fixed order)
-__global__ void __launch_bounds__(1024) k_mg_dots(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
-                                                  const double* __restrict__ diag, double* __restrict__ out) {
-    double a = 0.0, b = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-        a += x[i] * y[i];
-        b += x[i] * x[i] * diag[i];
-    }
-    a = block_sum<1024>(a);
-    b = block_sum<1024>(b);
-    if (threadIdx.x == 0) {
-        out[0] = a;
-        out[1] = b;
-    }
-}
-
 // ------------------------------------------------------------------------------------------
 // Lanczos by Jacobi-preconditioned CG (the extreme eigenvalue of D^-1 A from the CG coefficients): the
 // scalars stay on the device, s = [p.Ap, r.z, -, beta], hist = (alpha_k, beta_k) per step
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_mg_dot(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
-                                                 double* __restrict__ out) {
+// Dot products in two fixed-order passes: per-block partial sums (the block count depends on n only), then
+// one block adds them in block order.
+constexpr int kMgDotBlocks = 296;
+constexpr int kMgDotThreads = 256;
+
+static int mg_dot_blocks(int64_t n) {
+    const int64_t b = (n + 4 * kMgDotThreads - 1) / (4 * kMgDotThreads);
+    return (int)(b < 1 ? 1 : (b > kMgDotBlocks ? kMgDotBlocks : b));
+}
+
+__global__ void __launch_bounds__(kMgDotThreads) k_mg_dot_part(int64_t n, const double* __restrict__ x,
+                                                                const double* __restrict__ y, double* __restrict__ part) {
     double a = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) a += x[i] * y[i];
-    a = block_sum<1024>(a);
-    if (threadIdx.x == 0) *out = a;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a += x[i] * y[i];
+    a = block_sum<kMgDotThreads>(a);
+    if (threadIdx.x == 0) part[blockIdx.x] = a;
+}
+
+// LANCZOS: the sum is r.z of a CG step: alpha = s[1] / s[0], beta = sum / s[1] into hist, s[1] = sum, s[3] = beta
+template <bool LANCZOS>
+__global__ void __launch_bounds__(kMgDotThreads) k_mg_dot_final(int nb, const double* __restrict__ part,
+                                                                 double* __restrict__ out, double* __restrict__ hist, int k) {
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) a += part[b];
+    a = block_sum<kMgDotThreads>(a);
+    if (threadIdx.x == 0) {
+        if (LANCZOS) {
+            const double alpha = out[1] / out[0], beta = a / out[1];
+            hist[2 * k] = alpha;
+            hist[2 * k + 1] = beta;
+            out[1] = a;
+            out[3] = beta;
+        } else {
+            *out = a;
+        }
+    }
 }
 
 __global__ void k_mg_lanczos_step(int64_t n, const double* __restrict__ q, double* __restrict__ r, double* __restrict__ z,
@@ -400,20 +420,6 @@ __global__ void k_mg_lanczos_step(int64_t n, const double* __restrict__ q, doubl
     }
 }
 
-__global__ void __launch_bounds__(1024) k_mg_lanczos_dot(int64_t n, const double* __restrict__ r, const double* __restrict__ z,
-                                                         double* __restrict__ s, double* __restrict__ hist, int k) {
-    double a = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) a += r[i] * z[i];
-    a = block_sum<1024>(a);
-    if (threadIdx.x == 0) {
-        const double alpha = s[1] / s[0], beta = a / s[1];
-        hist[2 * k] = alpha;
-        hist[2 * k + 1] = beta;
-        s[1] = a;
-        s[3] = beta;
-    }
-}
-
 __global__ void k_mg_lanczos_p(int64_t n, double* __restrict__ p, const double* __restrict__ z, const double* __restrict__ s) {
     const double beta = s[3];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -423,10 +429,19 @@ __global__ void k_mg_lanczos_p(int64_t n, double* __restrict__ p, const double* 
 // ------------------------------------------------------------------------------------------
 // coarsest level: dense A (assembled in cell order), inverted by Gauss-Jordan (A is SPD: no pivoting)
 // ------------------------------------------------------------------------------------------
-constexpr int kMgDenseMax = 256;  // DOFs
+constexpr int kMgDenseMax = 256;     // DOFs
+constexpr int kMgDenseShared = 112;  // up to this many DOFs A, Ainv and the pivot column live in shared memory
 
-__global__ void __launch_bounds__(1024) k_mg_dense_inverse(MgGrid g, double* __restrict__ A, double* __restrict__ Ainv) {
+// SHARED: A and Ainv in dynamic shared memory (copied to Ainv_out at the end), else in global memory
+template <bool SHARED>
+__global__ void __launch_bounds__(1024) k_mg_dense_inverse(MgGrid g, double* __restrict__ A_glob, double* __restrict__ Ainv_out) {
+    extern __shared__ double dense_sm[];
     const int ny = g.gy + 1, nn = (g.gx + 1) * ny, n = 2 * nn, n_cells = g.gx * g.gy;
+    double* A = SHARED ? dense_sm : A_glob;
+    double* Ainv = SHARED ? dense_sm + n * n : Ainv_out;
+    double* fcol = SHARED ? dense_sm + 2 * n * n : nullptr;
+    __shared__ double fcol_glob[SHARED ? 1 : 2 * kMgDenseMax];
+    if (!SHARED) fcol = fcol_glob;
     for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
         A[k] = 0.0;
         Ainv[k] = (k / n == k % n) ? 1.0 : 0.0;
@@ -445,7 +460,6 @@ __global__ void __launch_bounds__(1024) k_mg_dense_inverse(MgGrid g, double* __r
     for (int d = threadIdx.x; d < n; d += blockDim.x)
         if ((g.fix[d >> 1] >> (d & 1)) & 1) A[d * n + d] += 1.0;
     __syncthreads();
-    __shared__ double fcol[2 * kMgDenseMax];
     for (int k = 0; k < n; ++k) {
         const double p = 1.0 / A[k * n + k];
         __syncthreads();
@@ -465,6 +479,8 @@ __global__ void __launch_bounds__(1024) k_mg_dense_inverse(MgGrid g, double* __r
         }
         __syncthreads();
     }
+    if (SHARED)
+        for (int t = threadIdx.x; t < n * n; t += blockDim.x) Ainv_out[t] = Ainv[t];
 }
 
 // x = Ainv b, one warp per row
@@ -580,8 +596,9 @@ extern "C" int dfea_mg_diag(const dfea_mg_grid* grid, double* diag, void* stream
     return launch_check("dfea_mg_diag");
 }
 
-extern "C" int dfea_mg_cheb_start(int64_t n, const double* r, const double* diag, double scale, double* d, void* stream) {
-    if (n < 0 || (n > 0 && (!r || !diag || !d))) return set_error(DFEA_ERR_INVALID, "dfea_mg_cheb_start: bad arguments");
+extern "C" int dfea_mg_cheb_start(int64_t n, const double* r, const double* diag, const double* scale, double* d,
+                                  void* stream) {
+    if (n < 0 || (n > 0 && (!r || !diag || !d || !scale))) return set_error(DFEA_ERR_INVALID, "dfea_mg_cheb_start: bad arguments");
     if (n == 0) return DFEA_OK;
     k_mg_cheb_start<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, r, diag, scale, d);
     note_launches(1);
@@ -589,21 +606,14 @@ extern "C" int dfea_mg_cheb_start(int64_t n, const double* r, const double* diag
 }
 
 extern "C" int dfea_mg_cheb_step(int64_t n, double* x, double* r, double* d, const double* q, const double* diag,
-                                 double c1, double c2, int32_t last, void* stream) {
-    if (n < 0 || (n > 0 && (!x || !r || !d || !q || !diag)))
+                                 const double* c, int32_t last, void* stream) {
+    if (n < 0 || (n > 0 && (!x || !r || !d || !q || !diag || (!last && !c))))
         return set_error(DFEA_ERR_INVALID, "dfea_mg_cheb_step: bad arguments");
     if (n == 0) return DFEA_OK;
-    k_mg_cheb_step<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, x, r, d, q, diag, c1,
-                                                                                                    c2, last);
+    k_mg_cheb_step<<<grid_for(n, kThreads, 8), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, x, r, d, q, diag, c,
+                                                                                                    last);
     note_launches(1);
     return launch_check("dfea_mg_cheb_step");
-}
-
-extern "C" int dfea_mg_dots(int64_t n, const double* x, const double* y, const double* diag, double* out, void* stream) {
-    if (n < 0 || !x || !y || !diag || !out) return set_error(DFEA_ERR_INVALID, "dfea_mg_dots: bad arguments");
-    k_mg_dots<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(n, x, y, diag, out);
-    note_launches(1);
-    return launch_check("dfea_mg_dots");
 }
 
 extern "C" int64_t dfea_mg_dense_max(void) { return kMgDenseMax; }
@@ -614,7 +624,21 @@ extern "C" int dfea_mg_dense_inverse(const dfea_mg_grid* grid, double* work, dou
     const int n = 2 * (grid->gx + 1) * (grid->gy + 1);
     if (n > kMgDenseMax) return set_error(DFEA_ERR_INVALID, "dfea_mg_dense_inverse: %d DOFs exceed %d", n, kMgDenseMax);
     if (!grid->K || !grid->fix || !work || !Ainv) return set_error(DFEA_ERR_INVALID, "dfea_mg_dense_inverse: NULL pointer");
-    k_mg_dense_inverse<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(mg_grid(*grid), work, Ainv);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n <= kMgDenseShared) {
+        const size_t smem = (size_t)(2 * n * n + n) * sizeof(double);
+        static bool attr_set = false;  // the attribute is a property of the function, set once per process
+        if (!attr_set) {
+            rc = check_cuda(cudaFuncSetAttribute(k_mg_dense_inverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)((2 * kMgDenseShared * kMgDenseShared + kMgDenseShared) * sizeof(double))),
+                            "cudaFuncSetAttribute");
+            if (rc) return rc;
+            attr_set = true;
+        }
+        k_mg_dense_inverse<true><<<1, 1024, smem, st>>>(mg_grid(*grid), work, Ainv);
+    } else {
+        k_mg_dense_inverse<false><<<1, 1024, 0, st>>>(mg_grid(*grid), work, Ainv);
+    }
     note_launches(1);
     return launch_check("dfea_mg_dense_inverse");
 }
@@ -626,22 +650,295 @@ extern "C" int dfea_mg_dense_solve(int32_t n, const double* Ainv, const double* 
     return launch_check("dfea_mg_dense_solve");
 }
 
-extern "C" int dfea_mg_dot(int64_t n, const double* x, const double* y, double* out, void* stream) {
-    if (n < 0 || !x || !y || !out) return set_error(DFEA_ERR_INVALID, "dfea_mg_dot: bad arguments");
-    k_mg_dot<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(n, x, y, out);
-    note_launches(1);
+extern "C" int64_t dfea_mg_dot_work(void) { return kMgDotBlocks; }
+
+extern "C" int dfea_mg_dot(int64_t n, const double* x, const double* y, double* out, double* work, void* stream) {
+    if (n < 0 || !x || !y || !out || !work) return set_error(DFEA_ERR_INVALID, "dfea_mg_dot: bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nb = mg_dot_blocks(n);
+    k_mg_dot_part<<<nb, kMgDotThreads, 0, st>>>(n, x, y, work);
+    k_mg_dot_final<false><<<1, kMgDotThreads, 0, st>>>(nb, work, out, nullptr, 0);
+    note_launches(2);
     return launch_check("dfea_mg_dot");
 }
 
 extern "C" int dfea_mg_lanczos_step(int64_t n, double* p, const double* q, double* r, double* z, const double* diag,
-                                    double* s, double* hist, int32_t k, void* stream) {
-    if (n < 1 || !p || !q || !r || !z || !diag || !s || !hist || k < 0)
+                                    double* s, double* hist, int32_t k, double* work, void* stream) {
+    if (n < 1 || !p || !q || !r || !z || !diag || !s || !hist || k < 0 || !work)
         return set_error(DFEA_ERR_INVALID, "dfea_mg_lanczos_step: bad arguments");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    k_mg_dot<<<1, 1024, 0, st>>>(n, p, q, s);
+    const int nb = mg_dot_blocks(n);
+    k_mg_dot_part<<<nb, kMgDotThreads, 0, st>>>(n, p, q, work);
+    k_mg_dot_final<false><<<1, kMgDotThreads, 0, st>>>(nb, work, s, nullptr, 0);
     k_mg_lanczos_step<<<grid_for(n, kThreads, 8), kThreads, 0, st>>>(n, q, r, z, diag, s);
-    k_mg_lanczos_dot<<<1, 1024, 0, st>>>(n, r, z, s, hist, k);
+    k_mg_dot_part<<<nb, kMgDotThreads, 0, st>>>(n, r, z, work);
+    k_mg_dot_final<true><<<1, kMgDotThreads, 0, st>>>(nb, work, s, hist, k);
     k_mg_lanczos_p<<<grid_for(n, kThreads, 8), kThreads, 0, st>>>(n, p, z, s);
-    note_launches(4);
+    note_launches(6);
     return launch_check("dfea_mg_lanczos_step");
+}
+
+// ------------------------------------------------------------------------------------------
+// the C++ driver: set-up, V-cycle, PCG
+// ------------------------------------------------------------------------------------------
+namespace dfea {
+
+__global__ void k_mg_start(int64_t n, double* __restrict__ r) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        r[i] = sin((double)(i + 1));
+}
+
+__global__ void k_mg_div(int64_t n, const double* __restrict__ r, const double* __restrict__ diag, double* __restrict__ z) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        z[i] = r[i] / diag[i];
+}
+
+// Largest eigenvalue of the symmetric tridiagonal matrix (diagonal a, off-diagonal e) by bisection on the
+// Sturm sequence count (number of eigenvalues below x), from the Gershgorin upper bound.
+static double tridiag_max_eig(const double* a, const double* e, int m) {
+    double lo = a[0], hi = a[0];
+    for (int i = 0; i < m; ++i) {
+        const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < m ? fabs(e[i]) : 0.0);
+        lo = fmin(lo, a[i] - r);
+        hi = fmax(hi, a[i] + r);
+    }
+    auto below = [&](double x) {
+        int c = 0;
+        double d = 1.0;
+        for (int i = 0; i < m; ++i) {
+            d = a[i] - x - (i > 0 ? e[i - 1] * e[i - 1] / d : 0.0);
+            if (d == 0.0) d = -1e-300;
+            if (d < 0.0) ++c;
+        }
+        return c;
+    };
+    for (int it = 0; it < 200 && hi - lo > 1e-14 * fmax(1.0, fabs(hi)); ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (below(mid) >= m) hi = mid;   // every eigenvalue is below mid
+        else lo = mid;
+    }
+    return hi;
+}
+
+// lambda_max of D^-1 A from Jacobi-CG coefficients (alpha_k, beta_k), over the prefix before a breakdown
+static double ritz_max(const double* hist, int steps) {
+    double a[64], e[64];
+    int m = 0;
+    for (; m < steps && m < 64; ++m) {
+        const double al = hist[2 * m], be = hist[2 * m + 1];
+        if (!(std::isfinite(al) && al > 0.0 && std::isfinite(be) && be >= 0.0)) break;
+    }
+    if (m == 0) return 2.5;
+    for (int k = 0; k < m; ++k) {
+        a[k] = 1.0 / hist[2 * k] + (k > 0 ? hist[2 * k - 1] / hist[2 * k - 2] : 0.0);
+        if (k + 1 < m) e[k] = sqrt(hist[2 * k + 1]) / hist[2 * k];
+    }
+    return tridiag_max_eig(a, e, m);
+}
+
+static void transfer_args(const dfea_mesh_view* mesh, const dfea_mg* mg, int l, const int32_t** gnode,
+                          const uint8_t** ffix) {
+    *gnode = l == 0 ? mg->gnode : nullptr;
+    *ffix = l == 0 ? mesh->node_fix : mg->level[l].grid.fix;
+}
+
+static int mg_apply(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, int l,
+                    const double* v, double* y, cudaStream_t s) {
+    if (l == 0) return dfea_tangent_apply(mesh, moduli, code, v, y, DFEA_F64, s);
+    return dfea_mg_apply(&mg->level[l].grid, v, y, s);
+}
+
+static int mg_cheb(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, int l, double* x,
+                   double* r, cudaStream_t s) {
+    const dfea_mg_level& lv = mg->level[l];
+    const double* row = mg->coef + (int64_t)l * 2 * DFEA_MG_MAX_DEGREE;
+    int rc = dfea_mg_cheb_start(lv.n, r, lv.diag, row, lv.d, s);
+    for (int k = 1; !rc && k <= mg->degree; ++k) {
+        const bool last = k == mg->degree;
+        if ((rc = mg_apply(mesh, mg, moduli, code, l, lv.d, lv.q, s))) break;
+        rc = dfea_mg_cheb_step(lv.n, x, r, lv.d, lv.q, lv.diag, last ? nullptr : row + 1 + 2 * (k - 1), last ? 1 : 0, s);
+    }
+    return rc;
+}
+
+static int mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, int l,
+                     const double* b, double* x, cudaStream_t s) {
+    const dfea_mg_level& lv = mg->level[l];
+    int rc;
+    if (l == mg->n_levels - 1) return dfea_mg_dense_solve((int32_t)lv.n, mg->Ainv, b, x, s);
+    if ((rc = check_cuda(cudaMemcpyAsync(lv.r, b, lv.n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")) ||
+        (rc = check_cuda(cudaMemsetAsync(x, 0, lv.n * sizeof(double), s), "cudaMemsetAsync")) ||
+        (rc = mg_cheb(mesh, mg, moduli, code, l, x, lv.r, s)))
+        return rc;
+    const dfea_mg_level& c = mg->level[l + 1];
+    const int32_t* gn;
+    const uint8_t* ffix;
+    transfer_args(mesh, mg, l, &gn, &ffix);
+    if ((rc = dfea_mg_restrict(&lv.grid, &c.grid, gn, ffix, lv.r, c.b, nullptr, s)) ||
+        (rc = mg_vcycle(mesh, mg, moduli, code, l + 1, c.b, c.x, s)) ||
+        (rc = dfea_mg_prolong_add(&lv.grid, &c.grid, gn, ffix, c.x, x, s)) ||
+        (rc = mg_apply(mesh, mg, moduli, code, l, x, lv.q, s)) ||
+        (rc = dfea_add_scaled(lv.n, b, -1.0, lv.q, lv.r, s)))
+        return rc;
+    return mg_cheb(mesh, mg, moduli, code, l, x, lv.r, s);
+}
+
+static int validate_mg(const dfea_mesh_view* mesh, const dfea_mg* mg, const char* what) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!mg || mg->n_levels < 2 || mg->n_levels > DFEA_MG_MAX_LEVELS || mg->degree < 1 ||
+        mg->degree > DFEA_MG_MAX_DEGREE || mg->lanczos_steps < 1 || mg->lanczos_steps > 64 || !(mg->ratio > 1.0))
+        return set_error(DFEA_ERR_INVALID, "%s: bad hierarchy parameters", what);
+    if (mg->level[0].n != 2 * mesh->n_nodes) return set_error(DFEA_ERR_INVALID, "%s: level 0 is not the mesh", what);
+    for (int l = 0; l < mg->n_levels; ++l) {
+        const dfea_mg_level& lv = mg->level[l];
+        if (lv.n != 2 * (int64_t)(lv.grid.gx + 1) * (lv.grid.gy + 1) || !lv.diag || !lv.b || !lv.x || !lv.r || !lv.d || !lv.q)
+            return set_error(DFEA_ERR_INVALID, "%s: level %d buffers", what, l);
+        if (l > 0 && (rc = validate_grid(&lv.grid, true, what))) return rc;
+    }
+    if (mg->level[mg->n_levels - 1].n > kMgDenseMax) return set_error(DFEA_ERR_INVALID, "%s: coarsest level too large", what);
+    if (!mg->node_ij || !mg->gnode || !mg->cell_slot || !mg->Ainv || !mg->dense_work || !mg->coef || !mg->lscal ||
+        !mg->lhist || !mg->dot_work || !mg->pcg || !mg->scal)
+        return set_error(DFEA_ERR_INVALID, "%s: NULL buffer", what);
+    return DFEA_OK;
+}
+
+static int read_scalars(double* host, const double* dev, int k, cudaStream_t s) {
+    int rc = check_cuda(cudaMemcpyAsync(host, dev, k * sizeof(double), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    return rc ? rc : check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+}
+
+}  // namespace dfea
+
+extern "C" int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
+                             const double* diag, void* stream) {
+    int rc = validate_mg(mesh, mg, "dfea_mg_setup");
+    if (rc) return rc;
+    if (!moduli || !diag) return set_error(DFEA_ERR_INVALID, "dfea_mg_setup: NULL pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int L = mg->n_levels;
+    if ((rc = check_cuda(cudaMemcpyAsync(mg->level[0].diag, diag, mg->level[0].n * sizeof(double), cudaMemcpyDeviceToDevice, s),
+                         "cudaMemcpyAsync")))
+        return rc;
+    for (int l = 1; l < L; ++l) {
+        const int32_t* gn;
+        const uint8_t* ffix;
+        transfer_args(mesh, mg, l - 1, &gn, &ffix);
+        if ((rc = dfea_mg_restrict(&mg->level[l - 1].grid, &mg->level[l].grid, gn, ffix, nullptr, nullptr,
+                                   mg->level[l].grid.fix, s)))
+            return rc;
+        rc = l == 1 ? dfea_mg_galerkin_fe(mesh, moduli, moduli_dtype, mg->node_ij, mg->cell_slot, mg->span,
+                                          &mg->level[0].grid, &mg->level[1].grid, s)
+                    : dfea_mg_galerkin(&mg->level[l - 1].grid, &mg->level[l].grid, s);
+        if (rc || (rc = dfea_mg_diag(&mg->level[l].grid, mg->level[l].diag, s))) return rc;
+    }
+    if ((rc = dfea_mg_dense_inverse(&mg->level[L - 1].grid, mg->dense_work, mg->Ainv, s))) return rc;
+    // Lanczos on every smoothed level, all levels in lockstep (p in x, z in d)
+    for (int l = 0; l < L - 1; ++l) {
+        const dfea_mg_level& lv = mg->level[l];
+        k_mg_start<<<grid_for(lv.n, kThreads, 8), kThreads, 0, s>>>(lv.n, lv.r);
+        k_mg_div<<<grid_for(lv.n, kThreads, 8), kThreads, 0, s>>>(lv.n, lv.r, lv.diag, lv.d);
+        note_launches(2);
+        if ((rc = check_cuda(cudaMemcpyAsync(lv.x, lv.d, lv.n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")) ||
+            (rc = dfea_mg_dot(lv.n, lv.r, lv.d, mg->lscal + 4 * l + 1, mg->dot_work, s)))
+            return rc;
+    }
+    for (int k = 0; k < mg->lanczos_steps; ++k)
+        for (int l = 0; l < L - 1; ++l) {
+            const dfea_mg_level& lv = mg->level[l];
+            if ((rc = mg_apply(mesh, mg, moduli, moduli_dtype, l, lv.x, lv.q, s)) ||
+                (rc = dfea_mg_lanczos_step(lv.n, lv.x, lv.q, lv.r, lv.d, lv.diag, mg->lscal + 4 * l,
+                                           mg->lhist + (int64_t)2 * mg->lanczos_steps * l, k, mg->dot_work, s)))
+                return rc;
+        }
+    const int nh = 2 * mg->lanczos_steps * (L - 1);
+    double hist[2 * 64 * DFEA_MG_MAX_LEVELS];
+    if ((rc = read_scalars(hist, mg->lhist, nh, s))) return rc;
+    double coef[DFEA_MG_MAX_LEVELS * 2 * DFEA_MG_MAX_DEGREE] = {0.0};
+    for (int l = 0; l < L - 1; ++l) {
+        const double lam = ritz_max(hist + 2 * mg->lanczos_steps * l, mg->lanczos_steps);
+        mg->lam[l] = lam;
+        const double hi = 1.1 * lam, lo = hi / mg->ratio;
+        const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+        double rho = 1.0 / sigma;
+        double* row = coef + l * 2 * DFEA_MG_MAX_DEGREE;
+        row[0] = 1.0 / theta;
+        for (int k = 1; k < mg->degree; ++k) {
+            const double rho_new = 1.0 / (2.0 * sigma - rho);
+            row[1 + 2 * (k - 1)] = rho_new * rho;
+            row[2 + 2 * (k - 1)] = 2.0 * rho_new / delta;
+            rho = rho_new;
+        }
+    }
+    if ((rc = check_cuda(cudaMemcpyAsync(mg->coef, coef, sizeof(double) * 2 * DFEA_MG_MAX_DEGREE * (L - 1),
+                                         cudaMemcpyHostToDevice, s), "cudaMemcpyAsync")))
+        return rc;
+    // the copy reads a stack array: it has completed when the stream has
+    return check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+}
+
+extern "C" int dfea_mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
+                              const double* r, double* z, void* stream) {
+    int rc = validate_mg(mesh, mg, "dfea_mg_vcycle");
+    if (rc) return rc;
+    if (!moduli || !r || !z) return set_error(DFEA_ERR_INVALID, "dfea_mg_vcycle: NULL pointer");
+    return mg_vcycle(mesh, mg, moduli, moduli_dtype, 0, r, z, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int dfea_mg_pcg(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
+                           const double* b, double* x, double rtol, int32_t max_iter, int32_t* iterations,
+                           int32_t* status, void* stream) {
+    int rc = validate_mg(mesh, mg, "dfea_mg_pcg");
+    if (rc) return rc;
+    if (!moduli || !b || !x || !iterations || !status || max_iter < 0)
+        return set_error(DFEA_ERR_INVALID, "dfea_mg_pcg: bad arguments");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = mg->level[0].n;
+    double *r = mg->pcg, *z = mg->pcg + n, *p = mg->pcg + 2 * n, *q = mg->pcg + 3 * n;
+    double h[1];
+    auto dot = [&](const double* u, const double* v, double* out) -> int {
+        int e = dfea_mg_dot(n, u, v, mg->scal, mg->dot_work, s);
+        return e ? e : read_scalars(out, mg->scal, 1, s);
+    };
+    *iterations = 0;
+    if ((rc = check_cuda(cudaMemsetAsync(x, 0, n * sizeof(double), s), "cudaMemsetAsync")) ||
+        (rc = check_cuda(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")) ||
+        (rc = dot(b, b, h)))
+        return rc;
+    const double nb2 = h[0];
+    if (nb2 == 0.0) {
+        *status = DFEA_PCG_ZERO_RHS;
+        return DFEA_OK;
+    }
+    const double tol2 = rtol * rtol * nb2;
+    if ((rc = mg_vcycle(mesh, mg, moduli, moduli_dtype, 0, r, z, s)) ||
+        (rc = check_cuda(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")) ||
+        (rc = dot(r, z, h)))
+        return rc;
+    double rz = h[0];
+    for (int k = 0; k < max_iter; ++k) {
+        if ((rc = mg_apply(mesh, mg, moduli, moduli_dtype, 0, p, q, s)) || (rc = dot(p, q, h))) return rc;
+        const double curv = h[0];
+        if (!(curv > 0.0)) {
+            if (k == 0)
+                rc = check_cuda(cudaMemcpyAsync(x, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
+            *iterations = k;
+            *status = DFEA_PCG_NEG_CURV;
+            return rc;
+        }
+        const double alpha = rz / curv;
+        if ((rc = dfea_axpy(n, alpha, p, x, s)) || (rc = dfea_axpy(n, -alpha, q, r, s)) || (rc = dot(r, r, h))) return rc;
+        if (h[0] <= tol2) {
+            *iterations = k + 1;
+            *status = DFEA_PCG_CONVERGED;
+            return DFEA_OK;
+        }
+        if ((rc = mg_vcycle(mesh, mg, moduli, moduli_dtype, 0, r, z, s)) || (rc = dot(r, z, h))) return rc;
+        const double rz_new = h[0];
+        if ((rc = dfea_add_scaled(n, z, rz_new / rz, p, p, s))) return rc;
+        rz = rz_new;
+    }
+    *iterations = max_iter;
+    *status = DFEA_PCG_MAX_ITER;
+    return DFEA_OK;
 }

@@ -61,6 +61,22 @@ class MgGrid(ctypes.Structure):
 
 
 _MGP = ctypes.POINTER(MgGrid)
+MG_MAX_LEVELS = 24
+MG_MAX_DEGREE = 8
+
+
+class MgLevel(ctypes.Structure):
+    """Mirror of ``dfea_mg_level``."""
+    _fields_ = [("grid", MgGrid), ("n", c_i64), ("diag", c_vp), ("b", c_vp), ("x", c_vp), ("r", c_vp), ("d", c_vp),
+                ("q", c_vp)]
+
+
+class Mg(ctypes.Structure):
+    """Mirror of ``dfea_mg``."""
+    _fields_ = [("n_levels", c_i32), ("degree", c_i32), ("lanczos_steps", c_i32), ("span", c_i32), ("ratio", c_f64),
+                ("node_ij", c_vp), ("gnode", c_vp), ("cell_slot", c_vp), ("level", MgLevel * MG_MAX_LEVELS),
+                ("Ainv", c_vp), ("dense_work", c_vp), ("coef", c_vp), ("lscal", c_vp), ("lhist", c_vp),
+                ("dot_work", c_vp), ("pcg", c_vp), ("scal", c_vp), ("lam", c_f64 * MG_MAX_LEVELS)]
 
 _PROTOS = {
     "dfea_last_error": (ctypes.c_char_p, []),
@@ -103,12 +119,16 @@ _PROTOS = {
     "dfea_mg_prolong_add": (ctypes.c_int, [_MGP, _MGP, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "dfea_mg_apply": (ctypes.c_int, [_MGP, c_vp, c_vp, c_vp]),
     "dfea_mg_diag": (ctypes.c_int, [_MGP, c_vp, c_vp]),
-    "dfea_mg_cheb_start": (ctypes.c_int, [c_i64, c_vp, c_vp, c_f64, c_vp, c_vp]),
-    "dfea_mg_cheb_step": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_f64, c_f64, c_i32, c_vp]),
-    "dfea_mg_dots": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
-    "dfea_mg_dot": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp]),
-    "dfea_mg_lanczos_step": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp]),
+    "dfea_mg_cheb_start": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "dfea_mg_cheb_step": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp]),
+    "dfea_mg_dot_work": (c_i64, []),
+    "dfea_mg_dot": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "dfea_mg_lanczos_step": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
     "dfea_mg_dense_max": (c_i64, []),
+    "dfea_mg_setup": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp]),
+    "dfea_mg_vcycle": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp, c_vp]),
+    "dfea_mg_pcg": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp, c_f64, c_i32,
+                                   ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_vp]),
     "dfea_mg_dense_inverse": (ctypes.c_int, [_MGP, c_vp, c_vp, c_vp]),
     "dfea_mg_dense_solve": (ctypes.c_int, [c_i32, c_vp, c_vp, c_vp, c_vp]),
     "dfea_batch_create": (ctypes.c_int, [c_i32, c_i32, c_vp]),

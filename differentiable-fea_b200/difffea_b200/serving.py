@@ -104,7 +104,21 @@ def with_arrivals(requests, rate, seed=1):
     return out
 
 
-def hbm_estimate(req, precision="fp32"):
+# "auto" preconditioner: geometric multigrid from this many nodes up (structured rectangles), Jacobi below.
+# Measured crossover on B200 (one request, FP32 operator, 1 load step, tol 1e-10 ||f||): Q4 64 x 16 (1,105
+# nodes) 15.6 ms Jacobi vs 18.1 ms multigrid, Q4 128 x 32 (4,257) 28.2 vs 21.0, Q9 64 x 16 (4,257) 40.0 vs
+# 24.0, Q9 512 x 128 (263,169) 381 vs 49.
+MULTIGRID_MIN_NODES = 2500
+
+
+def preconditioner_for(req, preconditioner="auto"):
+    """The preconditioner a request is solved with: "auto" picks multigrid for the larger requests."""
+    if preconditioner != "auto":
+        return preconditioner
+    return "multigrid" if req.n_nodes >= MULTIGRID_MIN_NODES else "jacobi"
+
+
+def hbm_estimate(req, precision="fp32", preconditioner="jacobi"):
     """Bytes a request holds on the device while it runs (problem, packed mesh, moduli, vectors)."""
     E, N = req.n_elements, req.n_nodes
     nen, nq = NEN[req.element_type], NQ[req.element_type]
@@ -114,6 +128,12 @@ def hbm_estimate(req, precision="fp32"):
                  else 128 * nq)                         # FP64 moduli
               + 16 * nen + 4 * nen)                     # gather form: element results, node incidence
     per_node = 16 + 2 * 8 * 14 + 2 * 4 * 6 + 1 + 4      # nodes, ~14 f64 and ~6 f32 DOF vectors, fix bits, ptr
+    if preconditioner_for(req, preconditioner) == "multigrid":
+        # 10 FP64 DOF vectors on the fine grid (6 of the cycle, 4 of its PCG), a third more over the coarse
+        # levels, their 8 x 8 element matrices (a quarter of the fine cells at level 1, Q9: as many), grid maps
+        cells1 = E if NEN[req.element_type] == 9 else E / 4
+        per_node += 10 * 16 * 4 / 3 + 8 + 4
+        return int(E * per_el + N * per_node + cells1 * 512 * 4 / 3 + 4 * 2 ** 20)
     return int(E * per_el + N * per_node + 4 * 2 ** 20)  # + reduction scratch and PCG state
 
 
@@ -146,9 +166,12 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     concurrent slots; 1: conditional-loop graph; 0: direct launches); ``pcg_form`` the product form inside
     it ("auto", "colour" or "gather", see DevicePCG and workspace.pcg_form_for); ``fp32_moduli`` the FP32
     operator's moduli ("ref": reference frame, no gradients read; "physical"); ``max_blocks`` the most blocks
-    per PCG launch (0: the whole GPU); ``preconditioner`` "jacobi" or "block_jacobi"; ``batch`` a
-    ``BatchExecutor`` that runs the PCG solves of all slots together.
+    per PCG launch (0: the whole GPU); ``preconditioner`` "jacobi", "block_jacobi", "multigrid" or "auto"
+    (``preconditioner_for``); ``batch`` a ``BatchExecutor`` that runs the PCG solves of all slots together.
     """
+    preconditioner = preconditioner_for(req, preconditioner)
+    if preconditioner == "multigrid":
+        batch = None                     # the multigrid PCG runs per request (host-driven, graph-replayed cycle)
     if host_params is not None:
         p = {k: (v.to(device, non_blocking=True) if torch.is_tensor(v) else v) for k, v in host_params.items()}
     else:
@@ -172,7 +195,7 @@ class ServingEngine:
 
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
                  pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
-                 fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="jacobi", batched=False):
+                 fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
@@ -265,7 +288,7 @@ class ServingEngine:
                 if req is None:
                     return
                 res = results[req.rid]
-                nbytes = hbm_estimate(req, self.precision)
+                nbytes = hbm_estimate(req, self.precision, self.solve_kw["preconditioner"])
                 reserved = False
                 try:
                     self._reserve(nbytes)
@@ -293,7 +316,7 @@ class ServingEngine:
             delay = req.arrival - (time.perf_counter() - t0)
             if delay > 0:
                 time.sleep(delay)
-            prio = -hbm_estimate(req, self.precision) if self.order == "largest_first" else 0
+            prio = -hbm_estimate(req, self.precision, self.solve_kw["preconditioner"]) if self.order == "largest_first" else 0
             q.put((prio, seq, req))
             seq += 1
         for _ in threads:

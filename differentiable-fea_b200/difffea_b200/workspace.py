@@ -88,7 +88,6 @@ class NewtonWorkspace:
             # geometric multigrid V-cycle (structured meshes) inside a PCG driven from the host
             from difffea_b200.multigrid import Multigrid
             self.mg = Multigrid(mesh, params)
-            self.mg_work = torch.empty(4, n, **f64)
             self.pcg = None
         else:
             self.pcg = DevicePCG(mesh, self.C, self.diag if self.blocks is None else self.blocks, self.b, self.du,
@@ -126,17 +125,12 @@ class NewtonWorkspace:
         """du = PCG(A, -R) to relative tolerance rtol; returns (du (FP64 buffer), iterations, status)."""
         torch.neg(R, out=self.b)
         if self.mg is not None:
-            from difffea_b200.multigrid import mg_pcg
-            iters, status = mg_pcg(self._apply, self.mg, self.b, self.du, rtol, max_iter, self.mg_work)
+            iters, status = self.mg.pcg(self.b, self.du, rtol, max_iter)
         elif self.batch is not None:
             iters, status = self.batch.solve(self.pcg, rtol, max_iter)
         else:
             iters, status = self.pcg.solve(rtol, max_iter)
         return self.du, iters, status
-
-    def _apply(self, v, y):
-        _lib.call("dfea_tangent_apply", self.mesh.view_ref, ptr(self.C), self.moduli_code, ptr(v), ptr(y),
-                  _lib.DFEA_F64, stream_handle())
 
     def trial(self, u, alpha, du, out):
         _lib.call("dfea_add_scaled", self.mesh.n_dof, ptr(u), float(alpha), ptr(du), ptr(out), stream_handle())

@@ -129,6 +129,7 @@ int dfea_version(void);
  * PCG graph are added when its solve returns).  A diagnostic for benchmarks. */
 int64_t dfea_launch_count(void);
 
+
 /* 1 if the (nen, n_q) pair is built: (3,1) tri3, (6,6) tri6, (4,4) quad4, (8,9) quad8, (9,9) quad9. */
 int dfea_element_supported(int32_t nen, int32_t n_q);
 
@@ -321,26 +322,75 @@ int dfea_mg_prolong_add(const dfea_mg_grid* fine, const dfea_mg_grid* coarse, co
 /* y = K v + (I - M) v on a coarse level; dfea_mg_diag: its diagonal. */
 int dfea_mg_apply(const dfea_mg_grid* grid, const double* v, double* y, void* stream);
 int dfea_mg_diag(const dfea_mg_grid* grid, double* diag, void* stream);
-/* Chebyshev smoothing (Jacobi-preconditioned Chebyshev iteration): d = scale r / diag; and one step
- * x += d, r -= q (q = A d), then unless last d = c1 d + c2 r / diag. */
-int dfea_mg_cheb_start(int64_t n, const double* r, const double* diag, double scale, double* d, void* stream);
+/* Chebyshev smoothing (Jacobi-preconditioned Chebyshev iteration): d = (*scale) r / diag; and one step
+ * x += d, r -= q (q = A d), then unless last d = c[0] d + c[1] r / diag.  scale and c are device
+ * pointers, so a captured CUDA graph of the cycle picks up new coefficients at every linearisation. */
+int dfea_mg_cheb_start(int64_t n, const double* r, const double* diag, const double* scale, double* d, void* stream);
 int dfea_mg_cheb_step(int64_t n, double* x, double* r, double* d, const double* q, const double* diag,
-                      double c1, double c2, int32_t last, void* stream);
-/* out[0] = x . y, out[1] = sum x_i^2 diag_i (device, fixed order). */
-int dfea_mg_dots(int64_t n, const double* x, const double* y, const double* diag, double* out, void* stream);
-/* Lanczos for lambda_max(D^-1 A) by Jacobi-preconditioned CG, scalars on the device: *out = x . y; and
+                      const double* c, int32_t last, void* stream);
+/* Lanczos for lambda_max(D^-1 A) by Jacobi-preconditioned CG, scalars on the device: *out = x . y (two
+ * fixed-order passes over dfea_mg_dot_work() doubles of caller scratch); and
  * after q = A p, one CG step: s[0] = p.q, alpha = s[1] / s[0], r -= alpha q, z = r / diag,
  * beta = r.z / s[1], p = z + beta p, s[1] = r.z, s[3] = beta, (alpha, beta) into hist[2k], hist[2k+1].
  * Start: r = b, z = r / diag, p = z, s[1] = r.z.  The eigenvalues of the tridiagonal matrix of the
  * coefficients approximate those of D^-1 A (Saad, Iterative Methods, section 6.7). */
-int dfea_mg_dot(int64_t n, const double* x, const double* y, double* out, void* stream);
+int64_t dfea_mg_dot_work(void); /* doubles of the work buffer of dfea_mg_dot and dfea_mg_lanczos_step */
+int dfea_mg_dot(int64_t n, const double* x, const double* y, double* out, double* work, void* stream);
 int dfea_mg_lanczos_step(int64_t n, double* p, const double* q, double* r, double* z, const double* diag,
-                         double* s, double* hist, int32_t k, void* stream);
+                         double* s, double* hist, int32_t k, double* work, void* stream);
 /* Coarsest level: the dense inverse of its operator (at most dfea_mg_dense_max() DOFs; work and Ainv
  * hold n x n doubles each), and x = Ainv b. */
 int64_t dfea_mg_dense_max(void);
 int dfea_mg_dense_inverse(const dfea_mg_grid* grid, double* work, double* Ainv, void* stream);
 int dfea_mg_dense_solve(int32_t n, const double* Ainv, const double* b, double* x, void* stream);
+
+/*
+ * The whole multigrid preconditioner and its PCG, driven from C++ (one call per set-up, per cycle, per
+ * solve; the host reads scalars with stream synchronisations, no other host work between launches).
+ * The caller owns every buffer and describes the hierarchy in a dfea_mg (levels[0] is the FE level:
+ * only gx, gy and its vectors; coarse levels carry their dfea_mg_grid).  Vectors of a level hold n doubles.
+ */
+#define DFEA_MG_MAX_LEVELS 24
+#define DFEA_MG_MAX_DEGREE 8
+typedef struct dfea_mg_level {
+    dfea_mg_grid grid;
+    int64_t n;                                 /* 2 (gx + 1)(gy + 1)                                */
+    double *diag, *b, *x, *r, *d, *q;          /* device vectors of n doubles                       */
+} dfea_mg_level;
+
+typedef struct dfea_mg {
+    int32_t n_levels;                          /* including level 0; the last one is solved densely */
+    int32_t degree;                            /* Chebyshev steps per smoothing (<= DFEA_MG_MAX_DEGREE) */
+    int32_t lanczos_steps;                     /* Jacobi-CG steps of the lambda_max estimate            */
+    int32_t span;                              /* FE element span in grid cells: 1 (Q4) or 2 (Q9)    */
+    double ratio;                              /* smoothing interval [lambda / ratio, lambda], lambda =
+                                                * 1.1 x the Lanczos estimate                            */
+    const int32_t* node_ij;                    /* FE node -> grid position (2N)                        */
+    const int32_t* gnode;                      /* grid node -> FE node                                 */
+    const int32_t* cell_slot;                  /* element cell -> packed element slot                  */
+    dfea_mg_level level[DFEA_MG_MAX_LEVELS];
+    double* Ainv;                              /* coarsest n x n inverse, and n x n of work            */
+    double* dense_work;
+    double* coef;                              /* [n_levels][2 DFEA_MG_MAX_DEGREE] Chebyshev coefficients */
+    double* lscal;                             /* [n_levels][4] Lanczos scalars                         */
+    double* lhist;                             /* [n_levels][2 lanczos_steps] Lanczos coefficients      */
+    double* dot_work;                          /* dfea_mg_dot_work() doubles                            */
+    double* pcg;                               /* 4 x level[0].n: the PCG's r, z, p, q                  */
+    double* scal;                              /* 4 device doubles                                      */
+    double lam[DFEA_MG_MAX_LEVELS];            /* out: the lambda_max estimates of the last set-up      */
+} dfea_mg;
+
+/* Set-up at a linearisation: coarse operators from the moduli, coarsest inverse, Lanczos estimates,
+ * Chebyshev coefficients (one host synchronisation). */
+int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
+                  const double* diag, void* stream);
+/* z = one V-cycle applied to r (the moduli of the set-up). */
+int dfea_mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
+                   const double* r, double* z, void* stream);
+/* PCG (x0 = 0) for A x = b with the V-cycle as preconditioner; status as dfea_pcg_solve's. */
+int dfea_mg_pcg(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
+                const double* b, double* x, double rtol, int32_t max_iter, int32_t* iterations, int32_t* status,
+                void* stream);
 
 /* ---------------------------------------------------------------- kernel (c): PCG ------------- */
 

@@ -19,7 +19,7 @@ import torch
 
 from oracle.reference_path import F64, make_operator
 
-COARSEST_NODES = 128
+COARSEST_NODES = 48
 
 
 def _coarser(g):

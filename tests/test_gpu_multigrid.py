@@ -114,3 +114,24 @@ def test_quarter_plate_grid_and_mixed_precision():
     print(f"\nplate 32x32 Q9: PCG iterations jacobi {i_j['total_cg']}, multigrid {i_m['total_cg']}")
     assert rel(u_m, u_j) < 1e-8
     assert i_m["total_cg"] * 5 < i_j["total_cg"]
+
+
+def test_cycle_and_pcg_are_deterministic_across_linearisations():
+    """The C++ driver's set-up, cycle and PCG give bit-identical results when repeated, at several states."""
+    p = build_rectangle_problem("quad4", 24, 6, 4.0, 1.0, load=(0.0, -0.01), device=DEV)
+    th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV)
+    ws = NewtonWorkspace(p, preconditioner="multigrid")
+    ws.set_theta(th)
+    r = torch.randn(p["f"].numel(), dtype=torch.float64, generator=torch.Generator().manual_seed(7)).to(DEV)
+    for amp in (0.0, 0.002, 0.005):                        # random states well below h = 1/6 (no inversion)
+        u, _, _ = _state(p, 11, amp) if amp else (torch.zeros_like(r), None, None)
+        out = []
+        for _ in range(2):
+            ws.linearize(u)
+            lams = [lv.lam for lv in ws.mg.levels[:-1]]
+            z = ws.mg(r)
+            du, it, status = ws.solve(-r, 1e-9, 200)
+            out.append((lams, z, du.clone(), it, status))
+        assert out[0][0] == out[1][0] and all(1.5 < x < 3.0 for x in out[0][0])
+        assert torch.isfinite(out[0][1]).all() and torch.equal(out[0][1], out[1][1])
+        assert torch.equal(out[0][2], out[1][2]) and out[0][3] == out[1][3] and out[0][4] == "converged"
