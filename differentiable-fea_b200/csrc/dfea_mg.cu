@@ -64,7 +64,7 @@ __device__ __forceinline__ double hat(const int32_t* X, int n_lines, int c, int 
 template <int NEN, int NQ, int MOD>
 __global__ void __launch_bounds__(128)
 k_mg_galerkin_fe(Mesh m, const void* __restrict__ moduli, RefGrad<NEN, NQ> rg, const int32_t* __restrict__ node_ij,
-                 const int32_t* __restrict__ cell_slot, int span, int ncy, MgGrid cg) {
+                 const int32_t* __restrict__ cell_slot, int span, int epc, int ncy, MgGrid cg) {
     const int n_cells = cg.gx * cg.gy;
     const int64_t S = m.stride;
     for (int C = blockIdx.x * blockDim.x + threadIdx.x; C < n_cells; C += gridDim.x * blockDim.x) {
@@ -76,8 +76,9 @@ k_mg_galerkin_fe(Mesh m, const void* __restrict__ moduli, RefGrad<NEN, NQ> rg, c
 #pragma unroll 1
         for (int fcx = x0 / span; fcx < x1 / span; ++fcx) {
 #pragma unroll 1
-            for (int fcy = y0 / span; fcy < y1 / span; ++fcy) {
-                const int64_t s = cell_slot[(int64_t)fcx * ncy + fcy];
+            for (int fce = (y0 / span) * epc; fce < (y1 / span) * epc; ++fce) {
+                // element fce % epc of the cell (fcx, fce / epc)
+                const int64_t s = cell_slot[((int64_t)fcx * ncy + fce / epc) * epc + fce % epc];
                 double P[NEN][4];
                 int fix[NEN];
 #pragma unroll
@@ -507,31 +508,29 @@ extern "C" int dfea_mg_galerkin_fe(const dfea_mesh_view* mesh, const void* modul
         return rc;
     if (!moduli || !node_ij || !cell_slot || !coarse->K) return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin_fe: NULL pointer");
     if (span != 1 && span != 2) return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin_fe: span must be 1 or 2");
-    if (fine->gx % span || fine->gy % span || (int64_t)(fine->gx / span) * (fine->gy / span) != mesh->n_el)
+    const int64_t n_cells = (int64_t)(fine->gx / span) * (fine->gy / span);
+    const int epc = n_cells > 0 ? (int)(mesh->n_el / n_cells) : 0;   // elements per cell: 1, or 2 triangles
+    if (fine->gx % span || fine->gy % span || (epc != 1 && epc != 2) || n_cells * epc != mesh->n_el)
         return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin_fe: the grid does not match the mesh's element count");
-    if (moduli_dtype == DFEA_F32REF && !(mesh->nen == 4 || mesh->nen == 9))
-        return set_error(DFEA_ERR_UNSUPPORTED, "dfea_mg_galerkin_fe: quadrilateral grids only");
     const Mesh m = kernel_mesh(*mesh);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int n_cells = coarse->gx * coarse->gy;
-    const int grid = grid_for(n_cells, 128, 8);
+    const int n_ccells = coarse->gx * coarse->gy;
+    const int grid = grid_for(n_ccells, 128, 8);
     const MgGrid cg = mg_grid(*coarse);
-    auto launch = [&](auto nen_c, auto nq_c) -> int {
+    const int ncy = fine->gy / span;
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
         constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
         const RefGrad<NEN, NQ> rg = ref_grad_of<NEN, NQ>(*mesh);
         if (moduli_dtype == DFEA_F64)
-            k_mg_galerkin_fe<NEN, NQ, 0><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, fine->gy / span, cg);
+            k_mg_galerkin_fe<NEN, NQ, 0><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, epc, ncy, cg);
         else if (moduli_dtype == DFEA_F32)
-            k_mg_galerkin_fe<NEN, NQ, 1><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, fine->gy / span, cg);
+            k_mg_galerkin_fe<NEN, NQ, 1><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, epc, ncy, cg);
         else if (moduli_dtype == DFEA_F32REF)
-            k_mg_galerkin_fe<NEN, NQ, 2><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, fine->gy / span, cg);
+            k_mg_galerkin_fe<NEN, NQ, 2><<<grid, 128, 0, s>>>(m, moduli, rg, node_ij, cell_slot, span, epc, ncy, cg);
         else
             return set_error(DFEA_ERR_INVALID, "dfea_mg_galerkin_fe: bad moduli dtype");
         return DFEA_OK;
-    };
-    if (mesh->nen == 4 && mesh->n_q == 4) rc = launch(IntC<4>{}, IntC<4>{});
-    else if (mesh->nen == 9 && mesh->n_q == 9) rc = launch(IntC<9>{}, IntC<9>{});
-    else return set_error(DFEA_ERR_UNSUPPORTED, "dfea_mg_galerkin_fe: Q4 and Q9 meshes only");
+    });
     if (rc) return rc;
     note_launches(1);
     return launch_check("dfea_mg_galerkin_fe");
@@ -792,7 +791,9 @@ static int validate_mg(const dfea_mesh_view* mesh, const dfea_mg* mg, const char
     if (mg->level[0].n != 2 * mesh->n_nodes) return set_error(DFEA_ERR_INVALID, "%s: level 0 is not the mesh", what);
     for (int l = 0; l < mg->n_levels; ++l) {
         const dfea_mg_level& lv = mg->level[l];
-        if (lv.n != 2 * (int64_t)(lv.grid.gx + 1) * (lv.grid.gy + 1) || !lv.diag || !lv.b || !lv.x || !lv.r || !lv.d || !lv.q)
+        // level 0 holds the mesh's DOFs (a Q8 grid has no nodes at the cell centres), the others their grid's
+        if ((l > 0 && lv.n != 2 * (int64_t)(lv.grid.gx + 1) * (lv.grid.gy + 1)) || !lv.diag || !lv.b || !lv.x || !lv.r ||
+            !lv.d || !lv.q)
             return set_error(DFEA_ERR_INVALID, "%s: level %d buffers", what, l);
         if (l > 0 && (rc = validate_grid(&lv.grid, true, what))) return rc;
     }

@@ -4,10 +4,10 @@ Geometric multigrid preconditioner for structured quadrilateral meshes (precondi
 The reference's preconditioners are Jacobi, nodal block-Jacobi and an incomplete LU on the CPU
 (operators.py:477-710); it names a scalable preconditioner as its main open item (docs/ROADMAP.md:11).
 This module builds one for the meshes whose cells form a logical grid (every rectangle of the
-structured mesher, Q4 or Q9, and the mapped quarter plate):
+structured mesher, any element type, and the mapped quarter plate):
 
     level 0     the finite-element mesh and its operator A = M K M + (I - M) (stored moduli, kernel (b))
-    level 1     a Q4 grid on the element corners (Q9: the element grid itself; Q4: every other line)
+    level 1     a Q4 grid on the element corners (Q9 / Q8 / Tri6: the element grid; Q4 / Tri3: every other line)
     level l+1   every other grid line of level l (a last cell one line wide when the count is odd),
                 down to at most 48 nodes, where the operator is inverted densely
 
@@ -41,54 +41,89 @@ LANCZOS_STEPS = 10
 # ---------------------------------------------------------------------------------------------
 # the grid behind a structured mesh
 # ---------------------------------------------------------------------------------------------
-def _grid_conn(ids, ncx, ncy, span):
-    """Connectivity of an ncx x ncy cell grid over node ids (grid of span*ncx+1 x span*ncy+1 nodes)."""
-    if span == 1:
+# per element type (nodes per element): grid cells spanned by an element, elements per cell
+_LAYOUT = {4: (1, 1), 9: (2, 1), 8: (2, 1), 3: (1, 2), 6: (2, 2)}
+
+
+def _grid_conn(ids, ncx, ncy, nen):
+    """
+    Connectivity of an ncx x ncy cell grid over the grid node ids, in the element library's local order:
+    Q4 / Q9 / Q8 one element per cell, Tri3 / Tri6 the lower-left triangles of all cells, then the
+    upper-right ones.
+    """
+    if nen in (4, 3):
         c = [ids[:ncx, :ncy], ids[1:ncx + 1, :ncy], ids[1:ncx + 1, 1:ncy + 1], ids[:ncx, 1:ncy + 1]]
-        return torch.stack([t.reshape(-1) for t in c], dim=1)
+        q4 = torch.stack([t.reshape(-1) for t in c], dim=1)
+        return q4 if nen == 4 else torch.cat([q4[:, [0, 1, 3]], q4[:, [1, 2, 3]]], dim=0)
     offs = [(0, 0), (2, 0), (2, 2), (0, 2), (1, 0), (2, 1), (1, 2), (0, 1), (1, 1)]
-    return torch.stack([ids[di:di + 2 * ncx:2, dj:dj + 2 * ncy:2].reshape(-1) for di, dj in offs], dim=1)
+    q9 = torch.stack([ids[di:di + 2 * ncx:2, dj:dj + 2 * ncy:2].reshape(-1) for di, dj in offs], dim=1)
+    if nen == 9:
+        return q9
+    if nen == 8:
+        return q9[:, :8]
+    return torch.cat([q9[:, [0, 1, 3, 4, 8, 7]], q9[:, [1, 2, 3, 5, 6, 8]]], dim=0)
+
+
+def _candidates(n_cells, n_nodes, span, q8):
+    """(ncx, ncy) with ncx ncy = n_cells and the node count of the grid: N = span^2 cells + span (ncx + ncy)
+    + 1, minus the cell centres for Q8; ncx and ncy are the roots of t^2 - (ncx + ncy) t + cells."""
+    rest = n_nodes - 1 - (span * span - (1 if q8 else 0)) * n_cells
+    if rest <= 0 or rest % span:
+        return []
+    ssum = rest // span
+    disc = ssum * ssum - 4 * n_cells
+    if disc < 0:
+        return []
+    root = math.isqrt(disc)
+    if root * root != disc or (ssum + root) % 2:
+        return []
+    out = []
+    for ncx in sorted({(ssum - root) // 2, (ssum + root) // 2}):
+        if ncx >= 1 and n_cells % ncx == 0:
+            out.append((ncx, n_cells // ncx))
+    return out
 
 
 def structured_grid(conn, n_nodes):
     """
-    The logical grid of a structured Q4 / Q9 mesh, or None: tries every cell count ncx x ncy = n_el
-    with the node numbering of the rectangle mesher (grid node (i, j) = i (gy + 1) + j) and of the
-    quarter-plate mesher (i + j (gx + 1)), and accepts one whose connectivity matches exactly.
-    Returns dict(span, ncx, ncy, gx, gy, gnode (grid -> FE node), node_ij (FE node -> grid)).
+    The logical grid of a structured mesh (any element type of the library), or None: the element count
+    and the node count fix at most two cell counts ncx x ncy; each is tried with the node numbering of the
+    rectangle mesher (grid node (i, j) = i (gy + 1) + j, Q8 without the cell centres) and, for Q4 / Q9, of
+    the quarter-plate mesher (i + j (gx + 1)), and accepted if the connectivity matches exactly.
+    Returns dict(span, epc (elements per cell), ncx, ncy, gx, gy, gnode (grid node -> FE node, -1 for a
+    Q8 cell centre), node_ij (FE node -> grid position)).
     """
     n_el, nen = conn.shape
-    span = {4: 1, 9: 2}.get(nen)
-    if span is None or n_el == 0:
+    if nen not in _LAYOUT or n_el == 0:
         return None
+    span, epc = _LAYOUT[nen]
+    if n_el % epc:
+        return None
+    n_cells = n_el // epc
     dev = conn.device
-    # (span ncx + 1)(span ncy + 1) = N and ncx ncy = n_el: ncx + ncy = (N - 1 - span^2 n_el) / span, so ncx and
-    # ncy are the two roots of t^2 - (ncx + ncy) t + n_el
-    rest = n_nodes - 1 - span * span * n_el
-    if rest <= 0 or rest % span:
-        return None
-    ssum = rest // span
-    disc = ssum * ssum - 4 * n_el
-    if disc < 0:
-        return None
-    root = math.isqrt(disc)
-    if root * root != disc or (ssum + root) % 2:
-        return None
-    for ncx in sorted({(ssum - root) // 2, (ssum + root) // 2}):
-        ncy = n_el // ncx if ncx > 0 else 0
-        if ncx < 1 or ncx * ncy != n_el:
-            continue
+    for ncx, ncy in _candidates(n_cells, n_nodes, span, nen == 8):
         gx, gy = span * ncx, span * ncy
-        lex = torch.arange((gx + 1) * (gy + 1), device=dev)
-        for ids in (lex.reshape(gx + 1, gy + 1), lex.reshape(gy + 1, gx + 1).t()):
-            if torch.equal(_grid_conn(ids, ncx, ncy, span), conn):
+        n_grid = (gx + 1) * (gy + 1)
+        lex = torch.arange(n_grid, device=dev)
+        numberings = [lex.reshape(gx + 1, gy + 1)]
+        if nen in (4, 9):
+            numberings.append(lex.reshape(gy + 1, gx + 1).t())
+        for ids in numberings:
+            if nen == 8:                     # drop the cell centres, renumber the other grid nodes in order
+                keep = torch.ones(gx + 1, gy + 1, dtype=torch.bool, device=dev)
+                keep[1:gx:2, 1:gy:2] = False
+                ids = torch.where(keep, torch.cumsum(keep.reshape(-1), 0).reshape(gx + 1, gy + 1) - 1,
+                                  torch.full_like(ids, -1))
+            if torch.equal(_grid_conn(ids, ncx, ncy, nen), conn):
                 gnode = ids.reshape(-1).to(torch.int32).contiguous()
                 node_ij = torch.empty(n_nodes, 2, dtype=torch.int32, device=dev)
                 ii = torch.arange(gx + 1, device=dev)[:, None].expand(gx + 1, gy + 1).reshape(-1)
                 jj = torch.arange(gy + 1, device=dev)[None, :].expand(gx + 1, gy + 1).reshape(-1)
-                node_ij[gnode.long(), 0] = ii.to(torch.int32)
-                node_ij[gnode.long(), 1] = jj.to(torch.int32)
-                return dict(span=span, ncx=ncx, ncy=ncy, gx=gx, gy=gy, gnode=gnode, node_ij=node_ij.contiguous())
+                present = gnode >= 0
+                node_ij[gnode[present].long(), 0] = ii[present].to(torch.int32)
+                node_ij[gnode[present].long(), 1] = jj[present].to(torch.int32)
+                return dict(span=span, epc=epc, ncx=ncx, ncy=ncy, gx=gx, gy=gy, gnode=gnode,
+                            node_ij=node_ij.contiguous())
     return None
 
 
@@ -96,10 +131,10 @@ def structured_grid(conn, n_nodes):
 # hierarchy
 # ---------------------------------------------------------------------------------------------
 class _Level:
-    def __init__(self, gx, gy, finer=None, device="cuda"):
+    def __init__(self, gx, gy, finer=None, device="cuda", n=None):
         self.gx, self.gy = gx, gy
         self.n_nodes = (gx + 1) * (gy + 1)
-        self.n = 2 * self.n_nodes
+        self.n = 2 * self.n_nodes if n is None else n       # level 0: the mesh's DOFs
         i32 = dict(dtype=torch.int32, device=device)
         self.keep = []
         self.grid = _lib.MgGrid()
@@ -142,7 +177,7 @@ class Multigrid:
     def __init__(self, mesh, params, degree=CHEB_DEGREE, ratio=CHEB_RATIO, lanczos_steps=LANCZOS_STEPS):
         g = structured_grid(params["conn"].to(mesh.device), mesh.n_nodes)
         if g is None:
-            raise ValueError("preconditioner='multigrid' needs a structured Q4 or Q9 mesh (a logical grid of cells)")
+            raise ValueError("preconditioner='multigrid' needs a structured mesh (a logical grid of cells)")
         if not 1 <= degree <= _lib.MG_MAX_DEGREE:
             raise ValueError(f"degree must be in [1, {_lib.MG_MAX_DEGREE}]")
         self.mesh, self.g = mesh, g
@@ -150,8 +185,12 @@ class Multigrid:
         dev = mesh.device
         inv_perm = torch.empty_like(mesh.perm)
         inv_perm[mesh.perm] = torch.arange(mesh.perm.numel(), device=dev)
-        self.cell_slot = inv_perm.to(torch.int32).contiguous()      # cells are numbered like the elements
-        self.levels = [_Level(g["gx"], g["gy"], None, dev)]
+        # the elements of cell c are c + k n_cells (k < epc: one quadrilateral, or the lower then the upper
+        # triangle), numbered like the mesher's
+        n_cells = g["ncx"] * g["ncy"]
+        elems = torch.arange(n_cells, device=dev)[:, None] + n_cells * torch.arange(g["epc"], device=dev)[None, :]
+        self.cell_slot = inv_perm[elems.reshape(-1)].to(torch.int32).contiguous()
+        self.levels = [_Level(g["gx"], g["gy"], None, dev, n=mesh.n_dof)]
         while True:
             f = self.levels[-1]
             if len(self.levels) > 1 and (f.n_nodes <= COARSEST_NODES or (f.gx == 1 and f.gy == 1)):

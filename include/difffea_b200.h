@@ -304,7 +304,9 @@ typedef struct dfea_mg_grid {
     uint8_t* fix;           /* [(gx + 1) (gy + 1)] fix bits (coarse levels)                          */
 } dfea_mg_grid;
 
-/* Level 1 from the stored moduli (DFEA_F64, DFEA_F32 or DFEA_F32REF) of a Q4 or Q9 mesh: coarse->K. */
+/* Level 1 from the stored moduli (DFEA_F64, DFEA_F32 or DFEA_F32REF) of the mesh: coarse->K.  Any element
+ * type on a grid: one element per cell (Q4, Q8, Q9; span 1 or 2 grid cells) or two triangles per cell (Tri3,
+ * Tri6); cell_slot lists the packed slots of the elements of cell c at [c epc .. c epc + epc). */
 int dfea_mg_galerkin_fe(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype,
                         const int32_t* node_ij, const int32_t* cell_slot, int32_t span,
                         const dfea_mg_grid* fine, const dfea_mg_grid* coarse, void* stream);
@@ -354,7 +356,8 @@ int dfea_mg_dense_solve(int32_t n, const double* Ainv, const double* b, double* 
 #define DFEA_MG_MAX_DEGREE 8
 typedef struct dfea_mg_level {
     dfea_mg_grid grid;
-    int64_t n;                                 /* 2 (gx + 1)(gy + 1)                                */
+    int64_t n;                                 /* 2 (gx + 1)(gy + 1); level 0: the mesh's 2N (a Q8 grid has
+                                                * no nodes at the cell centres)                        */
     double *diag, *b, *x, *r, *d, *q;          /* device vectors of n doubles                       */
 } dfea_mg_level;
 

@@ -38,8 +38,12 @@ def _interp_1d(gf, gc):
     return W
 
 
-def hierarchy(A0, gx, gy, fixed0, diag0=None):
-    """Levels [(A, P~ to the finer level, fixed)] of the V-cycle; fixed0: (2N,) bool."""
+def hierarchy(A0, gx, gy, fixed0, diag0=None, node_ij=None):
+    """
+    Levels [(A, P~ to the finer level, fixed)] of the V-cycle; fixed0: (2N,) bool.  node_ij: (N, 2) grid
+    position of every FE node (default: all grid nodes, numbered i (gy + 1) + j) -- level 0's interpolation
+    is evaluated at those positions, so meshes whose nodes are a subset of the grid (Q8) work alike.
+    """
     levels = [dict(A=A0, fixed=fixed0, gx=gx, gy=gy, diag=diag0 if diag0 is not None else torch.diagonal(A0).clone())]
     while True:
         f = levels[-1]
@@ -48,6 +52,8 @@ def hierarchy(A0, gx, gy, fixed0, diag0=None):
             break
         cgx, cgy = _coarser(f["gx"]), _coarser(f["gy"])
         Wn = torch.kron(_interp_1d(f["gx"], cgx), _interp_1d(f["gy"], cgy))          # nodes
+        if len(levels) == 1 and node_ij is not None:
+            Wn = Wn[node_ij[:, 0] * (f["gy"] + 1) + node_ij[:, 1]]
         P = torch.kron(Wn, torch.eye(2, dtype=F64))                                    # DOFs (2 node + comp)
         Pt = P * (~f["fixed"]).to(F64)[:, None]
         fixed_c = (Pt.abs().sum(0) == 0)
@@ -122,11 +128,11 @@ def vcycle(levels, b, l=0, lams=None):
     return x
 
 
-def preconditioner(u, theta, P, gx, gy, diag0=None):
-    """The V-cycle r -> z at (u, theta) for a structured rectangle mesh of gx x gy node-grid cells."""
+def preconditioner(u, theta, P, gx, gy, diag0=None, node_ij=None):
+    """The V-cycle r -> z at (u, theta) for a structured mesh of gx x gy node-grid cells."""
     A_fn = make_operator("qp", u, theta, P)
     n = u.numel()
     A0 = torch.stack([A_fn(torch.eye(n, dtype=F64)[i]) for i in range(n)], dim=1)
-    levels = hierarchy(A0, gx, gy, P["fixed"].clone(), diag0)
+    levels = hierarchy(A0, gx, gy, P["fixed"].clone(), diag0, node_ij)
     lams = [lambda_max(lv["A"], lv["diag"]) for lv in levels[:-1]]
     return (lambda r: vcycle(levels, r, 0, lams)), levels, lams

@@ -33,7 +33,8 @@ def _state(p, seed, amp):
 
 
 @pytest.mark.parametrize("et,nx,ny,fixed_dofs", [("quad4", 16, 4, "xy"), ("quad4", 13, 5, "xy"), ("quad4", 21, 3, "x"),
-                                                  ("quad9", 6, 3, "xy"), ("quad9", 5, 2, "xy")])
+                                                  ("quad9", 6, 3, "xy"), ("quad9", 5, 2, "xy"), ("quad8", 6, 3, "xy"),
+                                                  ("tri3", 13, 5, "xy"), ("tri6", 5, 3, "xy")])
 def test_vcycle_matches_the_oracle(et, nx, ny, fixed_dofs):
     p = build_rectangle_problem(et, nx, ny, 4.0, 1.0, load=(0.0, -0.01), fixed_dofs=fixed_dofs, device=DEV)
     if fixed_dofs == "x":                                  # rollers on x = 0 plus one pinned corner in y
@@ -42,9 +43,11 @@ def test_vcycle_matches_the_oracle(et, nx, ny, fixed_dofs):
     u, th, r = _state(p, 3, 0.01 * 4.0 / nx)
     z = make_preconditioner("multigrid", u, th, p)(r)
     P = oracle.as_problem(p)
-    span = 2 if et == "quad9" else 1
+    span = 2 if et in ("quad9", "quad8", "tri6") else 1
     uc, thc = u.cpu(), th.cpu()
-    M, levels, lams = omg.preconditioner(uc, thc, P, span * nx, span * ny, oracle.jacobi_diagonal(uc, thc, P))
+    gx, gy = span * nx, span * ny                          # grid positions from the coordinates (4 x 1 domain)
+    node_ij = torch.stack([torch.round(P["nodes"][:, 0] / 4.0 * gx), torch.round(P["nodes"][:, 1] * gy)], 1).long()
+    M, levels, lams = omg.preconditioner(uc, thc, P, gx, gy, oracle.jacobi_diagonal(uc, thc, P), node_ij)
     z_ref = M(r.cpu())
     assert rel(z, z_ref) < 1e-10
 
@@ -67,16 +70,11 @@ def test_vcycle_from_fp32_moduli(moduli):
 
 
 @pytest.mark.parametrize("name", ["solve_quad4_h0.25_cantilever", "solve_quad9_h0.5_cantilever", "solve_quad4_h0.2_tension",
-                                  "solve_tri6_h0.5_cantilever"])
+                                  "solve_tri6_h0.5_cantilever", "material_solve_fiber_reinforced_quad4_h0.5"])
 def test_multigrid_solves_match_reference(name):
     d = load(name)
     p = params_from(d, DEV)
     th = torch.as_tensor(d["theta"], device=DEV)
-    if d["conn"].shape[1] == 6:                           # triangles: no logical grid
-        with pytest.raises(ValueError, match="structured"):
-            newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False,
-                                preconditioner="multigrid")
-        return
     u, info = newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False,
                                   preconditioner="multigrid")
     assert info["converged"]
@@ -135,3 +133,13 @@ def test_cycle_and_pcg_are_deterministic_across_linearisations():
         assert out[0][0] == out[1][0] and all(1.5 < x < 3.0 for x in out[0][0])
         assert torch.isfinite(out[0][1]).all() and torch.equal(out[0][1], out[1][1])
         assert torch.equal(out[0][2], out[1][2]) and out[0][3] == out[1][3] and out[0][4] == "converged"
+
+
+def test_unstructured_mesh_is_refused():
+    d = load("operator_quad4_h0.5_unit")
+    p = params_from(d, DEV)
+    perm = torch.randperm(p["conn"].shape[0], generator=torch.Generator().manual_seed(0)).to(DEV)
+    p = dict(p, conn=p["conn"][perm], dN_dX=p["dN_dX"][perm], w_detJ=p["w_detJ"][perm])
+    th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV)
+    with pytest.raises(ValueError, match="structured"):
+        NewtonWorkspace(p, preconditioner="multigrid")

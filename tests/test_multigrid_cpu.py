@@ -30,11 +30,23 @@ def test_grid_of_the_quarter_plate(et):
     assert g is not None and (g["ncx"], g["ncy"]) == (4, 6)                          # radial cells first
 
 
-def test_no_grid_for_triangles_or_shuffled_meshes():
-    nodes, conn = create_rectangle_mesh("tri3", 1.0, 1.0, 4, 4)
-    assert structured_grid(conn, nodes.shape[0]) is None
+@pytest.mark.parametrize("et,span,epc", [("tri3", 1, 2), ("tri6", 2, 2), ("quad8", 2, 1)])
+def test_grid_of_triangle_and_serendipity_meshes(et, span, epc):
+    nodes, conn = create_rectangle_mesh(et, 2.0, 1.0, 5, 3)
+    g = structured_grid(conn, nodes.shape[0])
+    assert (g["span"], g["epc"], g["ncx"], g["ncy"]) == (span, epc, 5, 3)
+    ij = g["node_ij"].double()
+    assert torch.allclose(ij[:, 0] * 2.0 / (span * 5), nodes[:, 0], atol=1e-14)
+    assert torch.allclose(ij[:, 1] / (span * 3), nodes[:, 1], atol=1e-14)
+    if et == "quad8":                                   # the cell centres are not mesh nodes
+        assert int((g["gnode"] < 0).sum()) == 15
+
+
+def test_no_grid_for_shuffled_meshes():
     nodes, conn = create_rectangle_mesh("quad4", 1.0, 1.0, 4, 4)
     assert structured_grid(conn[torch.randperm(16, generator=torch.Generator().manual_seed(0))], 25) is None
+    nodes, conn = create_rectangle_mesh("tri3", 1.0, 1.0, 4, 4)
+    assert structured_grid(conn.flip(1), 25) is None
 
 
 @pytest.mark.parametrize("et,nx,ny,rtol_it", [("quad4", 16, 4, 16), ("quad4", 33, 9, 16), ("quad9", 8, 2, 16)])
