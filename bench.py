@@ -8,7 +8,7 @@ over the multiples of 4 in [16, 512], Q4/Q9 50/50, E log-uniform in [0.5, 2], nu
 axial dead traction uniform in [0.01, 0.05] (strain ~ load / E), 1 load step, Newton tol 1e-10 ||f||,
 PCG with Eisenstat-Walker forcing (cap 5000), preconditioned by geometric multigrid for requests of at
 least 2,500 nodes and by Jacobi below (serving.preconditioner_for).  One step = 32 consecutive requests of the stream; the
-K steps of the timed window are served continuously by the engine (24 slots, FP32 reference-frame
+K steps of the timed window are served continuously by the engine (32 slots, FP32 reference-frame
 operator / FP64 Newton and Krylov vectors, the largest waiting request first); value = requests/s over
 all ranks (each rank serves its own shard of the stream: replicas, weak scaling), device-timed with CUDA
 events joined over the slot streams.  Beside it:
@@ -57,7 +57,7 @@ MATVEC_N = 1600
 # one product: 570.0 + 47.6 MB against 532.6 MB algorithmic); traffic grows with the element count, so the
 # 2.56M launch is charged the same ratio (profiles/k_apply_640k.md)
 DRAM_PER_ALG_BYTE = 617.6e6 / 532.56e6
-SERVE = dict(stream=2000, seed=0, batch=32, slots=24, compare=64, latency_requests=48, cpu_sample_nx=64,
+SERVE = dict(stream=2000, seed=0, batch=32, slots=32, compare=64, latency_requests=48, cpu_sample_nx=64,
              cpu_budget_s=20.0)
 
 
