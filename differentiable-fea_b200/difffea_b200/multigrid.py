@@ -141,10 +141,12 @@ class _Level:
         self.grid.gx, self.grid.gy = gx, gy
         if finer is not None:
             fgx, fgy = finer.gx, finer.gy
-            lx = torch.tensor([min(2 * i, fgx) for i in range(gx + 1)], **i32)
-            ly = torch.tensor([min(2 * j, fgy) for j in range(gy + 1)], **i32)
-            cx = torch.tensor([min(i // 2, gx - 1) for i in range(fgx + 1)], **i32)
-            cy = torch.tensor([min(j // 2, gy - 1) for j in range(fgy + 1)], **i32)
+            # line I of this level lies on line min(2 I, fgx) of the finer one; finer line i lies in cell
+            # min(i // 2, gx - 1) of this level (computed on the device: no host-to-device copies)
+            lx = torch.clamp(2 * torch.arange(gx + 1, **i32), max=fgx)
+            ly = torch.clamp(2 * torch.arange(gy + 1, **i32), max=fgy)
+            cx = torch.clamp(torch.arange(fgx + 1, **i32) // 2, max=gx - 1)
+            cy = torch.clamp(torch.arange(fgy + 1, **i32) // 2, max=gy - 1)
             self.K = torch.empty(64 * gx * gy, dtype=torch.float64, device=device)
             self.fix = torch.empty(self.n_nodes, dtype=torch.uint8, device=device)
             self.keep += [lx, ly, cx, cy]
