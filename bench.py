@@ -302,6 +302,10 @@ def run_serve(args):
     from difffea_b200 import _lib
     from difffea_b200.serving import (ServingEngine, pcg_iteration_bytes, percentile, request_problem, run_plain,
                                       with_arrivals)
+    # the engine's slot threads outnumber the host's cores: threads waiting for the GPU sleep instead of
+    # spinning (per-process context flag, set before the context is created)
+    local_dev = int(os.environ.get("LOCAL_RANK", "0"))
+    blocking = _lib.load().dfea_set_blocking_sync(local_dev, 1) == 0
     rank, world, local = dist_init("nccl")
     dev = torch.device("cuda", torch.cuda.current_device())
     B = SERVE["batch"]
@@ -333,11 +337,17 @@ def run_serve(args):
         batched_ms = eng.device_ms
         s = torch.cuda.current_stream()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # the plain path is one host thread: timed with the default (spinning) synchronisation it would have
+        # in a user's process, not with the engine's blocking one
+        torch.cuda.synchronize()
+        plain_spin = blocking and _lib.load().dfea_set_blocking_sync(local_dev, 0) == 0
         e0.record(s)
         plain = run_plain(timed[:C], dev)
         e1.record(s)
         e1.synchronize()
         plain_ms = e0.elapsed_time(e1)
+        if plain_spin:
+            _lib.load().dfea_set_blocking_sync(local_dev, 1)
         err = max(float((a.u - b.u).abs().max() / b.u.abs().max()) for a, b in zip(results[:C], plain))
         # latency under Poisson arrivals at 80 % of the measured capacity of this replica
         rate = 0.8 * value / world
@@ -369,11 +379,13 @@ def run_serve(args):
                                       f"{B} requests per step ({len(timed)} served continuously, "
                                       f"largest waiting request first), {SERVE['slots']} slots",
                           "parallelism": f"replicas x{world} (stream sharded by request id)",
+                          "host_sync": "blocking" if blocking else "spin (blocking sync refused)",
                           "l2": "roofline leg inputs 2.2 GB > 126 MB L2; serving working sets stream from HBM"},
                "all_converged": ok,
                "batched_vs_plain": {"requests": C, "batched_solves_per_s": C / (batched_ms * 1e-3),
                                     "plain_fp64_solves_per_s": C / (plain_ms * 1e-3),
                                     "ratio": (plain_ms / batched_ms), "max_rel_err": err,
+                                    "plain_host_sync": "spin" if (plain_spin or not blocking) else "blocking",
                                     "plain": "newton_krylov_solve defaults, one request after another: FP64 "
                                              "moduli and gradients, Jacobi-PCG in 8-iteration graphs, product "
                                              "form by mesh size (fused gather below 1.5M elements)"},

@@ -90,6 +90,23 @@ extern "C" int dfea_version(void) { return 10000; }
 
 extern "C" int64_t dfea_launch_count(void) { return (int64_t)g_launches.load(std::memory_order_relaxed); }
 
+// Blocking synchronisation (on != 0) or the default spin/yield heuristic (on == 0) for this process's context
+// on `device`: with blocking, a host thread waiting for the GPU sleeps instead of spinning (many serving
+// threads on few host cores).
+extern "C" int dfea_set_blocking_sync(int32_t device, int32_t on) {
+    int rc = check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    if (rc) return rc;
+    const unsigned int want = on ? cudaDeviceScheduleBlockingSync : cudaDeviceScheduleAuto;
+    rc = check_cuda(cudaSetDeviceFlags(want), "cudaSetDeviceFlags");
+    if (rc) return rc;
+    unsigned int flags = 0;
+    rc = check_cuda(cudaGetDeviceFlags(&flags), "cudaGetDeviceFlags");
+    if (rc) return rc;
+    return (flags & cudaDeviceScheduleMask) == want
+               ? DFEA_OK
+               : set_error(DFEA_ERR_CUDA, "the scheduling flag was not applied (flags 0x%x)", flags);
+}
+
 extern "C" int dfea_element_supported(int32_t nen, int32_t n_q) {
     return (nen == 4 && n_q == 4) || (nen == 9 && n_q == 9) || (nen == 3 && n_q == 1) || (nen == 6 && n_q == 6) ||
            (nen == 8 && n_q == 9);

@@ -82,6 +82,7 @@ _PROTOS = {
     "dfea_last_error": (ctypes.c_char_p, []),
     "dfea_version": (ctypes.c_int, []),
     "dfea_launch_count": (c_i64, []),
+    "dfea_set_blocking_sync": (ctypes.c_int, [c_i32, c_i32]),
     "dfea_element_supported": (ctypes.c_int, [c_i32, c_i32]),
     "dfea_colour_elements": (ctypes.c_int, [c_vp, c_i64, c_i32, c_i64, c_vp, c_vp]),
     "dfea_mesh_pack": (ctypes.c_int, [c_i64, c_i64, c_i32, c_i32, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp,

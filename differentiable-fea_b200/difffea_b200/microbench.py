@@ -6,6 +6,8 @@ launches unless ``--no-flush``).
     python -m difffea_b200.microbench apply --element quad4 --elements 640000 --precision fp64
     python -m difffea_b200.microbench moduli|residual|sensitivity|fields|pcg --element quad4 --elements 640000
                                             [--material mooney_rivlin|...|all]
+    python -m difffea_b200.microbench vcycle --element quad4 --elements 1048576
+                                            multigrid set-up and one V-cycle (structured mesh)
     python -m difffea_b200.microbench solve --element quad4 --nx 256 --precision mixed
                                             one serving request (4:1 cantilever, E 1, nu 0.3, load 0.03)
                                             solved twice; the second solve is timed
@@ -223,6 +225,20 @@ def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters
     return row
 
 
+def vcycle_once(element, n_elements, precision, reps=10):
+    """Set-up and one V-cycle of the multigrid preconditioner on the microbench mesh (CUDA events)."""
+    from difffea_b200.multigrid import Multigrid
+    st = State(element, n_elements, precision)
+    code = _lib.DFEA_F32REF if precision == "ref" else (_lib.DFEA_F64 if st.C.dtype == torch.float64 else _lib.DFEA_F32)
+    mg = Multigrid(st.mesh, st.p)
+    r = torch.randn(st.N2, dtype=torch.float64, generator=torch.Generator().manual_seed(1)).to(st.device)
+    z = torch.empty_like(r)
+    setup_ms, _ = time_launches(lambda: mg.setup(st.C, code, st.diag), reps=3, warmup=1)
+    cycle_ms, cycle_min = time_launches(lambda: mg.apply(r, z), reps=reps)
+    return dict(kernel="vcycle", element=element, n_el=st.n_el, precision=precision,
+                levels=[(lv.gx, lv.gy) for lv in mg.levels], setup_ms=setup_ms, cycle_ms=cycle_ms, cycle_ms_min=cycle_min)
+
+
 def solve_once(element, nx, precision, pcg_graph, form="auto", preconditioner="jacobi"):
     """Wall and device milliseconds of one serving-type request (the second of two identical solves)."""
     import time
@@ -250,7 +266,8 @@ def solve_once(element, nx, precision, pcg_graph, form="auto", preconditioner="j
 
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m difffea_b200.microbench")
-    ap.add_argument("kind", choices=("sweep", "apply", "moduli", "residual", "sensitivity", "fields", "pcg", "solve"))
+    ap.add_argument("kind", choices=("sweep", "apply", "moduli", "residual", "sensitivity", "fields", "pcg", "solve",
+                                     "vcycle"))
     ap.add_argument("--element", default="quad4", choices=tuple(NEN))
     ap.add_argument("--elements", type=int, default=640_000)
     ap.add_argument("--precision", default="fp64", choices=tuple(_SIZES))
@@ -275,6 +292,9 @@ def main(argv=None):
         print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph,
                                     a.form or "auto", a.preconditioner)),
               flush=True)
+        return 0
+    if a.kind == "vcycle":
+        print(json.dumps(vcycle_once(a.element, a.elements, a.precision, a.reps)), flush=True)
         return 0
     if a.kind == "sweep":
         for element in ("quad4", "quad9"):

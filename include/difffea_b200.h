@@ -129,6 +129,12 @@ int dfea_version(void);
  * PCG graph are added when its solve returns).  A diagnostic for benchmarks. */
 int64_t dfea_launch_count(void);
 
+/* Blocking synchronisation (cudaDeviceScheduleBlockingSync, on != 0) or the default heuristic (on == 0)
+ * for this process's context on `device`: with blocking, host threads waiting for the GPU sleep instead of
+ * spinning.  For processes that run many host threads per GPU (the serving engine).  A per-process
+ * setting of this process's context, gone with the process. */
+int dfea_set_blocking_sync(int32_t device, int32_t on);
+
 
 /* 1 if the (nen, n_q) pair is built: (3,1) tri3, (6,6) tri6, (4,4) quad4, (8,9) quad8, (9,9) quad9. */
 int dfea_element_supported(int32_t nen, int32_t n_q);
