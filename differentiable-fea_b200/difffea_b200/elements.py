@@ -10,7 +10,6 @@ grad_shape_functions_2d.py:47-64).
 
 All functions here run on the host (set-up work); the kernels consume the tables they produce.
 """
-import math
 
 import numpy as np
 import torch

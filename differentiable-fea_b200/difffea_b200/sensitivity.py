@@ -1,5 +1,4 @@
 """compute_sensitivity (the reference's sensitivity.py:7-38): forward solve, dL/du, adjoint, implicit VJP."""
-import torch
 from torch.func import grad
 
 from difffea_b200.adjoint import compute_implicit_vjp, solve_adjoint

@@ -10,8 +10,6 @@ the solve ends: faster than the conditional-loop graph, 23 vs 28 us per iteratio
 calls the C ABI directly on these buffers (no allocation per Newton step), reading back only the
 scalars the algorithm branches on: ||R|| per residual evaluation and (status, iterations) per PCG.
 """
-import ctypes
-
 import torch
 
 from difffea_b200 import _lib
