@@ -14,14 +14,27 @@ import torch
 
 from difffea_b200 import ops
 from difffea_b200.newton_krylov import pcg
-from difffea_b200.operators import _f64c, _prepare, make_AT_operator, make_jacobi_preconditioner
+from difffea_b200.operators import _f64c, _prepare, make_AT_operator, make_preconditioner
 
 
-def solve_adjoint(u_star, theta, params, dL_du, rtol=1e-6, max_iter=500):
-    """(lambda (2N,), PCG iterations) of A^T lambda = m * dL/du at the converged state u_star."""
-    AT = make_AT_operator(u_star, theta, params)
-    Minv = make_jacobi_preconditioner(u_star, theta, params)
+def solve_adjoint(u_star, theta, params, dL_du, rtol=1e-6, max_iter=500, preconditioner="jacobi"):
+    """
+    (lambda (2N,), PCG iterations) of A^T lambda = m * dL/du at the converged state u_star.  ``preconditioner``:
+    "jacobi" (the reference's), "block_jacobi", or "multigrid" (structured meshes; the iteration count no
+    longer grows with the mesh, which matters for the tight adjoint tolerances of sensitivities).
+    """
     b = (params["m"] * dL_du).to(torch.float64).contiguous()
+    if preconditioner == "multigrid":
+        from difffea_b200 import _lib
+        from difffea_b200.operators import make_A_operator_cuda, multigrid_for
+        A = make_A_operator_cuda(u_star, theta, params)          # A^T = A: the tangent is symmetric
+        mg = multigrid_for(A.mesh, params)
+        mg.setup(A.C, _lib.DFEA_F64, A.diag)
+        lam = torch.empty_like(b)
+        iters, _ = mg.pcg(b, lam, rtol, max_iter)
+        return lam, iters
+    AT = make_AT_operator(u_star, theta, params)
+    Minv = make_preconditioner(preconditioner, u_star, theta, params)
     return pcg(AT, b, Minv, rtol=rtol, max_iter=max_iter)
 
 

@@ -2,6 +2,8 @@
 Differentiable equilibrium: u*(theta) as a torch.autograd.Function whose backward is the adjoint.
 
     u = equilibrium(theta, params, **solver_options)      forward: device Newton-Krylov solve
+                                                          (adjoint_rtol, adjoint_max_iter and
+                                                          adjoint_preconditioner configure the backward)
     L = compliance(theta, params, **solver_options)       f . u*(theta)
     L.backward()                                          theta.grad = dL/dtheta by the adjoint kernels
 
@@ -20,7 +22,7 @@ class EquilibriumSolve(torch.autograd.Function):
     @staticmethod
     def forward(ctx, theta, params, options):
         opts = dict(options)
-        adj = {k: opts.pop(k) for k in ("adjoint_rtol", "adjoint_max_iter") if k in opts}
+        adj = {k: opts.pop(k) for k in ("adjoint_rtol", "adjoint_max_iter", "adjoint_preconditioner") if k in opts}
         opts.setdefault("verbose", False)
         u = solve_newton_krylov(params, theta.detach(), **opts)
         ctx.save_for_backward(theta.detach(), u)
@@ -33,7 +35,8 @@ class EquilibriumSolve(torch.autograd.Function):
         theta, u = ctx.saved_tensors
         lam, iters = solve_adjoint(u, theta, ctx.params, grad_u.contiguous(),
                                    rtol=ctx.adjoint.get("adjoint_rtol", 1e-10),
-                                   max_iter=ctx.adjoint.get("adjoint_max_iter", 500))
+                                   max_iter=ctx.adjoint.get("adjoint_max_iter", 500),
+                                   preconditioner=ctx.adjoint.get("adjoint_preconditioner", "jacobi"))
         ctx.adjoint_iterations = iters
         return compute_implicit_vjp(u, theta, ctx.params, lam).to(theta.dtype), None, None
 

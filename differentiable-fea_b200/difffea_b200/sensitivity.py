@@ -6,7 +6,7 @@ from difffea_b200.newton_krylov import solve_newton_krylov
 
 
 def compute_sensitivity(params, theta, loss_fn, n_load_steps=5, tol=1e-8, max_newton=25, adjoint_rtol=1e-10,
-                        adjoint_max_iter=500, **solver_kw):
+                        adjoint_max_iter=500, adjoint_preconditioner="jacobi", **solver_kw):
     """
     (u_star, dL/dtheta) for a scalar loss L(u*): u* by the device Newton-Krylov solver, dL/du by
     autodiff of ``loss_fn``, the adjoint by the device PCG, dL/dtheta by the sensitivity kernel.
@@ -16,5 +16,6 @@ def compute_sensitivity(params, theta, loss_fn, n_load_steps=5, tol=1e-8, max_ne
     u_star = solve_newton_krylov(params, theta, n_load_steps=n_load_steps, tol=tol, max_newton=max_newton,
                                  verbose=False, **solver_kw)
     dL_du = grad(loss_fn)(u_star)
-    lam, _ = solve_adjoint(u_star, theta, params, dL_du, rtol=adjoint_rtol, max_iter=adjoint_max_iter)
+    lam, _ = solve_adjoint(u_star, theta, params, dL_du, rtol=adjoint_rtol, max_iter=adjoint_max_iter,
+                           preconditioner=adjoint_preconditioner)
     return u_star, compute_implicit_vjp(u_star, theta, params, lam)
