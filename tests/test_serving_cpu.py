@@ -13,8 +13,8 @@ import pytest
 import torch
 import torch.multiprocessing as mp
 
-from difffea_b200.serving import (Request, ServingEngine, hbm_estimate, percentile, request_problem, request_stream,
-                                  shard_requests, with_arrivals)
+from difffea_b200.serving import (MULTIGRID_MIN_NODES, Request, ServingEngine, hbm_estimate, percentile,
+                                  preconditioner_for, request_problem, request_stream, shard_requests, with_arrivals)
 
 
 def test_request_stream_is_seeded_and_follows_its_distributions():
@@ -60,6 +60,18 @@ def test_hbm_estimate_grows_with_size_and_precision():
     assert hbm_estimate(small) < hbm_estimate(large) < hbm_estimate(q9)
     assert hbm_estimate(large, "fp32") < hbm_estimate(large, "fp64")
     assert hbm_estimate(q9) < 2 ** 30                      # the largest request of the stream fits easily
+
+
+def test_auto_preconditioner_threshold_and_its_memory():
+    small, large = Request(0, "quad4", 64, 1, 0.3, 0.02), Request(1, "quad9", 512, 1, 0.3, 0.02)
+    assert small.n_nodes < MULTIGRID_MIN_NODES <= large.n_nodes
+    assert preconditioner_for(small) == "jacobi" and preconditioner_for(large) == "multigrid"
+    assert preconditioner_for(large, "jacobi") == "jacobi" and preconditioner_for(small, "multigrid") == "multigrid"
+    assert hbm_estimate(large, "fp32", "auto") > hbm_estimate(large, "fp32", "jacobi")
+    assert hbm_estimate(small, "fp32", "auto") == hbm_estimate(small, "fp32", "jacobi")
+    assert hbm_estimate(large, "fp32", "auto") < 2 ** 30
+    served = [preconditioner_for(r) for r in request_stream(400, seed=0)]
+    assert 0.7 < served.count("multigrid") / len(served) < 0.95        # most of the stream is large
 
 
 def test_percentile_is_nearest_rank():
