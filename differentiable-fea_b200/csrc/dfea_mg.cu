@@ -878,6 +878,11 @@ extern "C" int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void
     return check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
 }
 
+extern "C" double dfea_mg_lanczos_bound(const double* hist, int32_t steps) {
+    if (!hist || steps < 1 || steps > 64) return -1.0;
+    return ritz_max(hist, steps);
+}
+
 extern "C" int dfea_mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
                               const double* r, double* z, void* stream) {
     int rc = validate_mg(mesh, mg, "dfea_mg_vcycle");

@@ -126,6 +126,7 @@ _PROTOS = {
     "dfea_mg_dot": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "dfea_mg_lanczos_step": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
     "dfea_mg_dense_max": (c_i64, []),
+    "dfea_mg_lanczos_bound": (ctypes.c_double, [c_vp, c_i32]),
     "dfea_mg_setup": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp]),
     "dfea_mg_vcycle": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp, c_vp]),
     "dfea_mg_pcg": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp, c_f64, c_i32,

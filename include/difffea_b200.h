@@ -393,6 +393,10 @@ typedef struct dfea_mg {
  * Chebyshev coefficients (one host synchronisation). */
 int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
                   const double* diag, void* stream);
+/* Host arithmetic of the set-up: the largest eigenvalue of the Lanczos tridiagonal matrix of `steps`
+ * Jacobi-CG coefficients hist = (alpha_0, beta_0, alpha_1, ...), over the prefix before a breakdown (2.5 if
+ * none), by Sturm-sequence bisection; -1 for bad arguments.  No GPU involved. */
+double dfea_mg_lanczos_bound(const double* hist, int32_t steps);
 /* z = one V-cycle applied to r (the moduli of the set-up). */
 int dfea_mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
                    const double* r, double* z, void* stream);

@@ -64,3 +64,48 @@ def test_oracle_vcycle_is_spd_and_converges_fast(et, nx, ny, rtol_it):
     assert float(r1 @ M(r1)) > 0
     _, it = oracle.pcg(lambda v: A @ v, P["f"] * P["m"], M, rtol=1e-10, max_iter=500)
     assert it <= rtol_it
+
+
+def test_lanczos_bound_is_the_largest_ritz_value():
+    """The C++ set-up's bound (Sturm bisection on the CG tridiagonal) equals numpy's eigenvalue, on the CPU."""
+    import ctypes
+    import numpy as np
+    from difffea_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(0)
+    for steps in (1, 3, 10, 20):
+        hist = np.empty(2 * steps)
+        hist[0::2] = rng.uniform(0.3, 1.5, steps)          # alpha_k > 0
+        hist[1::2] = rng.uniform(0.0, 0.9, steps)          # beta_k >= 0
+        a, b = hist[0::2], hist[1::2]
+        T = np.zeros((steps, steps))
+        for k in range(steps):
+            T[k, k] = 1 / a[k] + (b[k - 1] / a[k - 1] if k else 0.0)
+            if k + 1 < steps:
+                T[k, k + 1] = T[k + 1, k] = np.sqrt(b[k]) / a[k]
+        got = lib.dfea_mg_lanczos_bound(hist.ctypes.data_as(ctypes.c_void_p), steps)
+        assert abs(got - np.linalg.eigvalsh(T).max()) < 1e-12 * abs(got)
+    # a breakdown (alpha <= 0) cuts the matrix; no valid step gives the default 2.5
+    hist = np.array([0.5, 0.2, -1.0, 0.1])
+    assert abs(lib.dfea_mg_lanczos_bound(hist.ctypes.data_as(ctypes.c_void_p), 2) - 2.0) < 1e-12
+    assert lib.dfea_mg_lanczos_bound(np.array([np.nan, 0.0]).ctypes.data_as(ctypes.c_void_p), 1) == 2.5
+    assert lib.dfea_mg_lanczos_bound(hist.ctypes.data_as(ctypes.c_void_p), 0) == -1.0
+
+
+def test_grid_inference_over_random_meshes():
+    """Every structured rectangle mesh (random element type and cell counts) is recognised with its exact
+    counts and node positions; a mesh with two nodes swapped is not."""
+    g = torch.Generator().manual_seed(3)
+    spans = {"quad4": 1, "tri3": 1, "quad9": 2, "quad8": 2, "tri6": 2}
+    for _ in range(25):
+        et = ["quad4", "quad9", "quad8", "tri3", "tri6"][int(torch.randint(0, 5, (1,), generator=g))]
+        nx, ny = (int(v) for v in torch.randint(1, 12, (2,), generator=g))
+        nodes, conn = create_rectangle_mesh(et, float(nx), float(ny), nx, ny)
+        grid = structured_grid(conn, nodes.shape[0])
+        assert grid is not None and (grid["ncx"], grid["ncy"]) == (nx, ny), (et, nx, ny)
+        span = spans[et]
+        assert torch.allclose(grid["node_ij"].double() / span, nodes, atol=1e-12)
+        if conn.shape[0] > 1:
+            bad = conn.clone()
+            bad[0, 0], bad[0, 1] = conn[0, 1], conn[0, 0]
+            assert structured_grid(bad, nodes.shape[0]) is None
