@@ -55,7 +55,7 @@ MATVEC_N = 1600
 # DRAM bytes per algorithmic byte of the FP64 product, from one ncu capture of the same kernel on 640,000 Q4
 # elements with L2 state kept (dram__bytes_read.sum + dram__bytes_write.sum over the four colour passes of
 # one product: 570.0 + 47.6 MB against 532.6 MB algorithmic); traffic grows with the element count, so the
-# 2.56M launch is charged the same ratio (profiles/k_apply_640k.md)
+# 2.56M launch is charged the same ratio
 DRAM_PER_ALG_BYTE = 617.6e6 / 532.56e6
 SERVE = dict(stream=2000, seed=0, batch=32, slots=32, compare=64, latency_requests=48, cpu_sample_nx=64,
              cpu_budget_s=20.0)

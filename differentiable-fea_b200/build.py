@@ -12,6 +12,7 @@ import argparse
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
@@ -54,7 +55,7 @@ def build(force=False, verbose_ptxas=False, quiet=False):
     os.makedirs(OBJ_DIR, exist_ok=True)
     nvcc = _nvcc()
     hdrs = headers()
-    objs = []
+    objs, jobs = [], []
     for src in sources():
         obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
         objs.append(obj)
@@ -64,13 +65,23 @@ def build(force=False, verbose_ptxas=False, quiet=False):
         cmd += ["-c", src, "-o", obj]
         if src.endswith(".cpp"):
             cmd = [nvcc, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC, "-c", src, "-o", obj]
+        jobs.append((src, cmd))
+
+    def compile_one(job):
+        src, cmd = job
         if not quiet:
             print(" ".join(cmd), flush=True)
-        res = subprocess.run(cmd, capture_output=True, text=True)
+        return src, subprocess.run(cmd, capture_output=True, text=True)
+
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        results = list(pool.map(compile_one, jobs))
+    for src, res in results:
         if verbose_ptxas or res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
-        if res.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {os.path.basename(src)}")
+    failed = [os.path.basename(src) for src, res in results if res.returncode != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed on {', '.join(failed)}")
     if force or _stale(LIB, objs):
         cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static"]
         if not quiet:

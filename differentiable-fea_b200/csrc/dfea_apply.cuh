@@ -23,6 +23,8 @@
 // window on the launch that marks them persisting (see `l2_window`).
 #pragma once
 
+#include <mutex>
+
 #include "dfea_common.cuh"
 
 namespace dfea {
@@ -548,17 +550,18 @@ k_apply_ref_elem(Mesh m, const float* __restrict__ C, const RefGrad<NEN, NQ> rg,
 // kMaxBlocks.
 template <auto Kernel, int SMEM, int NT>
 int resident_grid(int64_t n_elements) {
-    static unsigned long long configured = 0ull;  // one bit per device ordinal
+    // the shared-memory opt-in is a property of the function on each device: set once per device ordinal,
+    // race-free when several host threads launch their first product at the same time
+    static std::once_flag configured[64];
     static int blocks_per_sm[64] = {0};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
-    if (!(configured & (1ull << dev))) {
+    std::call_once(configured[dev], [dev] {
         cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
         int b = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, Kernel, NT, SMEM) != cudaSuccess || b < 1) b = 1;
         blocks_per_sm[dev] = b;
-        configured |= (1ull << dev);
-    }
+    });
     const int64_t tiles = (n_elements + NT - 1) / NT;
     int64_t grid = (int64_t)device_sm_count() * blocks_per_sm[dev];
     if (grid > kMaxBlocks) grid = kMaxBlocks;

@@ -36,15 +36,15 @@ static std::atomic<long long> g_launches{0};
 void note_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int device_sm_count() {
-    static int cache[64] = {0};
+    static std::atomic<int> cache[64];   // 0 until queried; threads that race store the same value
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-    if (cache[dev] == 0) {
-        int n = 0;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n == 0) {
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
-        cache[dev] = n;
+        cache[dev].store(n, std::memory_order_relaxed);
     }
-    return cache[dev];
+    return n;
 }
 
 // L2 set-aside for persisting accesses, configured once per device (before any stream capture).

@@ -13,6 +13,8 @@
 // Everything here is deterministic: node-centric gathers in a fixed order, single-block reductions.
 #include <cmath>
 #include <cstdio>
+#include <mutex>
+#include <new>
 
 #include "dfea_common.cuh"
 
@@ -626,13 +628,22 @@ extern "C" int dfea_mg_dense_inverse(const dfea_mg_grid* grid, double* work, dou
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (n <= kMgDenseShared) {
         const size_t smem = (size_t)(2 * n * n + n) * sizeof(double);
-        static bool attr_set = false;  // the attribute is a property of the function, set once per process
-        if (!attr_set) {
-            rc = check_cuda(cudaFuncSetAttribute(k_mg_dense_inverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)((2 * kMgDenseShared * kMgDenseShared + kMgDenseShared) * sizeof(double))),
-                            "cudaFuncSetAttribute");
-            if (rc) return rc;
-            attr_set = true;
+        // the shared-memory opt-in is a property of the function on each device: set once per device
+        // ordinal (a bit per device, set under a mutex so that concurrent first set-ups are safe)
+        static std::mutex attr_mutex;
+        static unsigned long long attr_set = 0ull;
+        int dev = 0;
+        if ((rc = check_cuda(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
+        if (dev < 0 || dev >= 64) return set_error(DFEA_ERR_INVALID, "dfea_mg_dense_inverse: device ordinal %d", dev);
+        {
+            std::lock_guard<std::mutex> lock(attr_mutex);
+            if (!(attr_set & (1ull << dev))) {
+                rc = check_cuda(cudaFuncSetAttribute(k_mg_dense_inverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)((2 * kMgDenseShared * kMgDenseShared + kMgDenseShared) * sizeof(double))),
+                                "cudaFuncSetAttribute");
+                if (rc) return rc;
+                attr_set |= 1ull << dev;
+            }
         }
         k_mg_dense_inverse<true><<<1, 1024, smem, st>>>(mg_grid(*grid), work, Ainv);
     } else {

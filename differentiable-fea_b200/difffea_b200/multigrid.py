@@ -226,6 +226,7 @@ class Multigrid:
             setattr(h, name, getattr(self, name).data_ptr())
         h.pcg = self.pcg_work.data_ptr()
         self.C, self.code = None, None
+        self.generation = 0          # set-ups so far: a preconditioner closure checks that it is still current
 
     @property
     def ref(self):
@@ -234,6 +235,7 @@ class Multigrid:
     def setup(self, C, moduli_code, diag):
         """Coarse operators from the fine moduli C (DFEA_F64 / DFEA_F32 / DFEA_F32REF) and the Jacobi diagonal."""
         self.C, self.code = C, moduli_code
+        self.generation += 1
         _lib.call("dfea_mg_setup", self.mesh.view_ref, self.ref, ptr(C), moduli_code, ptr(diag), stream_handle())
         for l, lv in enumerate(self.levels[:-1]):
             lv.lam = float(self.h.lam[l])

@@ -235,13 +235,29 @@ def make_block_jacobi_preconditioner(u, theta, params):
 
 
 class CudaMultigridPreconditioner:
-    """r -> one V-cycle of the geometric multigrid of a structured mesh (multigrid.py), set up at (u, theta)."""
+    """
+    r -> one V-cycle of the geometric multigrid of a structured mesh (multigrid.py), set up at (u, theta).
 
-    def __init__(self, mg):
-        self.mg = mg
+    The hierarchy's buffers are shared by every preconditioner of the same mesh (one ``Multigrid`` per mesh),
+    while each closure keeps the moduli and diagonal of its own linearisation point: when another set-up
+    has overwritten the coarse operators since this closure was made, the call sets them up again from its
+    own moduli first, so closures made at different states stay independent, as the reference's are.
+    """
+
+    def __init__(self, mg, A):
+        self.mg, self.A = mg, A
         self.mesh = mg.mesh
+        self.generation = mg.generation
+
+    def refresh(self):
+        """Set the shared hierarchy up at this closure's linearisation again if another set-up replaced it."""
+        if self.mg.generation != self.generation:
+            from difffea_b200 import _lib
+            self.mg.setup(self.A.C, _lib.DFEA_F64, self.A.diag)
+            self.generation = self.mg.generation
 
     def __call__(self, r):
+        self.refresh()
         return self.mg(r.to(torch.float64))
 
 
@@ -265,7 +281,7 @@ def make_multigrid_preconditioner(u, theta, params):
     mg = multigrid_for(A.mesh, params)
     from difffea_b200 import _lib
     mg.setup(A.C, _lib.DFEA_F64, A.diag)
-    return CudaMultigridPreconditioner(mg)
+    return CudaMultigridPreconditioner(mg, A)
 
 
 def make_preconditioner(kind, u, theta, params):

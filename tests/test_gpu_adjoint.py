@@ -72,3 +72,44 @@ def test_adjoint_gradient_matches_central_differences():
         Lm = torch.dot(f, solve_newton_krylov(p, tm, 2, 1e-12, verbose=False))
         g_fd[i] = (Lp - Lm) / (2 * eps)
     assert float(torch.norm(g - g_fd) / torch.norm(g_fd)) < 1e-6
+
+
+@pytest.mark.parametrize("preconditioner", ["jacobi", "multigrid"])
+def test_unconverged_adjoint_is_reported(preconditioner):
+    """An adjoint PCG stopped by its iteration cap warns (default) or raises; a converged one is silent."""
+    from difffea_b200.adjoint import AdjointConvergenceWarning
+    d = load("solve_quad4_h0.2_tension")
+    p = params_from(d, DEV)
+    th, u = _t(d, "theta"), _t(d, "u_star")
+    with pytest.warns(AdjointConvergenceWarning, match="max_iter"):
+        _, k, status = solve_adjoint(u, th, p, p["f"], rtol=1e-14, max_iter=2, preconditioner=preconditioner,
+                                     return_status=True)
+    assert (k, status) == (2, "max_iter")
+    with pytest.raises(RuntimeError, match="did not reach"):
+        solve_adjoint(u, th, p, p["f"], rtol=1e-14, max_iter=2, preconditioner=preconditioner, on_failure="raise")
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", AdjointConvergenceWarning)
+        _, _, status = solve_adjoint(u, th, p, p["f"], rtol=1e-10, max_iter=2000, preconditioner=preconditioner,
+                                     return_status=True)
+    assert status == "converged"
+
+
+def test_autograd_backward_reports_an_unconverged_adjoint():
+    from difffea_b200.adjoint import AdjointConvergenceWarning
+    d = load("sensitivity_quad4_h0.25")
+    p = params_from(d, DEV)
+    th = _t(d, "theta").requires_grad_(True)
+    L = compliance(th, p, n_load_steps=2, tol=1e-12, adjoint_max_iter=2, adjoint_preconditioner="jacobi")
+    with pytest.warns(AdjointConvergenceWarning):
+        L.backward()
+    th.grad = None
+    L = compliance(th, p, n_load_steps=2, tol=1e-12, adjoint_max_iter=2, adjoint_preconditioner="jacobi",
+                   adjoint_on_failure="raise")
+    with pytest.raises(RuntimeError, match="did not reach"):
+        L.backward()
+    # the default ("auto": multigrid on this structured mesh) converges and matches the reference
+    th.grad = None
+    L = compliance(th, p, n_load_steps=2, tol=1e-12)
+    L.backward()
+    assert rel(th.grad, d["dL_dtheta"]) < 1e-8

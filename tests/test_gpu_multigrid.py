@@ -143,3 +143,18 @@ def test_unstructured_mesh_is_refused():
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=DEV)
     with pytest.raises(ValueError, match="structured"):
         NewtonWorkspace(p, preconditioner="multigrid")
+
+
+def test_preconditioner_closures_at_different_states_stay_independent():
+    """Two make_preconditioner("multigrid") closures of one mesh share its hierarchy's buffers; the first still
+    applies its own linearisation after the second has been set up (it sets the hierarchy up again)."""
+    p = build_rectangle_problem("quad4", 32, 8, 4.0, 1.0, load=(0.0, -0.01), device=DEV)
+    u1, th, r = _state(p, 21, 0.002)
+    u2, _, _ = _state(p, 22, 0.004)
+    M1 = make_preconditioner("multigrid", u1, th, p)
+    z1 = M1(r).clone()
+    M2 = make_preconditioner("multigrid", u2, th, p)
+    z2 = M2(r).clone()
+    assert M1.mg is M2.mg and not torch.equal(z1, z2)
+    assert torch.equal(M1(r), z1)                          # re-set-up at u1: the same cycle, bit for bit
+    assert torch.equal(M2(r), z2)
