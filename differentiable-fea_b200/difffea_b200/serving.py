@@ -197,6 +197,8 @@ class ServingEngine:
                  pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
                  fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        if self.device.index is None:            # "cuda": the current device, by index (the slot threads set it)
+            self.device = torch.device(self.device.type, torch.cuda.current_device())
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = int(0.6 * free)

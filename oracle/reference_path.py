@@ -272,13 +272,48 @@ def block_jacobi(u, theta, P):
     return lambda r: torch.einsum("nij,nj->ni", Binv, r.reshape(N, 2)).reshape(-1)
 
 
+def assemble_tangent(u, theta, P):
+    """
+    The tangent as a SciPy CSC matrix with identity pivots on constrained DOFs (assemble_tangent_sparse,
+    operators.py:641-677).  The element matrices K_e[(a i), (b k)] = sum_q sum_JL dN_aJ C_(iJ)(kL) dN_bL come
+    from the stored moduli (the same second derivatives the reference takes by jacfwd of the element force),
+    scattered once as COO entries with the rows and columns of constrained DOFs dropped.
+    """
+    import numpy as np
+    import scipy.sparse as sp
+    conn, m, dN = P["conn"], P["m"], P["dN_dX"]
+    n_el, nen = conn.shape
+    C = moduli(u, theta, P).reshape(n_el, -1, 2, 2, 2, 2)                     # [e, q, i, J, k, L]
+    Ke = torch.einsum("eqaJ,eqiJkL,eqbL->eaibk", dN, C, dN).reshape(n_el, 2 * nen, 2 * nen)
+    dofs = (2 * conn[:, :, None] + torch.arange(2)).reshape(n_el, 2 * nen)
+    rows = dofs[:, :, None].expand(-1, -1, 2 * nen).reshape(-1)
+    cols = dofs[:, None, :].expand(-1, 2 * nen, -1).reshape(-1)
+    free = m > 0.5
+    vals = Ke.reshape(-1) * (free[rows] & free[cols])
+    fixed_ids = torch.nonzero(~free).reshape(-1)
+    rows = torch.cat([rows, fixed_ids]).numpy()
+    cols = torch.cat([cols, fixed_ids]).numpy()
+    vals = torch.cat([vals, torch.ones(fixed_ids.numel(), dtype=F64)]).numpy()
+    n = m.numel()
+    return sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsc().astype(np.float64)
+
+
+def ilu_preconditioner(u, theta, P, drop_tol=1e-5, fill_factor=30.0):
+    """Incomplete LU of the assembled tangent, SciPy spilu (make_ilu_preconditioner, operators.py:680-699)."""
+    from scipy.sparse.linalg import spilu
+    ilu = spilu(assemble_tangent(u, theta, P), drop_tol=drop_tol, fill_factor=fill_factor)
+    return lambda r: torch.as_tensor(ilu.solve(r.numpy()), dtype=F64)
+
+
 def preconditioner(kind, u, theta, P):
-    """M^-1 as a closure: "jacobi" (r / diag) or "block_jacobi"."""
+    """M^-1 as a closure: "jacobi" (r / diag), "block_jacobi" or "ilu" (operators.py:702-710)."""
     if kind == "jacobi":
         d = jacobi_diagonal(u, theta, P)
         return lambda r: r / d
     if kind == "block_jacobi":
         return block_jacobi(u, theta, P)
+    if kind == "ilu":
+        return ilu_preconditioner(u, theta, P)
     raise ValueError(kind)
 
 

@@ -274,6 +274,11 @@ EXTRA = {
                                         preconditioner="block_jacobi")),
     # the other materials of the library: operators, solves and sensitivities
     "materials": material_cases,
+    # incomplete-LU preconditioned PCG (operators.py:680-699), the oracle's solver for the large serving requests
+    "ilu": lambda: (solve_case("quad4", 0.2, (60.0, 0.0), 2, 1e-10, "solve_quad4_h0.2_tension_ilu",
+                               preconditioner="ilu"),
+                    solve_case("quad9", 0.5, (0.0, -40.0), 3, 1e-9, "solve_quad9_h0.5_cantilever_ilu",
+                               preconditioner="ilu")),
 }
 
 
