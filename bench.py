@@ -3,33 +3,37 @@ Benchmark of the matrix-free Newton-Krylov hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload serve|plain]
 
-Workload "serve" (default): the seeded 2,000-request serving stream -- 4:1 cantilever bars, nx uniform
+Workload "serve" (default), on the seeded 2,000-request serving stream -- 4:1 cantilever bars, nx uniform
 over the multiples of 4 in [16, 512], Q4/Q9 50/50, E log-uniform in [0.5, 2], nu uniform in [0.2, 0.45],
 axial dead traction uniform in [0.01, 0.05] (strain ~ load / E), 1 load step, Newton tol 1e-10 ||f||,
-PCG with Eisenstat-Walker forcing (cap 5000), preconditioned by geometric multigrid for requests of at
-least 2,500 nodes and by Jacobi below (serving.preconditioner_for).  One step = 32 consecutive requests of the stream; the
-K steps of the timed window are served continuously by the engine (32 slots, FP32 reference-frame
-operator / FP64 Newton and Krylov vectors, the largest waiting request first); value = requests/s over
-all ranks (each rank serves its own shard of the stream: replicas, weak scaling), device-timed with CUDA
-events joined over the slot streams.  Beside it:
-  batched_vs_plain  the first 64 requests of the window through the engine and, one after another,
-                    through the plain FP64 drop-in (newton_krylov_solve defaults): both solves/s, the
-                    ratio and the max relative difference of the solutions
-  serving_hbm       algorithmic bytes of all PCG iterations of the window / device time
-  latency_ms        p50 / p99 of (finish - arrival) for 48 further requests replayed with Poisson
-                    arrivals at 80 % of the measured capacity (first come, first served)
+PCG with Eisenstat-Walker forcing (cap 5000).
+
+The headline ``value`` is measured on the sample both arms can solve in full: the stream's requests with
+nx <= 64, in stream order (the reference's CPU path needs ~0.5 s for one of them and ~nx^3 more for larger
+ones).  One step = 4 consecutive requests of that sample; W steps warm up, the next K steps are timed.
+  ours       the K x 4 requests served continuously by the engine (32 slots, FP32 reference-frame operator /
+             FP64 Newton and Krylov vectors, multigrid-preconditioned from 2,500 nodes, Jacobi below, the
+             largest waiting request first); value = requests / device time (CUDA events joined over the slot
+             streams, max over ranks), each problem built on the device inside the timed region
+  reference  the same K x 4 requests solved one after another by the reference algorithm's CPU path (the
+             oracle: tangent "qp", Jacobi-PCG, newton_krylov.py defaults) on all host cores
+Beside the headline (ours):
+  e2e               the same requests again with each problem dictionary built on the host, pinned and
+                    copied to the device inside the timed region, solutions read back (host wall clock)
+  full_stream       K x 32 consecutive requests of the whole stream (nx 16..512) served continuously
+  batched_vs_plain  the first 64 of those through the engine (auto preconditioner, and Jacobi only) and, one
+                    after another, through the plain FP64 drop-in (newton_krylov_solve defaults): solves/s,
+                    both ratios, the max relative difference of the solutions
+  serving_hbm       algorithmic bytes of the full window's PCG iterations / its device time
+  latency_ms        p50 / p99 of (finish - arrival) over all 2,000 requests of the stream (this rank's shard)
+                    replayed with Poisson arrivals at 80 % of the full window's measured capacity, FIFO
   roofline          the tangent product (kernel (b), FP64 stored moduli) at the microbench size,
                     structured Q4 1600 x 1600 = 2.56M elements (inputs 2.2 GB >> L2), CUDA-event timed
-  cpu_baseline      the oracle (CPU restatement of the reference algorithm, tangent "qp") on the first
-                    requests of the window with nx <= 64, on this host's cores
-  e2e               the 64 requests again with each problem dictionary built on the host (pinned) and
-                    copied to the device inside the timed region, solutions read back to the host
+  cpu_baseline      the oracle on the first 24 requests of the sample, on this host's cores
 
 Workload "plain": one step = one complete FP64 solve of the 100 x 100 Q4 unit-square problem (left edge
-clamped, traction (0.1, 0) on the right edge, 3 load steps, tol 1e-10), the reference's CPU-runnable case.
-
---impl reference times the reference algorithm's CPU implementation (the oracle) on the workload's
-CPU sample.
+clamped, traction (0.1, 0) on the right edge, 3 load steps, tol 1e-10), the reference's CPU-runnable case;
+the reference arm times the same solve on the CPU.
 """
 import argparse
 import json
@@ -57,8 +61,8 @@ MATVEC_N = 1600
 # one product: 570.0 + 47.6 MB against 532.6 MB algorithmic); traffic grows with the element count, so the
 # 2.56M launch is charged the same ratio
 DRAM_PER_ALG_BYTE = 617.6e6 / 532.56e6
-SERVE = dict(stream=2000, seed=0, batch=32, slots=32, compare=64, latency_requests=48, cpu_sample_nx=64,
-             cpu_budget_s=20.0)
+SERVE = dict(stream=2000, seed=0, batch=32, slots=32, compare=64, sample_nx=64, sample_per_step=4,
+             cpu_baseline_requests=24, latency_load=0.8)
 
 
 def peaks():
@@ -154,6 +158,12 @@ def dist_barrier(world):
 # ------------------------------------------------------------------------------------------------
 # workloads
 # ------------------------------------------------------------------------------------------------
+def plain_config():
+    return {"workload": "plain: 100x100 Q4 (10,000 el), E=1 nu=0.3, traction (0.1, 0), 3 load steps, tol 1e-10, "
+                        "Jacobi-PCG (EW forcing, cap 500)",
+            "parallelism": "replicas"}
+
+
 def plain_problem(device):
     from difffea_b200.problem import build_rectangle_problem
     c = PLAIN
@@ -223,39 +233,51 @@ def cpu_oracle_solve(params_cpu, theta_cpu, n_load_steps, tol, pcg_max_iter=500)
     return time.perf_counter() - t, u, info
 
 
-def serve_cpu_sample(requests, budget_s):
-    """The oracle on the window's requests with nx <= cpu_sample_nx, in stream order, until the budget."""
-    from difffea_b200.serving import request_problem
-    done, spent = [], 0.0
-    for r in requests:
-        if r.nx > SERVE["cpu_sample_nx"]:
-            continue
-        p = request_problem(r, "cpu")
-        tol = 1e-10 * float(torch.linalg.vector_norm(p["f"]))
-        dt, _, info = cpu_oracle_solve(p, torch.ones(p["conn"].shape[0], dtype=torch.float64), 1, tol, 5000)
-        done.append((r.rid, r.element_type, r.nx, dt))
-        spent += dt
-        if spent >= budget_s:
-            break
-    if not done:                                   # no small request in the window: the smallest one
-        r = min(requests, key=lambda q: q.nx)
-        p = request_problem(r, "cpu")
-        tol = 1e-10 * float(torch.linalg.vector_norm(p["f"]))
-        dt, _, _ = cpu_oracle_solve(p, torch.ones(p["conn"].shape[0], dtype=torch.float64), 1, tol, 5000)
-        done, spent = [(r.rid, r.element_type, r.nx, dt)], dt
-    return done, spent
+def serve_config(steps):
+    """The workload description both arms print (the same dictionary: the driver compares them)."""
+    S = SERVE["sample_per_step"]
+    return {"workload": f"serve, like-for-like sample: the requests of the seeded 2000-request stream with nx <= "
+                        f"{SERVE['sample_nx']} in stream order (4:1 cantilever bars, Q4/Q9, E 0.5..2, nu 0.2..0.45, "
+                        f"axial load 0.01..0.05, 1 load step, tol 1e-10 ||f||), {S} requests per step, {steps * S} "
+                        f"timed; nx 16..512 stream window under full_stream",
+            "parallelism": "replicas (stream sharded by request id)",
+            "l2": "serving working sets stream from HBM; roofline leg inputs 2.2 GB > 126 MB L2"}
 
 
-def stream_windows(rank, world, steps, warmup):
-    """This rank's shard of the request stream: timed window, warm-up window, latency window."""
+def stream_shard(rank, world):
     from difffea_b200.serving import request_stream, shard_requests
-    mine = shard_requests(request_stream(SERVE["stream"], seed=SERVE["seed"]), rank, world)
+    return shard_requests(request_stream(SERVE["stream"], seed=SERVE["seed"]), rank, world)
+
+
+def sample_windows(rank, world, steps, warmup):
+    """This rank's like-for-like sample (nx <= sample_nx, stream order): warm-up requests, timed requests."""
+    S = SERVE["sample_per_step"]
+    small = [r for r in stream_shard(rank, world) if r.nx <= SERVE["sample_nx"]]
+    need = (warmup + steps) * S
+    if len(small) < need:                       # more steps than the stream holds: cycle through it again
+        small = (small * (need // max(1, len(small)) + 1))[:need]
+    return small[:warmup * S], small[warmup * S:need]
+
+
+def full_windows(rank, world, steps, warmup):
+    """This rank's whole-stream windows (nx 16..512): timed window and warm-up window."""
+    mine = stream_shard(rank, world)
     B = SERVE["batch"]
     timed = mine[:steps * B]
-    rest = mine[steps * B:]
-    lat = rest[:SERVE["latency_requests"]]
-    warm = rest[SERVE["latency_requests"]:SERVE["latency_requests"] + warmup * B] or mine[:warmup * B]
-    return timed, warm, lat
+    warm = mine[steps * B:(steps + warmup) * B] or mine[:warmup * B]
+    return timed, warm
+
+
+def oracle_request_solve(req):
+    """One request by the oracle on this host's cores (tangent "qp", Jacobi-PCG): (seconds, u, info)."""
+    from difffea_b200.serving import request_problem
+    p = request_problem(req, "cpu")
+    tol = 1e-10 * float(torch.linalg.vector_norm(p["f"]))
+    return cpu_oracle_solve(p, torch.ones(p["conn"].shape[0], dtype=torch.float64), 1, tol, 5000)
+
+
+def describe(reqs):
+    return ", ".join(f"{r.element_type} nx={r.nx}" for r in reqs)
 
 
 # ------------------------------------------------------------------------------------------------
@@ -270,28 +292,28 @@ def run_reference(args):
         p = build_rectangle_problem(c["element_type"], c["nx"], c["ny"], c["width"], c["height"], E=c["E"],
                                     nu=c["nu"], load=c["load"])
         th = torch.ones(p["conn"].shape[0], dtype=torch.float64)
-        times, spent = [], 0.0
-        for i in range(args.warmup + args.steps):
+        cpu_oracle_solve(p, th, c["n_load_steps"], c["tol"])          # one warm-up solve
+        times = []
+        for i in range(args.steps):
             dt, _, _ = cpu_oracle_solve(p, th, c["n_load_steps"], c["tol"])
-            spent += dt
-            if i >= args.warmup:
-                times.append(dt)
-            if spent > 240.0 and times:
-                break
+            times.append(dt)
         sample = f"{len(times)} complete solves of the plain problem (oracle restatement, tangent qp)"
-        workload = "plain: 100x100 Q4 neo-Hookean, 3 load steps, Newton tol 1e-10, Jacobi-PCG"
+        config = plain_config()
+        n_solves = len(times)
     else:
-        timed, _, _ = stream_windows(0, 1, args.steps, args.warmup)
-        done, _ = serve_cpu_sample(timed, SERVE["cpu_budget_s"] * 3)
-        times = [d[3] for d in done]
-        sample = (f"{len(done)} requests of the timed window with nx <= {SERVE['cpu_sample_nx']} in stream order "
-                  f"({', '.join(f'{d[1]} nx={d[2]}' for d in done)}); larger requests cost the CPU ~nx^3 more")
-        workload = "serve: seeded 2000-request cantilever stream (CPU sample)"
-    v = len(times) / sum(times)
+        warm, timed = sample_windows(0, 1, args.steps, args.warmup)
+        for r in warm[:1]:                                              # warm-up: CPU kernels and allocator
+            oracle_request_solve(r)
+        times = [oracle_request_solve(r)[0] for r in timed]
+        sample = (f"the {len(timed)} timed requests of the like-for-like sample, one after another "
+                  f"({describe(timed)})")
+        config = serve_config(args.steps)
+        n_solves = len(timed)
+    v = n_solves / sum(times)
     line = {"metric": METRIC, "value": v, "unit": "solves/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload, "parallelism": "host CPU"},
+            "config": config,
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -309,11 +331,13 @@ def run_serve(args):
     rank, world, local = dist_init("nccl")
     dev = torch.device("cuda", torch.cuda.current_device())
     B = SERVE["batch"]
-    timed, warm, lat_reqs = stream_windows(rank, world, args.steps, args.warmup)
-    # the timed window is a backlog: slots take the largest waiting request first
+    warm_s, timed_s = sample_windows(rank, world, args.steps, args.warmup)
+    timed_f, warm_f = full_windows(rank, world, args.steps, args.warmup)
+    # a backlog: slots take the largest waiting request first
     eng = ServingEngine(n_slots=SERVE["slots"], device=dev, precision="fp32", order="largest_first")
-    eng.run(warm, keep_solutions=False)                        # W steps of warm-up, served continuously
-    run_plain(warm[:2], dev)                                   # plain path warm-up (kernels, graphs)
+    eng.run(warm_f, keep_solutions=False)                      # warm-up over the whole size range
+    eng.run(warm_s, keep_solutions=False)                      # W steps of the sample
+    run_plain(warm_f[:2], dev)                                 # plain path warm-up (kernels, graphs)
     torch.cuda.synchronize()
 
     lib = _lib.load()
@@ -321,20 +345,49 @@ def run_serve(args):
         dist_barrier(world)
         torch.cuda.synchronize()
         n0 = lib.dfea_launch_count()
-        results = eng.run(timed)                               # K steps of B requests, served continuously
+        results_s = eng.run(timed_s)                           # K steps of the sample, served continuously
         launches = lib.dfea_launch_count() - n0
         torch.cuda.synchronize()
         dist_barrier(world)
-    total_ms = dist_max(eng.device_ms, world, dev)
-    value = world * len(timed) / (total_ms * 1e-3)
-    ok = all(r.converged and not r.error for r in results)
+        sample_ms = dist_max(eng.device_ms, world, dev)
+        # end to end, the same requests: each problem built on the host, pinned, copied inside the slot
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        results_e = eng.run(timed_s, source="host")
+        e2e_s = dist_max(eng.wall, world, dev)
+        # the whole stream's window
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        results_f = eng.run(timed_f)
+        torch.cuda.synchronize()
+        full_ms = dist_max(eng.device_ms, world, dev)
+        dist_barrier(world)
+    value = world * len(timed_s) / (sample_ms * 1e-3)
+    full_value = world * len(timed_f) / (full_ms * 1e-3)
+    ok = all(r.converged and not r.error for r in results_s + results_e + results_f)
+    e2e_same = max(float((a.u - b.u).abs().max() / b.u.abs().max()) for a, b in zip(results_e, results_s))
+    h2d = sum(v.numel() * v.element_size() for r in timed_s for v in request_problem(r, "cpu").values()
+              if torch.is_tensor(v))
+    d2h = sum(r.u.numel() * 8 for r in results_e)
+
+    # latency over the whole stream (this rank's shard), Poisson arrivals at 80 % of the measured capacity
+    rate = SERVE["latency_load"] * full_value / world
+    eng_fifo = ServingEngine(n_slots=SERVE["slots"], device=dev, precision="fp32", order="fifo")
+    lat_res = eng_fifo.run(with_arrivals(stream_shard(rank, world), rate, seed=7), keep_solutions=False)
+    lat = [1e3 * r.latency for r in lat_res]
+    lat_ok = all(r.converged and not r.error for r in lat_res)
 
     out = None
     if rank == 0:
-        # the same requests through the engine and through the plain FP64 drop-in, one after another
-        C = min(SERVE["compare"], len(timed))
-        eng.run(timed[:C], keep_solutions=False)
-        batched_ms = eng.device_ms
+        # the same requests through the engine (auto preconditioner; Jacobi only) and through the plain FP64
+        # drop-in, one after another
+        C = min(SERVE["compare"], len(timed_f))
+        eng.run(timed_f[:C], keep_solutions=False)
+        auto_ms = eng.device_ms
+        eng_j = ServingEngine(n_slots=SERVE["slots"], device=dev, precision="fp32", order="largest_first",
+                              preconditioner="jacobi")
+        jac_res = eng_j.run(timed_f[:C])
+        jac_ms = eng_j.device_ms
         s = torch.cuda.current_stream()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         # the plain path is one host thread: timed with the default (spinning) synchronisation it would have
@@ -342,73 +395,64 @@ def run_serve(args):
         torch.cuda.synchronize()
         plain_spin = blocking and _lib.load().dfea_set_blocking_sync(local_dev, 0) == 0
         e0.record(s)
-        plain = run_plain(timed[:C], dev)
+        plain = run_plain(timed_f[:C], dev)
         e1.record(s)
         e1.synchronize()
         plain_ms = e0.elapsed_time(e1)
         if plain_spin:
             _lib.load().dfea_set_blocking_sync(local_dev, 1)
-        err = max(float((a.u - b.u).abs().max() / b.u.abs().max()) for a, b in zip(results[:C], plain))
-        # latency under Poisson arrivals at 80 % of the measured capacity of this replica
-        rate = 0.8 * value / world
-        eng_fifo = ServingEngine(n_slots=SERVE["slots"], device=dev, precision="fp32", order="fifo")
-        lat_res = eng_fifo.run(with_arrivals(lat_reqs, rate, seed=7), keep_solutions=False)
-        lat = [1e3 * r.latency for r in lat_res]
-        # end to end: problems built on the host (pinned), copied inside the timed region
-        host = {}
-        for r in timed[:C]:
-            hp = request_problem(r, "cpu")
-            host[r.rid] = {k: (v.pin_memory() if torch.is_tensor(v) else v) for k, v in hp.items()}
-        h2d = sum(v.numel() * v.element_size() for hp in host.values() for v in hp.values() if torch.is_tensor(v))
-        torch.cuda.synchronize()
-        e2e_res = eng.run(timed[:C], host_params=host)
-        e2e = C / eng.wall                             # host wall clock: copies, solves and read-back
-        d2h = sum(r.u.numel() * 8 for r in e2e_res)
-        # aggregate traffic of the PCG iterations in the timed window (algorithmic bytes / device time)
-        pcg_bytes = sum(r.cg * pcg_iteration_bytes(q) for r, q in zip(results, timed))
+        err = max(float((a.u - b.u).abs().max() / b.u.abs().max()) for a, b in zip(results_f[:C], plain))
+        err_j = max(float((a.u - b.u).abs().max() / b.u.abs().max()) for a, b in zip(jac_res, plain))
+        pcg_bytes = sum(r.cg * pcg_iteration_bytes(q) for r, q in zip(results_f, timed_f))
         roof = matvec_roofline(dev)
         hbm, kind = peaks()
-        cpu_done, cpu_s = serve_cpu_sample(timed, SERVE["cpu_budget_s"])
+        cpu_reqs = timed_s[:SERVE["cpu_baseline_requests"]]
+        cpu_s = sum(oracle_request_solve(r)[0] for r in cpu_reqs)
         out = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+               "warmup": args.warmup, "ms_per_step": sample_ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32 operator / f64 Newton and Krylov vectors",
-               "data": "synthetic (seeded request stream)",
-               "config": {"workload": "serve: seeded 2000-request stream of 4:1 cantilever bars (nx 16..512, Q4/Q9, "
-                                      "E 0.5..2, nu 0.2..0.45, axial load 0.01..0.05), 1 load step, tol 1e-10 ||f||, "
-                                      "PCG cap 5000, multigrid-preconditioned from 2500 nodes, Jacobi below; "
-                                      f"{B} requests per step ({len(timed)} served continuously, "
-                                      f"largest waiting request first), {SERVE['slots']} slots",
-                          "parallelism": f"replicas x{world} (stream sharded by request id)",
-                          "host_sync": "blocking" if blocking else "spin (blocking sync refused)",
-                          "l2": "roofline leg inputs 2.2 GB > 126 MB L2; serving working sets stream from HBM"},
-               "all_converged": ok,
-               "batched_vs_plain": {"requests": C, "batched_solves_per_s": C / (batched_ms * 1e-3),
-                                    "plain_fp64_solves_per_s": C / (plain_ms * 1e-3),
-                                    "ratio": (plain_ms / batched_ms), "max_rel_err": err,
+               "data": "synthetic (seeded request stream)", "config": serve_config(args.steps),
+               "engine": f"{SERVE['slots']} slots, largest waiting request first, multigrid-preconditioned from "
+                         f"2500 nodes, Jacobi below, host sync "
+                         f"{'blocking' if blocking else 'spin (blocking sync refused)'}",
+               "all_converged": ok and lat_ok,
+               "e2e": {"value": world * len(timed_s) / e2e_s, "unit": "solves/s", "requests": len(timed_s),
+                       "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+                       "max_rel_diff_vs_value_run": e2e_same,
+                       "covers": "problem build on the host, pinned H2D copy, solve, D2H of u, per request"},
+               "full_stream": {"value": full_value, "unit": "solves/s", "requests": len(timed_f) * world,
+                               "window": f"{len(timed_f)} consecutive requests of the stream per rank (nx 16..512, "
+                                         f"{B} per step), served continuously",
+                               "ms": full_ms},
+               "batched_vs_plain": {"requests": C, "plain_fp64_solves_per_s": C / (plain_ms * 1e-3),
+                                    "engine_auto_solves_per_s": C / (auto_ms * 1e-3),
+                                    "engine_jacobi_solves_per_s": C / (jac_ms * 1e-3),
+                                    "ratio_auto": plain_ms / auto_ms, "ratio_jacobi": plain_ms / jac_ms,
+                                    "max_rel_err_auto": err, "max_rel_err_jacobi": err_j,
                                     "plain_host_sync": "spin" if (plain_spin or not blocking) else "blocking",
                                     "plain": "newton_krylov_solve defaults, one request after another: FP64 "
                                              "moduli and gradients, Jacobi-PCG in 8-iteration graphs, product "
-                                             "form by mesh size (fused gather below 1.5M elements)"},
-               "serving_hbm": {"achieved_gbs": pcg_bytes / (total_ms * 1e-3) / 1e9,
-                               "frac": pcg_bytes / (total_ms * 1e-3) / 1e9 / hbm,
-                               "pcg_iterations": int(sum(r.cg for r in results)),
-                               "bytes": "serving.pcg_iteration_bytes x PCG iterations, over the timed window (the "
+                                             "form by mesh size (fused gather below 1.5M elements)",
+                                    "reading": "ratio_jacobi isolates the engine (batching, FP32 operator); "
+                                               "ratio_auto adds the multigrid preconditioner"},
+               "serving_hbm": {"achieved_gbs": pcg_bytes / (full_ms * 1e-3) / 1e9,
+                               "frac": pcg_bytes / (full_ms * 1e-3) / 1e9 / hbm,
+                               "pcg_iterations": int(sum(r.cg for r in results_f)),
+                               "bytes": "serving.pcg_iteration_bytes x PCG iterations over the full window (the "
                                         "operator's bytes per iteration; a multigrid iteration moves more: its "
                                         "cycle's products and transfers are not counted)"},
                "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99), "requests": len(lat),
-                              "arrival_rate_per_s": rate},
+                              "arrival_rate_per_s": rate, "load": SERVE["latency_load"], "order": "fifo"},
                "roofline": {"bound": "hbm", "achieved": roof["gbs"], "peak": hbm, "unit": "GB/s",
                             "frac": roof["gbs"] / hbm, "traffic": roof["bytes"] * DRAM_PER_ALG_BYTE, "peak_kind": kind,
                             "traffic_source": "ncu, 640k-element capture scaled by element count",
                             "kernel": "k_apply<4,4,double,double> (A(v), FP64 stored moduli)",
                             "workload": f"structured Q4 {MATVEC_N}x{MATVEC_N} = {roof['n_el']} elements",
                             "alg_bytes_per_launch": roof["bytes"], "ms_per_product": roof["ms"]},
-               "cpu_baseline": {"value": len(cpu_done) / cpu_s, "unit": "solves/s", "cores": os.cpu_count(),
+               "cpu_baseline": {"value": len(cpu_reqs) / cpu_s, "unit": "solves/s", "cores": os.cpu_count(),
                                 "kind": "port",
-                                "sample": f"{len(cpu_done)} requests of the timed window with nx <= "
-                                          f"{SERVE['cpu_sample_nx']} ({', '.join(f'{d[1]} nx={d[2]}' for d in cpu_done)})"},
-               "e2e": {"value": e2e, "unit": "solves/s", "requests": C, "h2d_bytes_per_step": int(h2d * B / C),
-                       "d2h_bytes_per_step": int(d2h * B / C)},
+                                "sample": f"the first {len(cpu_reqs)} timed requests of the like-for-like sample "
+                                          f"({describe(cpu_reqs)})"},
                "gpu_launches": int(launches),
                "clocks": clocks.summary()}
         print(json.dumps(out))
@@ -477,9 +521,7 @@ def run_plain_workload(args):
         print(json.dumps({"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
                           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                          "config": {"workload": "plain: 100x100 Q4 (10,000 el), E=1 nu=0.3, traction (0.1, 0), "
-                                                 "3 load steps, tol 1e-10, Jacobi-PCG (EW forcing, cap 500)",
-                                     "parallelism": f"replicas x{world}"},
+                          "config": plain_config(),
                           "latency_ms": {"p50": ls[len(ls) // 2], "p99": ls[min(len(ls) - 1, int(0.99 * len(ls)))]},
                           "accuracy": {"rel_err_vs_oracle": err, "newton": info["total_newton"], "cg": info["total_cg"],
                                        "newton_oracle": info_ref["total_newton"], "cg_oracle": info_ref["total_cg"]},

@@ -265,13 +265,17 @@ class ServingEngine:
         return self._streams
 
     # run --------------------------------------------------------------------------------------------
-    def run(self, requests, keep_solutions=True, host_params=None):
+    def run(self, requests, keep_solutions=True, host_params=None, source="device"):
         """
-        Serve ``requests``; ``host_params`` (rid -> problem dictionary in pinned host memory) makes each
-        slot copy its problem to the device instead of building it there.  After the call
-        ``self.device_ms`` is the device time from the first slot's start to the last slot's end
-        (CUDA events joined over the slot streams) and ``self.wall`` the host wall time.
+        Serve ``requests``.  Where a slot gets a request's problem dictionary: ``source="device"`` builds it on
+        the GPU (torch ops on the slot's stream); ``source="host"`` builds it on the CPU, pins it and copies it
+        to the device inside the slot (the path of a client that submits requests from host memory);
+        ``host_params`` (rid -> problem dictionary in pinned host memory) copies a dictionary built before the
+        call.  After the call ``self.device_ms`` is the device time from the first slot's start to the last
+        slot's end (CUDA events joined over the slot streams) and ``self.wall`` the host wall time.
         """
+        if source not in ("device", "host"):
+            raise ValueError("source must be 'device' or 'host'")
         results = {r.rid: Result(r.rid, arrival=r.arrival) for r in requests}
         q = queue.PriorityQueue()      # entries (priority, sequence, request); None ends a worker
         streams = self._slot_streams()
@@ -298,6 +302,9 @@ class ServingEngine:
                     res.admitted = time.perf_counter() - t0
                     with torch.cuda.stream(stream):
                         hp = host_params.get(req.rid) if host_params is not None else None
+                        if hp is None and source == "host":
+                            hp = {k: (v.pin_memory() if torch.is_tensor(v) else v)
+                                  for k, v in request_problem(req, "cpu").items()}
                         u, info = solve_request(req, self.device, host_params=hp, **self.solve_kw)
                         res.u = u.to("cpu") if keep_solutions else None
                         stream.synchronize()

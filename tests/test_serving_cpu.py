@@ -134,11 +134,13 @@ def _rank_main(rank, world, port, out):
     assert (r, w) == (rank, world)
     bench.dist_barrier(w)
     m = bench.dist_max(float(10 * rank + 1), w, torch.device("cpu"))
-    timed, warm, lat = bench.stream_windows(r, w, steps=2, warmup=3)
+    timed, warm = bench.full_windows(r, w, steps=2, warmup=3)
+    warm_s, timed_s = bench.sample_windows(r, w, steps=2, warmup=3)
     import torch.distributed as dist
-    ids = [None] * w
+    ids, sample_ids = [None] * w, [None] * w
     dist.all_gather_object(ids, [q.rid for q in timed])
-    out[rank] = (m, ids, len(warm), len(lat))
+    dist.all_gather_object(sample_ids, [q.rid for q in warm_s + timed_s])
+    out[rank] = (m, ids, len(warm), sample_ids, max(q.nx for q in timed_s), bench.serve_config(2))
     dist.destroy_process_group()
 
 
@@ -147,9 +149,14 @@ def test_two_rank_bench_helpers_over_gloo():
     out = mp.get_context("spawn").Manager().dict()
     mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
     for rank in range(world):
-        m, ids, n_warm, n_lat = out[rank]
+        m, ids, n_warm, sample_ids, max_nx, config = out[rank]
         assert m == 11.0                                      # max over ranks of (1, 11)
         assert set(ids[0]).isdisjoint(ids[1])                 # each replica serves its own requests
         assert all(i % world == 0 for i in ids[0]) and all(i % world == 1 for i in ids[1])
         assert len(ids[0]) == len(ids[1]) == 2 * 32
-        assert n_warm > 0 and n_lat == 48
+        assert n_warm > 0
+        # the like-for-like sample: disjoint per replica, 4 requests per step, small requests only
+        assert set(sample_ids[0]).isdisjoint(sample_ids[1])
+        assert len(sample_ids[0]) == len(sample_ids[1]) == (3 + 2) * 4
+        assert max_nx <= 64
+        assert config == out[0][5]                            # both arms and all ranks print one config
