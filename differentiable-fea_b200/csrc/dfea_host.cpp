@@ -139,3 +139,19 @@ extern "C" int dfea_colour_elements(const int64_t* conn, int64_t n_el, int32_t n
     *n_colours = n_used > 0 ? n_used : 1;
     return DFEA_OK;
 }
+
+// sizeof of the public structs, by name: lets a binding check its mirrors against this build's layout
+extern "C" int64_t dfea_struct_size(const char* name) {
+    if (!name) return -1;
+    struct Entry { const char* name; int64_t size; };
+    static const Entry table[] = {
+        {"dfea_material", (int64_t)sizeof(dfea_material)},   {"dfea_mesh_view", (int64_t)sizeof(dfea_mesh_view)},
+        {"dfea_mg_grid", (int64_t)sizeof(dfea_mg_grid)},     {"dfea_mg_level", (int64_t)sizeof(dfea_mg_level)},
+        {"dfea_mg", (int64_t)sizeof(dfea_mg)},               {"dfea_newton", (int64_t)sizeof(dfea_newton)},
+        {"dfea_newton_record", (int64_t)sizeof(dfea_newton_record)},
+        {"dfea_newton_info", (int64_t)sizeof(dfea_newton_info)},
+    };
+    for (const Entry& e : table)
+        if (std::strcmp(e.name, name) == 0) return e.size;
+    return -1;
+}

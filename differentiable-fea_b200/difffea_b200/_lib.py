@@ -78,12 +78,34 @@ class Mg(ctypes.Structure):
                 ("Ainv", c_vp), ("dense_work", c_vp), ("coef", c_vp), ("lscal", c_vp), ("lhist", c_vp),
                 ("dot_work", c_vp), ("pcg", c_vp), ("scal", c_vp), ("lam", c_f64 * MG_MAX_LEVELS)]
 
+class Newton(ctypes.Structure):
+    """Mirror of ``dfea_newton``: the problem, the buffers and the linear solver of one Newton-Krylov solve."""
+    _fields_ = [("mesh", ctypes.POINTER(MeshView)), ("material", Material), ("theta", c_vp), ("f", c_vp),
+                ("u_D", c_vp), ("u", c_vp), ("w", c_vp), ("uc", c_vp), ("R", c_vp), ("Rc", c_vp), ("du", c_vp),
+                ("b", c_vp), ("diag", c_vp), ("blocks", c_vp), ("moduli", c_vp), ("moduli_dtype", c_i32),
+                ("reserved", c_i32), ("reduce_work", c_vp), ("scal", c_vp), ("scal_host", c_vp), ("pcg", c_vp),
+                ("mg", ctypes.POINTER(Mg)), ("min_rtol", c_f64)]
+
+
+class NewtonRecord(ctypes.Structure):
+    """Mirror of ``dfea_newton_record``."""
+    _fields_ = [("step", c_i32), ("iteration", c_i32), ("cg_iters", c_i32), ("pcg_status", c_i32),
+                ("load_factor", c_f64), ("residual", c_f64), ("alpha", c_f64)]
+
+
+class NewtonInfo(ctypes.Structure):
+    """Mirror of ``dfea_newton_info``."""
+    _fields_ = [("converged", c_i32), ("total_newton", c_i32), ("total_cg", c_i32), ("n_cutbacks", c_i32),
+                ("load_factor", c_f64), ("n_records", c_i32), ("reserved", c_i32)]
+
+
 _PROTOS = {
     "dfea_last_error": (ctypes.c_char_p, []),
     "dfea_version": (ctypes.c_int, []),
     "dfea_launch_count": (c_i64, []),
     "dfea_set_blocking_sync": (ctypes.c_int, [c_i32, c_i32]),
     "dfea_element_supported": (ctypes.c_int, [c_i32, c_i32]),
+    "dfea_struct_size": (c_i64, [ctypes.c_char_p]),
     "dfea_colour_elements": (ctypes.c_int, [c_vp, c_i64, c_i32, c_i64, c_vp, c_vp]),
     "dfea_mesh_pack": (ctypes.c_int, [c_i64, c_i64, c_i32, c_i32, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp,
                                       c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
@@ -145,6 +167,8 @@ _PROTOS = {
     "dfea_pcg_destroy": (ctypes.c_int, [c_vp]),
     "dfea_pcg_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp, c_i32, c_f64, c_i32,
                                               ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_vp]),
+    "dfea_newton_solve": (ctypes.c_int, [ctypes.POINTER(Newton), c_i32, c_f64, c_i32, c_i32, c_i32,
+                                         ctypes.POINTER(NewtonInfo), ctypes.POINTER(NewtonRecord), c_i32, c_vp]),
     "dfea_axpy": (ctypes.c_int, [c_i64, c_f64, c_vp, c_vp, c_vp]),
     "dfea_add_scaled": (ctypes.c_int, [c_i64, c_vp, c_f64, c_vp, c_vp, c_vp]),
     "dfea_f64_to_f32": (ctypes.c_int, [c_i64, c_vp, c_vp, c_vp]),

@@ -16,7 +16,7 @@ import warnings
 
 import torch
 
-from difffea_b200 import _lib
+from difffea_b200 import _lib, ops
 from difffea_b200.cuda_mesh import ptr, stream_handle
 
 
@@ -97,15 +97,14 @@ class DevicePCG:
         self.use_graph = use_graph
         self.form = form
         self.last_status = None
+        self.id = ops.register_handle(self)
 
     def solve(self, rtol, max_iter=500):
-        """Run PCG on the bound buffers; returns (iterations, status string).  Blocks until done."""
-        iters, status = ctypes.c_int32(0), ctypes.c_int32(0)
-        with torch.cuda.device(self.mesh.device):
-            _lib.call("dfea_pcg_solve", self._h, float(rtol), int(max_iter), ctypes.byref(iters), ctypes.byref(status),
-                      stream_handle())
-        self.last_status = _lib.PCG_STATUS.get(status.value, str(status.value))
-        return iters.value, self.last_status
+        """Run PCG on the bound buffers (custom op pcg_solve); returns (iterations, status string).  Blocks
+        until done."""
+        it, st = torch.ops.difffea_b200.pcg_solve(self.id, self.x, float(rtol), int(max_iter)).tolist()
+        self.last_status = _lib.PCG_STATUS.get(st, str(st))
+        return it, self.last_status
 
     def close(self):
         if self._h and self._h.value:

@@ -28,8 +28,7 @@ import math
 
 import torch
 
-from difffea_b200 import _lib
-from difffea_b200.cuda_mesh import ptr, stream_handle
+from difffea_b200 import _lib, ops
 
 COARSEST_NODES = 48           # levels are coarsened until a level has at most this many nodes (96 DOFs: the
                               # dense Gauss-Jordan of the coarsest operator then runs in shared memory)
@@ -226,6 +225,7 @@ class Multigrid:
             setattr(h, name, getattr(self, name).data_ptr())
         h.pcg = self.pcg_work.data_ptr()
         self.C, self.code = None, None
+        self.id = ops.register_handle(self)
         self.generation = 0          # set-ups so far: a preconditioner closure checks that it is still current
 
     @property
@@ -233,26 +233,23 @@ class Multigrid:
         return ctypes.byref(self.h)
 
     def setup(self, C, moduli_code, diag):
-        """Coarse operators from the fine moduli C (DFEA_F64 / DFEA_F32 / DFEA_F32REF) and the Jacobi diagonal."""
+        """Coarse operators from the fine moduli C (DFEA_F64 / DFEA_F32 / DFEA_F32REF) and the Jacobi diagonal
+        (custom op mg_setup)."""
         self.C, self.code = C, moduli_code
         self.generation += 1
-        _lib.call("dfea_mg_setup", self.mesh.view_ref, self.ref, ptr(C), moduli_code, ptr(diag), stream_handle())
-        for l, lv in enumerate(self.levels[:-1]):
-            lv.lam = float(self.h.lam[l])
+        lam = torch.ops.difffea_b200.mg_setup(self.id, C, int(moduli_code), diag).tolist()
+        for lv, x in zip(self.levels[:-1], lam):
+            lv.lam = x
 
     def apply(self, r, z):
-        """z = M^-1 r (one V-cycle); r and z are (2N,) float64 device vectors."""
-        _lib.call("dfea_mg_vcycle", self.mesh.view_ref, self.ref, ptr(self.C), self.code, ptr(r), ptr(z),
-                  stream_handle())
+        """z = M^-1 r (one V-cycle, custom op mg_vcycle); r and z are (2N,) float64 device vectors."""
+        z.copy_(torch.ops.difffea_b200.mg_vcycle(self.id, self.C, int(self.code), r.contiguous()))
         return z
 
     def __call__(self, r):
-        z = torch.empty_like(r)
-        return self.apply(r.contiguous(), z)
+        return torch.ops.difffea_b200.mg_vcycle(self.id, self.C, int(self.code), r.contiguous())
 
     def pcg(self, b, x, rtol, max_iter):
-        """x = PCG(A, b) with the V-cycle, x0 = 0; returns (iterations, status name)."""
-        it, st = ctypes.c_int32(0), ctypes.c_int32(0)
-        _lib.call("dfea_mg_pcg", self.mesh.view_ref, self.ref, ptr(self.C), self.code, ptr(b), ptr(x), float(rtol),
-                  int(max_iter), ctypes.byref(it), ctypes.byref(st), stream_handle())
-        return it.value, _lib.PCG_STATUS.get(st.value, str(st.value))
+        """x = PCG(A, b) with the V-cycle, x0 = 0 (custom op mg_pcg); returns (iterations, status name)."""
+        it, st = torch.ops.difffea_b200.mg_pcg(self.id, self.C, int(self.code), b, x, float(rtol), int(max_iter)).tolist()
+        return it, _lib.PCG_STATUS.get(st, str(st))

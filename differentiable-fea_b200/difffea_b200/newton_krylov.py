@@ -162,17 +162,35 @@ def newton_at_load(u0, theta, params, load_factor, tol, max_newton, verbose, cal
 @torch.no_grad()
 def newton_krylov_solve(params, theta, n_load_steps=5, tol=1e-8, max_newton=25, verbose=True, callback=None,
                         max_cutbacks=8, preconditioner="jacobi", tangent="auto", *, pcg_max_iter=500,
-                        precision="fp64", workspace=None):
+                        precision="fp64", workspace=None, driver="python"):
     """
     Solve R(u, theta) = 0 with load continuation; returns (u, info) with info keys converged,
     load_factor, history, total_newton, total_cg, n_cutbacks, snapshots (as the reference).
+
+    ``driver``: "python" runs the loop here (per-step callback, verbose printing, a snapshot per load step);
+    "native" runs the same loop in the library's C++ driver (dfea_newton_solve), the same iterates bit for
+    bit, in one call that holds no interpreter lock -- for many solves on concurrent host threads.  It takes
+    no callback, prints the history after the solve when verbose, and keeps the initial and final
+    snapshots only.
     """
     _check_kinds(tangent, preconditioner)
     nodes = params["nodes"]
     if not nodes.is_cuda:
         raise RuntimeError("difffea_b200 solves on CUDA devices only: move the problem with "
                            "problem.to_device(params, 'cuda')")
+    if driver not in ("python", "native"):
+        raise ValueError("driver must be 'python' or 'native'")
     ws = _workspace(params, theta, precision, workspace, preconditioner)
+    if driver == "native":
+        if callback is not None:
+            raise ValueError("the native driver takes no callback (use driver='python')")
+        u, info = ws.native_solve(theta, n_load_steps, tol, max_newton=max_newton, max_cutbacks=max_cutbacks,
+                                  pcg_max_iter=pcg_max_iter)
+        if verbose:
+            for r in info["history"]:
+                print(f"  step {r['step']} iter {r['iteration']:2d} | ||R|| = {r['residual']:.4e} | "
+                      f"CG = {r['cg_iters']:3d} | alpha = {r['alpha']:.4f}")
+        return u, info
     u = torch.zeros(2 * nodes.shape[0], dtype=torch.float64, device=nodes.device)
     info = {"converged": False, "load_factor": 0.0, "history": [], "total_newton": 0, "total_cg": 0,
             "n_cutbacks": 0, "snapshots": [(0.0, u.clone())]}

@@ -187,11 +187,11 @@ def compute_jacobi_diagonal(u, theta, params):
 
 def _diag_only(mesh, u, theta, mat):
     from difffea_b200 import _lib
-    from difffea_b200.cuda_mesh import ptr, stream_handle
     u64, th64 = _f64c(u), _f64c(theta)
     diag = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_qp_moduli_mat", mesh.view_ref, ptr(u64), ptr(th64), mat, ptr(None), _lib.DFEA_F64, ptr(diag),
-              ptr(None), stream_handle())
+    empty = torch.empty(0, dtype=torch.float64, device=mesh.device)
+    torch.ops.difffea_b200.qp_moduli_out(ops.register_mesh(mesh), u64, th64, *ops.material_args(mat), empty,
+                                         _lib.DFEA_F64, diag, empty)
     return diag
 
 
@@ -219,13 +219,13 @@ class CudaBlockJacobiPreconditioner:
 def compute_block_jacobi(u, theta, params):
     """The (4N,) inverse 2x2 node blocks of the tangent at (u, theta) (kernel (a) with the coupling term)."""
     from difffea_b200 import _lib
-    from difffea_b200.cuda_mesh import ptr, stream_handle
     mesh, mid, mat = _prepare(u, theta, params)
     u64, th64 = _f64c(u), _f64c(theta)
     diag = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
     blocks = torch.empty(2 * mesh.n_dof, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_qp_moduli_mat", mesh.view_ref, ptr(u64), ptr(th64), mat, ptr(None), _lib.DFEA_F64,
-              ptr(diag), ptr(blocks), stream_handle())
+    torch.ops.difffea_b200.qp_moduli_out(mid, u64, th64, *ops.material_args(mat),
+                                         torch.empty(0, dtype=torch.float64, device=mesh.device), _lib.DFEA_F64,
+                                         diag, blocks)
     return blocks
 
 

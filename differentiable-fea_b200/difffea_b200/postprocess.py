@@ -14,8 +14,7 @@ support reactions are the internal force with no mask (every DOF) summed over th
 """
 import torch
 
-from difffea_b200 import _lib
-from difffea_b200.cuda_mesh import ptr, stream_handle
+from difffea_b200 import ops
 from difffea_b200.operators import _f64c, _prepare
 
 ELEMENT_FIELDS = ("J", "sxx", "syy", "sxy", "mises", "energy_density")
@@ -23,11 +22,8 @@ ELEMENT_FIELDS = ("J", "sxx", "syy", "sxy", "mises", "energy_density")
 
 def element_fields(u, theta, params):
     """(7, n_el) per original element: area, then the weighted means J, sxx, syy, sxy, mises, psi."""
-    mesh, _, mat = _prepare(u, theta, params)
-    u, theta = _f64c(u), _f64c(theta)
-    out = torch.empty(7, mesh.n_el, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_element_fields_mat", mesh.view_ref, ptr(u), ptr(theta), mat, ptr(out), stream_handle())
-    return out
+    mesh, mid, mat = _prepare(u, theta, params)
+    return torch.ops.difffea_b200.element_fields(mid, _f64c(u), _f64c(theta), *ops.material_args(mat))
 
 
 def compute_fields(u, theta, params) -> dict:
@@ -37,11 +33,9 @@ def compute_fields(u, theta, params) -> dict:
         per node (N,):        ux, uy, u_mag (and ux_n, uy_n, u_mag_n), and J_n ... energy_density_n
         scalars (0-d):        strain_energy, min_J
     """
-    mesh, _, _ = _prepare(u, theta, params)
+    mesh, mid, _ = _prepare(u, theta, params)
     el = element_fields(u, theta, params)
-    mesh.ensure_node_incidence()
-    nodal = torch.empty(6, mesh.n_nodes, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_node_fields", mesh.view_ref, ptr(el), ptr(nodal), stream_handle())
+    nodal = torch.ops.difffea_b200.node_fields(mid, el)
     un = _f64c(u).view(mesh.n_nodes, 2)
     out = {name: el[k + 1] for k, name in enumerate(ELEMENT_FIELDS)}
     out.update(ux=un[:, 0], uy=un[:, 1], u_mag=torch.linalg.norm(un, dim=1),
@@ -55,11 +49,8 @@ def compute_fields(u, theta, params) -> dict:
 
 def internal_force(u, theta, params):
     """R_int(u) at every DOF, the constrained ones included (no mask, no external load)."""
-    mesh, _, mat = _prepare(u, theta, params)
-    u, theta = _f64c(u), _f64c(theta)
-    R = torch.empty(mesh.n_dof, dtype=torch.float64, device=mesh.device)
-    _lib.call("dfea_internal_force_mat", mesh.view_ref, ptr(u), ptr(theta), mat, ptr(R), stream_handle())
-    return R
+    mesh, mid, mat = _prepare(u, theta, params)
+    return torch.ops.difffea_b200.internal_force(mid, _f64c(u), _f64c(theta), *ops.material_args(mat))
 
 
 def support_reactions(u, theta, params) -> torch.Tensor:

@@ -56,6 +56,19 @@ class Request:
         k = 2 if self.element_type == "quad9" else 1
         return (k * self.nx + 1) * (k * self.ny + 1)
 
+    def validate(self):
+        """Raise ValueError for a request the solver cannot take (checked on the host before any GPU work)."""
+        if self.element_type not in NEN:
+            raise ValueError(f"request {self.rid}: element type '{self.element_type}' is not served ({sorted(NEN)})")
+        if not (isinstance(self.nx, int) and self.nx >= 4 and self.nx % 4 == 0):
+            raise ValueError(f"request {self.rid}: nx must be a positive multiple of 4, got {self.nx}")
+        if not (math.isfinite(self.E) and self.E > 0):
+            raise ValueError(f"request {self.rid}: E must be finite and positive, got {self.E}")
+        if not (math.isfinite(self.nu) and 0.0 <= self.nu < 0.5):
+            raise ValueError(f"request {self.rid}: nu must lie in [0, 0.5), got {self.nu}")
+        if not math.isfinite(self.load):
+            raise ValueError(f"request {self.rid}: load must be finite, got {self.load}")
+
 
 @dataclass
 class Result:
@@ -68,6 +81,7 @@ class Result:
     finished: float = 0.0
     arrival: float = 0.0
     error: str = ""
+    load_factor: float = 0.0      # the load factor reached (1.0 when converged)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -159,7 +173,7 @@ def request_problem(req, device="cpu", build_on_device=False):
 
 def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2,
                   host_params=None, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
-                  preconditioner="jacobi", batch=None):
+                  preconditioner="jacobi", batch=None, driver="native", max_newton=25, max_cutbacks=8):
     """
     Build (or copy from ``host_params``) and solve one request on the current stream; returns
     (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
@@ -167,8 +181,11 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     it ("auto", "colour" or "gather", see DevicePCG and workspace.pcg_form_for); ``fp32_moduli`` the FP32
     operator's moduli ("ref": reference frame, no gradients read; "physical"); ``max_blocks`` the most blocks
     per PCG launch (0: the whole GPU); ``preconditioner`` "jacobi", "block_jacobi", "multigrid" or "auto"
-    (``preconditioner_for``); ``batch`` a ``BatchExecutor`` that runs the PCG solves of all slots together.
+    (``preconditioner_for``); ``batch`` a ``BatchExecutor`` that runs the PCG solves of all slots together;
+    ``driver`` the Newton loop: "native" (the library's C++ driver, one call per solve) or "python".  The request
+    is validated on the host first (``Request.validate``).
     """
+    req.validate()
     preconditioner = preconditioner_for(req, preconditioner)
     if preconditioner == "multigrid":
         batch = None                     # the multigrid PCG runs per request (host-driven, graph-replayed cycle)
@@ -180,8 +197,11 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
     ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli,
                          max_blocks=max_blocks, preconditioner=preconditioner, batch=batch)
-    u, info = newton_krylov_solve(p, th, n_load_steps, tol, verbose=False, workspace=ws, precision=precision,
-                                  pcg_max_iter=pcg_max_iter, preconditioner=preconditioner)
+    if batch is not None:
+        driver = "python"                # the batched PCG is driven from the executor's thread
+    u, info = newton_krylov_solve(p, th, n_load_steps, tol, max_newton=max_newton, verbose=False, workspace=ws,
+                                  precision=precision, pcg_max_iter=pcg_max_iter, preconditioner=preconditioner,
+                                  driver=driver, max_cutbacks=max_cutbacks)
     if ws.pcg is not None:
         ws.pcg.close()
     return u, info
@@ -195,7 +215,8 @@ class ServingEngine:
 
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
                  pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
-                 fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False):
+                 fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False,
+                 driver="native", max_newton=25, max_cutbacks=8):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if self.device.index is None:            # "cuda": the current device, by index (the slot threads set it)
             self.device = torch.device(self.device.type, torch.cuda.current_device())
@@ -211,7 +232,8 @@ class ServingEngine:
             self.batch = BatchExecutor(self.device, capacity=n_slots, max_blocks=max_blocks)
         self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter,
                              pcg_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli, max_blocks=max_blocks,
-                             preconditioner=preconditioner, batch=self.batch)
+                             preconditioner=preconditioner, batch=self.batch, driver=driver, max_newton=max_newton,
+                             max_cutbacks=max_cutbacks)
         # torch's caching allocator keeps one pool per stream; a slot whose pool already holds a block of
         # the largest request never calls cudaMalloc (which synchronises the whole device) mid-run
         self.prewarm_bytes = int(prewarm_bytes)
@@ -294,9 +316,10 @@ class ServingEngine:
                 if req is None:
                     return
                 res = results[req.rid]
-                nbytes = hbm_estimate(req, self.precision, self.solve_kw["preconditioner"])
                 reserved = False
                 try:
+                    req.validate()
+                    nbytes = hbm_estimate(req, self.precision, self.solve_kw["preconditioner"])
                     self._reserve(nbytes)
                     reserved = True
                     res.admitted = time.perf_counter() - t0
@@ -309,6 +332,9 @@ class ServingEngine:
                         res.u = u.to("cpu") if keep_solutions else None
                         stream.synchronize()
                     res.converged, res.newton, res.cg = info["converged"], info["total_newton"], info["total_cg"]
+                    res.load_factor = info["load_factor"]
+                    if not res.converged:
+                        res.error = f"NotConverged: the load continuation stopped at load factor {res.load_factor:g}"
                 except Exception as exc:  # a failed request must not take the engine down
                     res.error = f"{type(exc).__name__}: {exc}"
                     errors.append(res.error)
@@ -325,7 +351,12 @@ class ServingEngine:
             delay = req.arrival - (time.perf_counter() - t0)
             if delay > 0:
                 time.sleep(delay)
-            prio = -hbm_estimate(req, self.precision, self.solve_kw["preconditioner"]) if self.order == "largest_first" else 0
+            prio = 0
+            if self.order == "largest_first":
+                try:
+                    prio = -hbm_estimate(req, self.precision, self.solve_kw["preconditioner"])
+                except (KeyError, ValueError, TypeError):   # a malformed request: its slot reports the error
+                    prio = 0
             q.put((prio, seq, req))
             seq += 1
         for _ in threads:
@@ -347,8 +378,9 @@ class ServingEngine:
 def run_plain(requests, device, precision="fp64", pcg_graph=2, **kw):
     """
     The same requests one after another on one stream -- the plain drop-in path (FP64, the PCG form of
-    newton_krylov_solve's default workspace); Results in order.
+    newton_krylov_solve's default workspace, its Python driver); Results in order.
     """
+    kw.setdefault("driver", "python")
     out = []
     t0 = time.perf_counter()
     for req in requests:

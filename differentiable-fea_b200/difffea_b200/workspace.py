@@ -12,8 +12,8 @@ scalars the algorithm branches on: ||R|| per residual evaluation and (status, it
 """
 import torch
 
-from difffea_b200 import _lib
-from difffea_b200.cuda_mesh import _require_cuda, cuda_mesh, ptr, stream_handle
+from difffea_b200 import _lib, ops
+from difffea_b200.cuda_mesh import _require_cuda, cuda_mesh
 from difffea_b200.krylov import DevicePCG
 from difffea_b200.materials import device_material
 
@@ -92,8 +92,13 @@ class NewtonWorkspace:
                                  use_graph=use_graph, form=pcg_form_for(mesh, pcg_form), moduli=self.moduli_kind,
                                  max_blocks=max_blocks, preconditioner=preconditioner)
         self.work = mesh.reduce_work()
+        self.mesh_id = ops.register_mesh(mesh)
+        self.mat_args = ops.material_args(self.material)
+        self._empty = torch.empty(0, dtype=torch.float64, device=dev)
+        self.id = ops.register_handle(self)
         self.theta = None
         self.n_launch_groups = 0
+        self._native = None           # the dfea_newton description, built on the first native solve
 
     # ---------------------------------------------------------------------------------------------
     def set_theta(self, theta):
@@ -104,9 +109,8 @@ class NewtonWorkspace:
 
     def residual(self, u, load_factor, out, energy=False):
         """out = R(u) (FP64); returns ||R|| (and the strain energy if asked) as Python floats."""
-        _lib.call("dfea_residual_mat", self.mesh.view_ref, ptr(u), ptr(self.theta), self.material, ptr(self.f),
-                  float(load_factor), ptr(out), ptr(self.scal), ptr(self.scal[1:]) if energy else ptr(None),
-                  ptr(self.work), stream_handle())
+        torch.ops.difffea_b200.residual_out(self.mesh_id, u, self.theta, *self.mat_args, self.f, float(load_factor),
+                                            out, self.scal, bool(energy))
         self.scal_host.copy_(self.scal, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         rn = float(self.scal_host[0]) ** 0.5
@@ -114,8 +118,8 @@ class NewtonWorkspace:
 
     def linearize(self, u):
         """Kernel (a): moduli C and the preconditioner at u (into the buffers the PCG graph is bound to)."""
-        _lib.call("dfea_qp_moduli_mat", self.mesh.view_ref, ptr(u), ptr(self.theta), self.material, ptr(self.C),
-                  self.moduli_code, ptr(self.diag), ptr(self.blocks), stream_handle())
+        torch.ops.difffea_b200.qp_moduli_out(self.mesh_id, u, self.theta, *self.mat_args, self.C, self.moduli_code,
+                                             self.diag, self.blocks if self.blocks is not None else self._empty)
         if self.mg is not None:
             self.mg.setup(self.C, self.moduli_code, self.diag)
 
@@ -130,8 +134,69 @@ class NewtonWorkspace:
             iters, status = self.pcg.solve(rtol, max_iter)
         return self.du, iters, status
 
+    # ---------------------------------------------------------------------------------------------
+    # the whole solve in the library's C++ driver (dfea_newton_solve, custom op newton_solve)
+    # ---------------------------------------------------------------------------------------------
+    MAX_RECORDS = 1024
+
+    def native_solve(self, theta, n_load_steps, tol, max_newton=25, max_cutbacks=8, pcg_max_iter=500):
+        """
+        newton_krylov_solve's loop in C++ on this workspace's buffers (one call, no interpreter lock held):
+        returns (u (2N,) float64, info) with the reference's info keys; ``history`` holds the Newton records
+        (at most MAX_RECORDS), ``snapshots`` the initial and the final state only.
+        """
+        if self.batch is not None:
+            raise ValueError("the native driver runs its own PCG; a workspace bound to a BatchExecutor cannot use it")
+        self.set_theta(theta)
+        if self._native is None:
+            self._build_native()
+        u, stats = torch.ops.difffea_b200.newton_solve(self.id, self.theta, int(n_load_steps), float(tol),
+                                                        int(max_newton), int(max_cutbacks), int(pcg_max_iter))
+        converged, load_factor, total_newton, total_cg, n_cutbacks, n_records = stats.tolist()
+        history = [dict(step=r.step, load_factor=r.load_factor, iteration=r.iteration, residual=r.residual,
+                        cg_iters=r.cg_iters, alpha=r.alpha) for r in self._records[:int(n_records)]]
+        return u, {"converged": bool(converged), "load_factor": float(load_factor), "history": history,
+                   "total_newton": int(total_newton), "total_cg": int(total_cg), "n_cutbacks": int(n_cutbacks),
+                   "snapshots": [(0.0, torch.zeros_like(u)), (float(load_factor), u.clone())]}
+
+    def _build_native(self):
+        import ctypes
+        mesh, n, dev = self.mesh, self.mesh.n_dof, self.mesh.device
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.w = torch.empty(n, **f64)
+        uD = self.params.get("u_D")
+        self.u_D = None if uD is None or not bool((uD != 0).any()) else uD.detach().to(**f64).contiguous()
+        self._records = (_lib.NewtonRecord * self.MAX_RECORDS)()
+        nw = _lib.Newton()
+        nw.mesh = ctypes.pointer(mesh.view)
+        for name, t in (("f", self.f), ("u_D", self.u_D), ("w", self.w), ("uc", self.uc), ("R", self.R),
+                        ("Rc", self.Rc), ("du", self.du), ("b", self.b), ("diag", self.diag), ("blocks", self.blocks),
+                        ("moduli", self.C), ("reduce_work", self.work), ("scal", self.scal),
+                        ("scal_host", self.scal_host)):
+            setattr(nw, name, t.data_ptr() if t is not None else None)
+        nw.moduli_dtype = self.moduli_code
+        if self.mg is not None:
+            nw.mg = ctypes.pointer(self.mg.h)
+        else:
+            nw.pcg = self.pcg._h.value
+        from difffea_b200.newton_krylov import FP32_MIN_RTOL
+        nw.min_rtol = FP32_MIN_RTOL if self.precision == "fp32" else 0.0
+        self._native = nw
+
+    def _native_args(self, theta):
+        """The dfea_newton description for a solve at theta (this workspace's buffers) and a fresh u."""
+        self.set_theta(theta)
+        if self._native is None:
+            self._build_native()
+        nw = self._native
+        nw.material = self.material
+        nw.theta = self.theta.data_ptr()
+        u = torch.empty(self.mesh.n_dof, dtype=torch.float64, device=self.mesh.device)
+        nw.u = u.data_ptr()
+        return nw, u
+
     def trial(self, u, alpha, du, out):
-        _lib.call("dfea_add_scaled", self.mesh.n_dof, ptr(u), float(alpha), ptr(du), ptr(out), stream_handle())
+        torch.ops.difffea_b200.add_scaled_out(u, float(alpha), du, out)
         return out
 
 

@@ -136,6 +136,11 @@ int64_t dfea_launch_count(void);
 int dfea_set_blocking_sync(int32_t device, int32_t on);
 
 
+/* sizeof of a public struct of this header, by its type name ("dfea_mesh_view", "dfea_material", "dfea_mg_grid",
+ * "dfea_mg_level", "dfea_mg", "dfea_newton", "dfea_newton_record", "dfea_newton_info"); -1 for other names.
+ * Host function: lets a binding check its mirrors of these structs against the library's layout. */
+int64_t dfea_struct_size(const char* name);
+
 /* 1 if the (nen, n_q) pair is built: (3,1) tri3, (6,6) tri6, (4,4) quad4, (8,9) quad8, (9,9) quad9. */
 int dfea_element_supported(int32_t nen, int32_t n_q);
 
@@ -492,6 +497,59 @@ int dfea_batch_iterate(dfea_batch* batch, int32_t n_iterations, int32_t* status,
 int dfea_pcg_solve_noalloc(const dfea_mesh_view* mesh, const void* moduli, const void* diag,
                            const void* b, void* x, int32_t vec_dtype, double rtol, int32_t max_iter,
                            int32_t* iters, int32_t* status, void* stream);
+
+/* ---------------------------------------------------------------- Newton-Krylov driver -------- */
+
+/*
+ * One complete solve R(u, theta) = 0 driven from C++: load continuation with cut-backs
+ * (newton_krylov_solve, newton_krylov.py:185-264), inexact Newton with the Eisenstat-Walker forcing term
+ * eta = min(0.5, sqrt(||R|| / ||R_0||)) (newton_at_load, :126-179) and Armijo backtracking from alpha = 1
+ * down to 2^-5 with c1 = 1e-4, NaN rejecting a step (armijo_line_search, :94-120).  Each linearisation
+ * runs kernel (a) (dfea_qp_moduli_mat) and, with a multigrid hierarchy, dfea_mg_setup; each linear solve
+ * negates R into b and runs the bound PCG handle (dfea_pcg_solve, which must be bound to b and du) or
+ * dfea_mg_pcg.  The caller owns every buffer (device unless noted).  The host reads one scalar per residual
+ * and (status, iterations) per linear solve; nothing here holds a lock of the calling language, so threads
+ * solving different problems proceed side by side.  Blocks the host until the solve ends.
+ */
+typedef struct dfea_newton {
+    const dfea_mesh_view* mesh;  /* host pointer                                                     */
+    dfea_material material;
+    const double* theta;         /* [n_el] design field, ORIGINAL element order                      */
+    const double* f;             /* [2N] external load at load factor 1                              */
+    const double* u_D;           /* [2N] prescribed displacements at load factor 1, or NULL (zero)   */
+    double* u;                   /* [2N] out: the last accepted state (the solution when converged)  */
+    double *w, *uc;              /* [2N] scratch: the Newton iterate and the line-search trial       */
+    double *R, *Rc;              /* [2N] scratch: their residuals                                    */
+    double *du, *b;              /* [2N] the Newton step and -R (the PCG handle's x and b)           */
+    double* diag;                /* [2N] Jacobi diagonal (written by kernel (a))                     */
+    double* blocks;              /* [4N] inverse 2x2 node blocks for block-Jacobi, or NULL           */
+    void* moduli;                /* moduli buffer of moduli_dtype (DFEA_F64, DFEA_F32 or DFEA_F32REF) */
+    int32_t moduli_dtype;
+    int32_t reserved;
+    void* reduce_work;           /* dfea_reduce_work_bytes(mesh) bytes                               */
+    double* scal;                /* 4 device doubles                                                 */
+    double* scal_host;           /* 4 host doubles (pinned)                                          */
+    dfea_pcg* pcg;               /* exactly one of pcg (bound to b, du) and mg                       */
+    dfea_mg* mg;
+    double min_rtol;             /* floor of the inner tolerance: 0 (FP64 operator) or, for an FP32
+                                  * operator, the accuracy it can deliver (1e-5)                     */
+} dfea_newton;
+
+typedef struct dfea_newton_record {  /* one Newton iteration, as the reference's history records     */
+    int32_t step, iteration, cg_iters, pcg_status;
+    double load_factor, residual, alpha;
+} dfea_newton_record;
+
+typedef struct dfea_newton_info {
+    int32_t converged, total_newton, total_cg, n_cutbacks;
+    double load_factor;            /* the load factor reached                                        */
+    int32_t n_records;             /* records written (at most max_records; total_newton counts all) */
+    int32_t reserved;
+} dfea_newton_info;
+
+int dfea_newton_solve(const dfea_newton* nw, int32_t n_load_steps, double tol, int32_t max_newton,
+                      int32_t max_cutbacks, int32_t pcg_max_iter, dfea_newton_info* info,
+                      dfea_newton_record* records, int32_t max_records, void* stream);
 
 /* ---------------------------------------------------------------- vector helpers -------------- */
 

@@ -78,3 +78,22 @@ def test_compute_entry_points_validate_before_touching_the_gpu():
     view = _lib.MeshView()            # all zero: invalid
     rc = _lib.load().dfea_tangent_apply(ctypes.byref(view), None, 0, None, None, 0, None)
     assert rc != 0
+
+
+def test_ctypes_mirrors_match_the_library_struct_layouts():
+    """Every struct the binding mirrors has the size the library was compiled with (a host query)."""
+    lib = _lib.load()
+    mirrors = {"dfea_material": _lib.Material, "dfea_mesh_view": _lib.MeshView, "dfea_mg_grid": _lib.MgGrid,
+               "dfea_mg_level": _lib.MgLevel, "dfea_mg": _lib.Mg, "dfea_newton": _lib.Newton,
+               "dfea_newton_record": _lib.NewtonRecord, "dfea_newton_info": _lib.NewtonInfo}
+    for name, cls in mirrors.items():
+        assert lib.dfea_struct_size(name.encode()) == ctypes.sizeof(cls), name
+    assert lib.dfea_struct_size(b"no_such_struct") == -1
+
+
+def test_newton_driver_validates_before_touching_the_gpu():
+    lib = _lib.load()
+    info = _lib.NewtonInfo()
+    assert lib.dfea_newton_solve(None, 1, 1e-8, 25, 8, 500, ctypes.byref(info), None, 0, None) == 1
+    nw = _lib.Newton()                 # no mesh, no buffers
+    assert lib.dfea_newton_solve(ctypes.byref(nw), 1, 1e-8, 25, 8, 500, ctypes.byref(info), None, 0, None) == 1

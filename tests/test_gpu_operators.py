@@ -127,8 +127,10 @@ def test_inverted_element_propagates_nan_like_the_reference():
 
 
 def test_custom_ops_are_registered():
-    assert hasattr(torch.ops.difffea_b200, "tangent_apply")
-    assert hasattr(torch.ops.difffea_b200, "qp_moduli")
+    for name in ("tangent_apply", "qp_moduli", "residual", "element_sensitivity", "element_fields", "node_fields",
+                 "internal_force", "pcg_solve", "mg_setup", "mg_vcycle", "mg_pcg", "newton_solve", "residual_out",
+                 "qp_moduli_out", "add_scaled_out"):
+        assert hasattr(torch.ops.difffea_b200, name), name
     d, p, u, v, th = golden_case("operator_quad4_h0.5_unit")
     mesh = cuda_mesh(p)
     mid = ops.register_mesh(mesh)

@@ -59,3 +59,43 @@ def test_batched_engine_gives_the_slot_results_bit_for_bit():
     for a, b in zip(slots, batched):
         assert b.error == "" and b.converged
         assert torch.equal(a.u, b.u) and (a.newton, a.cg) == (b.newton, b.cg)
+
+
+def test_faulty_requests_in_the_mix_are_reported_and_leave_the_others_unchanged():
+    """A request whose load inverts elements (a strain of ~10 in one step: NaN residuals, rejected line searches,
+    cut-backs) and malformed requests run inside a mix; they are reported, every other result is bit for bit
+    the one of the clean mix."""
+    reqs = _requests()
+    clean = ServingEngine(n_slots=4, device=DEV, max_cutbacks=2).run(reqs)
+    inverting = Request(100, "quad4", 32, 0.5, 0.3, 5.0, arrival=0.003)
+    malformed = [Request(101, "quad5", 16, 1.0, 0.3, 0.02, arrival=0.004),
+                 Request(102, "quad4", 0, 1.0, 0.3, 0.02, arrival=0.005),
+                 Request(103, "quad9", 16, float("nan"), 0.3, 0.02, arrival=0.006),
+                 Request(104, "quad4", 16, 1.0, 0.5, 0.02, arrival=0.007)]
+    mix = reqs[:3] + [inverting] + malformed + reqs[3:]
+    res = {r.rid: r for r in ServingEngine(n_slots=4, device=DEV, max_cutbacks=2).run(mix)}
+    for a in clean:
+        b = res[a.rid]
+        assert a.converged and b.converged and b.error == ""
+        assert torch.equal(a.u, b.u) and (a.newton, a.cg) == (b.newton, b.cg)
+    bad = res[100]
+    assert not bad.converged and bad.error.startswith("NotConverged") and bad.load_factor < 1.0
+    for m in malformed:
+        assert res[m.rid].error.startswith("ValueError"), res[m.rid].error
+
+
+@pytest.mark.parametrize("et,nx,preconditioner", [("quad4", 32, "jacobi"), ("quad9", 24, "jacobi"),
+                                                  ("quad4", 256, "multigrid"), ("quad9", 128, "multigrid")])
+def test_hbm_estimate_bounds_the_memory_a_request_allocates(et, nx, preconditioner):
+    """The admission estimate covers what a request really allocates on the device (torch's peak counter)."""
+    from difffea_b200.serving import solve_request
+    req = Request(7, et, nx, 1.0, 0.3, 0.03)
+    torch.cuda.synchronize()
+    base = torch.cuda.memory_allocated(DEV)
+    torch.cuda.reset_peak_memory_stats(DEV)
+    u, info = solve_request(req, DEV, preconditioner=preconditioner, pcg_form="gather", max_blocks=64)
+    torch.cuda.synchronize()
+    peak = torch.cuda.max_memory_allocated(DEV) - base
+    est = hbm_estimate(req, "fp32", preconditioner)
+    print(f"\n{et} nx={nx} {preconditioner}: peak {peak / 2**20:.1f} MiB, estimate {est / 2**20:.1f} MiB")
+    assert info["converged"] and peak <= est
