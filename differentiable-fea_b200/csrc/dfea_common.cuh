@@ -26,6 +26,8 @@ int set_error(int code, const char* fmt, ...);
 int check_cuda(cudaError_t err, const char* what);
 int launch_check(const char* what);
 void note_launches(long long n);
+long long thread_launch_count();  // launches noted by the calling thread (kernels captured into a graph are
+                                  // noted while capturing; the capture subtracts them again)
 int device_sm_count();
 long long persisting_l2_bytes(long long* max_window);
 

@@ -33,7 +33,12 @@ int launch_check(const char* what) { return check_cuda(cudaGetLastError(), what)
 // Kernels this library has launched in the process (direct launches when issued, graph-executed
 // kernels when the graph's solve returns): the evidence behind a benchmark's "gpu_launches".
 static std::atomic<long long> g_launches{0};
-void note_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local long long t_launches = 0;  // the same count for the calling thread alone
+void note_launches(long long n) {
+    g_launches.fetch_add(n, std::memory_order_relaxed);
+    t_launches += n;
+}
+long long thread_launch_count() { return t_launches; }
 
 int device_sm_count() {
     static std::atomic<int> cache[64];   // 0 until queried; threads that race store the same value

@@ -822,12 +822,60 @@ static int read_scalars(double* host, const double* dev, int k, cudaStream_t s) 
 
 }  // namespace dfea
 
-extern "C" int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
-                             const double* diag, void* stream) {
-    int rc = validate_mg(mesh, mg, "dfea_mg_setup");
-    if (rc) return rc;
-    if (!moduli || !diag) return set_error(DFEA_ERR_INVALID, "dfea_mg_setup: NULL pointer");
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
+namespace dfea {
+
+// ------------------------------------------------------------------------------------------
+// graph-driven mode: the captured set-up and the device-side PCG loop
+// ------------------------------------------------------------------------------------------
+// State of a device-side PCG solve (mg->pcg_state, 16 doubles).
+struct MgPcgState {
+    double rz, curv, rr, rz_new, nb2, tol2, rtol2, spare;
+    int32_t k, max_iter, status, iters, guard, spare_i[3];
+};
+static_assert(sizeof(MgPcgState) <= 16 * sizeof(double), "pcg_state holds 16 doubles");
+
+// the graphs of one hierarchy, each bound to the buffers it was captured with
+struct MgGraphs {
+    cudaStream_t capture = nullptr;
+    // set-up: moduli, diag and the mesh arrays the level-0 product reads
+    const void* key_setup[6] = {};
+    int32_t code_setup = -1;
+    int calls_setup = 0;
+    cudaGraphExec_t setup = nullptr;
+    long long kernels_setup = 0;
+    // PCG: moduli, b, x and the mesh arrays
+    const void* key_pcg[7] = {};
+    int32_t code_pcg = -1;
+    int calls_pcg = 0;
+    cudaGraphExec_t start = nullptr, loop = nullptr;
+    long long kernels_start = 0, kernels_body = 0;
+
+    void drop_setup() {
+        if (setup) cudaGraphExecDestroy(setup);
+        setup = nullptr;
+    }
+    void drop_pcg() {
+        if (start) cudaGraphExecDestroy(start);
+        if (loop) cudaGraphExecDestroy(loop);
+        start = loop = nullptr;
+    }
+    ~MgGraphs() {
+        drop_setup();
+        drop_pcg();
+        if (capture) cudaStreamDestroy(capture);
+    }
+};
+
+static bool same_key(const void* const* a, const void* const* b, int n) {
+    for (int i = 0; i < n; ++i)
+        if (a[i] != b[i]) return false;
+    return true;
+}
+
+// the device part of a set-up: coarse operators, coarsest inverse, Lanczos coefficients into mg->lhist
+static int setup_device_part(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
+                             const double* diag, cudaStream_t s) {
+    int rc;
     const int L = mg->n_levels;
     if ((rc = check_cuda(cudaMemcpyAsync(mg->level[0].diag, diag, mg->level[0].n * sizeof(double), cudaMemcpyDeviceToDevice, s),
                          "cudaMemcpyAsync")))
@@ -863,6 +911,250 @@ extern "C" int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void
                                            mg->lhist + (int64_t)2 * mg->lanczos_steps * l, k, mg->dot_work, s)))
                 return rc;
         }
+    return DFEA_OK;
+}
+
+// Capture `body(stream)` into a new graph on the hierarchy's capture stream and instantiate it; the kernels
+// the body notes while capturing are not launches yet (they are counted per replay instead).
+template <typename F>
+static int capture_exec(MgGraphs* g, F&& body, cudaGraphExec_t* out, long long* kernels) {
+    int rc;
+    if (!g->capture && (rc = check_cuda(cudaStreamCreateWithFlags(&g->capture, cudaStreamNonBlocking), "cudaStreamCreate")))
+        return rc;
+    const long long before = thread_launch_count();
+    if ((rc = check_cuda(cudaStreamBeginCapture(g->capture, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")))
+        return rc;
+    rc = body(g->capture);
+    cudaGraph_t graph = nullptr;
+    const int rc_end = check_cuda(cudaStreamEndCapture(g->capture, &graph), "cudaStreamEndCapture");
+    *kernels = thread_launch_count() - before;
+    note_launches(-*kernels);
+    if (!rc && !rc_end) rc = check_cuda(cudaGraphInstantiate(out, graph, 0), "cudaGraphInstantiate");
+    if (graph) cudaGraphDestroy(graph);
+    return rc ? rc : rc_end;
+}
+
+__global__ void k_mgp_init(MgPcgState* st, double rtol, int max_iter) {
+    st->rtol2 = rtol * rtol;
+    st->max_iter = max_iter;
+    st->k = 0;
+    st->iters = 0;
+    st->guard = 0;
+    st->status = DFEA_PCG_RUNNING;
+}
+
+// after |b|^2: the tolerance, and the ends that need no iteration
+__global__ void k_mgp_check(MgPcgState* st) {
+    st->tol2 = st->rtol2 * st->nb2;
+    if (st->nb2 == 0.0) {
+        st->status = DFEA_PCG_ZERO_RHS;
+    } else if (st->max_iter <= 0) {
+        st->status = DFEA_PCG_MAX_ITER;
+        st->iters = st->max_iter;
+    }
+}
+
+// x += alpha p, r -= alpha q (alpha = rz / p.q); on p.q <= 0 only x = z at the first iteration
+__global__ void k_mgp_update(int64_t n, const MgPcgState* __restrict__ st, double* __restrict__ x, double* __restrict__ r,
+                             const double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ z) {
+    if (st->status != DFEA_PCG_RUNNING) return;
+    const double curv = st->curv;
+    if (!(curv > 0.0)) {
+        if (st->k == 0)
+            for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+                x[i] = z[i];
+        return;
+    }
+    const double alpha = st->rz / curv, neg = -alpha;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        r[i] += neg * q[i];
+    }
+}
+
+// p = z + (r.z_new / r.z) p while the solve goes on
+__global__ void k_mgp_direction(int64_t n, const MgPcgState* __restrict__ st, double* __restrict__ p,
+                                const double* __restrict__ z) {
+    if (st->status != DFEA_PCG_RUNNING || !(st->curv > 0.0) || st->rr <= st->tol2) return;
+    const double beta = st->rz_new / st->rz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+// end of an iteration: the status, the counters and the loop condition.  The loop runs at most
+// max_iter + 4 bodies whatever the numbers do.
+__global__ void k_mgp_end(MgPcgState* st, cudaGraphConditionalHandle cond) {
+    st->guard += 1;
+    if (st->status == DFEA_PCG_RUNNING) {
+        if (!(st->curv > 0.0)) {
+            st->status = DFEA_PCG_NEG_CURV;
+            st->iters = st->k;
+        } else if (st->rr <= st->tol2) {
+            st->status = DFEA_PCG_CONVERGED;
+            st->iters = st->k + 1;
+        } else {
+            st->rz = st->rz_new;
+            st->k += 1;
+            if (st->k >= st->max_iter) {
+                st->status = DFEA_PCG_MAX_ITER;
+                st->iters = st->max_iter;
+            }
+        }
+    }
+    cudaGraphSetConditional(cond, (st->status == DFEA_PCG_RUNNING && st->guard < st->max_iter + 4) ? 1u : 0u);
+}
+
+__global__ void k_mgp_begin(const MgPcgState* st, cudaGraphConditionalHandle cond) {
+    cudaGraphSetConditional(cond, st->status == DFEA_PCG_RUNNING ? 1u : 0u);
+}
+
+// start of a solve: x = 0, r = b, |b|^2, z = V(r), p = z, r.z
+static int pcg_start_part(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code,
+                          const double* b, double* x, cudaStream_t s) {
+    const int64_t n = mg->level[0].n;
+    double *r = mg->pcg, *z = mg->pcg + n, *p = mg->pcg + 2 * n;
+    MgPcgState* st = reinterpret_cast<MgPcgState*>(mg->pcg_state);
+    int rc;
+    if ((rc = check_cuda(cudaMemsetAsync(x, 0, n * sizeof(double), s), "cudaMemsetAsync")) ||
+        (rc = check_cuda(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")) ||
+        (rc = dfea_mg_dot(n, b, b, &st->nb2, mg->dot_work, s)))
+        return rc;
+    k_mgp_check<<<1, 1, 0, s>>>(st);
+    note_launches(1);
+    if ((rc = launch_check("dfea_mg_pcg: check")) || (rc = mg_vcycle(mesh, mg, moduli, code, 0, r, z, s)) ||
+        (rc = check_cuda(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")))
+        return rc;
+    return dfea_mg_dot(n, r, z, &st->rz, mg->dot_work, s);
+}
+
+// one iteration of the device-side loop
+static int pcg_body_part(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, double* x,
+                         cudaGraphConditionalHandle cond, cudaStream_t s) {
+    const int64_t n = mg->level[0].n;
+    double *r = mg->pcg, *z = mg->pcg + n, *p = mg->pcg + 2 * n, *q = mg->pcg + 3 * n;
+    MgPcgState* st = reinterpret_cast<MgPcgState*>(mg->pcg_state);
+    int rc;
+    if ((rc = mg_apply(mesh, mg, moduli, code, 0, p, q, s)) || (rc = dfea_mg_dot(n, p, q, &st->curv, mg->dot_work, s)))
+        return rc;
+    k_mgp_update<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(n, st, x, r, p, q, z);
+    note_launches(1);
+    if ((rc = launch_check("dfea_mg_pcg: update")) || (rc = dfea_mg_dot(n, r, r, &st->rr, mg->dot_work, s)) ||
+        (rc = mg_vcycle(mesh, mg, moduli, code, 0, r, z, s)) || (rc = dfea_mg_dot(n, r, z, &st->rz_new, mg->dot_work, s)))
+        return rc;
+    k_mgp_direction<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(n, st, p, z);
+    k_mgp_end<<<1, 1, 0, s>>>(st, cond);
+    note_launches(2);
+    return launch_check("dfea_mg_pcg: end");
+}
+
+// the loop graph: a node that sets the condition from the status, then a while node around one iteration
+static int build_loop_graph(MgGraphs* g, const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli,
+                            int32_t code, double* x) {
+    int rc;
+    if (!g->capture && (rc = check_cuda(cudaStreamCreateWithFlags(&g->capture, cudaStreamNonBlocking), "cudaStreamCreate")))
+        return rc;
+    cudaGraph_t graph = nullptr;
+    if ((rc = check_cuda(cudaGraphCreate(&graph, 0), "cudaGraphCreate"))) return rc;
+    auto fail = [&](int code_) {
+        cudaGraphDestroy(graph);
+        return code_;
+    };
+    cudaGraphConditionalHandle cond;
+    if ((rc = check_cuda(cudaGraphConditionalHandleCreate(&cond, graph, 0u, cudaGraphCondAssignDefault),
+                         "cudaGraphConditionalHandleCreate")))
+        return fail(rc);
+    MgPcgState* st = reinterpret_cast<MgPcgState*>(mg->pcg_state);
+    if ((rc = check_cuda(cudaStreamBeginCaptureToGraph(g->capture, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                         "cudaStreamBeginCaptureToGraph")))
+        return fail(rc);
+    k_mgp_begin<<<1, 1, 0, g->capture>>>(st, cond);
+    rc = launch_check("dfea_mg_pcg: begin");
+    cudaGraph_t cap = graph;
+    int rc_end = check_cuda(cudaStreamEndCapture(g->capture, &cap), "cudaStreamEndCapture");
+    if (rc || rc_end) return fail(rc ? rc : rc_end);
+    cudaGraphNode_t first = nullptr;
+    size_t n_nodes = 1;
+    if ((rc = check_cuda(cudaGraphGetNodes(graph, &first, &n_nodes), "cudaGraphGetNodes"))) return fail(rc);
+    if (n_nodes != 1) return fail(set_error(DFEA_ERR_CUDA, "dfea_mg_pcg: unexpected loop-graph prologue"));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if ((rc = check_cuda(cudaGraphAddNode(&node, graph, &first, 1, &cp), "cudaGraphAddNode(while)"))) return fail(rc);
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const long long before = thread_launch_count();
+    if ((rc = check_cuda(cudaStreamBeginCaptureToGraph(g->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                         "cudaStreamBeginCaptureToGraph")))
+        return fail(rc);
+    rc = pcg_body_part(mesh, mg, moduli, code, x, cond, g->capture);
+    cudaGraph_t body_cap = body;
+    rc_end = check_cuda(cudaStreamEndCapture(g->capture, &body_cap), "cudaStreamEndCapture");
+    g->kernels_body = thread_launch_count() - before;
+    note_launches(-g->kernels_body);
+    if (rc || rc_end) return fail(rc ? rc : rc_end);
+    rc = check_cuda(cudaGraphInstantiate(&g->loop, graph, 0), "cudaGraphInstantiate");
+    cudaGraphDestroy(graph);
+    return rc;
+}
+
+// graph-driven PCG: init kernel, start graph, loop graph, one status read
+static int pcg_graph_solve(MgGraphs* g, const dfea_mg* mg, double rtol, int32_t max_iter, int32_t* iterations,
+                           int32_t* status, cudaStream_t s) {
+    MgPcgState* st = reinterpret_cast<MgPcgState*>(mg->pcg_state);
+    k_mgp_init<<<1, 1, 0, s>>>(st, rtol, max_iter);
+    int rc = launch_check("dfea_mg_pcg: init");
+    if (rc || (rc = check_cuda(cudaGraphLaunch(g->start, s), "cudaGraphLaunch")) ||
+        (rc = check_cuda(cudaGraphLaunch(g->loop, s), "cudaGraphLaunch")))
+        return rc;
+    int32_t host[5];  // k, max_iter, status, iters, guard
+    if ((rc = check_cuda(cudaMemcpyAsync(host, &st->k, sizeof(host), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync")) ||
+        (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+        return rc;
+    note_launches(2 + g->kernels_start + (long long)host[4] * g->kernels_body);
+    if (host[2] == DFEA_PCG_RUNNING) return set_error(DFEA_ERR_INVALID, "dfea_mg_pcg: the device loop ended without a status");
+    *status = host[2];
+    *iterations = host[3];
+    return DFEA_OK;
+}
+
+}  // namespace dfea
+
+extern "C" int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
+                             const double* diag, void* stream) {
+    int rc = validate_mg(mesh, mg, "dfea_mg_setup");
+    if (rc) return rc;
+    if (!moduli || !diag) return set_error(DFEA_ERR_INVALID, "dfea_mg_setup: NULL pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int L = mg->n_levels;
+    if (mg->pcg_state) {
+        if (!mg->graphs) {
+            MgGraphs* g = new (std::nothrow) MgGraphs;
+            if (!g) return set_error(DFEA_ERR_INVALID, "dfea_mg_setup: out of host memory");
+            mg->graphs = g;
+        }
+        MgGraphs* g = static_cast<MgGraphs*>(mg->graphs);
+        const void* key[6] = {moduli, diag, mesh->conn, mesh->grad, mesh->grad32, mesh->jinv};
+        if (!same_key(key, g->key_setup, 6) || g->code_setup != moduli_dtype) {
+            g->drop_setup();
+            for (int i = 0; i < 6; ++i) g->key_setup[i] = key[i];
+            g->code_setup = moduli_dtype;
+            g->calls_setup = 0;
+        }
+        if (g->calls_setup++ == 0) {
+            rc = setup_device_part(mesh, mg, moduli, moduli_dtype, diag, s);       // direct, the first time
+        } else {
+            if (!g->setup &&
+                (rc = capture_exec(g, [&](cudaStream_t cs) { return setup_device_part(mesh, mg, moduli, moduli_dtype, diag, cs); },
+                                   &g->setup, &g->kernels_setup)))
+                return rc;
+            rc = check_cuda(cudaGraphLaunch(g->setup, s), "cudaGraphLaunch");
+            note_launches(g->kernels_setup);
+        }
+    } else {
+        rc = setup_device_part(mesh, mg, moduli, moduli_dtype, diag, s);
+    }
+    if (rc) return rc;
     const int nh = 2 * mg->lanczos_steps * (L - 1);
     double hist[2 * 64 * DFEA_MG_MAX_LEVELS];
     if ((rc = read_scalars(hist, mg->lhist, nh, s))) return rc;
@@ -889,6 +1181,14 @@ extern "C" int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void
     return check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
 }
 
+extern "C" int dfea_mg_release(dfea_mg* mg) {
+    if (mg && mg->graphs) {
+        delete static_cast<MgGraphs*>(mg->graphs);
+        mg->graphs = nullptr;
+    }
+    return DFEA_OK;
+}
+
 extern "C" double dfea_mg_lanczos_bound(const double* hist, int32_t steps) {
     if (!hist || steps < 1 || steps > 64) return -1.0;
     return ritz_max(hist, steps);
@@ -910,6 +1210,29 @@ extern "C" int dfea_mg_pcg(const dfea_mesh_view* mesh, const dfea_mg* mg, const 
     if (!moduli || !b || !x || !iterations || !status || max_iter < 0)
         return set_error(DFEA_ERR_INVALID, "dfea_mg_pcg: bad arguments");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (mg->pcg_state && mg->graphs) {
+        // graph-driven: the second solve with the same buffers captures the loop, later ones replay it
+        MgGraphs* g = static_cast<MgGraphs*>(mg->graphs);
+        const void* key[7] = {moduli, b, x, mesh->conn, mesh->grad, mesh->grad32, mesh->jinv};
+        if (!same_key(key, g->key_pcg, 7) || g->code_pcg != moduli_dtype) {
+            g->drop_pcg();
+            for (int i = 0; i < 7; ++i) g->key_pcg[i] = key[i];
+            g->code_pcg = moduli_dtype;
+            g->calls_pcg = 0;
+        }
+        if (g->calls_pcg++ > 0) {
+            if (!g->start) {
+                rc = capture_exec(g, [&](cudaStream_t cs) { return pcg_start_part(mesh, mg, moduli, moduli_dtype, b, x, cs); },
+                                  &g->start, &g->kernels_start);
+                if (!rc) rc = build_loop_graph(g, mesh, mg, moduli, moduli_dtype, x);
+                if (rc) {
+                    g->drop_pcg();
+                    return rc;
+                }
+            }
+            return pcg_graph_solve(g, mg, rtol, max_iter, iterations, status, s);
+        }
+    }
     const int64_t n = mg->level[0].n;
     double *r = mg->pcg, *z = mg->pcg + n, *p = mg->pcg + 2 * n, *q = mg->pcg + 3 * n;
     double h[1];

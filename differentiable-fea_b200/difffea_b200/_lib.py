@@ -76,7 +76,8 @@ class Mg(ctypes.Structure):
     _fields_ = [("n_levels", c_i32), ("degree", c_i32), ("lanczos_steps", c_i32), ("span", c_i32), ("ratio", c_f64),
                 ("node_ij", c_vp), ("gnode", c_vp), ("cell_slot", c_vp), ("level", MgLevel * MG_MAX_LEVELS),
                 ("Ainv", c_vp), ("dense_work", c_vp), ("coef", c_vp), ("lscal", c_vp), ("lhist", c_vp),
-                ("dot_work", c_vp), ("pcg", c_vp), ("scal", c_vp), ("lam", c_f64 * MG_MAX_LEVELS)]
+                ("dot_work", c_vp), ("pcg", c_vp), ("scal", c_vp), ("lam", c_f64 * MG_MAX_LEVELS),
+                ("pcg_state", c_vp), ("graphs", c_vp)]
 
 class Newton(ctypes.Structure):
     """Mirror of ``dfea_newton``: the problem, the buffers and the linear solver of one Newton-Krylov solve."""
@@ -151,6 +152,7 @@ _PROTOS = {
     "dfea_mg_lanczos_bound": (ctypes.c_double, [c_vp, c_i32]),
     "dfea_mg_setup": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp]),
     "dfea_mg_vcycle": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp, c_vp]),
+    "dfea_mg_release": (ctypes.c_int, [ctypes.POINTER(Mg)]),
     "dfea_mg_pcg": (ctypes.c_int, [ctypes.POINTER(MeshView), ctypes.POINTER(Mg), c_vp, c_i32, c_vp, c_vp, c_f64, c_i32,
                                    ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_vp]),
     "dfea_mg_dense_inverse": (ctypes.c_int, [_MGP, c_vp, c_vp, c_vp]),

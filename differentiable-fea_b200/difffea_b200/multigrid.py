@@ -175,7 +175,10 @@ class Multigrid:
     concurrent serving threads do not queue behind one another's launches).
     """
 
-    def __init__(self, mesh, params, degree=CHEB_DEGREE, ratio=CHEB_RATIO, lanczos_steps=LANCZOS_STEPS):
+    def __init__(self, mesh, params, degree=CHEB_DEGREE, ratio=CHEB_RATIO, lanczos_steps=LANCZOS_STEPS, graphs=True):
+        """``graphs``: graph-driven mode (set-ups replay a captured graph from the second on, the PCG iterates
+        in a device-side loop, one graph launch and one status read per solve); False: every launch issued
+        from the host.  Both give the same iterates."""
         g = structured_grid(params["conn"].to(mesh.device), mesh.n_nodes)
         if g is None:
             raise ValueError("preconditioner='multigrid' needs a structured mesh (a logical grid of cells)")
@@ -212,6 +215,8 @@ class Multigrid:
         self.dot_work = torch.zeros(int(_lib.load().dfea_mg_dot_work()), **f64)
         self.pcg_work = torch.empty(4, self.levels[0].n, **f64)
         self.scal = torch.zeros(4, **f64)
+        # graph-driven mode: set-ups replay a captured graph, the PCG iterates in a device-side loop
+        self.pcg_state = torch.zeros(16, **f64) if graphs else None
         h = self.h = _lib.Mg()
         h.n_levels, h.degree, h.lanczos_steps, h.span, h.ratio = L, degree, lanczos_steps, g["span"], float(ratio)
         h.node_ij, h.gnode, h.cell_slot = g["node_ij"].data_ptr(), g["gnode"].data_ptr(), self.cell_slot.data_ptr()
@@ -224,6 +229,8 @@ class Multigrid:
         for name in ("Ainv", "dense_work", "coef", "lscal", "lhist", "dot_work", "scal"):
             setattr(h, name, getattr(self, name).data_ptr())
         h.pcg = self.pcg_work.data_ptr()
+        h.pcg_state = self.pcg_state.data_ptr() if graphs else None
+        h.graphs = None
         self.C, self.code = None, None
         self.id = ops.register_handle(self)
         self.generation = 0          # set-ups so far: a preconditioner closure checks that it is still current
@@ -248,6 +255,18 @@ class Multigrid:
 
     def __call__(self, r):
         return torch.ops.difffea_b200.mg_vcycle(self.id, self.C, int(self.code), r.contiguous())
+
+    def close(self):
+        """Release the CUDA graphs the library captured for this hierarchy (graph-driven mode)."""
+        h = getattr(self, "h", None)
+        if h is not None and h.graphs:
+            _lib.load().dfea_mg_release(ctypes.byref(h))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def pcg(self, b, x, rtol, max_iter):
         """x = PCG(A, b) with the V-cycle, x0 = 0 (custom op mg_pcg); returns (iterations, status name)."""

@@ -392,6 +392,14 @@ typedef struct dfea_mg {
     double* pcg;                               /* 4 x level[0].n: the PCG's r, z, p, q                  */
     double* scal;                              /* 4 device doubles                                      */
     double lam[DFEA_MG_MAX_LEVELS];            /* out: the lambda_max estimates of the last set-up      */
+    /* Graph-driven mode (optional): with pcg_state set, dfea_mg_setup replays its launch sequence as a CUDA
+     * graph and dfea_mg_pcg runs its iteration as a device-side loop (scalars on the device, one graph
+     * launch and one status read per solve), the same iterates bit for bit as the host-driven loop.  The
+     * graphs are captured at the second call with the same buffers (the first runs directly, which also
+     * sets up every lazily configured kernel attribute) and are owned by the library through `graphs`
+     * (NULL at first; release them with dfea_mg_release).  NULL pcg_state: everything host-driven. */
+    double* pcg_state;                         /* 16 device doubles, or NULL                            */
+    void* graphs;                              /* library-owned, NULL until the first graph is captured */
 } dfea_mg;
 
 /* Set-up at a linearisation: coarse operators from the moduli, coarsest inverse, Lanczos estimates,
@@ -405,6 +413,8 @@ double dfea_mg_lanczos_bound(const double* hist, int32_t steps);
 /* z = one V-cycle applied to r (the moduli of the set-up). */
 int dfea_mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
                    const double* r, double* z, void* stream);
+/* Release the graphs a hierarchy captured in graph-driven mode (mg->graphs); no-op when there are none. */
+int dfea_mg_release(dfea_mg* mg);
 /* PCG (x0 = 0) for A x = b with the V-cycle as preconditioner; status as dfea_pcg_solve's. */
 int dfea_mg_pcg(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
                 const double* b, double* x, double rtol, int32_t max_iter, int32_t* iterations, int32_t* status,

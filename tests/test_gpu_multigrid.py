@@ -158,3 +158,34 @@ def test_preconditioner_closures_at_different_states_stay_independent():
     assert M1.mg is M2.mg and not torch.equal(z1, z2)
     assert torch.equal(M1(r), z1)                          # re-set-up at u1: the same cycle, bit for bit
     assert torch.equal(M2(r), z2)
+
+
+@pytest.mark.parametrize("et,code", [("quad4", "f64"), ("quad9", "f32ref")])
+def test_graph_driven_hierarchy_matches_the_host_driven_one_bit_for_bit(et, code):
+    """Set-ups replayed from a captured graph and the device-side PCG loop give the host-driven iterates: the
+    same smoother bounds, solutions and iteration counts over several linearisations and solves (the first
+    set-up and solve run directly, the second capture, the later ones replay)."""
+    p = build_rectangle_problem(et, 48, 12, 4.0, 1.0, load=(0.02, 0.0), device=DEV)
+    mesh = cuda_mesh(p)
+    if code == "f32ref":
+        mesh.ensure_ref_frame()
+    hosted, graphed = Multigrid(mesh, p, graphs=False), Multigrid(mesh, p, graphs=True)
+    n = mesh.n_dof
+    b = torch.empty(n, dtype=torch.float64, device=DEV)
+    xs = [torch.empty(n, dtype=torch.float64, device=DEV) for _ in range(2)]
+    ws = NewtonWorkspace(p, "fp32" if code == "f32ref" else "fp64", preconditioner="jacobi")
+    for step in range(4):
+        u, th, r = _state(p, 40 + step, 0.003)
+        ws.set_theta(th)
+        ws.linearize(u)                                   # moduli and diagonal at this state
+        b.copy_(r * p["m"])
+        out = []
+        for mg, x in zip((hosted, graphed), xs):
+            mg.setup(ws.C, ws.moduli_code, ws.diag)
+            k, status = mg.pcg(b, x, 1e-10, 200)
+            out.append((k, status, [lv.lam for lv in mg.levels[:-1]]))
+        assert out[0] == out[1] and out[0][1] == "converged"
+        assert torch.equal(xs[0], xs[1])
+    assert graphed.h.graphs and not hosted.h.graphs
+    graphed.close()
+    assert not graphed.h.graphs
