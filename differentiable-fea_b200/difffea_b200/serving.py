@@ -171,9 +171,108 @@ def request_problem(req, device="cpu", build_on_device=False):
                                    load=(req.load * 1.0, 0.0), device=device, build_on_device=build_on_device)
 
 
+class PooledSolve:
+    """
+    A served mesh kept for the next request on it: the device problem dictionary and the solver workspace
+    (packed mesh, moduli, Krylov vectors, the bound PCG graph or multigrid hierarchy and its captured graphs),
+    plus what rebuilding the load vector needs.  A request on the same mesh differs only in its load
+    magnitude and material, which ``retarget`` sets; the load vector comes from the same function as in a
+    fresh build, so a pooled solve gives the fresh solve's result bit for bit.
+    """
+
+    def __init__(self, req, params, ws, nbytes):
+        from difffea_b200.boundary_conditions import boundary_edges, select_boundary_nodes
+        from difffea_b200.elements import get_element
+        el = get_element(req.element_type)
+        self.params, self.ws, self.nbytes = params, ws, nbytes
+        self.order = el["order"]
+        self.edges = boundary_edges(params["conn"], el["edges"])
+        self.load_nodes = select_boundary_nodes(params["nodes"], "right")
+
+    def retarget(self, req):
+        """The problem dictionary of ``req`` on this mesh (new load vector and material), bound to the workspace."""
+        from difffea_b200.boundary_conditions import edge_traction_load
+        from difffea_b200.materials import lame_parameters, material_vector
+        p = self.params
+        f = edge_traction_load(p["nodes"], self.edges, self.order, self.load_nodes, (float(req.load * 1.0), 0.0))
+        mu0, lmbda0 = lame_parameters(req.E, req.nu)
+        mat_p, _ = material_vector("neo_hookean", {"mu": mu0, "lmbda": lmbda0}, dtype=p["nodes"].dtype)
+        self.params = {**p, "f": f.reshape(-1), "mat_p": mat_p.to(p["nodes"].device)}
+        self.ws.retarget(self.params)
+        return self.params
+
+    def close(self):
+        if self.ws.pcg is not None:
+            self.ws.pcg.close()
+        if self.ws.mg is not None:
+            self.ws.mg.close()
+
+
+class WorkspacePool:
+    """
+    Idle ``PooledSolve`` entries by (mesh, solver configuration), least recently used first out, within a
+    byte budget (device memory the idle entries hold, beside the engine's admission budget).  Thread-safe:
+    a slot takes an entry for the length of one solve and gives it back; two requests on one mesh in
+    flight at once each get their own entry.
+    """
+
+    def __init__(self, budget_bytes):
+        from collections import OrderedDict
+        self.budget = int(budget_bytes)
+        self._idle = OrderedDict()           # key -> [PooledSolve]
+        self._bytes = 0
+        self._lock = threading.Lock()
+        self.hits = self.misses = self.evictions = 0
+
+    def take(self, key):
+        with self._lock:
+            entries = self._idle.get(key)
+            if entries:
+                entry = entries.pop()
+                if not entries:
+                    del self._idle[key]
+                self._bytes -= entry.nbytes
+                self.hits += 1
+                return entry
+            self.misses += 1
+            return None
+
+    def give(self, key, entry):
+        drop = []
+        with self._lock:
+            if entry.nbytes > self.budget:
+                drop.append(entry)
+            else:
+                while self._bytes + entry.nbytes > self.budget and self._idle:
+                    old_key, entries = next(iter(self._idle.items()))
+                    victim = entries.pop(0)
+                    if not entries:
+                        del self._idle[old_key]
+                    self._bytes -= victim.nbytes
+                    self.evictions += 1
+                    drop.append(victim)
+                self._idle.setdefault(key, []).append(entry)
+                self._idle.move_to_end(key)
+                self._bytes += entry.nbytes
+        for e in drop:
+            e.close()
+
+    @property
+    def idle_bytes(self):
+        return self._bytes
+
+    def clear(self):
+        with self._lock:
+            entries = [e for es in self._idle.values() for e in es]
+            self._idle.clear()
+            self._bytes = 0
+        for e in entries:
+            e.close()
+
+
 def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2,
                   host_params=None, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
-                  preconditioner="jacobi", batch=None, driver="native", max_newton=25, max_cutbacks=8):
+                  preconditioner="jacobi", batch=None, driver="native", max_newton=25, max_cutbacks=8, pool=None):
     """
     Build (or copy from ``host_params``) and solve one request on the current stream; returns
     (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
@@ -182,27 +281,45 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     operator's moduli ("ref": reference frame, no gradients read; "physical"); ``max_blocks`` the most blocks
     per PCG launch (0: the whole GPU); ``preconditioner`` "jacobi", "block_jacobi", "multigrid" or "auto"
     (``preconditioner_for``); ``batch`` a ``BatchExecutor`` that runs the PCG solves of all slots together;
-    ``driver`` the Newton loop: "native" (the library's C++ driver, one call per solve) or "python".  The request
-    is validated on the host first (``Request.validate``).
+    ``driver`` the Newton loop: "native" (the library's C++ driver, one call per solve) or "python"; ``pool`` a
+    ``WorkspacePool`` that keeps the mesh and workspace of a solved request for the next request on the same
+    mesh (not used with ``host_params``, whose dictionary the caller built).  The request is validated on
+    the host first (``Request.validate``).
     """
     req.validate()
     preconditioner = preconditioner_for(req, preconditioner)
     if preconditioner == "multigrid":
         batch = None                     # the multigrid PCG runs per request (host-driven, graph-replayed cycle)
-    if host_params is not None:
-        p = {k: (v.to(device, non_blocking=True) if torch.is_tensor(v) else v) for k, v in host_params.items()}
+    if batch is not None:
+        pool = None                      # workspaces bound to a batch executor are not kept
+    key = (req.element_type, req.nx, precision, preconditioner, pcg_form, fp32_moduli, max_blocks, pcg_graph,
+           str(device)) if (pool is not None and host_params is None) else None
+    entry = pool.take(key) if key is not None else None
+    if entry is not None:
+        p, ws = entry.retarget(req), entry.ws
     else:
-        p = request_problem(req, device, build_on_device=True)
+        if host_params is not None:
+            p = {k: (v.to(device, non_blocking=True) if torch.is_tensor(v) else v) for k, v in host_params.items()}
+        else:
+            p = request_problem(req, device, build_on_device=True)
+        ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli,
+                             max_blocks=max_blocks, preconditioner=preconditioner, batch=batch)
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
-    ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli,
-                         max_blocks=max_blocks, preconditioner=preconditioner, batch=batch)
     if batch is not None:
         driver = "python"                # the batched PCG is driven from the executor's thread
-    u, info = newton_krylov_solve(p, th, n_load_steps, tol, max_newton=max_newton, verbose=False, workspace=ws,
-                                  precision=precision, pcg_max_iter=pcg_max_iter, preconditioner=preconditioner,
-                                  driver=driver, max_cutbacks=max_cutbacks)
-    if ws.pcg is not None:
+    try:
+        u, info = newton_krylov_solve(p, th, n_load_steps, tol, max_newton=max_newton, verbose=False, workspace=ws,
+                                      precision=precision, pcg_max_iter=pcg_max_iter, preconditioner=preconditioner,
+                                      driver=driver, max_cutbacks=max_cutbacks)
+    except BaseException:
+        if entry is not None:
+            entry.close()
+        raise
+    if key is not None:
+        pool.give(key, entry if entry is not None else
+                  PooledSolve(req, p, ws, hbm_estimate(req, precision, preconditioner)))
+    elif ws.pcg is not None:
         ws.pcg.close()
     return u, info
 
@@ -216,7 +333,7 @@ class ServingEngine:
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
                  pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
                  fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False,
-                 driver="native", max_newton=25, max_cutbacks=8):
+                 driver="native", max_newton=25, max_cutbacks=8, pool_bytes=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if self.device.index is None:            # "cuda": the current device, by index (the slot threads set it)
             self.device = torch.device(self.device.type, torch.cuda.current_device())
@@ -224,6 +341,13 @@ class ServingEngine:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = int(0.6 * free)
         self.n_slots, self.hbm_budget, self.precision = n_slots, int(hbm_budget), precision
+        # meshes of served requests are kept for later requests on the same mesh (their workspaces, PCG graphs
+        # and multigrid hierarchies), within pool_bytes of device memory beside the admission budget (default
+        # 20 % of the free memory; 0: build every request from scratch)
+        if pool_bytes is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            pool_bytes = int(0.2 * free)
+        self.pool = WorkspacePool(pool_bytes) if pool_bytes > 0 else None
         # batched: the PCG solves of all slots advance together on one stream (BatchExecutor), one set of
         # launches per iteration for all of them
         self.batch = None
@@ -233,7 +357,7 @@ class ServingEngine:
         self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter,
                              pcg_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli, max_blocks=max_blocks,
                              preconditioner=preconditioner, batch=self.batch, driver=driver, max_newton=max_newton,
-                             max_cutbacks=max_cutbacks)
+                             max_cutbacks=max_cutbacks, pool=self.pool)
         # torch's caching allocator keeps one pool per stream; a slot whose pool already holds a block of
         # the largest request never calls cudaMalloc (which synchronises the whole device) mid-run
         self.prewarm_bytes = int(prewarm_bytes)

@@ -101,6 +101,20 @@ class NewtonWorkspace:
         self._native = None           # the dfea_newton description, built on the first native solve
 
     # ---------------------------------------------------------------------------------------------
+    def retarget(self, params):
+        """
+        Bind this workspace to another problem on the same mesh (the same conn, geometry and supports): its
+        load vector and material replace the current ones; every device buffer, the bound PCG graph and the
+        multigrid hierarchy are kept.
+        """
+        for k in ("conn", "dN_dX", "w_detJ", "m"):
+            if params[k] is not self.params[k]:
+                raise ValueError(f"retarget needs the same mesh: params['{k}'] differs")
+        self.params = params
+        self.f.copy_(params["f"].detach().to(torch.float64))
+        self.material = device_material(params)
+        self.mat_args = ops.material_args(self.material)
+
     def set_theta(self, theta):
         _require_cuda(theta)
         if theta.numel() != self.mesh.n_el or theta.device != self.mesh.device:

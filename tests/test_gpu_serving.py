@@ -99,3 +99,22 @@ def test_hbm_estimate_bounds_the_memory_a_request_allocates(et, nx, precondition
     est = hbm_estimate(req, "fp32", preconditioner)
     print(f"\n{et} nx={nx} {preconditioner}: peak {peak / 2**20:.1f} MiB, estimate {est / 2**20:.1f} MiB")
     assert info["converged"] and peak <= est
+
+
+def test_pooled_meshes_give_the_fresh_results_bit_for_bit():
+    """Requests on meshes the engine has served before reuse the kept mesh and workspace (new load and
+    material only); every result equals the one of an engine that builds each request from scratch."""
+    specs = [("quad4", 32, 1.0, 0.3, 0.03), ("quad9", 24, 0.7, 0.25, 0.02), ("quad4", 128, 1.8, 0.42, 0.05),
+             ("quad4", 32, 0.6, 0.4, 0.011), ("quad9", 24, 1.9, 0.21, 0.045), ("quad4", 128, 0.9, 0.33, 0.02),
+             ("quad4", 32, 1.3, 0.35, 0.04), ("quad9", 64, 1.1, 0.3, 0.03), ("quad9", 64, 0.8, 0.27, 0.015)]
+    reqs = [Request(i, et, nx, E, nu, ld) for i, (et, nx, E, nu, ld) in enumerate(specs)]
+    fresh = ServingEngine(n_slots=1, device=DEV, pool_bytes=0).run(reqs)
+    eng = ServingEngine(n_slots=1, device=DEV)
+    pooled = eng.run(reqs)
+    assert eng.pool.hits >= 4                               # the repeated meshes were served from the pool
+    for a, b in zip(fresh, pooled):
+        assert a.converged and b.converged and b.error == ""
+        assert torch.equal(a.u, b.u) and (a.newton, a.cg) == (b.newton, b.cg)
+    again = eng.run(reqs)                                   # every mesh pooled now, several slots
+    for a, b in zip(fresh, again):
+        assert torch.equal(a.u, b.u)
