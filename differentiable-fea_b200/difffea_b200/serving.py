@@ -140,14 +140,18 @@ def hbm_estimate(req, precision="fp32", preconditioner="jacobi"):
               + 4 * nen + 4 + 16 * nq * nen + 8 * nq + 8  # packed mesh (FP64 gradients)
               + ((40 + 32) * nq if precision == "fp32"  # reference-frame FP32 moduli + inverse Jacobians
                  else 128 * nq)                         # FP64 moduli
-              + 16 * nen + 4 * nen)                     # gather form: element results, node incidence
+              + 16 * nen + 4 * nen                      # gather form: element results, node incidence
+              + 32 * nen)                               # int64 keys, values and order of the incidence sort
     per_node = 16 + 2 * 8 * 14 + 2 * 4 * 6 + 1 + 4      # nodes, ~14 f64 and ~6 f32 DOF vectors, fix bits, ptr
     if preconditioner_for(req, preconditioner) == "multigrid":
         # 10 FP64 DOF vectors on the fine grid (6 of the cycle, 4 of its PCG), a third more over the coarse
         # levels, their 8 x 8 element matrices (a quarter of the fine cells at level 1, Q9: as many), grid maps
         cells1 = E if NEN[req.element_type] == 9 else E / 4
         per_node += 10 * 16 * 4 / 3 + 8 + 4
-        return int(E * per_el + N * per_node + cells1 * 512 * 4 / 3 + 4 * 2 ** 20)
+        # the grid inference's int64 temporaries (connectivity built per candidate numbering, grid maps)
+        per_el += 8 * nen + 96
+        per_node += 96
+        return int(1.1 * (E * per_el + N * per_node + cells1 * 512 * 4 / 3) + 4 * 2 ** 20)
     return int(E * per_el + N * per_node + 4 * 2 ** 20)  # + reduction scratch and PCG state
 
 

@@ -175,7 +175,7 @@ def test_graph_driven_hierarchy_matches_the_host_driven_one_bit_for_bit(et, code
     xs = [torch.empty(n, dtype=torch.float64, device=DEV) for _ in range(2)]
     ws = NewtonWorkspace(p, "fp32" if code == "f32ref" else "fp64", preconditioner="jacobi")
     for step in range(4):
-        u, th, r = _state(p, 40 + step, 0.003)
+        u, th, r = _state(p, 40 + step, 0.01 * 4.0 / 48)
         ws.set_theta(th)
         ws.linearize(u)                                   # moduli and diagonal at this state
         b.copy_(r * p["m"])

@@ -62,12 +62,12 @@ def test_batched_engine_gives_the_slot_results_bit_for_bit():
 
 
 def test_faulty_requests_in_the_mix_are_reported_and_leave_the_others_unchanged():
-    """A request whose load inverts elements (a strain of ~10 in one step: NaN residuals, rejected line searches,
-    cut-backs) and malformed requests run inside a mix; they are reported, every other result is bit for bit
-    the one of the clean mix."""
+    """A request whose load inverts elements at every attempt (a traction of 4,000 E: NaN residuals, rejected
+    line searches, two cut-backs allowed) and malformed requests run inside a mix; they are reported, every
+    other result is bit for bit the one of the clean mix."""
     reqs = _requests()
     clean = ServingEngine(n_slots=4, device=DEV, max_cutbacks=2).run(reqs)
-    inverting = Request(100, "quad4", 32, 0.5, 0.3, 5.0, arrival=0.003)
+    inverting = Request(100, "quad4", 32, 0.5, 0.3, 2000.0, arrival=0.003)
     malformed = [Request(101, "quad5", 16, 1.0, 0.3, 0.02, arrival=0.004),
                  Request(102, "quad4", 0, 1.0, 0.3, 0.02, arrival=0.005),
                  Request(103, "quad9", 16, float("nan"), 0.3, 0.02, arrival=0.006),
