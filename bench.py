@@ -20,8 +20,6 @@ ones).  One step = 4 consecutive requests of that sample; W steps warm up, the n
 Beside the headline (ours):
   e2e               the same requests again with each problem dictionary built on the host, pinned and
                     copied to the device inside the timed region, solutions read back (host wall clock)
-  mesh_pool         hits of the engine's per-mesh workspace pool in the timed window, and the same requests
-                    served by an engine that builds every mesh from scratch
   full_stream       K x 32 consecutive requests of the whole stream (nx 16..512) served continuously
   batched_vs_plain  the first 64 of those through the engine (auto preconditioner, and Jacobi only) and, one
                     after another, through the plain FP64 drop-in (newton_krylov_solve defaults): solves/s,
@@ -347,21 +345,11 @@ def run_serve(args):
         dist_barrier(world)
         torch.cuda.synchronize()
         n0 = lib.dfea_launch_count()
-        hits0, misses0 = (eng.pool.hits, eng.pool.misses) if eng.pool else (0, 0)
         results_s = eng.run(timed_s)                           # K steps of the sample, served continuously
         launches = lib.dfea_launch_count() - n0
-        pool_hits = (eng.pool.hits - hits0, eng.pool.misses - misses0) if eng.pool else (0, 0)
         torch.cuda.synchronize()
         dist_barrier(world)
         sample_ms = dist_max(eng.device_ms, world, dev)
-        # the same requests with every mesh built from scratch (no pool)
-        eng_fresh = ServingEngine(n_slots=SERVE["slots"], device=dev, precision="fp32", order="largest_first",
-                                  pool_bytes=0)
-        eng_fresh.run(warm_s, keep_solutions=False)
-        dist_barrier(world)
-        torch.cuda.synchronize()
-        eng_fresh.run(timed_s, keep_solutions=False)
-        fresh_ms = dist_max(eng_fresh.device_ms, world, dev)
         # end to end, the same requests: each problem built on the host, pinned, copied inside the slot
         dist_barrier(world)
         torch.cuda.synchronize()
@@ -428,11 +416,6 @@ def run_serve(args):
                          f"2500 nodes, Jacobi below, host sync "
                          f"{'blocking' if blocking else 'spin (blocking sync refused)'}",
                "all_converged": ok and lat_ok,
-               "mesh_pool": {"hits": pool_hits[0], "misses": pool_hits[1],
-                             "value_fresh_meshes": world * len(timed_s) / (fresh_ms * 1e-3),
-                             "reading": "the engine keeps the mesh and workspace of a served request for later requests "
-                                        "on the same mesh (warm-up and timed requests share meshes); "
-                                        "value_fresh_meshes serves the same requests building every mesh anew"},
                "e2e": {"value": world * len(timed_s) / e2e_s, "unit": "solves/s", "requests": len(timed_s),
                        "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                        "max_rel_diff_vs_value_run": e2e_same,

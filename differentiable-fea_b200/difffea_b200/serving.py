@@ -276,7 +276,8 @@ class WorkspacePool:
 
 def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2,
                   host_params=None, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
-                  preconditioner="jacobi", batch=None, driver="native", max_newton=25, max_cutbacks=8, pool=None):
+                  preconditioner="jacobi", batch=None, driver="native", max_newton=25, max_cutbacks=8, pool=None,
+                  mg_graphs=True):
     """
     Build (or copy from ``host_params``) and solve one request on the current stream; returns
     (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
@@ -287,8 +288,9 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     (``preconditioner_for``); ``batch`` a ``BatchExecutor`` that runs the PCG solves of all slots together;
     ``driver`` the Newton loop: "native" (the library's C++ driver, one call per solve) or "python"; ``pool`` a
     ``WorkspacePool`` that keeps the mesh and workspace of a solved request for the next request on the same
-    mesh (not used with ``host_params``, whose dictionary the caller built).  The request is validated on
-    the host first (``Request.validate``).
+    mesh (not used with ``host_params``, whose dictionary the caller built); ``mg_graphs`` the multigrid
+    hierarchy's graph-driven mode (see multigrid.Multigrid).  The request is validated on the host first
+    (``Request.validate``).
     """
     req.validate()
     preconditioner = preconditioner_for(req, preconditioner)
@@ -297,7 +299,7 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     if batch is not None:
         pool = None                      # workspaces bound to a batch executor are not kept
     key = (req.element_type, req.nx, precision, preconditioner, pcg_form, fp32_moduli, max_blocks, pcg_graph,
-           str(device)) if (pool is not None and host_params is None) else None
+           mg_graphs, str(device)) if (pool is not None and host_params is None) else None
     entry = pool.take(key) if key is not None else None
     if entry is not None:
         p, ws = entry.retarget(req), entry.ws
@@ -307,7 +309,7 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
         else:
             p = request_problem(req, device, build_on_device=True)
         ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli,
-                             max_blocks=max_blocks, preconditioner=preconditioner, batch=batch)
+                             max_blocks=max_blocks, preconditioner=preconditioner, batch=batch, mg_graphs=mg_graphs)
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
     if batch is not None:
@@ -337,7 +339,7 @@ class ServingEngine:
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
                  pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
                  fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False,
-                 driver="native", max_newton=25, max_cutbacks=8, pool_bytes=None):
+                 driver="native", max_newton=25, max_cutbacks=8, pool_bytes=0, mg_graphs=False):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if self.device.index is None:            # "cuda": the current device, by index (the slot threads set it)
             self.device = torch.device(self.device.type, torch.cuda.current_device())
@@ -345,9 +347,14 @@ class ServingEngine:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = int(0.6 * free)
         self.n_slots, self.hbm_budget, self.precision = n_slots, int(hbm_budget), precision
-        # meshes of served requests are kept for later requests on the same mesh (their workspaces, PCG graphs
-        # and multigrid hierarchies), within pool_bytes of device memory beside the admission budget (default
-        # 20 % of the free memory; 0: build every request from scratch)
+        # pool_bytes > 0 keeps the meshes of served requests for later requests on the same mesh (their
+        # workspaces, PCG graphs and multigrid hierarchies) within that much device memory beside the admission
+        # budget (None: 20 % of the free memory).  Off by default: on the seeded stream few requests share a
+        # mesh (16 % of a 256-request window), and the memory the idle entries hold makes the other requests
+        # allocate anew (measured: 80.9 vs 93.8 solves/s with 32 slots).
+        # mg_graphs: the multigrid hierarchies' graph-driven mode.  Off by default in the engine: a request's
+        # ~6 set-ups do not repay capturing and instantiating its graphs while 31 other slots launch (measured:
+        # 59.4 vs 93.8 solves/s), although one request alone is faster with it (54.5 vs 72.9 ms).
         if pool_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             pool_bytes = int(0.2 * free)
@@ -361,7 +368,7 @@ class ServingEngine:
         self.solve_kw = dict(precision=precision, n_load_steps=n_load_steps, tol_rel=tol_rel, pcg_max_iter=pcg_max_iter,
                              pcg_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli, max_blocks=max_blocks,
                              preconditioner=preconditioner, batch=self.batch, driver=driver, max_newton=max_newton,
-                             max_cutbacks=max_cutbacks, pool=self.pool)
+                             max_cutbacks=max_cutbacks, pool=self.pool, mg_graphs=mg_graphs)
         # torch's caching allocator keeps one pool per stream; a slot whose pool already holds a block of
         # the largest request never calls cudaMalloc (which synchronises the whole device) mid-run
         self.prewarm_bytes = int(prewarm_bytes)

@@ -103,13 +103,14 @@ def test_hbm_estimate_bounds_the_memory_a_request_allocates(et, nx, precondition
 
 def test_pooled_meshes_give_the_fresh_results_bit_for_bit():
     """Requests on meshes the engine has served before reuse the kept mesh and workspace (new load and
-    material only); every result equals the one of an engine that builds each request from scratch."""
+    material only; with graph-driven multigrid, also the graphs an earlier request captured); every result
+    equals the one of an engine that builds each request from scratch."""
     specs = [("quad4", 32, 1.0, 0.3, 0.03), ("quad9", 24, 0.7, 0.25, 0.02), ("quad4", 128, 1.8, 0.42, 0.05),
              ("quad4", 32, 0.6, 0.4, 0.011), ("quad9", 24, 1.9, 0.21, 0.045), ("quad4", 128, 0.9, 0.33, 0.02),
              ("quad4", 32, 1.3, 0.35, 0.04), ("quad9", 64, 1.1, 0.3, 0.03), ("quad9", 64, 0.8, 0.27, 0.015)]
     reqs = [Request(i, et, nx, E, nu, ld) for i, (et, nx, E, nu, ld) in enumerate(specs)]
     fresh = ServingEngine(n_slots=1, device=DEV, pool_bytes=0).run(reqs)
-    eng = ServingEngine(n_slots=1, device=DEV)
+    eng = ServingEngine(n_slots=1, device=DEV, pool_bytes=None, mg_graphs=True)
     pooled = eng.run(reqs)
     assert eng.pool.hits >= 4                               # the repeated meshes were served from the pool
     for a, b in zip(fresh, pooled):
