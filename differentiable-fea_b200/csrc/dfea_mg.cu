@@ -837,12 +837,12 @@ static_assert(sizeof(MgPcgState) <= 16 * sizeof(double), "pcg_state holds 16 dou
 // the graphs of one hierarchy, each bound to the buffers it was captured with
 struct MgGraphs {
     cudaStream_t capture = nullptr;
-    // set-up: moduli, diag and the mesh arrays the level-0 product reads
+    // set-up: moduli, diag and the mesh arrays the level-0 product reads; with and without the Lanczos bounds
     const void* key_setup[6] = {};
     int32_t code_setup = -1;
-    int calls_setup = 0;
-    cudaGraphExec_t setup = nullptr;
-    long long kernels_setup = 0;
+    int calls_setup[2] = {0, 0};
+    cudaGraphExec_t setup[2] = {nullptr, nullptr};
+    long long kernels_setup[2] = {0, 0};
     // PCG: moduli, b, x and the mesh arrays
     const void* key_pcg[7] = {};
     int32_t code_pcg = -1;
@@ -851,8 +851,11 @@ struct MgGraphs {
     long long kernels_start = 0, kernels_body = 0;
 
     void drop_setup() {
-        if (setup) cudaGraphExecDestroy(setup);
-        setup = nullptr;
+        for (int i = 0; i < 2; ++i) {
+            if (setup[i]) cudaGraphExecDestroy(setup[i]);
+            setup[i] = nullptr;
+            calls_setup[i] = 0;
+        }
     }
     void drop_pcg() {
         if (start) cudaGraphExecDestroy(start);
@@ -874,7 +877,7 @@ static bool same_key(const void* const* a, const void* const* b, int n) {
 
 // the device part of a set-up: coarse operators, coarsest inverse, Lanczos coefficients into mg->lhist
 static int setup_device_part(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t moduli_dtype,
-                             const double* diag, cudaStream_t s) {
+                             const double* diag, cudaStream_t s, bool lanczos) {
     int rc;
     const int L = mg->n_levels;
     if ((rc = check_cuda(cudaMemcpyAsync(mg->level[0].diag, diag, mg->level[0].n * sizeof(double), cudaMemcpyDeviceToDevice, s),
@@ -893,6 +896,7 @@ static int setup_device_part(const dfea_mesh_view* mesh, const dfea_mg* mg, cons
         if (rc || (rc = dfea_mg_diag(&mg->level[l].grid, mg->level[l].diag, s))) return rc;
     }
     if ((rc = dfea_mg_dense_inverse(&mg->level[L - 1].grid, mg->dense_work, mg->Ainv, s))) return rc;
+    if (!lanczos) return DFEA_OK;
     // Lanczos on every smoothed level, all levels in lockstep (p in x, z in d)
     for (int l = 0; l < L - 1; ++l) {
         const dfea_mg_level& lv = mg->level[l];
@@ -1127,6 +1131,9 @@ extern "C" int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void
     if (!moduli || !diag) return set_error(DFEA_ERR_INVALID, "dfea_mg_setup: NULL pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int L = mg->n_levels;
+    // the smoother bounds: estimated now, or kept from an earlier set-up of this hierarchy
+    const bool lanczos = mg->bounds_every <= 0 || mg->setups <= 0 || (mg->setups % mg->bounds_every) == 0;
+    mg->setups = mg->setups < 0 ? 1 : mg->setups + 1;
     if (mg->pcg_state) {
         if (!mg->graphs) {
             MgGraphs* g = new (std::nothrow) MgGraphs;
@@ -1139,22 +1146,23 @@ extern "C" int dfea_mg_setup(const dfea_mesh_view* mesh, dfea_mg* mg, const void
             g->drop_setup();
             for (int i = 0; i < 6; ++i) g->key_setup[i] = key[i];
             g->code_setup = moduli_dtype;
-            g->calls_setup = 0;
         }
-        if (g->calls_setup++ == 0) {
-            rc = setup_device_part(mesh, mg, moduli, moduli_dtype, diag, s);       // direct, the first time
+        const int v = lanczos ? 1 : 0;
+        if (g->calls_setup[v]++ == 0) {
+            rc = setup_device_part(mesh, mg, moduli, moduli_dtype, diag, s, lanczos);   // direct, the first time
         } else {
-            if (!g->setup &&
-                (rc = capture_exec(g, [&](cudaStream_t cs) { return setup_device_part(mesh, mg, moduli, moduli_dtype, diag, cs); },
-                                   &g->setup, &g->kernels_setup)))
+            if (!g->setup[v] &&
+                (rc = capture_exec(g, [&](cudaStream_t cs) { return setup_device_part(mesh, mg, moduli, moduli_dtype, diag, cs, lanczos); },
+                                   &g->setup[v], &g->kernels_setup[v])))
                 return rc;
-            rc = check_cuda(cudaGraphLaunch(g->setup, s), "cudaGraphLaunch");
-            note_launches(g->kernels_setup);
+            rc = check_cuda(cudaGraphLaunch(g->setup[v], s), "cudaGraphLaunch");
+            note_launches(g->kernels_setup[v]);
         }
     } else {
-        rc = setup_device_part(mesh, mg, moduli, moduli_dtype, diag, s);
+        rc = setup_device_part(mesh, mg, moduli, moduli_dtype, diag, s, lanczos);
     }
     if (rc) return rc;
+    if (!lanczos) return DFEA_OK;   // bounds, coefficients and lam[] of the last estimate stay in force
     const int nh = 2 * mg->lanczos_steps * (L - 1);
     double hist[2 * 64 * DFEA_MG_MAX_LEVELS];
     if ((rc = read_scalars(hist, mg->lhist, nh, s))) return rc;

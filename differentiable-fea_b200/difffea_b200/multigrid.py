@@ -175,10 +175,13 @@ class Multigrid:
     concurrent serving threads do not queue behind one another's launches).
     """
 
-    def __init__(self, mesh, params, degree=CHEB_DEGREE, ratio=CHEB_RATIO, lanczos_steps=LANCZOS_STEPS, graphs=True):
+    def __init__(self, mesh, params, degree=CHEB_DEGREE, ratio=CHEB_RATIO, lanczos_steps=LANCZOS_STEPS, graphs=True,
+                 bounds_every=0):
         """``graphs``: graph-driven mode (set-ups replay a captured graph from the second on, the PCG iterates
         in a device-side loop, one graph launch and one status read per solve); False: every launch issued
-        from the host.  Both give the same iterates."""
+        from the host.  Both give the same iterates.  ``bounds_every``: 0 estimates the smoother bounds by
+        Lanczos at every set-up; k > 0 at the first set-up and every k-th after it, keeping the last estimates
+        in between (a set-up then rebuilds the coarse operators only)."""
         g = structured_grid(params["conn"].to(mesh.device), mesh.n_nodes)
         if g is None:
             raise ValueError("preconditioner='multigrid' needs a structured mesh (a logical grid of cells)")
@@ -231,6 +234,7 @@ class Multigrid:
         h.pcg = self.pcg_work.data_ptr()
         h.pcg_state = self.pcg_state.data_ptr() if graphs else None
         h.graphs = None
+        h.bounds_every, h.setups = int(bounds_every), 0
         self.C, self.code = None, None
         self.id = ops.register_handle(self)
         self.generation = 0          # set-ups so far: a preconditioner closure checks that it is still current

@@ -400,6 +400,12 @@ typedef struct dfea_mg {
      * (NULL at first; release them with dfea_mg_release).  NULL pcg_state: everything host-driven. */
     double* pcg_state;                         /* 16 device doubles, or NULL                            */
     void* graphs;                              /* library-owned, NULL until the first graph is captured */
+    /* Smoother bounds: 0 (or less) estimates lambda_max by Lanczos at every set-up; k > 0 at the first set-up
+     * and every k-th one after it, the others keeping the last estimates (and the Chebyshev coefficients
+     * on the device): such a set-up rebuilds the coarse operators and the coarsest inverse only, with no
+     * host synchronisation.  setups counts the set-ups so far (the library increments it). */
+    int32_t bounds_every;
+    int32_t setups;
 } dfea_mg;
 
 /* Set-up at a linearisation: coarse operators from the moduli, coarsest inverse, Lanczos estimates,

@@ -189,3 +189,25 @@ def test_graph_driven_hierarchy_matches_the_host_driven_one_bit_for_bit(et, code
     assert graphed.h.graphs and not hosted.h.graphs
     graphed.close()
     assert not graphed.h.graphs
+
+
+@pytest.mark.parametrize("name", ["solve_quad4_h0.25_cantilever", "solve_quad9_h0.5_cantilever"])
+def test_kept_smoother_bounds_still_reach_the_reference_solution(name):
+    """Smoother bounds estimated at the first set-up only (bounds_every large): the later set-ups rebuild the
+    coarse operators but keep lambda_max, and the Newton solve still meets the reference's solution."""
+    d = load(name)
+    p = params_from(d, DEV)
+    th = torch.as_tensor(d["theta"], dtype=torch.float64, device=DEV)
+    ws = NewtonWorkspace(p, preconditioner="multigrid", mg_bounds_every=1000)
+    seen = []
+    setup = ws.mg.setup
+
+    def record(C, code, diag):
+        setup(C, code, diag)
+        seen.append([lv.lam for lv in ws.mg.levels[:-1]])
+    ws.mg.setup = record
+    u, info = newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False, workspace=ws,
+                                  preconditioner="multigrid")
+    assert info["converged"] and rel(u, d["u_star"]) < 1e-9
+    assert len(seen) >= 2 and all(s == seen[0] for s in seen)
+    assert ws.mg.h.setups == len(seen)
