@@ -754,7 +754,10 @@ static void transfer_args(const dfea_mesh_view* mesh, const dfea_mg* mg, int l, 
 
 static int mg_apply(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, int l,
                     const double* v, double* y, cudaStream_t s) {
-    if (l == 0) return dfea_tangent_apply(mesh, moduli, code, v, y, DFEA_F64, s);
+    if (l == 0)
+        return (mg->fe_work && mesh->node_elem_ptr && mesh->node_elem)
+                   ? dfea_tangent_apply_gather(mesh, moduli, code, v, y, DFEA_F64, mg->fe_work, s)
+                   : dfea_tangent_apply(mesh, moduli, code, v, y, DFEA_F64, s);
     return dfea_mg_apply(&mg->level[l].grid, v, y, s);
 }
 

@@ -77,7 +77,7 @@ class Mg(ctypes.Structure):
                 ("node_ij", c_vp), ("gnode", c_vp), ("cell_slot", c_vp), ("level", MgLevel * MG_MAX_LEVELS),
                 ("Ainv", c_vp), ("dense_work", c_vp), ("coef", c_vp), ("lscal", c_vp), ("lhist", c_vp),
                 ("dot_work", c_vp), ("pcg", c_vp), ("scal", c_vp), ("lam", c_f64 * MG_MAX_LEVELS),
-                ("pcg_state", c_vp), ("graphs", c_vp), ("bounds_every", c_i32), ("setups", c_i32)]
+                ("pcg_state", c_vp), ("graphs", c_vp), ("bounds_every", c_i32), ("setups", c_i32), ("fe_work", c_vp)]
 
 class Newton(ctypes.Structure):
     """Mirror of ``dfea_newton``: the problem, the buffers and the linear solver of one Newton-Krylov solve."""

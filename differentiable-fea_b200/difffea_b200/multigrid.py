@@ -176,12 +176,13 @@ class Multigrid:
     """
 
     def __init__(self, mesh, params, degree=CHEB_DEGREE, ratio=CHEB_RATIO, lanczos_steps=LANCZOS_STEPS, graphs=True,
-                 bounds_every=0):
+                 bounds_every=0, gather=False):
         """``graphs``: graph-driven mode (set-ups replay a captured graph from the second on, the PCG iterates
         in a device-side loop, one graph launch and one status read per solve); False: every launch issued
         from the host.  Both give the same iterates.  ``bounds_every``: 0 estimates the smoother bounds by
         Lanczos at every set-up; k > 0 at the first set-up and every k-th after it, keeping the last estimates
-        in between (a set-up then rebuilds the coarse operators only)."""
+        in between (a set-up then rebuilds the coarse operators only).  ``gather``: the level-0 products in the
+        gather form (2 launches each; the mesh's node incidence is built here) instead of one per colour."""
         g = structured_grid(params["conn"].to(mesh.device), mesh.n_nodes)
         if g is None:
             raise ValueError("preconditioner='multigrid' needs a structured mesh (a logical grid of cells)")
@@ -235,6 +236,12 @@ class Multigrid:
         h.pcg_state = self.pcg_state.data_ptr() if graphs else None
         h.graphs = None
         h.bounds_every, h.setups = int(bounds_every), 0
+        self.fe_work = None
+        if gather:
+            mesh.ensure_node_incidence()
+            self.fe_work = torch.empty(int(_lib.load().dfea_gather_work_bytes(mesh.view_ref, _lib.DFEA_F64)),
+                                       dtype=torch.uint8, device=dev)
+            h.fe_work = self.fe_work.data_ptr()
         self.C, self.code = None, None
         self.id = ops.register_handle(self)
         self.generation = 0          # set-ups so far: a preconditioner closure checks that it is still current

@@ -277,7 +277,7 @@ class WorkspacePool:
 def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, pcg_max_iter=5000, pcg_graph=2,
                   host_params=None, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
                   preconditioner="jacobi", batch=None, driver="native", max_newton=25, max_cutbacks=8, pool=None,
-                  mg_graphs=True, mg_bounds_every=0):
+                  mg_graphs=True, mg_bounds_every=0, mg_gather=False):
     """
     Build (or copy from ``host_params``) and solve one request on the current stream; returns
     (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
@@ -299,7 +299,7 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     if batch is not None:
         pool = None                      # workspaces bound to a batch executor are not kept
     key = (req.element_type, req.nx, precision, preconditioner, pcg_form, fp32_moduli, max_blocks, pcg_graph,
-           mg_graphs, mg_bounds_every, str(device)) if (pool is not None and host_params is None) else None
+           mg_graphs, mg_bounds_every, mg_gather, str(device)) if (pool is not None and host_params is None) else None
     entry = pool.take(key) if key is not None else None
     if entry is not None:
         p, ws = entry.retarget(req), entry.ws
@@ -310,7 +310,7 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
             p = request_problem(req, device, build_on_device=True)
         ws = NewtonWorkspace(p, precision, use_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli,
                              max_blocks=max_blocks, preconditioner=preconditioner, batch=batch, mg_graphs=mg_graphs,
-                             mg_bounds_every=mg_bounds_every)
+                             mg_bounds_every=mg_bounds_every, mg_gather=mg_gather)
     th = torch.ones(p["conn"].shape[0], dtype=torch.float64, device=device)
     tol = tol_rel * float(torch.linalg.vector_norm(p["f"]))
     if batch is not None:
@@ -340,7 +340,8 @@ class ServingEngine:
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
                  pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
                  fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False,
-                 driver="native", max_newton=25, max_cutbacks=8, pool_bytes=0, mg_graphs=False, mg_bounds_every=0):
+                 driver="native", max_newton=25, max_cutbacks=8, pool_bytes=0, mg_graphs=False, mg_bounds_every=0,
+                 mg_gather=False):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if self.device.index is None:            # "cuda": the current device, by index (the slot threads set it)
             self.device = torch.device(self.device.type, torch.cuda.current_device())
@@ -370,7 +371,7 @@ class ServingEngine:
                              pcg_graph=pcg_graph, pcg_form=pcg_form, fp32_moduli=fp32_moduli, max_blocks=max_blocks,
                              preconditioner=preconditioner, batch=self.batch, driver=driver, max_newton=max_newton,
                              max_cutbacks=max_cutbacks, pool=self.pool, mg_graphs=mg_graphs,
-                             mg_bounds_every=mg_bounds_every)
+                             mg_bounds_every=mg_bounds_every, mg_gather=mg_gather)
         # torch's caching allocator keeps one pool per stream; a slot whose pool already holds a block of
         # the largest request never calls cudaMalloc (which synchronises the whole device) mid-run
         self.prewarm_bytes = int(prewarm_bytes)

@@ -36,7 +36,7 @@ def pcg_form_for(mesh, pcg_form="auto"):
 
 class NewtonWorkspace:
     def __init__(self, params, precision="fp64", use_graph=2, pcg_form="auto", fp32_moduli="ref", max_blocks=0,
-                 preconditioner="jacobi", batch=None, mg_graphs=True, mg_bounds_every=0):
+                 preconditioner="jacobi", batch=None, mg_graphs=True, mg_bounds_every=0, mg_gather=False):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32' (FP32 moduli and PCG, FP64 Newton)")
         if preconditioner not in ("jacobi", "block_jacobi", "multigrid"):
@@ -85,7 +85,7 @@ class NewtonWorkspace:
         if preconditioner == "multigrid":
             # geometric multigrid V-cycle (structured meshes) inside a PCG driven from the host
             from difffea_b200.multigrid import Multigrid
-            self.mg = Multigrid(mesh, params, graphs=mg_graphs, bounds_every=mg_bounds_every)
+            self.mg = Multigrid(mesh, params, graphs=mg_graphs, bounds_every=mg_bounds_every, gather=mg_gather)
             self.pcg = None
         else:
             self.pcg = DevicePCG(mesh, self.C, self.diag if self.blocks is None else self.blocks, self.b, self.du,

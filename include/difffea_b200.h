@@ -406,6 +406,10 @@ typedef struct dfea_mg {
      * host synchronisation.  setups counts the set-ups so far (the library increments it). */
     int32_t bounds_every;
     int32_t setups;
+    /* Optional element-result buffer (dfea_gather_work_bytes(mesh, DFEA_F64) bytes): when set and the mesh has
+     * its node incidence, every level-0 product of the hierarchy runs in the gather form (an element pass and
+     * the node sums: 2 launches) instead of one launch per colour; NULL: the colour form. */
+    void* fe_work;
 } dfea_mg;
 
 /* Set-up at a linearisation: coarse operators from the moduli, coarsest inverse, Lanczos estimates,

@@ -211,3 +211,21 @@ def test_kept_smoother_bounds_still_reach_the_reference_solution(name):
     assert info["converged"] and rel(u, d["u_star"]) < 1e-9
     assert len(seen) >= 2 and all(s == seen[0] for s in seen)
     assert ws.mg.h.setups == len(seen)
+
+
+@pytest.mark.parametrize("name,graphs", [("solve_quad4_h0.25_cantilever", False), ("solve_quad9_h0.5_cantilever", True),
+                                         ("solve_tri6_h0.5_cantilever", True)])
+def test_gather_form_level0_products_reach_the_reference_solution(name, graphs):
+    """The hierarchy's level-0 products in the gather form (element pass + node sums), host- or graph-driven:
+    the Newton solve meets the reference's solution, and one V-cycle agrees with the colour form's to rounding."""
+    d = load(name)
+    p = params_from(d, DEV)
+    th = torch.as_tensor(d["theta"], dtype=torch.float64, device=DEV)
+    ws = NewtonWorkspace(p, preconditioner="multigrid", mg_gather=True, mg_graphs=graphs)
+    u, info = newton_krylov_solve(p, th, int(d["n_load_steps"]), float(d["tol"]), verbose=False, workspace=ws,
+                                  preconditioner="multigrid")
+    assert info["converged"] and rel(u, d["u_star"]) < 1e-9
+    colour = Multigrid(ws.mesh, p, graphs=False)
+    colour.setup(ws.C, ws.moduli_code, ws.diag)
+    r = torch.randn(ws.mesh.n_dof, dtype=torch.float64, generator=torch.Generator().manual_seed(9)).to(DEV)
+    assert rel(ws.mg(r), colour(r)) < 1e-12
