@@ -56,11 +56,11 @@ METRIC = "solves/s + p50/p99 latency, batched vs plain, at <=1e-8 rel err; A(v) 
 PLAIN = dict(element_type="quad4", nx=100, ny=100, width=1.0, height=1.0, E=1.0, nu=0.3, load=(0.1, 0.0),
              n_load_steps=3, tol=1e-10)
 MATVEC_N = 1600
-# DRAM bytes per algorithmic byte of the FP64 product, from one ncu capture of the same kernel on 640,000 Q4
-# elements with L2 state kept (dram__bytes_read.sum + dram__bytes_write.sum over the four colour passes of
-# one product: 570.0 + 47.6 MB against 532.6 MB algorithmic); traffic grows with the element count, so the
-# 2.56M launch is charged the same ratio
-DRAM_PER_ALG_BYTE = 617.6e6 / 532.56e6
+# DRAM bytes of one FP64 product at 2.56M Q4 elements, from ncu (dram__bytes_read.sum + dram__bytes_write.sum of
+# the four colour passes, L2 state kept, two products averaged: 2,335.1 MB read + 131.0 MB written; the pass that
+# initialises y with the Dirichlet pivot is not counted) against 2,130.1 MB algorithmic: 1.158 per byte, the
+# excess being v gathered and y read back by every colour pass
+DRAM_BYTES_PER_PRODUCT = 2.466e9
 SERVE = dict(stream=2000, seed=0, batch=32, slots=32, compare=64, sample_nx=64, sample_per_step=4,
              cpu_baseline_requests=24, latency_load=0.8)
 
@@ -444,8 +444,8 @@ def run_serve(args):
                "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99), "requests": len(lat),
                               "arrival_rate_per_s": rate, "load": SERVE["latency_load"], "order": "fifo"},
                "roofline": {"bound": "hbm", "achieved": roof["gbs"], "peak": hbm, "unit": "GB/s",
-                            "frac": roof["gbs"] / hbm, "traffic": roof["bytes"] * DRAM_PER_ALG_BYTE, "peak_kind": kind,
-                            "traffic_source": "ncu, 640k-element capture scaled by element count",
+                            "frac": roof["gbs"] / hbm, "traffic": DRAM_BYTES_PER_PRODUCT, "peak_kind": kind,
+                            "traffic_source": "ncu capture of the same product at the same size (four colour passes)",
                             "kernel": "k_apply<4,4,double,double> (A(v), FP64 stored moduli)",
                             "workload": f"structured Q4 {MATVEC_N}x{MATVEC_N} = {roof['n_el']} elements",
                             "alg_bytes_per_launch": roof["bytes"], "ms_per_product": roof["ms"]},
@@ -526,8 +526,8 @@ def run_plain_workload(args):
                           "accuracy": {"rel_err_vs_oracle": err, "newton": info["total_newton"], "cg": info["total_cg"],
                                        "newton_oracle": info_ref["total_newton"], "cg_oracle": info_ref["total_cg"]},
                           "roofline": {"bound": "hbm", "achieved": roof["gbs"], "peak": hbm, "unit": "GB/s",
-                                       "frac": roof["gbs"] / hbm, "traffic": roof["bytes"] * DRAM_PER_ALG_BYTE, "peak_kind": kind,
-                            "traffic_source": "ncu, 640k-element capture scaled by element count",
+                                       "frac": roof["gbs"] / hbm, "traffic": DRAM_BYTES_PER_PRODUCT, "peak_kind": kind,
+                            "traffic_source": "ncu capture of the same product at the same size (four colour passes)",
                                        "kernel": "k_apply<4,4,double,double>",
                                        "workload": f"structured Q4 {MATVEC_N}x{MATVEC_N}",
                                        "alg_bytes_per_launch": roof["bytes"], "ms_per_product": roof["ms"]},
