@@ -310,26 +310,12 @@ k_apply_elem(Mesh m, const SD* __restrict__ C, const SD* __restrict__ G, const T
 template <typename T>
 __device__ __forceinline__ v2_t<T> node_sum(const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc,
                                             const v2_t<T>* __restrict__ fe2, int64_t n) {
-    // Slots in groups of four: the group's incidence entries are loaded together, then its element results
-    // together, so a node costs two dependent loads per group instead of two per slot.  The sum still runs
-    // over the slots in incidence order, and slots past the node's end are skipped (never added as zeros,
-    // which could flip the sign of a zero sum): the same bits as a slot-by-slot loop.
     T sx = T(0), sy = T(0);
     const int j1 = inc_ptr[n + 1];
-    for (int j = inc_ptr[n]; j < j1; j += 4) {
-        int idx[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) idx[k] = (j + k < j1) ? __ldg(inc + j + k) : -1;
-        v2_t<T> f[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (idx[k] >= 0) f[k] = fe2[idx[k]];
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (idx[k] >= 0) {
-                sx += f[k].x;
-                sy += f[k].y;
-            }
+    for (int j = inc_ptr[n]; j < j1; ++j) {
+        const v2_t<T> f = fe2[inc[j]];
+        sx += f.x;
+        sy += f.y;
     }
     return make_v2<T>(sx, sy);
 }

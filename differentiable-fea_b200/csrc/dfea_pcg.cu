@@ -160,52 +160,27 @@ __device__ __forceinline__ void pcg_update1_body(const Mesh& m, int n_colours, c
     const double alpha = st->rz / curv;
     const T a = (T)alpha;
     double rr = 0.0, rz = 0.0;
-    const T2* P = reinterpret_cast<const T2*>(p);
-    T2* X = reinterpret_cast<T2*>(x);
-    T2* Rv = reinterpret_cast<T2*>(r);
-    auto load_y = [&](int64_t n, T2 pn) -> T2 {
+    for (int64_t n = blk * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)nblk * blockDim.x) {
+        const T2 pn = reinterpret_cast<const T2*>(p)[n];
+        T2 yn;
         if constexpr (GATHER) {
             const int fix = m.node_fix[n];
             const T2 f = node_sum<T>(inc_ptr, inc, reinterpret_cast<const T2*>(fe), n);
-            return make_v2<T>((fix & 1) ? pn.x : f.x, (fix & 2) ? pn.y : f.y);
+            yn = make_v2<T>((fix & 1) ? pn.x : f.x, (fix & 2) ? pn.y : f.y);
         } else {
-            return reinterpret_cast<const T2*>(y)[n];
+            yn = reinterpret_cast<const T2*>(y)[n];
         }
-    };
-    auto update = [&](int64_t n, T2 pn, T2 yn, T2 xn, T2 rn) {
+        T2 xn = reinterpret_cast<const T2*>(x)[n];
+        T2 rn = reinterpret_cast<const T2*>(r)[n];
         xn.x += a * pn.x;
         xn.y += a * pn.y;
         rn.x -= a * yn.x;
         rn.y -= a * yn.y;
-        X[n] = xn;
-        Rv[n] = rn;
+        reinterpret_cast<T2*>(x)[n] = xn;
+        reinterpret_cast<T2*>(r)[n] = rn;
         rr += (double)rn.x * rn.x + (double)rn.y * rn.y;
         const T2 zn = precond<BJ, T>(d, n, rn);
         rz += (double)rn.x * zn.x + (double)rn.y * zn.y;
-    };
-    // colour form: a thread's nodes in pairs (n, n + stride), both nodes' loads issued before either is
-    // used; the partial sums take the nodes in the same order as one node at a time.  (The gather form keeps
-    // one node at a time: its node sums already load a node's slots together, and a pair of them would
-    // double the registers.)
-    const int64_t stride = (int64_t)nblk * blockDim.x;
-    int64_t n = blk * (int64_t)blockDim.x + threadIdx.x;
-    if constexpr (GATHER) {
-        for (; n < m.n_nodes; n += stride) {
-            const T2 pa = P[n];
-            update(n, pa, load_y(n, pa), X[n], Rv[n]);
-        }
-    }
-    for (; n + stride < m.n_nodes; n += 2 * stride) {
-        const int64_t n2 = n + stride;
-        const T2 pa = P[n], pb = P[n2];
-        const T2 xa = X[n], xb = X[n2], ra = Rv[n], rb = Rv[n2];
-        const T2 ya = load_y(n, pa), yb = load_y(n2, pb);
-        update(n, pa, ya, xa, ra);
-        update(n2, pb, yb, xb, rb);
-    }
-    if (n < m.n_nodes) {
-        const T2 pa = P[n];
-        update(n, pa, load_y(n, pa), X[n], Rv[n]);
     }
     const double vals[2] = {block_sum<kThreads>(rr), block_sum<kThreads>(rz)};
     double tot[2];
@@ -217,7 +192,7 @@ __device__ __forceinline__ void pcg_update1_body(const Mesh& m, int n_colours, c
 }
 
 template <typename T, bool GATHER, bool BJ>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads)
 k_pcg_update1(Mesh m, int n_colours, const T* __restrict__ p, const T* __restrict__ y, const T* __restrict__ d,
               T* __restrict__ x, T* __restrict__ r, PcgState* st, RedSite site, const int32_t* __restrict__ inc_ptr,
               const int32_t* __restrict__ inc, const T* __restrict__ fe) {
@@ -247,28 +222,18 @@ __device__ __forceinline__ void pcg_update2_body(const Mesh& m, const T* __restr
     const double beta = st->rz_new / st->rz;
     const T bt = (T)beta;
     double pf = 0.0;
-    const T2* Rv = reinterpret_cast<const T2*>(r);
-    T2* P = reinterpret_cast<T2*>(p);
-    auto update = [&](int64_t n, int fix, T2 rn, T2 pn) {
+    for (int64_t n = blk * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)nblk * blockDim.x) {
+        const int fix = m.node_fix[n];
+        const T2 rn = reinterpret_cast<const T2*>(r)[n];
         const T2 zn = precond<BJ, T>(d, n, rn);
+        T2 pn = reinterpret_cast<const T2*>(p)[n];
         pn.x = zn.x + bt * pn.x;
         pn.y = zn.y + bt * pn.y;
-        P[n] = pn;
+        reinterpret_cast<T2*>(p)[n] = pn;
         if (PIVOT) reinterpret_cast<T2*>(y)[n] = make_v2<T>((fix & 1) ? pn.x : T(0), (fix & 2) ? pn.y : T(0));
         if (fix & 1) pf += (double)pn.x * pn.x;
         if (fix & 2) pf += (double)pn.y * pn.y;
-    };
-    // nodes in pairs, loads first (as in update 1); the same order of the partial sums
-    const int64_t stride = (int64_t)nblk * blockDim.x;
-    int64_t n = blk * (int64_t)blockDim.x + threadIdx.x;
-    for (; n + stride < m.n_nodes; n += 2 * stride) {
-        const int64_t n2 = n + stride;
-        const int fa = m.node_fix[n], fb = m.node_fix[n2];
-        const T2 ra = Rv[n], rb = Rv[n2], pa = P[n], pb = P[n2];
-        update(n, fa, ra, pa);
-        update(n2, fb, rb, pb);
     }
-    if (n < m.n_nodes) update(n, m.node_fix[n], Rv[n], P[n]);
     const double vals[1] = {block_sum<kThreads>(pf)};
     double tot[1];
     if (last_block_sum_in<kThreads, 1>(vals, site, tot, blk, nblk) && threadIdx.x == 0) {
@@ -283,7 +248,7 @@ __device__ __forceinline__ void pcg_update2_body(const Mesh& m, const T* __restr
 }
 
 template <typename T, bool PIVOT, bool BJ>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads)
 k_pcg_update2(Mesh m, const T* __restrict__ r, const T* __restrict__ d, T* __restrict__ p, T* __restrict__ y,
               PcgState* st, RedSite site) {
     grid_dependency_wait();
