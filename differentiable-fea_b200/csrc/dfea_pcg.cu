@@ -449,7 +449,10 @@ struct dfea_pcg {
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int32_t* host_status = nullptr;  // pinned: [done, iters]
+    // [done, iters, bodies]: read after the stream has reached the copy.  Ordinary host memory (the handle's
+    // own buffer): a page-locked allocation per handle cost a device-wide driver call for every solve set up.
+    int32_t status_buf[4] = {0, 0, 0, 0};
+    int32_t* host_status = status_buf;
 
     PcgState* state() const { return reinterpret_cast<PcgState*>(work + layout.off_state); }
     RedSite site(int i, int k_slot_results) const {
@@ -648,7 +651,6 @@ void release(dfea_pcg* h) {
     if (h->exec) cudaGraphExecDestroy(h->exec);
     if (h->graph) cudaGraphDestroy(h->graph);
     if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
-    if (h->host_status) cudaFreeHost(h->host_status);
     delete h;
 }
 
@@ -737,9 +739,7 @@ extern "C" int dfea_pcg_create(const dfea_mesh_view* mesh, const void* moduli, c
         }
         return DFEA_OK;
     });
-    if ((rc = check_cuda(cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
-        (rc = check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&h->host_status), 4 * sizeof(int32_t), cudaHostAllocDefault),
-                         "cudaHostAlloc"))) {
+    if ((rc = check_cuda(cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking), "cudaStreamCreate"))) {
         release(h);
         return rc;
     }

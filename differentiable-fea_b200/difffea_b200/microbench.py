@@ -239,7 +239,8 @@ def vcycle_once(element, n_elements, precision, reps=10):
                 levels=[(lv.gx, lv.gy) for lv in mg.levels], setup_ms=setup_ms, cycle_ms=cycle_ms, cycle_ms_min=cycle_min)
 
 
-def solve_once(element, nx, precision, pcg_graph, form="auto", preconditioner="jacobi"):
+def solve_once(element, nx, precision, pcg_graph, form="auto", preconditioner="jacobi", mg_graphs=False,
+               mg_bounds_every=3):
     """Wall and device milliseconds of one serving-type request (the second of two identical solves)."""
     import time
     from difffea_b200.serving import Request, solve_request
@@ -253,7 +254,7 @@ def solve_once(element, nx, precision, pcg_graph, form="auto", preconditioner="j
         t = time.perf_counter()
         e0.record(s)
         u, info = solve_request(req, "cuda", precision=prec, pcg_graph=pcg_graph, pcg_form=form,
-                                preconditioner=preconditioner)
+                                preconditioner=preconditioner, mg_graphs=mg_graphs, mg_bounds_every=mg_bounds_every)
         e1.record(s)
         torch.cuda.synchronize()
         out = dict(kernel="solve", element=element, nx=nx, n_el=req.n_elements, precision=precision,
@@ -283,6 +284,9 @@ def main(argv=None):
                     help="material of the moduli / residual / sensitivity / fields kernels (library defaults); "
                          "all = every material in turn")
     ap.add_argument("--preconditioner", default="jacobi", choices=("jacobi", "block_jacobi", "multigrid"),
+    ap.add_argument("--mg-graphs", action="store_true", help="solve: graph-driven multigrid (default: host-driven, "
+                    "as the serving engine)")
+    ap.add_argument("--mg-bounds-every", type=int, default=3, help="solve: multigrid smoother bounds every k-th set-up")
                     help="preconditioner of the solve kind")
     ap.add_argument("--pcg-graph", type=int, default=None,
                     help="PCG form: 0 direct launches (solve's default), 1 loop graph (pcg's default), "
@@ -290,7 +294,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     if a.kind == "solve":
         print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph,
-                                    a.form or "auto", a.preconditioner)),
+                                    a.form or "auto", a.preconditioner, a.mg_graphs, a.mg_bounds_every)),
               flush=True)
         return 0
     if a.kind == "vcycle":
