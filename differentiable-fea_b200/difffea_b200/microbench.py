@@ -284,10 +284,10 @@ def main(argv=None):
                     help="material of the moduli / residual / sensitivity / fields kernels (library defaults); "
                          "all = every material in turn")
     ap.add_argument("--preconditioner", default="jacobi", choices=("jacobi", "block_jacobi", "multigrid"),
+                    help="preconditioner of the solve kind")
     ap.add_argument("--mg-graphs", action="store_true", help="solve: graph-driven multigrid (default: host-driven, "
                     "as the serving engine)")
     ap.add_argument("--mg-bounds-every", type=int, default=3, help="solve: multigrid smoother bounds every k-th set-up")
-                    help="preconditioner of the solve kind")
     ap.add_argument("--pcg-graph", type=int, default=None,
                     help="PCG form: 0 direct launches (solve's default), 1 loop graph (pcg's default), "
                          "2 unrolled graph")
