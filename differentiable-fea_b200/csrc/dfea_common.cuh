@@ -30,6 +30,8 @@ long long thread_launch_count();  // launches noted by the calling thread (kerne
                                   // noted while capturing; the capture subtracts them again)
 int device_sm_count();
 long long persisting_l2_bytes(long long* max_window);
+// copy `bytes` from the device to `host` once stream `s` reaches the copy, through a pooled page-locked block
+int read_to_host(void* host, const void* dev, size_t bytes, cudaStream_t s);
 
 // Partial sums per reduction site; grids of reducing kernels never exceed this many blocks.
 constexpr int kMaxBlocks = 2048;

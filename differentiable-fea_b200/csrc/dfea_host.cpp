@@ -40,6 +40,50 @@ void note_launches(long long n) {
 }
 long long thread_launch_count() { return t_launches; }
 
+// Page-locked staging for the small reads that end a stream's work (PCG status words, host-driven dot
+// products, Lanczos histories).  A device-to-host copy into pageable memory goes through the driver's
+// staging path, which all threads of the process share, so with many solver threads waiting on their
+// streams the reads queue behind one another.  Blocks are allocated page-locked (portable across
+// devices) on first need and reused for the life of the process: the pool holds as many blocks as reads
+// were ever in flight at once.  Allocation failure falls back to a pageable read.
+static constexpr size_t kHostBlockBytes = 32 * 1024;
+static std::mutex g_host_blocks_mutex;
+static std::vector<void*> g_host_blocks;
+
+static void* acquire_host_block() {
+    {
+        std::lock_guard<std::mutex> lock(g_host_blocks_mutex);
+        if (!g_host_blocks.empty()) {
+            void* p = g_host_blocks.back();
+            g_host_blocks.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, kHostBlockBytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+static void release_host_block(void* p) {
+    std::lock_guard<std::mutex> lock(g_host_blocks_mutex);
+    g_host_blocks.push_back(p);
+}
+
+int read_to_host(void* host, const void* dev, size_t bytes, cudaStream_t s) {
+    void* block = bytes <= kHostBlockBytes ? acquire_host_block() : nullptr;
+    void* dst = block ? block : host;
+    int rc = check_cuda(cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    if (!rc) rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (block) {
+        if (!rc) std::memcpy(host, block, bytes);
+        release_host_block(block);
+    }
+    return rc;
+}
+
 int device_sm_count() {
     static std::atomic<int> cache[64];   // 0 until queried; threads that race store the same value
     int dev = 0;

@@ -819,8 +819,7 @@ static int validate_mg(const dfea_mesh_view* mesh, const dfea_mg* mg, const char
 }
 
 static int read_scalars(double* host, const double* dev, int k, cudaStream_t s) {
-    int rc = check_cuda(cudaMemcpyAsync(host, dev, k * sizeof(double), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
-    return rc ? rc : check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    return read_to_host(host, dev, k * sizeof(double), s);
 }
 
 }  // namespace dfea
@@ -1115,9 +1114,7 @@ static int pcg_graph_solve(MgGraphs* g, const dfea_mg* mg, double rtol, int32_t 
         (rc = check_cuda(cudaGraphLaunch(g->loop, s), "cudaGraphLaunch")))
         return rc;
     int32_t host[5];  // k, max_iter, status, iters, guard
-    if ((rc = check_cuda(cudaMemcpyAsync(host, &st->k, sizeof(host), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync")) ||
-        (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
-        return rc;
+    if ((rc = read_to_host(host, &st->k, sizeof(host), s))) return rc;
     note_launches(2 + g->kernels_start + (long long)host[4] * g->kernels_body);
     if (host[2] == DFEA_PCG_RUNNING) return set_error(DFEA_ERR_INVALID, "dfea_mg_pcg: the device loop ended without a status");
     *status = host[2];

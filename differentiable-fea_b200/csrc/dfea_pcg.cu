@@ -449,8 +449,8 @@ struct dfea_pcg {
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    // [done, iters, bodies]: read after the stream has reached the copy.  Ordinary host memory (the handle's
-    // own buffer): a page-locked allocation per handle cost a device-wide driver call for every solve set up.
+    // [done, iters, bodies]: read after the stream has reached the copy, staged through the library's pool of
+    // page-locked blocks (a page-locked allocation per handle cost a device-wide driver call per solve set up).
     int32_t status_buf[4] = {0, 0, 0, 0};
     int32_t* host_status = status_buf;
 
@@ -779,19 +779,13 @@ extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_
         while (true) {
             if ((rc = check_cuda(cudaGraphLaunch(h->exec, s), "cudaGraphLaunch"))) return rc;
             launched += kUnrolled;
-            if ((rc = check_cuda(cudaMemcpyAsync(h->host_status, &st->done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
-                                 "cudaMemcpyAsync")) ||
-                (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
-                return rc;
+            if ((rc = read_to_host(h->host_status, &st->done, 2 * sizeof(int32_t), s))) return rc;
             if (h->host_status[0] != DFEA_PCG_RUNNING || launched > max_iter + kUnrolled) break;
         }
         note_launches((long long)launched * kernels_per_iteration(*h));
     } else if (h->use_graph) {
         if ((rc = check_cuda(cudaGraphLaunch(h->exec, s), "cudaGraphLaunch"))) return rc;
-        if ((rc = check_cuda(cudaMemcpyAsync(h->host_status, &st->done, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
-                             "cudaMemcpyAsync")) ||
-            (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
-            return rc;
+        if ((rc = read_to_host(h->host_status, &st->done, 3 * sizeof(int32_t), s))) return rc;
         // each executed body ran one iteration's kernels and the loop condition
         note_launches((long long)h->host_status[2] * (kernels_per_iteration(*h) + 1));
     } else {
@@ -805,10 +799,7 @@ extern "C" int dfea_pcg_solve(dfea_pcg* h, double rtol, int32_t max_iter, int32_
                 if (rc) return rc;
             }
             launched += chunk;
-            if ((rc = check_cuda(cudaMemcpyAsync(h->host_status, &st->done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
-                                 "cudaMemcpyAsync")) ||
-                (rc = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
-                return rc;
+            if ((rc = read_to_host(h->host_status, &st->done, 2 * sizeof(int32_t), s))) return rc;
             if (h->host_status[0] != DFEA_PCG_RUNNING || launched > max_iter + chunk) break;
         }
     }
