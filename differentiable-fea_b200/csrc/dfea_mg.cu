@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <mutex>
 #include <new>
+#include <utility>
 
 #include "dfea_common.cuh"
 
@@ -302,46 +303,53 @@ __global__ void k_mg_prolong_add(MgGrid fg, MgGrid cg, const int32_t* __restrict
 // ------------------------------------------------------------------------------------------
 // coarse-level operator: y = K v + (I - M) v (K has zero rows and columns at fixed DOFs); DIAG: diag(A)
 // ------------------------------------------------------------------------------------------
+// row of node n = I * ny + J (both DOFs); the standalone product and the fused smoothing steps below share it,
+// so they compute the same sums in the same order
 template <bool DIAG>
-__global__ void __launch_bounds__(256) k_mg_apply(MgGrid g, const double* __restrict__ v, double* __restrict__ y) {
-    const int nx = g.gx + 1, ny = g.gy + 1, n_cells = g.gx * g.gy;
-    const double2* v2 = reinterpret_cast<const double2*>(v);
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nx * ny; n += gridDim.x * blockDim.x) {
-        const int I = n / ny, J = n % ny;
-        double y0 = 0.0, y1 = 0.0;
+__device__ __forceinline__ double2 mg_node_row(const MgGrid& g, const double2* __restrict__ v2, int n) {
+    const int ny = g.gy + 1, n_cells = g.gx * g.gy;
+    const int I = n / ny, J = n % ny;
+    double y0 = 0.0, y1 = 0.0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            // cells around the node and the node's corner in each: (I-1,J-1):2 (I,J-1):3 (I,J):0 (I-1,J):1
-            const int CX = (k == 0 || k == 3) ? I - 1 : I, CY = (k <= 1) ? J - 1 : J;
-            const int b = k == 0 ? 2 : k == 1 ? 3 : k == 2 ? 0 : 1;
-            if (CX < 0 || CY < 0 || CX >= g.gx || CY >= g.gy) continue;
-            const int c = CX * g.gy + CY;
-            if (DIAG) {
-                y0 += g.K[(int64_t)((2 * b) * 8 + 2 * b) * n_cells + c];
-                y1 += g.K[(int64_t)((2 * b + 1) * 8 + 2 * b + 1) * n_cells + c];
-            } else {
-                const int cn[4] = {CX * ny + CY, (CX + 1) * ny + CY, (CX + 1) * ny + CY + 1, CX * ny + CY + 1};
+    for (int k = 0; k < 4; ++k) {
+        // cells around the node and the node's corner in each: (I-1,J-1):2 (I,J-1):3 (I,J):0 (I-1,J):1
+        const int CX = (k == 0 || k == 3) ? I - 1 : I, CY = (k <= 1) ? J - 1 : J;
+        const int b = k == 0 ? 2 : k == 1 ? 3 : k == 2 ? 0 : 1;
+        if (CX < 0 || CY < 0 || CX >= g.gx || CY >= g.gy) continue;
+        const int c = CX * g.gy + CY;
+        if (DIAG) {
+            y0 += g.K[(int64_t)((2 * b) * 8 + 2 * b) * n_cells + c];
+            y1 += g.K[(int64_t)((2 * b + 1) * 8 + 2 * b + 1) * n_cells + c];
+        } else {
+            const int cn[4] = {CX * ny + CY, (CX + 1) * ny + CY, (CX + 1) * ny + CY + 1, CX * ny + CY + 1};
 #pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const double2 t = v2[cn[a]];
-                    y0 += g.K[(int64_t)((2 * b) * 8 + 2 * a) * n_cells + c] * t.x +
-                          g.K[(int64_t)((2 * b) * 8 + 2 * a + 1) * n_cells + c] * t.y;
-                    y1 += g.K[(int64_t)((2 * b + 1) * 8 + 2 * a) * n_cells + c] * t.x +
-                          g.K[(int64_t)((2 * b + 1) * 8 + 2 * a + 1) * n_cells + c] * t.y;
-                }
+            for (int a = 0; a < 4; ++a) {
+                const double2 t = v2[cn[a]];
+                y0 += g.K[(int64_t)((2 * b) * 8 + 2 * a) * n_cells + c] * t.x +
+                      g.K[(int64_t)((2 * b) * 8 + 2 * a + 1) * n_cells + c] * t.y;
+                y1 += g.K[(int64_t)((2 * b + 1) * 8 + 2 * a) * n_cells + c] * t.x +
+                      g.K[(int64_t)((2 * b + 1) * 8 + 2 * a + 1) * n_cells + c] * t.y;
             }
         }
-        const int f = g.fix[n];
-        if (DIAG) {
-            y0 = (f & 1) ? 1.0 : y0;
-            y1 = (f & 2) ? 1.0 : y1;
-        } else {
-            const double2 t = v2[n];
-            if (f & 1) y0 += t.x;
-            if (f & 2) y1 += t.y;
-        }
-        reinterpret_cast<double2*>(y)[n] = make_double2(y0, y1);
     }
+    const int f = g.fix[n];
+    if (DIAG) {
+        y0 = (f & 1) ? 1.0 : y0;
+        y1 = (f & 2) ? 1.0 : y1;
+    } else {
+        const double2 t = v2[n];
+        if (f & 1) y0 += t.x;
+        if (f & 2) y1 += t.y;
+    }
+    return make_double2(y0, y1);
+}
+
+template <bool DIAG>
+__global__ void __launch_bounds__(256) k_mg_apply(MgGrid g, const double* __restrict__ v, double* __restrict__ y) {
+    const int n_nodes = (g.gx + 1) * (g.gy + 1);
+    const double2* v2 = reinterpret_cast<const double2*>(v);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x)
+        reinterpret_cast<double2*>(y)[n] = mg_node_row<DIAG>(g, v2, n);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -367,6 +375,79 @@ __global__ void k_mg_cheb_step(int64_t n, double* __restrict__ x, double* __rest
         const double ri = r[i] - q[i];
         r[i] = ri;
         if (!last) d[i] = c1 * di + c2 * ri / diag[i];
+    }
+}
+
+// Fused forms used inside a V-cycle; each computes exactly the expressions of the separate kernels it
+// replaces (the copy and reset before the pre-smoothing, k_mg_cheb_start, k_mg_apply + k_mg_cheb_step,
+// k_mg_apply / the tangent product + r = b - q + k_mg_cheb_start), in one launch instead of two or three.
+
+// start of the pre-smoothing from x = 0: r = b, x = 0, d = s r / D
+__global__ void k_mg_cheb_first(int64_t n, const double* __restrict__ b, const double* __restrict__ diag,
+                                const double* __restrict__ scale, double* __restrict__ r, double* __restrict__ x,
+                                double* __restrict__ d) {
+    const double s = *scale;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double bi = b[i];
+        r[i] = bi;
+        x[i] = 0.0;
+        d[i] = s * bi / diag[i];
+    }
+}
+
+// start of the post-smoothing from the product q = A x in memory: r = b - q, d = s r / D
+__global__ void k_mg_cheb_restart(int64_t n, const double* __restrict__ b, const double* __restrict__ q,
+                                  const double* __restrict__ diag, const double* __restrict__ scale,
+                                  double* __restrict__ r, double* __restrict__ d) {
+    const double s = *scale;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ri = b[i] - q[i];
+        r[i] = ri;
+        d[i] = s * ri / diag[i];
+    }
+}
+
+// the same on a coarse level with the product computed at the node: r = b - A x, d = s r / D
+__global__ void __launch_bounds__(256) k_mg_residual_restart(MgGrid g, const double* __restrict__ b,
+                                                             const double* __restrict__ x, const double* __restrict__ diag,
+                                                             const double* __restrict__ scale, double* __restrict__ r,
+                                                             double* __restrict__ d) {
+    const double s = *scale;
+    const int n_nodes = (g.gx + 1) * (g.gy + 1);
+    const double2 *x2 = reinterpret_cast<const double2*>(x), *b2 = reinterpret_cast<const double2*>(b),
+                  *D2 = reinterpret_cast<const double2*>(diag);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
+        const double2 q = mg_node_row<false>(g, x2, n), bn = b2[n], dn = D2[n];
+        const double r0 = bn.x - q.x, r1 = bn.y - q.y;
+        reinterpret_cast<double2*>(r)[n] = make_double2(r0, r1);
+        reinterpret_cast<double2*>(d)[n] = make_double2(s * r0 / dn.x, s * r1 / dn.y);
+    }
+}
+
+// one Chebyshev step on a coarse level with its product computed at the node: q = A d_in, x += d_in,
+// r -= q, d_out = c1 d_in + c2 r / D (not written by the last step).  d is double-buffered because
+// neighbouring nodes read d_in.
+__global__ void __launch_bounds__(256) k_mg_cheb_apply_step(MgGrid g, double* __restrict__ x, double* __restrict__ r,
+                                                            const double* __restrict__ d_in, double* __restrict__ d_out,
+                                                            const double* __restrict__ diag,
+                                                            const double* __restrict__ c, int last) {
+    const double c1 = last ? 0.0 : c[0], c2 = last ? 0.0 : c[1];
+    const int n_nodes = (g.gx + 1) * (g.gy + 1);
+    const double2 *d2 = reinterpret_cast<const double2*>(d_in), *D2 = reinterpret_cast<const double2*>(diag);
+    double2 *x2 = reinterpret_cast<double2*>(x), *r2 = reinterpret_cast<double2*>(r);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
+        const double2 q = mg_node_row<false>(g, d2, n), dn = d2[n];
+        double2 xn = x2[n];
+        xn.x += dn.x;
+        xn.y += dn.y;
+        x2[n] = xn;
+        const double2 rn = r2[n];
+        const double r0 = rn.x - q.x, r1 = rn.y - q.y;
+        r2[n] = make_double2(r0, r1);
+        if (!last) {
+            const double2 Dn = D2[n];
+            reinterpret_cast<double2*>(d_out)[n] = make_double2(c1 * dn.x + c2 * r0 / Dn.x, c1 * dn.y + c2 * r1 / Dn.y);
+        }
     }
 }
 
@@ -761,15 +842,27 @@ static int mg_apply(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* m
     return dfea_mg_apply(&mg->level[l].grid, v, y, s);
 }
 
-static int mg_cheb(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, int l, double* x,
-                   double* r, cudaStream_t s) {
+// the Chebyshev steps of one smoothing pass at level l, from the first direction in lv.d; on coarse levels
+// each step is one fused launch with d alternating between lv.d and lv.q
+static int mg_cheb_steps(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, int l,
+                         double* x, double* r, cudaStream_t s) {
     const dfea_mg_level& lv = mg->level[l];
     const double* row = mg->coef + (int64_t)l * 2 * DFEA_MG_MAX_DEGREE;
-    int rc = dfea_mg_cheb_start(lv.n, r, lv.diag, row, lv.d, s);
+    double *d_in = lv.d, *d_out = lv.q;
+    int rc = DFEA_OK;
     for (int k = 1; !rc && k <= mg->degree; ++k) {
-        const bool last = k == mg->degree;
-        if ((rc = mg_apply(mesh, mg, moduli, code, l, lv.d, lv.q, s))) break;
-        rc = dfea_mg_cheb_step(lv.n, x, r, lv.d, lv.q, lv.diag, last ? nullptr : row + 1 + 2 * (k - 1), last ? 1 : 0, s);
+        const int last = k == mg->degree ? 1 : 0;
+        const double* c = last ? nullptr : row + 1 + 2 * (k - 1);
+        if (l == 0) {
+            if (!(rc = mg_apply(mesh, mg, moduli, code, 0, lv.d, lv.q, s)))
+                rc = dfea_mg_cheb_step(lv.n, x, r, lv.d, lv.q, lv.diag, c, last, s);
+            continue;
+        }
+        const int n_nodes = (lv.grid.gx + 1) * (lv.grid.gy + 1);
+        k_mg_cheb_apply_step<<<grid_for(n_nodes, 256, 8), 256, 0, s>>>(mg_grid(lv.grid), x, r, d_in, d_out, lv.diag, c, last);
+        note_launches(1);
+        rc = launch_check("dfea_mg_vcycle: smoothing step");
+        std::swap(d_in, d_out);
     }
     return rc;
 }
@@ -779,9 +872,10 @@ static int mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* 
     const dfea_mg_level& lv = mg->level[l];
     int rc;
     if (l == mg->n_levels - 1) return dfea_mg_dense_solve((int32_t)lv.n, mg->Ainv, b, x, s);
-    if ((rc = check_cuda(cudaMemcpyAsync(lv.r, b, lv.n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")) ||
-        (rc = check_cuda(cudaMemsetAsync(x, 0, lv.n * sizeof(double), s), "cudaMemsetAsync")) ||
-        (rc = mg_cheb(mesh, mg, moduli, code, l, x, lv.r, s)))
+    const double* scale = mg->coef + (int64_t)l * 2 * DFEA_MG_MAX_DEGREE;
+    k_mg_cheb_first<<<grid_for(lv.n, kThreads, 8), kThreads, 0, s>>>(lv.n, b, lv.diag, scale, lv.r, x, lv.d);
+    note_launches(1);
+    if ((rc = launch_check("dfea_mg_vcycle: smoothing start")) || (rc = mg_cheb_steps(mesh, mg, moduli, code, l, x, lv.r, s)))
         return rc;
     const dfea_mg_level& c = mg->level[l + 1];
     const int32_t* gn;
@@ -789,11 +883,18 @@ static int mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* 
     transfer_args(mesh, mg, l, &gn, &ffix);
     if ((rc = dfea_mg_restrict(&lv.grid, &c.grid, gn, ffix, lv.r, c.b, nullptr, s)) ||
         (rc = mg_vcycle(mesh, mg, moduli, code, l + 1, c.b, c.x, s)) ||
-        (rc = dfea_mg_prolong_add(&lv.grid, &c.grid, gn, ffix, c.x, x, s)) ||
-        (rc = mg_apply(mesh, mg, moduli, code, l, x, lv.q, s)) ||
-        (rc = dfea_add_scaled(lv.n, b, -1.0, lv.q, lv.r, s)))
+        (rc = dfea_mg_prolong_add(&lv.grid, &c.grid, gn, ffix, c.x, x, s)))
         return rc;
-    return mg_cheb(mesh, mg, moduli, code, l, x, lv.r, s);
+    if (l == 0) {
+        if ((rc = mg_apply(mesh, mg, moduli, code, 0, x, lv.q, s))) return rc;
+        k_mg_cheb_restart<<<grid_for(lv.n, kThreads, 8), kThreads, 0, s>>>(lv.n, b, lv.q, lv.diag, scale, lv.r, lv.d);
+    } else {
+        const int n_nodes = (lv.grid.gx + 1) * (lv.grid.gy + 1);
+        k_mg_residual_restart<<<grid_for(n_nodes, 256, 8), 256, 0, s>>>(mg_grid(lv.grid), b, x, lv.diag, scale, lv.r, lv.d);
+    }
+    note_launches(1);
+    if ((rc = launch_check("dfea_mg_vcycle: residual"))) return rc;
+    return mg_cheb_steps(mesh, mg, moduli, code, l, x, lv.r, s);
 }
 
 static int validate_mg(const dfea_mesh_view* mesh, const dfea_mg* mg, const char* what) {
