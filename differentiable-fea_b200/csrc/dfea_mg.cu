@@ -245,59 +245,73 @@ __device__ __forceinline__ int fine_node(const int32_t* gnode, int fgy, int i, i
 
 // rc = P~^T r (masked at fixed fine DOFs); with fix_out, also the coarse fix bits (a coarse DOF is fixed
 // when every fine DOF it interpolates to is fixed)
-__global__ void k_mg_restrict(MgGrid fg, MgGrid cg, const int32_t* __restrict__ gnode, const uint8_t* __restrict__ ffix,
-                              const double* __restrict__ r, double* __restrict__ rc, uint8_t* __restrict__ fix_out) {
+// coarse node n of the restriction r_c = P~^T r (and the coarse fixed-DOF bits); the kernels below and the
+// one-block tail of the V-cycle share these per-node functions, whose pointers carry no __restrict__ because
+// the tail reads in one phase what it wrote in the previous one
+__device__ __forceinline__ void mg_restrict_node(const MgGrid& fg, const MgGrid& cg, const int32_t* gnode,
+                                                 const uint8_t* ffix, const double* r, double* rc, uint8_t* fix_out,
+                                                 int n) {
     const int nx = cg.gx + 1, ny = cg.gy + 1;
     const double2* r2 = reinterpret_cast<const double2*>(r);
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nx * ny; n += gridDim.x * blockDim.x) {
-        const int I = n / ny, J = n % ny;
-        const int ilo = I > 0 ? cg.line_x[I - 1] + 1 : cg.line_x[I], ihi = I < cg.gx ? cg.line_x[I + 1] - 1 : cg.line_x[I];
-        const int jlo = J > 0 ? cg.line_y[J - 1] + 1 : cg.line_y[J], jhi = J < cg.gy ? cg.line_y[J + 1] - 1 : cg.line_y[J];
-        double ax = 0.0, ay = 0.0;
-        int free_bits = 0;
-        for (int i = ilo; i <= ihi; ++i) {
-            const double wx = hat(cg.line_x, nx, I, i);
-            for (int j = jlo; j <= jhi; ++j) {
-                const int id = fine_node(gnode, fg.gy, i, j);
-                if (id < 0) continue;
-                const double w = wx * hat(cg.line_y, ny, J, j);
-                const int f = ffix[id];
-                if (r) {
-                    const double2 t = r2[id];
-                    if (!(f & 1)) ax += w * t.x;
-                    if (!(f & 2)) ay += w * t.y;
-                }
-                if (w > 0.0) free_bits |= (~f) & 3;
+    const int I = n / ny, J = n % ny;
+    const int ilo = I > 0 ? cg.line_x[I - 1] + 1 : cg.line_x[I], ihi = I < cg.gx ? cg.line_x[I + 1] - 1 : cg.line_x[I];
+    const int jlo = J > 0 ? cg.line_y[J - 1] + 1 : cg.line_y[J], jhi = J < cg.gy ? cg.line_y[J + 1] - 1 : cg.line_y[J];
+    double ax = 0.0, ay = 0.0;
+    int free_bits = 0;
+    for (int i = ilo; i <= ihi; ++i) {
+        const double wx = hat(cg.line_x, nx, I, i);
+        for (int j = jlo; j <= jhi; ++j) {
+            const int id = fine_node(gnode, fg.gy, i, j);
+            if (id < 0) continue;
+            const double w = wx * hat(cg.line_y, ny, J, j);
+            const int f = ffix[id];
+            if (r) {
+                const double2 t = r2[id];
+                if (!(f & 1)) ax += w * t.x;
+                if (!(f & 2)) ay += w * t.y;
             }
+            if (w > 0.0) free_bits |= (~f) & 3;
         }
-        if (rc) reinterpret_cast<double2*>(rc)[n] = make_double2(ax, ay);
-        if (fix_out) fix_out[n] = (uint8_t)((~free_bits) & 3);
     }
+    if (rc) reinterpret_cast<double2*>(rc)[n] = make_double2(ax, ay);
+    if (fix_out) fix_out[n] = (uint8_t)((~free_bits) & 3);
 }
 
-// x += P~ ec (x untouched at fixed fine DOFs)
-__global__ void k_mg_prolong_add(MgGrid fg, MgGrid cg, const int32_t* __restrict__ gnode, const uint8_t* __restrict__ ffix,
-                                 const double* __restrict__ ec, double* __restrict__ x) {
-    const int fnx = fg.gx + 1, fny = fg.gy + 1, cny = cg.gy + 1;
+__global__ void k_mg_restrict(MgGrid fg, MgGrid cg, const int32_t* __restrict__ gnode, const uint8_t* __restrict__ ffix,
+                              const double* __restrict__ r, double* __restrict__ rc, uint8_t* __restrict__ fix_out) {
+    const int n_nodes = (cg.gx + 1) * (cg.gy + 1);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x)
+        mg_restrict_node(fg, cg, gnode, ffix, r, rc, fix_out, n);
+}
+
+// x += P~ ec (x untouched at fixed fine DOFs) at fine grid node n
+__device__ __forceinline__ void mg_prolong_node(const MgGrid& fg, const MgGrid& cg, const int32_t* gnode,
+                                                const uint8_t* ffix, const double* ec, double* x, int n) {
+    const int fny = fg.gy + 1, cny = cg.gy + 1;
     const double2* e2 = reinterpret_cast<const double2*>(ec);
     double2* x2 = reinterpret_cast<double2*>(x);
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < fnx * fny; n += gridDim.x * blockDim.x) {
-        const int i = n / fny, j = n % fny;
-        const int id = gnode ? gnode[n] : n;
-        if (id < 0) continue;
-        const int f = ffix[id];
-        if ((f & 3) == 3) continue;
-        const int CX = cg.cell_x[i], CY = cg.cell_y[j];
-        const int x0 = cg.line_x[CX], x1 = cg.line_x[CX + 1], y0 = cg.line_y[CY], y1 = cg.line_y[CY + 1];
-        const double wx1 = (double)(i - x0) / (double)(x1 - x0), wy1 = (double)(j - y0) / (double)(y1 - y0);
-        const double wx0 = 1.0 - wx1, wy0 = 1.0 - wy1;
-        const double2 e00 = e2[CX * cny + CY], e10 = e2[(CX + 1) * cny + CY];
-        const double2 e11 = e2[(CX + 1) * cny + CY + 1], e01 = e2[CX * cny + CY + 1];
-        double2 t = x2[id];
-        if (!(f & 1)) t.x += wx0 * wy0 * e00.x + wx1 * wy0 * e10.x + wx1 * wy1 * e11.x + wx0 * wy1 * e01.x;
-        if (!(f & 2)) t.y += wx0 * wy0 * e00.y + wx1 * wy0 * e10.y + wx1 * wy1 * e11.y + wx0 * wy1 * e01.y;
-        x2[id] = t;
-    }
+    const int i = n / fny, j = n % fny;
+    const int id = gnode ? gnode[n] : n;
+    if (id < 0) return;
+    const int f = ffix[id];
+    if ((f & 3) == 3) return;
+    const int CX = cg.cell_x[i], CY = cg.cell_y[j];
+    const int x0 = cg.line_x[CX], x1 = cg.line_x[CX + 1], y0 = cg.line_y[CY], y1 = cg.line_y[CY + 1];
+    const double wx1 = (double)(i - x0) / (double)(x1 - x0), wy1 = (double)(j - y0) / (double)(y1 - y0);
+    const double wx0 = 1.0 - wx1, wy0 = 1.0 - wy1;
+    const double2 e00 = e2[CX * cny + CY], e10 = e2[(CX + 1) * cny + CY];
+    const double2 e11 = e2[(CX + 1) * cny + CY + 1], e01 = e2[CX * cny + CY + 1];
+    double2 t = x2[id];
+    if (!(f & 1)) t.x += wx0 * wy0 * e00.x + wx1 * wy0 * e10.x + wx1 * wy1 * e11.x + wx0 * wy1 * e01.x;
+    if (!(f & 2)) t.y += wx0 * wy0 * e00.y + wx1 * wy0 * e10.y + wx1 * wy1 * e11.y + wx0 * wy1 * e01.y;
+    x2[id] = t;
+}
+
+__global__ void k_mg_prolong_add(MgGrid fg, MgGrid cg, const int32_t* __restrict__ gnode, const uint8_t* __restrict__ ffix,
+                                 const double* __restrict__ ec, double* __restrict__ x) {
+    const int n_nodes = (fg.gx + 1) * (fg.gy + 1);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x)
+        mg_prolong_node(fg, cg, gnode, ffix, ec, x, n);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -306,7 +320,7 @@ __global__ void k_mg_prolong_add(MgGrid fg, MgGrid cg, const int32_t* __restrict
 // row of node n = I * ny + J (both DOFs); the standalone product and the fused smoothing steps below share it,
 // so they compute the same sums in the same order
 template <bool DIAG>
-__device__ __forceinline__ double2 mg_node_row(const MgGrid& g, const double2* __restrict__ v2, int n) {
+__device__ __forceinline__ double2 mg_node_row(const MgGrid& g, const double2* v2, int n) {
     const int ny = g.gy + 1, n_cells = g.gx * g.gy;
     const int I = n / ny, J = n % ny;
     double y0 = 0.0, y1 = 0.0;
@@ -407,48 +421,57 @@ __global__ void k_mg_cheb_restart(int64_t n, const double* __restrict__ b, const
     }
 }
 
-// the same on a coarse level with the product computed at the node: r = b - A x, d = s r / D
+// the same on a coarse level with the product computed at node n: r = b - A x, d = s r / D
+__device__ __forceinline__ void mg_residual_restart_node(const MgGrid& g, const double* b, const double* x,
+                                                         const double* diag, double s, double* r, double* d, int n) {
+    const double2 q = mg_node_row<false>(g, reinterpret_cast<const double2*>(x), n);
+    const double2 bn = reinterpret_cast<const double2*>(b)[n], dn = reinterpret_cast<const double2*>(diag)[n];
+    const double r0 = bn.x - q.x, r1 = bn.y - q.y;
+    reinterpret_cast<double2*>(r)[n] = make_double2(r0, r1);
+    reinterpret_cast<double2*>(d)[n] = make_double2(s * r0 / dn.x, s * r1 / dn.y);
+}
+
 __global__ void __launch_bounds__(256) k_mg_residual_restart(MgGrid g, const double* __restrict__ b,
                                                              const double* __restrict__ x, const double* __restrict__ diag,
                                                              const double* __restrict__ scale, double* __restrict__ r,
                                                              double* __restrict__ d) {
     const double s = *scale;
     const int n_nodes = (g.gx + 1) * (g.gy + 1);
-    const double2 *x2 = reinterpret_cast<const double2*>(x), *b2 = reinterpret_cast<const double2*>(b),
-                  *D2 = reinterpret_cast<const double2*>(diag);
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
-        const double2 q = mg_node_row<false>(g, x2, n), bn = b2[n], dn = D2[n];
-        const double r0 = bn.x - q.x, r1 = bn.y - q.y;
-        reinterpret_cast<double2*>(r)[n] = make_double2(r0, r1);
-        reinterpret_cast<double2*>(d)[n] = make_double2(s * r0 / dn.x, s * r1 / dn.y);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x)
+        mg_residual_restart_node(g, b, x, diag, s, r, d, n);
+}
+
+// one Chebyshev step on a coarse level with its product computed at node n: q = A d_in, x += d_in,
+// r -= q, d_out = c1 d_in + c2 r / D (not written by the last step).  d is double-buffered because
+// neighbouring nodes read d_in.
+__device__ __forceinline__ void mg_cheb_apply_step_node(const MgGrid& g, double* x, double* r, const double* d_in,
+                                                        double* d_out, const double* diag, double c1, double c2,
+                                                        int last, int n) {
+    const double2* d2 = reinterpret_cast<const double2*>(d_in);
+    const double2 q = mg_node_row<false>(g, d2, n), dn = d2[n];
+    double2* x2 = reinterpret_cast<double2*>(x);
+    double2* r2 = reinterpret_cast<double2*>(r);
+    double2 xn = x2[n];
+    xn.x += dn.x;
+    xn.y += dn.y;
+    x2[n] = xn;
+    const double2 rn = r2[n];
+    const double r0 = rn.x - q.x, r1 = rn.y - q.y;
+    r2[n] = make_double2(r0, r1);
+    if (!last) {
+        const double2 Dn = reinterpret_cast<const double2*>(diag)[n];
+        reinterpret_cast<double2*>(d_out)[n] = make_double2(c1 * dn.x + c2 * r0 / Dn.x, c1 * dn.y + c2 * r1 / Dn.y);
     }
 }
 
-// one Chebyshev step on a coarse level with its product computed at the node: q = A d_in, x += d_in,
-// r -= q, d_out = c1 d_in + c2 r / D (not written by the last step).  d is double-buffered because
-// neighbouring nodes read d_in.
 __global__ void __launch_bounds__(256) k_mg_cheb_apply_step(MgGrid g, double* __restrict__ x, double* __restrict__ r,
                                                             const double* __restrict__ d_in, double* __restrict__ d_out,
                                                             const double* __restrict__ diag,
                                                             const double* __restrict__ c, int last) {
     const double c1 = last ? 0.0 : c[0], c2 = last ? 0.0 : c[1];
     const int n_nodes = (g.gx + 1) * (g.gy + 1);
-    const double2 *d2 = reinterpret_cast<const double2*>(d_in), *D2 = reinterpret_cast<const double2*>(diag);
-    double2 *x2 = reinterpret_cast<double2*>(x), *r2 = reinterpret_cast<double2*>(r);
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
-        const double2 q = mg_node_row<false>(g, d2, n), dn = d2[n];
-        double2 xn = x2[n];
-        xn.x += dn.x;
-        xn.y += dn.y;
-        x2[n] = xn;
-        const double2 rn = r2[n];
-        const double r0 = rn.x - q.x, r1 = rn.y - q.y;
-        r2[n] = make_double2(r0, r1);
-        if (!last) {
-            const double2 Dn = D2[n];
-            reinterpret_cast<double2*>(d_out)[n] = make_double2(c1 * dn.x + c2 * r0 / Dn.x, c1 * dn.y + c2 * r1 / Dn.y);
-        }
-    }
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x)
+        mg_cheb_apply_step_node(g, x, r, d_in, d_out, diag, c1, c2, last, n);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -568,13 +591,104 @@ __global__ void __launch_bounds__(1024) k_mg_dense_inverse(MgGrid g, double* __r
 }
 
 // x = Ainv b, one warp per row
+// row r of x = Ainv b by one warp (lane-strided partial sums, then the warp's butterfly sum)
+__device__ __forceinline__ void mg_dense_row(int n, const double* Ainv, const double* b, double* x, int r, int lane) {
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += Ainv[(int64_t)r * n + j] * b[j];
+    s = warp_sum(s);
+    if (lane == 0) x[r] = s;
+}
+
 __global__ void k_mg_dense_solve(int n, const double* __restrict__ Ainv, const double* __restrict__ b, double* __restrict__ x) {
     const int lane = threadIdx.x & 31;
-    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
-        double s = 0.0;
-        for (int j = lane; j < n; j += 32) s += Ainv[(int64_t)r * n + j] * b[j];
-        s = warp_sum(s);
-        if (lane == 0) x[r] = s;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5)
+        mg_dense_row(n, Ainv, b, x, r, lane);
+}
+
+// ------------------------------------------------------------------------------------------
+// the coarse tail of a V-cycle in one block: levels t .. L-1 are small enough that a launch per smoothing
+// step costs more than the step, so one block runs the restriction from level t - 1, the smoothing of
+// every tail level, the coarsest solve and the prolongation back to level t - 1, with a block barrier
+// between phases.  Each phase calls the per-node function of the kernel it replaces, so the result is
+// bitwise that of the separate launches.
+// ------------------------------------------------------------------------------------------
+constexpr int kMgTailThreads = 512;
+constexpr int kMgTailNodes = 1536;   // levels of at most this many nodes run in the tail
+
+struct MgTailLevel {
+    MgGrid grid;
+    int n;                       // DOFs
+    const double* diag;
+    const double* coef;          // [scale, (c1, c2) per step]
+    double *b, *x, *r, *d, *q;
+};
+
+struct MgTail {
+    MgGrid fine;                 // level t - 1 (the transfers' fine side)
+    const int32_t* gnode;
+    const uint8_t* ffix;
+    const double* r_fine;        // level t - 1's residual, restricted into level t's right-hand side
+    double* x_fine;              // level t - 1's iterate, corrected by the prolongation of level t's
+    const double* Ainv;
+    int n_levels, degree;        // tail levels; the last is the coarsest
+    MgTailLevel lv[DFEA_MG_MAX_LEVELS];
+};
+
+__device__ __forceinline__ void tail_smooth(const MgTailLevel& L, int degree) {
+    const int n_nodes = L.n / 2;
+    double *d_in = L.d, *d_out = L.q;
+    for (int k = 1; k <= degree; ++k) {
+        const int last = k == degree ? 1 : 0;
+        const double c1 = last ? 0.0 : L.coef[1 + 2 * (k - 1)], c2 = last ? 0.0 : L.coef[2 + 2 * (k - 1)];
+        for (int n = threadIdx.x; n < n_nodes; n += blockDim.x)
+            mg_cheb_apply_step_node(L.grid, L.x, L.r, d_in, d_out, L.diag, c1, c2, last, n);
+        __syncthreads();
+        double* t = d_in;
+        d_in = d_out;
+        d_out = t;
+    }
+}
+
+__global__ void __launch_bounds__(kMgTailThreads) k_mg_tail(const __grid_constant__ MgTail T) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+    const int last = T.n_levels - 1;
+    for (int l = 0; l <= last; ++l) {
+        const MgTailLevel& L = T.lv[l];
+        const MgGrid& fg = l == 0 ? T.fine : T.lv[l - 1].grid;
+        const int32_t* gn = l == 0 ? T.gnode : nullptr;
+        const uint8_t* ffix = l == 0 ? T.ffix : T.lv[l - 1].grid.fix;
+        const double* r = l == 0 ? T.r_fine : T.lv[l - 1].r;
+        for (int n = threadIdx.x; n < L.n / 2; n += blockDim.x) mg_restrict_node(fg, L.grid, gn, ffix, r, L.b, nullptr, n);
+        __syncthreads();
+        if (l == last) break;
+        const double s = L.coef[0];
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+            const double bi = L.b[i];
+            L.r[i] = bi;
+            L.x[i] = 0.0;
+            L.d[i] = s * bi / L.diag[i];
+        }
+        __syncthreads();
+        tail_smooth(L, T.degree);
+    }
+    const MgTailLevel& C = T.lv[last];
+    for (int r = warp; r < C.n; r += n_warps) mg_dense_row(C.n, T.Ainv, C.b, C.x, r, lane);
+    __syncthreads();
+    for (int l = last; l >= 0; --l) {
+        const MgTailLevel& L = T.lv[l];
+        const MgGrid& fg = l == 0 ? T.fine : T.lv[l - 1].grid;
+        const int32_t* gn = l == 0 ? T.gnode : nullptr;
+        const uint8_t* ffix = l == 0 ? T.ffix : T.lv[l - 1].grid.fix;
+        double* xf = l == 0 ? T.x_fine : T.lv[l - 1].x;
+        const int fine_nodes = (fg.gx + 1) * (fg.gy + 1);
+        for (int n = threadIdx.x; n < fine_nodes; n += blockDim.x) mg_prolong_node(fg, L.grid, gn, ffix, L.x, xf, n);
+        __syncthreads();
+        if (l == 0) break;
+        const MgTailLevel& F = T.lv[l - 1];
+        const double s = F.coef[0];
+        for (int n = threadIdx.x; n < F.n / 2; n += blockDim.x) mg_residual_restart_node(F.grid, F.b, F.x, F.diag, s, F.r, F.d, n);
+        __syncthreads();
+        tail_smooth(F, T.degree);
     }
 }
 
@@ -867,6 +981,34 @@ static int mg_cheb_steps(const dfea_mesh_view* mesh, const dfea_mg* mg, const vo
     return rc;
 }
 
+// first level (>= 1) of the one-block tail: levels shrink, so every level from it on is small enough
+static int tail_start(const dfea_mg* mg) {
+    for (int l = 1; l < mg->n_levels; ++l)
+        if (mg->level[l].n / 2 <= kMgTailNodes) return l;
+    return mg->n_levels;
+}
+
+// restriction of level l's residual, the cycle of levels l + 1 .. L - 1 and the prolongation into x, in one launch
+static int launch_tail(const dfea_mesh_view* mesh, const dfea_mg* mg, int l, double* x, cudaStream_t s) {
+    MgTail T = {};
+    const dfea_mg_level& lv = mg->level[l];
+    T.fine = mg_grid(lv.grid);
+    transfer_args(mesh, mg, l, &T.gnode, &T.ffix);
+    T.r_fine = lv.r;
+    T.x_fine = x;
+    T.Ainv = mg->Ainv;
+    T.n_levels = mg->n_levels - (l + 1);
+    T.degree = mg->degree;
+    for (int k = 0; k < T.n_levels; ++k) {
+        const dfea_mg_level& c = mg->level[l + 1 + k];
+        T.lv[k] = MgTailLevel{mg_grid(c.grid), (int)c.n, c.diag, mg->coef + (int64_t)(l + 1 + k) * 2 * DFEA_MG_MAX_DEGREE,
+                              c.b, c.x, c.r, c.d, c.q};
+    }
+    k_mg_tail<<<1, kMgTailThreads, 0, s>>>(T);
+    note_launches(1);
+    return launch_check("dfea_mg_vcycle: coarse tail");
+}
+
 static int mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, int l,
                      const double* b, double* x, cudaStream_t s) {
     const dfea_mg_level& lv = mg->level[l];
@@ -881,10 +1023,13 @@ static int mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* 
     const int32_t* gn;
     const uint8_t* ffix;
     transfer_args(mesh, mg, l, &gn, &ffix);
-    if ((rc = dfea_mg_restrict(&lv.grid, &c.grid, gn, ffix, lv.r, c.b, nullptr, s)) ||
-        (rc = mg_vcycle(mesh, mg, moduli, code, l + 1, c.b, c.x, s)) ||
-        (rc = dfea_mg_prolong_add(&lv.grid, &c.grid, gn, ffix, c.x, x, s)))
+    if (l + 1 == tail_start(mg)) {
+        if ((rc = launch_tail(mesh, mg, l, x, s))) return rc;
+    } else if ((rc = dfea_mg_restrict(&lv.grid, &c.grid, gn, ffix, lv.r, c.b, nullptr, s)) ||
+               (rc = mg_vcycle(mesh, mg, moduli, code, l + 1, c.b, c.x, s)) ||
+               (rc = dfea_mg_prolong_add(&lv.grid, &c.grid, gn, ffix, c.x, x, s))) {
         return rc;
+    }
     if (l == 0) {
         if ((rc = mg_apply(mesh, mg, moduli, code, 0, x, lv.q, s))) return rc;
         k_mg_cheb_restart<<<grid_for(lv.n, kThreads, 8), kThreads, 0, s>>>(lv.n, b, lv.q, lv.diag, scale, lv.r, lv.d);
