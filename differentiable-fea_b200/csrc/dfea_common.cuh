@@ -32,6 +32,13 @@ int device_sm_count();
 long long persisting_l2_bytes(long long* max_window);
 // copy `bytes` from the device to `host` once stream `s` reaches the copy, through a pooled page-locked block
 int read_to_host(void* host, const void* dev, size_t bytes, cudaStream_t s);
+// gather-form product on the finite-element level of the multigrid V-cycle with the smoothing update in its
+// node pass (dfea_kernels.cu): MG_FE_STEP, one Chebyshev step from direction v = d; MG_FE_RESTART, the
+// residual r = b - A v and first direction after the coarse-grid correction (v = x)
+enum { MG_FE_STEP = 0, MG_FE_RESTART = 1 };
+int mg_fe_gather_cheb(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype, void* fe_work, int mode,
+                      const double* v, double* x, double* r, double* d, const double* b, const double* diag,
+                      const double* coef, int last, cudaStream_t s);
 
 // Partial sums per reduction site; grids of reducing kernels never exceed this many blocks.
 constexpr int kMaxBlocks = 2048;

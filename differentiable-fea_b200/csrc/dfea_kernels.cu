@@ -546,6 +546,49 @@ __global__ void k_zero_tickets(unsigned* t, int n, double* results, int nr) {
     if (i < nr) results[i] = 0.0;
 }
 
+// Node pass of the gather-form product q = A v on the finite-element level of the multigrid V-cycle, with
+// the smoothing arithmetic that follows the product applied at the node (each node's q is complete here and
+// the element pass has finished reading v):
+//   MG_FE_STEP    (v = d): x += d, r -= q, d = c1 d + c2 r / D (d kept by the last step), coef = (c1, c2);
+//   MG_FE_RESTART (v = x): r = b - q, d = s r / D, coef = (s).
+// The expressions are those of k_node_gather followed by the multigrid's separate Chebyshev kernels, so the
+// iterates are bitwise the same.  d and v alias in MG_FE_STEP (read and written at the thread's own node).
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+k_node_gather_cheb(Mesh m, const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc, const double* __restrict__ fe,
+                   const double* v, double* __restrict__ x, double* __restrict__ r, double* d, const double* __restrict__ b,
+                   const double* __restrict__ diag, const double* __restrict__ coef, int last) {
+    grid_dependency_wait();
+    grid_dependents_launch();
+    const double2* fe2 = reinterpret_cast<const double2*>(fe);
+    const double c1 = (MODE == MG_FE_RESTART || last) ? 0.0 : coef[0];
+    const double c2 = (MODE == MG_FE_RESTART || last) ? 0.0 : coef[1];
+    const double sc = MODE == MG_FE_RESTART ? coef[0] : 0.0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < m.n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fix = m.node_fix[n];
+        const double2 f = node_sum<double>(inc_ptr, inc, fe2, n);
+        const double2 vn = reinterpret_cast<const double2*>(v)[n];
+        const double q0 = (fix & 1) ? vn.x : f.x, q1 = (fix & 2) ? vn.y : f.y;
+        const double2 Dn = reinterpret_cast<const double2*>(diag)[n];
+        if (MODE == MG_FE_STEP) {
+            const double2 dn = reinterpret_cast<const double2*>(d)[n];
+            double2 xn = reinterpret_cast<const double2*>(x)[n];
+            xn.x += dn.x;
+            xn.y += dn.y;
+            reinterpret_cast<double2*>(x)[n] = xn;
+            const double2 rn = reinterpret_cast<const double2*>(r)[n];
+            const double r0 = rn.x - q0, r1 = rn.y - q1;
+            reinterpret_cast<double2*>(r)[n] = make_double2(r0, r1);
+            if (!last) reinterpret_cast<double2*>(d)[n] = make_double2(c1 * dn.x + c2 * r0 / Dn.x, c1 * dn.y + c2 * r1 / Dn.y);
+        } else {
+            const double2 bn = reinterpret_cast<const double2*>(b)[n];
+            const double r0 = bn.x - q0, r1 = bn.y - q1;
+            reinterpret_cast<double2*>(r)[n] = make_double2(r0, r1);
+            reinterpret_cast<double2*>(d)[n] = make_double2(sc * r0 / Dn.x, sc * r1 / Dn.y);
+        }
+    }
+}
+
 }  // namespace dfea
 
 using namespace dfea;
@@ -781,6 +824,47 @@ extern "C" int dfea_tangent_apply_gather(const dfea_mesh_view* mesh, const void*
     if (rc) return rc;
     note_launches(2);
     return launch_check("dfea_tangent_apply_gather");
+}
+
+int dfea::mg_fe_gather_cheb(const dfea_mesh_view* mesh, const void* moduli, int32_t moduli_dtype, void* fe_work, int mode,
+                           const double* v, double* x, double* r, double* d, const double* b, const double* diag,
+                           const double* coef, int last, cudaStream_t s) {
+    int rc = validate_mesh(mesh, moduli_dtype == DFEA_F32);
+    if (rc) return rc;
+    if (!mesh->node_elem_ptr || !mesh->node_elem) return set_error(DFEA_ERR_INVALID, "multigrid smoothing: no node incidence");
+    if (!moduli || !v || !fe_work || !r || !d || !diag || (!last && !coef) || (mode == MG_FE_STEP && !x) ||
+        (mode == MG_FE_RESTART && !b))
+        return set_error(DFEA_ERR_INVALID, "multigrid smoothing: NULL pointer");
+    if (!aligned16(moduli) || !aligned16(v) || !aligned16(fe_work))
+        return set_error(DFEA_ERR_INVALID, "multigrid smoothing: moduli, v and fe_work must be 16-byte aligned");
+    if (moduli_dtype != DFEA_F64 && moduli_dtype != DFEA_F32 && moduli_dtype != DFEA_F32REF)
+        return set_error(DFEA_ERR_INVALID, "bad moduli dtype");
+    const Mesh m = kernel_mesh(*mesh);
+    const int gn = grid_for(mesh->n_nodes, kThreads, 4);
+    const RedSite none{nullptr, nullptr, nullptr};
+    LaunchOpts pdl;
+    pdl.pdl = true;
+    double* fe = static_cast<double*>(fe_work);
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        if (moduli_dtype == DFEA_F32REF)
+            return launch_apply_ref_elem<NEN, NQ, double, false>(*mesh, static_cast<const float*>(moduli), v, fe, none,
+                                                                nullptr, s);
+        if (moduli_dtype == DFEA_F64)
+            return launch_apply_elem<NEN, NQ, double, double, false>(*mesh, static_cast<const double*>(moduli), mesh->grad,
+                                                                    v, fe, none, nullptr, s);
+        return launch_apply_elem<NEN, NQ, float, double, false>(*mesh, static_cast<const float*>(moduli), mesh->grad32, v,
+                                                               fe, none, nullptr, s);
+    });
+    if (rc) return rc;
+    rc = mode == MG_FE_STEP
+             ? launch_kernel(k_node_gather_cheb<MG_FE_STEP>, dim3(gn), dim3(kThreads), 0, s, pdl, m, mesh->node_elem_ptr,
+                             mesh->node_elem, (const double*)fe, v, x, r, d, b, diag, coef, last)
+             : launch_kernel(k_node_gather_cheb<MG_FE_RESTART>, dim3(gn), dim3(kThreads), 0, s, pdl, m,
+                             mesh->node_elem_ptr, mesh->node_elem, (const double*)fe, v, x, r, d, b, diag, coef, last);
+    if (rc) return rc;
+    note_launches(2);
+    return launch_check("multigrid smoothing");
 }
 
 extern "C" int64_t dfea_reduce_work_bytes(const dfea_mesh_view* mesh) {

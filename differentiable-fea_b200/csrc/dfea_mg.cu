@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(256) k_mg_cheb_apply_step(MgGrid g, double* __
 constexpr int kMgDotBlocks = 296;
 constexpr int kMgDotThreads = 256;
 
-static int mg_dot_blocks(int64_t n) {
+__host__ __device__ static int mg_dot_blocks(int64_t n) {
     const int64_t b = (n + 4 * kMgDotThreads - 1) / (4 * kMgDotThreads);
     return (int)(b < 1 ? 1 : (b > kMgDotBlocks ? kMgDotBlocks : b));
 }
@@ -531,6 +531,114 @@ __global__ void k_mg_lanczos_p(int64_t n, double* __restrict__ p, const double* 
     const double beta = s[3];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = z[i] + beta * p[i];
+}
+
+// ------------------------------------------------------------------------------------------
+// Lanczos of the small levels in one block (levels of at most kMgTailNodes nodes, each smoothed level's
+// start and all its steps).  The dot products reproduce dfea_mg_dot inside the block: nb = mg_dot_blocks(n)
+// virtual blocks of kMgDotThreads threads with the same grid-stride accumulation, the same warp and block
+// trees, then the final block's tree over the nb partials, so the coefficients, the bounds and every later
+// iterate are bitwise those of the separate launches.
+// ------------------------------------------------------------------------------------------
+constexpr int kMgTailLanczosThreads = 2 * kMgDotThreads;
+
+struct MgLanczosLevel {
+    MgGrid grid;
+    int n;                       // DOFs
+    const double* diag;
+    double *r, *z, *p, *q;       // the level's r, d, x and q buffers
+    double* s;                   // [p.Ap, r.z, -, beta]
+    double* hist;                // (alpha_k, beta_k) per step
+};
+
+struct MgLanczosTail {
+    int n_levels, steps;
+    MgLanczosLevel lv[DFEA_MG_MAX_LEVELS];
+};
+
+// x.y, returned to every thread; every thread of the block calls it
+__device__ double tail_dot(int n, const double* x, const double* y) {
+    constexpr int NW = kMgDotThreads / 32;
+    __shared__ double warp_part[kMgTailLanczosThreads / 32];
+    __shared__ double block_part[kMgDotBlocks];
+    __shared__ double result;
+    const int half = threadIdx.x / kMgDotThreads, vt = threadIdx.x % kMgDotThreads;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nb = mg_dot_blocks(n);
+    for (int vb0 = 0; vb0 < nb; vb0 += 2) {
+        const int vb = vb0 + half;
+        double a = 0.0;
+        if (vb < nb)
+            for (int64_t i = vb * (int64_t)kMgDotThreads + vt; i < n; i += (int64_t)nb * kMgDotThreads) a += x[i] * y[i];
+        a = warp_sum(a);
+        if (lane == 0) warp_part[warp] = a;
+        __syncthreads();
+        if (warp % NW == 0) {
+            double r = (lane < NW) ? warp_part[warp + lane] : 0.0;
+            r = warp_sum(r);
+            if (lane == 0 && vb < nb) block_part[vb] = r;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < kMgDotThreads) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < nb; b += kMgDotThreads) a += block_part[b];
+        a = warp_sum(a);
+        if (lane == 0) warp_part[warp] = a;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double r = (lane < NW) ? warp_part[lane] : 0.0;
+        r = warp_sum(r);
+        if (lane == 0) result = r;
+    }
+    __syncthreads();
+    const double out = result;
+    __syncthreads();
+    return out;
+}
+
+__global__ void __launch_bounds__(kMgTailLanczosThreads) k_mg_tail_lanczos(const __grid_constant__ MgLanczosTail T) {
+    for (int l = 0; l < T.n_levels; ++l) {
+        const MgLanczosLevel& L = T.lv[l];
+        const int n_nodes = L.n / 2;
+        // start: r = sin(i + 1), z = r / D, p = z, s[1] = r.z
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+            const double ri = sin((double)(i + 1));
+            L.r[i] = ri;
+            const double zi = ri / L.diag[i];
+            L.z[i] = zi;
+            L.p[i] = zi;
+        }
+        __syncthreads();
+        double rz = tail_dot(L.n, L.r, L.z);
+        if (threadIdx.x == 0) L.s[1] = rz;
+        for (int k = 0; k < T.steps; ++k) {
+            for (int n = threadIdx.x; n < n_nodes; n += blockDim.x)
+                reinterpret_cast<double2*>(L.q)[n] = mg_node_row<false>(L.grid, reinterpret_cast<const double2*>(L.p), n);
+            __syncthreads();
+            const double pq = tail_dot(L.n, L.p, L.q);
+            const double alpha = rz / pq;
+            for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+                const double ri = L.r[i] - alpha * L.q[i];
+                L.r[i] = ri;
+                L.z[i] = ri / L.diag[i];
+            }
+            __syncthreads();
+            const double rz_new = tail_dot(L.n, L.r, L.z);
+            const double beta = rz_new / rz;
+            if (threadIdx.x == 0) {
+                L.hist[2 * k] = alpha;
+                L.hist[2 * k + 1] = beta;
+                L.s[0] = pq;
+                L.s[1] = rz_new;
+                L.s[3] = beta;
+            }
+            rz = rz_new;
+            for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.p[i] = L.z[i] + beta * L.p[i];
+            __syncthreads();
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -947,10 +1055,15 @@ static void transfer_args(const dfea_mesh_view* mesh, const dfea_mg* mg, int l, 
     *ffix = l == 0 ? mesh->node_fix : mg->level[l].grid.fix;
 }
 
+// level 0 in the gather form (the hierarchy was given element-product scratch and the mesh has node incidence)
+static bool fe_gather(const dfea_mesh_view* mesh, const dfea_mg* mg) {
+    return mg->fe_work && mesh->node_elem_ptr && mesh->node_elem;
+}
+
 static int mg_apply(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* moduli, int32_t code, int l,
                     const double* v, double* y, cudaStream_t s) {
     if (l == 0)
-        return (mg->fe_work && mesh->node_elem_ptr && mesh->node_elem)
+        return fe_gather(mesh, mg)
                    ? dfea_tangent_apply_gather(mesh, moduli, code, v, y, DFEA_F64, mg->fe_work, s)
                    : dfea_tangent_apply(mesh, moduli, code, v, y, DFEA_F64, s);
     return dfea_mg_apply(&mg->level[l].grid, v, y, s);
@@ -967,6 +1080,11 @@ static int mg_cheb_steps(const dfea_mesh_view* mesh, const dfea_mg* mg, const vo
     for (int k = 1; !rc && k <= mg->degree; ++k) {
         const int last = k == mg->degree ? 1 : 0;
         const double* c = last ? nullptr : row + 1 + 2 * (k - 1);
+        if (l == 0 && fe_gather(mesh, mg)) {
+            rc = mg_fe_gather_cheb(mesh, moduli, code, mg->fe_work, MG_FE_STEP, lv.d, x, r, lv.d, nullptr, lv.diag, c,
+                                   last, s);
+            continue;
+        }
         if (l == 0) {
             if (!(rc = mg_apply(mesh, mg, moduli, code, 0, lv.d, lv.q, s)))
                 rc = dfea_mg_cheb_step(lv.n, x, r, lv.d, lv.q, lv.diag, c, last, s);
@@ -1029,6 +1147,12 @@ static int mg_vcycle(const dfea_mesh_view* mesh, const dfea_mg* mg, const void* 
                (rc = mg_vcycle(mesh, mg, moduli, code, l + 1, c.b, c.x, s)) ||
                (rc = dfea_mg_prolong_add(&lv.grid, &c.grid, gn, ffix, c.x, x, s))) {
         return rc;
+    }
+    if (l == 0 && fe_gather(mesh, mg)) {
+        if ((rc = mg_fe_gather_cheb(mesh, moduli, code, mg->fe_work, MG_FE_RESTART, x, nullptr, lv.r, lv.d, b, lv.diag,
+                                    scale, 0, s)))
+            return rc;
+        return mg_cheb_steps(mesh, mg, moduli, code, l, x, lv.r, s);
     }
     if (l == 0) {
         if ((rc = mg_apply(mesh, mg, moduli, code, 0, x, lv.q, s))) return rc;
@@ -1145,8 +1269,22 @@ static int setup_device_part(const dfea_mesh_view* mesh, const dfea_mg* mg, cons
     }
     if ((rc = dfea_mg_dense_inverse(&mg->level[L - 1].grid, mg->dense_work, mg->Ainv, s))) return rc;
     if (!lanczos) return DFEA_OK;
-    // Lanczos on every smoothed level, all levels in lockstep (p in x, z in d)
-    for (int l = 0; l < L - 1; ++l) {
+    // Lanczos on every smoothed level (p in x, z in d): the small levels in one block, the others in lockstep
+    const int t = tail_start(mg) < L - 1 ? tail_start(mg) : L - 1;
+    if (t < L - 1) {
+        MgLanczosTail T = {};
+        T.n_levels = L - 1 - t;
+        T.steps = mg->lanczos_steps;
+        for (int k = 0; k < T.n_levels; ++k) {
+            const dfea_mg_level& lv = mg->level[t + k];
+            T.lv[k] = MgLanczosLevel{mg_grid(lv.grid), (int)lv.n, lv.diag, lv.r, lv.d, lv.x, lv.q, mg->lscal + 4 * (t + k),
+                                     mg->lhist + (int64_t)2 * mg->lanczos_steps * (t + k)};
+        }
+        k_mg_tail_lanczos<<<1, kMgTailLanczosThreads, 0, s>>>(T);
+        note_launches(1);
+        if ((rc = launch_check("dfea_mg_setup: Lanczos of the small levels"))) return rc;
+    }
+    for (int l = 0; l < t; ++l) {
         const dfea_mg_level& lv = mg->level[l];
         k_mg_start<<<grid_for(lv.n, kThreads, 8), kThreads, 0, s>>>(lv.n, lv.r);
         k_mg_div<<<grid_for(lv.n, kThreads, 8), kThreads, 0, s>>>(lv.n, lv.r, lv.diag, lv.d);
@@ -1156,7 +1294,7 @@ static int setup_device_part(const dfea_mesh_view* mesh, const dfea_mg* mg, cons
             return rc;
     }
     for (int k = 0; k < mg->lanczos_steps; ++k)
-        for (int l = 0; l < L - 1; ++l) {
+        for (int l = 0; l < t; ++l) {
             const dfea_mg_level& lv = mg->level[l];
             if ((rc = mg_apply(mesh, mg, moduli, moduli_dtype, l, lv.x, lv.q, s)) ||
                 (rc = dfea_mg_lanczos_step(lv.n, lv.x, lv.q, lv.r, lv.d, lv.diag, mg->lscal + 4 * l,
