@@ -497,6 +497,25 @@ __global__ void __launch_bounds__(kMgDotThreads) k_mg_dot_part(int64_t n, const 
     if (threadIdx.x == 0) part[blockIdx.x] = a;
 }
 
+// x += alpha p, r += neg q (neg = -alpha) and the per-block partial sums of r.r in the grid and accumulation
+// order of k_mg_dot_part: the PCG update of dfea_mg_pcg's host-driven loop (two axpys and the first pass of
+// its r.r) in one launch, with the same expressions, so the iterates and the norm are bitwise the same
+__global__ void __launch_bounds__(kMgDotThreads) k_mg_update_rr(int64_t n, double alpha, double neg,
+                                                                 const double* __restrict__ p, const double* __restrict__ q,
+                                                                 double* __restrict__ x, double* __restrict__ r,
+                                                                 double* __restrict__ part) {
+    double a = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        double ri = r[i];
+        ri += neg * q[i];
+        r[i] = ri;
+        a += ri * ri;
+    }
+    a = block_sum<kMgDotThreads>(a);
+    if (threadIdx.x == 0) part[blockIdx.x] = a;
+}
+
 // LANCZOS: the sum is r.z of a CG step: alpha = s[1] / s[0], beta = sum / s[1] into hist, s[1] = sum, s[3] = beta
 template <bool LANCZOS>
 __global__ void __launch_bounds__(kMgDotThreads) k_mg_dot_final(int nb, const double* __restrict__ part,
@@ -1659,7 +1678,11 @@ extern "C" int dfea_mg_pcg(const dfea_mesh_view* mesh, const dfea_mg* mg, const 
             return rc;
         }
         const double alpha = rz / curv;
-        if ((rc = dfea_axpy(n, alpha, p, x, s)) || (rc = dfea_axpy(n, -alpha, q, r, s)) || (rc = dot(r, r, h))) return rc;
+        const int nb = mg_dot_blocks(n);
+        k_mg_update_rr<<<nb, kMgDotThreads, 0, s>>>(n, alpha, -alpha, p, q, x, r, mg->dot_work);
+        k_mg_dot_final<false><<<1, kMgDotThreads, 0, s>>>(nb, mg->dot_work, mg->scal, nullptr, 0);
+        note_launches(2);
+        if ((rc = launch_check("dfea_mg_pcg: update")) || (rc = read_scalars(h, mg->scal, 1, s))) return rc;
         if (h[0] <= tol2) {
             *iterations = k + 1;
             *status = DFEA_PCG_CONVERGED;
