@@ -281,7 +281,7 @@ def solve_request(req, device, precision="fp32", n_load_steps=1, tol_rel=1e-10, 
     """
     Build (or copy from ``host_params``) and solve one request on the current stream; returns
     (u on device, info).  ``pcg_graph`` is the PCG launch form (2: unrolled graph, the default for
-    concurrent slots; 1: conditional-loop graph; 0: direct launches); ``pcg_form`` the product form inside
+    a request solved alone; 1: conditional-loop graph; 0: direct launches, the serving engine's default); ``pcg_form`` the product form inside
     it ("auto", "colour" or "gather", see DevicePCG and workspace.pcg_form_for); ``fp32_moduli`` the FP32
     operator's moduli ("ref": reference frame, no gradients read; "physical"); ``max_blocks`` the most blocks
     per PCG launch (0: the whole GPU); ``preconditioner`` "jacobi", "block_jacobi", "multigrid" or "auto"
@@ -338,7 +338,7 @@ class ServingEngine:
     """
 
     def __init__(self, n_slots=16, hbm_budget=None, precision="fp32", device=None, n_load_steps=1, tol_rel=1e-10,
-                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=2, pcg_form="gather",
+                 pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=0, pcg_form="gather",
                  fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False,
                  driver="native", max_newton=25, max_cutbacks=8, pool_bytes=0, mg_graphs=False, mg_bounds_every=3,
                  mg_gather=False):
@@ -360,6 +360,10 @@ class ServingEngine:
         # mg_bounds_every=3: the smoother bounds are estimated at a request's first set-up and every third one
         # after it (measured: 101-113 vs 70-75 solves/s with estimates at every set-up, the same Newton and
         # PCG iteration counts to 0.05 %).  mg_gather: off (no gain measured on the stream).
+        # pcg_graph=0: the Jacobi PCG launches its kernels directly (status read every 16 iterations).  Capturing
+        # and instantiating a graph per request made the 32-slot engine stall from run to run (80 small requests:
+        # 42-181 solves/s with unrolled graphs, 168-178 with direct launches, 132-139 with the conditional loop);
+        # a request served alone keeps solve_request's unrolled graph.
         if pool_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             pool_bytes = int(0.2 * free)
