@@ -35,13 +35,21 @@ def dofs_from_node_mask(node_mask, components=(0, 1)):
     return out.reshape(-1)
 
 
-def boundary_edges(conn, edge_local_nodes):
-    """Edges used by exactly one element, as (E, k) global node ids [start, end(, mid)], element order."""
+def boundary_edges(conn, edge_local_nodes, node_mask=None, n_nodes=None):
+    """
+    Edges used by exactly one element, as (E, k) global node ids [start, end(, mid)], element order.
+    ``node_mask`` (N,) keeps only the edges whose nodes all lie in it; the two copies of an inner edge have
+    the same nodes, so they pass or fail the mask together and counting among the kept edges gives the same
+    boundary edges as counting among all.  ``n_nodes`` (more than the largest node id) spares reading that
+    id back from the device.
+    """
     k = len(edge_local_nodes[0])
     all_edges = conn[:, torch.tensor(edge_local_nodes, device=conn.device)].reshape(-1, k)
+    if node_mask is not None:
+        all_edges = all_edges[node_mask[all_edges].all(dim=1)]
     lo = torch.minimum(all_edges[:, 0], all_edges[:, 1])
     hi = torch.maximum(all_edges[:, 0], all_edges[:, 1])
-    key = lo * (int(conn.max()) + 1) + hi
+    key = lo * (int(n_nodes) if n_nodes is not None else int(conn.max()) + 1) + hi
     _, inverse, counts = torch.unique(key, return_inverse=True, return_counts=True)
     return all_edges[counts[inverse] == 1]
 

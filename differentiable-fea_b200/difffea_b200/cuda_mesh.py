@@ -18,7 +18,7 @@ import numpy as np
 import torch
 
 from difffea_b200 import _lib
-from difffea_b200.elements import element_quadrature, shape_gradients
+from difffea_b200.elements import default_rule, element_quadrature, quadrature_gradients
 
 _SUPPORTED = {(4, 4): "quad4", (9, 9): "quad9", (3, 1): "tri3", (6, 6): "tri6", (8, 9): "quad8"}
 
@@ -85,7 +85,8 @@ class CudaMesh:
         S = self.stride
 
         dev = self.device
-        self.perm = torch.from_numpy(order.astype(np.int64)).to(dev)
+        self.perm_host = order.astype(np.int64)          # packed slot -> element, on the host
+        self.perm = torch.from_numpy(self.perm_host).to(dev)
         self.conn = torch.empty(nen * S, dtype=torch.int32, device=dev)
         self.orig = torch.empty(S, dtype=torch.int32, device=dev)
         self.grad = torch.empty(n_q * nen * S * 2, dtype=torch.float64, device=dev)
@@ -118,10 +119,12 @@ class CudaMesh:
         # reference shape gradients at the Gauss points (host values in the view) and, built on demand,
         # the inverse element Jacobians of the reference-frame FP32 operator
         GP = params.get("GP")
-        if GP is None:
-            GP, _ = element_quadrature(self.element_type)
-        GP = GP.detach().to("cpu", torch.float64)
-        self.ref_grad = shape_gradients(self.element_type, GP[:, 0], GP[:, 1]).to(torch.float64)  # (n_q, nen, 2)
+        self._default_rule = GP is None or (GP.dtype == torch.float64 and default_rule(self.element_type, GP))
+        if self._default_rule:
+            GP = element_quadrature(self.element_type)[0]          # the same points, on the host (shared)
+        else:
+            GP = GP.detach().to("cpu", torch.float64)
+        self.ref_grad = quadrature_gradients(self.element_type, GP).to(torch.float64)  # (n_q, nen, 2), host
         flat = self.ref_grad.reshape(-1).tolist()
         for i, x in enumerate(flat):
             v.ref_grad[i] = x
@@ -179,7 +182,8 @@ class CudaMesh:
             dev, S, nq, nen, n = self.device, self.stride, self.n_q, self.nen, self.n_el
             conn = self.conn.view(nen, S)[:, :n] >> 2                                     # packed order
             X = self._nodes.detach().to(dev, torch.float64)[conn.to(torch.int64).t()]     # (n, nen, 2)
-            dNr = self.ref_grad.to(dev)                                                   # (nq, nen, 2)
+            dNr = (quadrature_gradients(self.element_type, element_quadrature(self.element_type, torch.float64, dev)[0])
+                   if self._default_rule else self.ref_grad.to(dev))                   # (nq, nen, 2)
             J = torch.einsum("eai,qaj->eqij", X, dNr)                                     # dX_i / dxi_j
             det = J[..., 0, 0] * J[..., 1, 1] - J[..., 0, 1] * J[..., 1, 0]
             Jinv = torch.stack([torch.stack([J[..., 1, 1], -J[..., 0, 1]], -1),

@@ -49,10 +49,33 @@ _TRI6_A = (0.445948490915965, 0.091576213509771)
 _TRI6_W = (0.223381589678011, 0.109951743655322)
 
 
+# Quadrature rules depend on (rule, dtype, device) only: each is built once and shared, so a serving thread
+# does not rebuild them (and copy them to the device) for every request.  The returned tensors are shared:
+# callers must not modify them.  A CUDA rule is cached after its blocking host-to-device copy has completed,
+# so threads on other streams may read it at once.
+_QUADRATURE = {}
+
+
+def _device_key(device):
+    d = torch.device(device)
+    if d.type == "cuda" and d.index is None:
+        d = torch.device("cuda", torch.cuda.current_device())
+    return str(d)
+
+
+def _cached_rule(key, build):
+    rule = _QUADRATURE.get(key)
+    if rule is None:
+        rule = _QUADRATURE.setdefault(key, build())
+    return rule
+
+
 def gauss_1d(n, dtype=torch.float64, device="cpu"):
-    """n-point Gauss-Legendre rule on [-1, 1] (points, weights)."""
-    x, w = np.polynomial.legendre.leggauss(n)
-    return torch.tensor(x, dtype=dtype, device=device), torch.tensor(w, dtype=dtype, device=device)
+    """n-point Gauss-Legendre rule on [-1, 1] (points, weights); cached and shared (do not modify)."""
+    def build():
+        x, w = np.polynomial.legendre.leggauss(n)
+        return torch.tensor(x, dtype=dtype, device=device), torch.tensor(w, dtype=dtype, device=device)
+    return _cached_rule(("gauss_1d", n, dtype, _device_key(device)), build)
 
 
 def gauss_square(n, dtype=torch.float64, device="cpu"):
@@ -78,10 +101,39 @@ def gauss_triangle(degree, dtype=torch.float64, device="cpu"):
     return torch.tensor(pts, dtype=dtype, device=device), torch.tensor(wts, dtype=dtype, device=device)
 
 
+def default_rule(name, points):
+    """True when ``points`` is the (shared) point tensor of this library's default rule of element ``name``."""
+    rule = _QUADRATURE.get(("element", name, points.dtype, _device_key(points.device)))
+    return rule is not None and rule[0] is points
+
+
+_RULE_GRADIENTS = {}
+
+
+def quadrature_gradients(name, points):
+    """
+    shape_gradients of element ``name`` at the points (n_q, 2).  For the default rule's shared point tensor
+    the result is computed once and shared as well (do not modify); a CUDA result is cached after its
+    stream has finished computing it, so threads on other streams may read it at once.
+    """
+    key = (name, id(points))
+    hit = _RULE_GRADIENTS.get(key)
+    if hit is not None and hit[0] is points:
+        return hit[1]
+    g = shape_gradients(name, points[:, 0], points[:, 1])
+    if default_rule(name, points):
+        if g.is_cuda:
+            torch.cuda.current_stream(g.device).synchronize()
+        _RULE_GRADIENTS[key] = (points, g)
+    return g
+
+
 def element_quadrature(name, dtype=torch.float64, device="cpu"):
-    """Default Gauss rule (points (n_q, 2), weights (n_q,)) of an element type."""
+    """Default Gauss rule (points (n_q, 2), weights (n_q,)) of an element type; cached and shared (do not
+    modify)."""
     kind, n = get_element(name)["gauss"]
-    return gauss_square(n, dtype, device) if kind == "tensor" else gauss_triangle(n, dtype, device)
+    return _cached_rule(("element", name, dtype, _device_key(device)),
+                        lambda: gauss_square(n, dtype, device) if kind == "tensor" else gauss_triangle(n, dtype, device))
 
 
 # ---------------------------------------------------------------------------------------------

@@ -26,6 +26,7 @@ dfea_mg_pcg); this module builds the grid description and owns the buffers.
 import ctypes
 import math
 
+import numpy as np
 import torch
 
 from difffea_b200 import _lib, ops
@@ -46,21 +47,21 @@ _LAYOUT = {4: (1, 1), 9: (2, 1), 8: (2, 1), 3: (1, 2), 6: (2, 2)}
 
 def _grid_conn(ids, ncx, ncy, nen):
     """
-    Connectivity of an ncx x ncy cell grid over the grid node ids, in the element library's local order:
-    Q4 / Q9 / Q8 one element per cell, Tri3 / Tri6 the lower-left triangles of all cells, then the
-    upper-right ones.
+    Connectivity of an ncx x ncy cell grid over the grid node ids (a numpy array), in the element library's
+    local order: Q4 / Q9 / Q8 one element per cell, Tri3 / Tri6 the lower-left triangles of all cells, then
+    the upper-right ones.
     """
     if nen in (4, 3):
         c = [ids[:ncx, :ncy], ids[1:ncx + 1, :ncy], ids[1:ncx + 1, 1:ncy + 1], ids[:ncx, 1:ncy + 1]]
-        q4 = torch.stack([t.reshape(-1) for t in c], dim=1)
-        return q4 if nen == 4 else torch.cat([q4[:, [0, 1, 3]], q4[:, [1, 2, 3]]], dim=0)
+        q4 = np.stack([t.reshape(-1) for t in c], axis=1)
+        return q4 if nen == 4 else np.concatenate([q4[:, [0, 1, 3]], q4[:, [1, 2, 3]]], axis=0)
     offs = [(0, 0), (2, 0), (2, 2), (0, 2), (1, 0), (2, 1), (1, 2), (0, 1), (1, 1)]
-    q9 = torch.stack([ids[di:di + 2 * ncx:2, dj:dj + 2 * ncy:2].reshape(-1) for di, dj in offs], dim=1)
+    q9 = np.stack([ids[di:di + 2 * ncx:2, dj:dj + 2 * ncy:2].reshape(-1) for di, dj in offs], axis=1)
     if nen == 9:
         return q9
     if nen == 8:
         return q9[:, :8]
-    return torch.cat([q9[:, [0, 1, 3, 4, 8, 7]], q9[:, [1, 2, 3, 5, 6, 8]]], dim=0)
+    return np.concatenate([q9[:, [0, 1, 3, 4, 8, 7]], q9[:, [1, 2, 3, 5, 6, 8]]], axis=0)
 
 
 def _candidates(n_cells, n_nodes, span, q8):
@@ -88,9 +89,10 @@ def structured_grid(conn, n_nodes):
     The logical grid of a structured mesh (any element type of the library), or None: the element count
     and the node count fix at most two cell counts ncx x ncy; each is tried with the node numbering of the
     rectangle mesher (grid node (i, j) = i (gy + 1) + j, Q8 without the cell centres) and, for Q4 / Q9, of
-    the quarter-plate mesher (i + j (gx + 1)), and accepted if the connectivity matches exactly.
+    the quarter-plate mesher (i + j (gx + 1)), and accepted if the connectivity matches exactly.  The
+    candidate connectivity is built on the host and compared with ``conn`` where it lies (one comparison).
     Returns dict(span, epc (elements per cell), ncx, ncy, gx, gy, gnode (grid node -> FE node, -1 for a
-    Q8 cell centre), node_ij (FE node -> grid position)).
+    Q8 cell centre), node_ij (FE node -> grid position)), the tensors on ``conn``'s device.
     """
     n_el, nen = conn.shape
     if nen not in _LAYOUT or n_el == 0:
@@ -102,27 +104,25 @@ def structured_grid(conn, n_nodes):
     dev = conn.device
     for ncx, ncy in _candidates(n_cells, n_nodes, span, nen == 8):
         gx, gy = span * ncx, span * ncy
-        n_grid = (gx + 1) * (gy + 1)
-        lex = torch.arange(n_grid, device=dev)
+        lex = np.arange((gx + 1) * (gy + 1), dtype=np.int64)
         numberings = [lex.reshape(gx + 1, gy + 1)]
         if nen in (4, 9):
-            numberings.append(lex.reshape(gy + 1, gx + 1).t())
+            numberings.append(lex.reshape(gy + 1, gx + 1).T)
         for ids in numberings:
             if nen == 8:                     # drop the cell centres, renumber the other grid nodes in order
-                keep = torch.ones(gx + 1, gy + 1, dtype=torch.bool, device=dev)
+                keep = np.ones((gx + 1, gy + 1), dtype=bool)
                 keep[1:gx:2, 1:gy:2] = False
-                ids = torch.where(keep, torch.cumsum(keep.reshape(-1), 0).reshape(gx + 1, gy + 1) - 1,
-                                  torch.full_like(ids, -1))
-            if torch.equal(_grid_conn(ids, ncx, ncy, nen), conn):
-                gnode = ids.reshape(-1).to(torch.int32).contiguous()
-                node_ij = torch.empty(n_nodes, 2, dtype=torch.int32, device=dev)
-                ii = torch.arange(gx + 1, device=dev)[:, None].expand(gx + 1, gy + 1).reshape(-1)
-                jj = torch.arange(gy + 1, device=dev)[None, :].expand(gx + 1, gy + 1).reshape(-1)
-                present = gnode >= 0
-                node_ij[gnode[present].long(), 0] = ii[present].to(torch.int32)
-                node_ij[gnode[present].long(), 1] = jj[present].to(torch.int32)
-                return dict(span=span, epc=epc, ncx=ncx, ncy=ncy, gx=gx, gy=gy, gnode=gnode,
-                            node_ij=node_ij.contiguous())
+                ids = np.where(keep, np.cumsum(keep.reshape(-1)).reshape(gx + 1, gy + 1) - 1, -1)
+            expect = _grid_conn(ids, ncx, ncy, nen)
+            if expect.shape != tuple(conn.shape) or not torch.equal(torch.from_numpy(expect).to(dev), conn):
+                continue
+            gnode = ids.reshape(-1).astype(np.int32)
+            node_ij = np.empty((n_nodes, 2), dtype=np.int32)
+            present = gnode >= 0
+            node_ij[gnode[present], 0] = np.repeat(np.arange(gx + 1, dtype=np.int32), gy + 1)[present]
+            node_ij[gnode[present], 1] = np.tile(np.arange(gy + 1, dtype=np.int32), gx + 1)[present]
+            return dict(span=span, epc=epc, ncx=ncx, ncy=ncy, gx=gx, gy=gy, gnode=torch.from_numpy(gnode).to(dev),
+                        node_ij=torch.from_numpy(node_ij).to(dev))
     return None
 
 
@@ -130,37 +130,32 @@ def structured_grid(conn, n_nodes):
 # hierarchy
 # ---------------------------------------------------------------------------------------------
 class _Level:
-    def __init__(self, gx, gy, finer=None, device="cuda", n=None):
+    """One level's grid (its buffers live in the hierarchy's arenas; ``grid`` holds their addresses)."""
+
+    def __init__(self, gx, gy, n=None):
         self.gx, self.gy = gx, gy
         self.n_nodes = (gx + 1) * (gy + 1)
         self.n = 2 * self.n_nodes if n is None else n       # level 0: the mesh's DOFs
-        i32 = dict(dtype=torch.int32, device=device)
-        self.keep = []
         self.grid = _lib.MgGrid()
         self.grid.gx, self.grid.gy = gx, gy
-        if finer is not None:
-            fgx, fgy = finer.gx, finer.gy
-            # line I of this level lies on line min(2 I, fgx) of the finer one; finer line i lies in cell
-            # min(i // 2, gx - 1) of this level (computed on the device: no host-to-device copies)
-            lx = torch.clamp(2 * torch.arange(gx + 1, **i32), max=fgx)
-            ly = torch.clamp(2 * torch.arange(gy + 1, **i32), max=fgy)
-            cx = torch.clamp(torch.arange(fgx + 1, **i32) // 2, max=gx - 1)
-            cy = torch.clamp(torch.arange(fgy + 1, **i32) // 2, max=gy - 1)
-            self.K = torch.empty(64 * gx * gy, dtype=torch.float64, device=device)
-            self.fix = torch.empty(self.n_nodes, dtype=torch.uint8, device=device)
-            self.keep += [lx, ly, cx, cy]
-            for name, t in (("line_x", lx), ("line_y", ly), ("cell_x", cx), ("cell_y", cy), ("K", self.K),
-                            ("fix", self.fix)):
-                setattr(self.grid, name, t.data_ptr())
-        f64 = dict(dtype=torch.float64, device=device)
-        self.diag = torch.empty(self.n, **f64)
-        self.b, self.x, self.r = (torch.empty(self.n, **f64) for _ in range(3))
-        self.d, self.q = torch.empty(self.n, **f64), torch.empty(self.n, **f64)
         self.lam = 1.0
 
     @property
     def ref(self):
         return ctypes.byref(self.grid)
+
+
+class _Arena:
+    """Offsets of the pieces of one device buffer, each aligned to 256 bytes."""
+
+    def __init__(self, itemsize):
+        self.itemsize, self.size, self.at = itemsize, 0, {}
+
+    def add(self, key, count):
+        align = 256 // self.itemsize
+        self.at[key] = (self.size, count)
+        self.size += (count + align - 1) // align * align
+        return self.at[key][0]
 
 
 def _coarser(g):
@@ -191,49 +186,89 @@ class Multigrid:
         self.mesh, self.g = mesh, g
         self.degree, self.ratio, self.lanczos_steps = degree, ratio, lanczos_steps
         dev = mesh.device
-        inv_perm = torch.empty_like(mesh.perm)
-        inv_perm[mesh.perm] = torch.arange(mesh.perm.numel(), device=dev)
-        # the elements of cell c are c + k n_cells (k < epc: one quadrilateral, or the lower then the upper
-        # triangle), numbered like the mesher's
-        n_cells = g["ncx"] * g["ncy"]
-        elems = torch.arange(n_cells, device=dev)[:, None] + n_cells * torch.arange(g["epc"], device=dev)[None, :]
-        self.cell_slot = inv_perm[elems.reshape(-1)].to(torch.int32).contiguous()
-        self.levels = [_Level(g["gx"], g["gy"], None, dev, n=mesh.n_dof)]
+        self.levels = [_Level(g["gx"], g["gy"], n=mesh.n_dof)]
         while True:
             f = self.levels[-1]
             if len(self.levels) > 1 and (f.n_nodes <= COARSEST_NODES or (f.gx == 1 and f.gy == 1)):
                 break
-            self.levels.append(_Level(_coarser(f.gx), _coarser(f.gy), f, dev))
+            self.levels.append(_Level(_coarser(f.gx), _coarser(f.gy)))
         if len(self.levels) > _lib.MG_MAX_LEVELS:
             raise ValueError("multigrid: too many levels")
         last = self.levels[-1]
         if last.n > int(_lib.load().dfea_mg_dense_max()):
             raise ValueError("multigrid: the coarsest level is too large for the dense solve")
-        f64 = dict(dtype=torch.float64, device=dev)
         L = len(self.levels)
-        self.Ainv = torch.empty(last.n * last.n, **f64)
-        self.dense_work = torch.empty_like(self.Ainv)
-        self.coef = torch.zeros(L, 2 * _lib.MG_MAX_DEGREE, **f64)
-        self.lscal = torch.zeros(L, 4, **f64)
-        self.lhist = torch.zeros(L, 2 * lanczos_steps, **f64)
-        self.dot_work = torch.zeros(int(_lib.load().dfea_mg_dot_work()), **f64)
-        self.pcg_work = torch.empty(4, self.levels[0].n, **f64)
-        self.scal = torch.zeros(4, **f64)
-        # graph-driven mode: set-ups replay a captured graph, the PCG iterates in a device-side loop
-        self.pcg_state = torch.zeros(16, **f64) if graphs else None
+        # Integer maps, built on the host and copied in one transfer: the element slot of every cell's elements
+        # (cell c holds elements c + k n_cells, k < epc: one quadrilateral, or the lower then the upper
+        # triangle, numbered like the mesher's) and per coarse level its line and cell maps -- line I of a
+        # level lies on line min(2 I, fgx) of the finer one, finer line i lies in cell min(i // 2, gx - 1).
+        n_cells = g["ncx"] * g["ncy"]
+        inv_perm = np.empty_like(mesh.perm_host)
+        inv_perm[mesh.perm_host] = np.arange(mesh.perm_host.size)
+        elems = np.arange(n_cells)[:, None] + n_cells * np.arange(g["epc"])[None, :]
+        pieces = {"cell_slot": inv_perm[elems.reshape(-1)]}
+        for l in range(1, L):
+            f, lv = self.levels[l - 1], self.levels[l]
+            pieces[(l, "line_x")] = np.minimum(2 * np.arange(lv.gx + 1), f.gx)
+            pieces[(l, "line_y")] = np.minimum(2 * np.arange(lv.gy + 1), f.gy)
+            pieces[(l, "cell_x")] = np.minimum(np.arange(f.gx + 1) // 2, lv.gx - 1)
+            pieces[(l, "cell_y")] = np.minimum(np.arange(f.gy + 1) // 2, lv.gy - 1)
+        ia = _Arena(4)
+        for k, v in pieces.items():
+            ia.add(k, v.size)
+        host = np.zeros(ia.size, dtype=np.int32)
+        for k, v in pieces.items():
+            o, c = ia.at[k]
+            host[o:o + c] = v
+        self._ints = torch.from_numpy(host).to(dev)
+        # Float64 buffers in one allocation, the zero-initialised ones first: coefficients, Lanczos scalars and
+        # history, dot partials, PCG scalars and the graph-driven loop's state; then the coarsest inverse and
+        # its work, the PCG vectors and every level's vectors and element matrices.
+        fa = _Arena(8)
+        fa.add("coef", L * 2 * _lib.MG_MAX_DEGREE)
+        fa.add("lscal", L * 4)
+        fa.add("lhist", L * 2 * lanczos_steps)
+        fa.add("dot_work", int(_lib.load().dfea_mg_dot_work()))
+        fa.add("scal", 4)
+        if graphs:
+            fa.add("pcg_state", 16)
+        zero_end = fa.size
+        fa.add("Ainv", last.n * last.n)
+        fa.add("dense_work", last.n * last.n)
+        fa.add("pcg", 4 * self.levels[0].n)
+        for l, lv in enumerate(self.levels):
+            for name in ("diag", "b", "x", "r", "d", "q"):
+                fa.add((l, name), lv.n)
+            if l > 0:
+                fa.add((l, "K"), 64 * lv.gx * lv.gy)
+        self._f64 = torch.empty(fa.size, dtype=torch.float64, device=dev)
+        self._f64[:zero_end].zero_()
+        ba = _Arena(1)
+        for l in range(1, L):
+            ba.add(l, self.levels[l].n_nodes)
+        self._fix = torch.empty(max(ba.size, 1), dtype=torch.uint8, device=dev)
+        self._fa = fa
+        ib, fb, bb = self._ints.data_ptr(), self._f64.data_ptr(), self._fix.data_ptr()
+        iptr = lambda k: ib + 4 * ia.at[k][0]
+        fptr = lambda k: fb + 8 * fa.at[k][0]
         h = self.h = _lib.Mg()
         h.n_levels, h.degree, h.lanczos_steps, h.span, h.ratio = L, degree, lanczos_steps, g["span"], float(ratio)
-        h.node_ij, h.gnode, h.cell_slot = g["node_ij"].data_ptr(), g["gnode"].data_ptr(), self.cell_slot.data_ptr()
+        h.node_ij, h.gnode, h.cell_slot = g["node_ij"].data_ptr(), g["gnode"].data_ptr(), iptr("cell_slot")
         for l, lv in enumerate(self.levels):
+            if l > 0:
+                for name in ("line_x", "line_y", "cell_x", "cell_y"):
+                    setattr(lv.grid, name, iptr((l, name)))
+                lv.grid.K = fptr((l, "K"))
+                lv.grid.fix = bb + ba.at[l][0]
             dst = h.level[l]
             dst.grid = lv.grid
             dst.n = lv.n
             for name in ("diag", "b", "x", "r", "d", "q"):
-                setattr(dst, name, getattr(lv, name).data_ptr())
+                setattr(dst, name, fptr((l, name)))
         for name in ("Ainv", "dense_work", "coef", "lscal", "lhist", "dot_work", "scal"):
-            setattr(h, name, getattr(self, name).data_ptr())
-        h.pcg = self.pcg_work.data_ptr()
-        h.pcg_state = self.pcg_state.data_ptr() if graphs else None
+            setattr(h, name, fptr(name))
+        h.pcg = fptr("pcg")
+        h.pcg_state = fptr("pcg_state") if graphs else None
         h.graphs = None
         h.bounds_every, h.setups = int(bounds_every), 0
         self.fe_work = None
@@ -249,6 +284,17 @@ class Multigrid:
     @property
     def ref(self):
         return ctypes.byref(self.h)
+
+    def buffer(self, name):
+        """A view of one of the hierarchy's float64 buffers ("coef", "lscal", "lhist", "Ainv", "pcg", or a level's
+        (l, "diag" | "b" | "x" | "r" | "d" | "q" | "K")), for inspection."""
+        o, c = self._fa.at[name]
+        return self._f64.narrow(0, o, c)
+
+    @property
+    def lhist(self):
+        """Lanczos coefficients (alpha_k, beta_k) per level, (levels, 2 * lanczos_steps)."""
+        return self.buffer("lhist").view(len(self.levels), 2 * self.lanczos_steps)
 
     def setup(self, C, moduli_code, diag):
         """Coarse operators from the fine moduli C (DFEA_F64 / DFEA_F32 / DFEA_F32REF) and the Jacobi diagonal

@@ -13,7 +13,7 @@ import torch
 
 from difffea_b200.boundary_conditions import (boundary_edges, dofs_from_node_mask, edge_traction_load,
                                               select_boundary_nodes)
-from difffea_b200.elements import element_quadrature, get_element, make_shape_fn, shape_gradients
+from difffea_b200.elements import element_quadrature, get_element, make_shape_fn, quadrature_gradients
 from difffea_b200.materials import lame_parameters, material_vector
 from difffea_b200.mesh import create_quarter_plate_mesh, create_rectangle_mesh
 
@@ -48,7 +48,7 @@ def precompute_geometry(params):
     name = params.get("element_type") or getattr(params.get("shape_fn"), "element_type", None)
     if name is None:
         raise ValueError("precompute_geometry needs params['element_type']")
-    dNr = shape_gradients(name, GP[:, 0], GP[:, 1]).to(nodes.dtype)            # (n_q, nen, 2)
+    dNr = quadrature_gradients(name, GP).to(nodes.dtype)                        # (n_q, nen, 2)
     Xe = nodes[conn]                                                            # (n_el, nen, 2)
     J = torch.einsum("eai,qaj->eqij", Xe, dNr)                                  # dX_i / dxi_j
     det = J[..., 0, 0] * J[..., 1, 1] - J[..., 0, 1] * J[..., 1, 0]
@@ -79,7 +79,7 @@ def _assemble(nodes, conn, element_type, spec, dtype):
             fixed = fixed | mask
             u_D = torch.where(mask, torch.as_tensor(float(val), dtype=dtype, device=dev), u_D)
     else:
-        edges = boundary_edges(conn, el["edges"])
+        edges = boundary_edges(conn, el["edges"], node_mask=load_nodes, n_nodes=N)
         f = edge_traction_load(nodes, edges, el["order"], load_nodes, (float(value[0]), float(value[1])))
     m = torch.where(fixed, 0.0, 1.0).to(dtype)
     material = spec.get("material", "neo_hookean")
