@@ -546,6 +546,72 @@ __global__ void k_zero_tickets(unsigned* t, int n, double* results, int nr) {
     if (i < nr) results[i] = 0.0;
 }
 
+// Inverse element Jacobians of the reference-frame FP32 operator, packed [q][row][stride] as (col 0, col 1)
+// pairs (zeros in the padding slots), from the packed connectivity and the node coordinates:
+// J_ij = sum_a X_a,i dN_a/dxi_j, Jinv = J^-1.  check[0] and check[1] receive the largest |Jinv^T dN/dxi -
+// dN/dX| and |dN/dX| over every element, Gauss point and node (maxima of non-negative values, combined by
+// atomic maxima of their bit patterns: order-independent; a NaN wins, as in a propagating maximum).
+__device__ __forceinline__ void nan_max(double& m, double v) {
+    if (v > m || v != v) m = (m != m) ? m : v;
+}
+
+template <int NEN, int NQ>
+__global__ void __launch_bounds__(128) k_ref_frame(Mesh m, RefGrad<NEN, NQ> rg, const double* __restrict__ nodes,
+                                                   double* __restrict__ jinv, double* __restrict__ check) {
+    const int64_t S = m.stride;
+    double2* out = reinterpret_cast<double2*>(jinv);
+    const double2* g2 = reinterpret_cast<const double2*>(m.grad);
+    double dmax = 0.0, smax = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < S; e += (int64_t)gridDim.x * blockDim.x) {
+        if (e >= m.n_el) {
+#pragma unroll
+            for (int k = 0; k < 2 * NQ; ++k) out[k * S + e] = make_double2(0.0, 0.0);
+            continue;
+        }
+        double X[NEN][2];
+#pragma unroll
+        for (int a = 0; a < NEN; ++a) {
+            const int64_t node = m.conn[a * S + e] >> 2;
+            X[a][0] = nodes[2 * node];
+            X[a][1] = nodes[2 * node + 1];
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                J00 += X[a][0] * rg.g[q][a][0];
+                J01 += X[a][0] * rg.g[q][a][1];
+                J10 += X[a][1] * rg.g[q][a][0];
+                J11 += X[a][1] * rg.g[q][a][1];
+            }
+            const double det = J00 * J11 - J01 * J10;
+            const double i00 = J11 / det, i01 = -J01 / det, i10 = -J10 / det, i11 = J00 / det;
+            out[(2 * q) * S + e] = make_double2(i00, i01);
+            out[(2 * q + 1) * S + e] = make_double2(i10, i11);
+#pragma unroll
+            for (int a = 0; a < NEN; ++a) {
+                const double r0 = rg.g[q][a][0] * i00 + rg.g[q][a][1] * i10;
+                const double r1 = rg.g[q][a][0] * i01 + rg.g[q][a][1] * i11;
+                const double2 g = g2[(q * NEN + a) * S + e];
+                nan_max(dmax, fabs(r0 - g.x));
+                nan_max(dmax, fabs(r1 - g.y));
+                nan_max(smax, fabs(g.x));
+                nan_max(smax, fabs(g.y));
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nan_max(dmax, __shfl_down_sync(0xffffffffu, dmax, o));
+        nan_max(smax, __shfl_down_sync(0xffffffffu, smax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(reinterpret_cast<unsigned long long*>(check), (unsigned long long)__double_as_longlong(dmax));
+        atomicMax(reinterpret_cast<unsigned long long*>(check + 1), (unsigned long long)__double_as_longlong(smax));
+    }
+}
+
 // Node pass of the gather-form product q = A v on the finite-element level of the multigrid V-cycle, with
 // the smoothing arithmetic that follows the product applied at the node (each node's q is complete here and
 // the element pass has finished reading v):
@@ -618,6 +684,26 @@ extern "C" int dfea_mesh_pack(int64_t n_el, int64_t stride, int32_t nen, int32_t
     k_node_fix<<<grid_for(n_nodes, kThreads, 8), kThreads, 0, s>>>(n_nodes, m, node_fix_out);
     note_launches(1);
     return launch_check("dfea_mesh_pack");
+}
+
+extern "C" int dfea_mesh_ref_frame(const dfea_mesh_view* mesh, const double* nodes, double* jinv_out, double* check,
+                                   void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!nodes || !jinv_out || !check) return set_error(DFEA_ERR_INVALID, "dfea_mesh_ref_frame: NULL pointer");
+    if (!aligned16(jinv_out)) return set_error(DFEA_ERR_INVALID, "dfea_mesh_ref_frame: jinv_out must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if ((rc = check_cuda(cudaMemsetAsync(check, 0, 2 * sizeof(double), s), "cudaMemsetAsync"))) return rc;
+    const Mesh m = kernel_mesh(*mesh);
+    rc = dispatch_element(mesh->nen, mesh->n_q, [&](auto nen_c, auto nq_c) -> int {
+        constexpr int NEN = decltype(nen_c)::value, NQ = decltype(nq_c)::value;
+        k_ref_frame<NEN, NQ><<<grid_for(mesh->stride, 128, 8), 128, 0, s>>>(m, ref_grad_of<NEN, NQ>(*mesh), nodes, jinv_out,
+                                                                             check);
+        return DFEA_OK;
+    });
+    if (rc) return rc;
+    note_launches(1);
+    return launch_check("dfea_mesh_ref_frame");
 }
 
 extern "C" int dfea_mesh_grad_to_f32(const dfea_mesh_view* mesh, float* grad32_out, void* stream) {

@@ -12,19 +12,22 @@ import torch
 from difffea_b200.elements import edge_shape, gauss_1d
 
 
-def select_boundary_nodes(nodes, side, tol=1e-6):
-    """(N,) bool mask of the nodes on side "left" | "right" | "bottom" | "top" of the bounding box."""
-    x, y = nodes[:, 0], nodes[:, 1]
-    eps = tol * torch.max(x.max() - x.min(), y.max() - y.min())
-    if side == "left":
-        return x <= x.min() + eps
-    if side == "right":
-        return x >= x.max() - eps
-    if side == "bottom":
-        return y <= y.min() + eps
-    if side == "top":
-        return y >= y.max() - eps
-    raise ValueError("side must be 'left', 'right', 'bottom' or 'top'")
+def bounding_box(nodes):
+    """(lo, hi): the per-coordinate minima and maxima of the nodes, (2,) each."""
+    return torch.aminmax(nodes, dim=0)
+
+
+def select_boundary_nodes(nodes, side, tol=1e-6, box=None):
+    """(N,) bool mask of the nodes on side "left" | "right" | "bottom" | "top" of the bounding box (``box``:
+    ``bounding_box(nodes)``, when the caller has it already)."""
+    if side not in ("left", "right", "bottom", "top"):
+        raise ValueError("side must be 'left', 'right', 'bottom' or 'top'")
+    lo, hi = bounding_box(nodes) if box is None else box
+    eps = tol * (hi - lo).max()
+    c = 0 if side in ("left", "right") else 1
+    if side in ("left", "bottom"):
+        return nodes[:, c] <= lo[c] + eps
+    return nodes[:, c] >= hi[c] - eps
 
 
 def dofs_from_node_mask(node_mask, components=(0, 1)):

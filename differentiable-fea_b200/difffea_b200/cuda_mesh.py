@@ -119,8 +119,7 @@ class CudaMesh:
         # reference shape gradients at the Gauss points (host values in the view) and, built on demand,
         # the inverse element Jacobians of the reference-frame FP32 operator
         GP = params.get("GP")
-        self._default_rule = GP is None or (GP.dtype == torch.float64 and default_rule(self.element_type, GP))
-        if self._default_rule:
+        if GP is None or (GP.dtype == torch.float64 and default_rule(self.element_type, GP)):
             GP = element_quadrature(self.element_type)[0]          # the same points, on the host (shared)
         else:
             GP = GP.detach().to("cpu", torch.float64)
@@ -179,24 +178,17 @@ class CudaMesh:
         operator.
         """
         if self.jinv is None:
-            dev, S, nq, nen, n = self.device, self.stride, self.n_q, self.nen, self.n_el
-            conn = self.conn.view(nen, S)[:, :n] >> 2                                     # packed order
-            X = self._nodes.detach().to(dev, torch.float64)[conn.to(torch.int64).t()]     # (n, nen, 2)
-            dNr = (quadrature_gradients(self.element_type, element_quadrature(self.element_type, torch.float64, dev)[0])
-                   if self._default_rule else self.ref_grad.to(dev))                   # (nq, nen, 2)
-            J = torch.einsum("eai,qaj->eqij", X, dNr)                                     # dX_i / dxi_j
-            det = J[..., 0, 0] * J[..., 1, 1] - J[..., 0, 1] * J[..., 1, 0]
-            Jinv = torch.stack([torch.stack([J[..., 1, 1], -J[..., 0, 1]], -1),
-                                torch.stack([-J[..., 1, 0], J[..., 0, 0]], -1)], -2) / det[..., None, None]
-            dN = self.grad.view(nq, nen, S, 2)[:, :, :n, :]                               # packed (nq, nen, n, 2)
-            dN_ref = torch.einsum("qaj,eqji->qaei", dNr, Jinv)
-            scale = float(dN.abs().max()) if n else 1.0
-            if n and float((dN_ref - dN).abs().max()) > 1e-9 * scale:
+            dev, S, nq = self.device, self.stride, self.n_q
+            nodes = self._nodes.detach().to(dev, torch.float64).contiguous()
+            jinv = torch.empty(nq * 2 * S * 2, dtype=torch.float64, device=dev)
+            check = torch.empty(2, dtype=torch.float64, device=dev)
+            with torch.cuda.device(dev):
+                _lib.call("dfea_mesh_ref_frame", self.view_ref, ptr(nodes), ptr(jinv), ptr(check), stream_handle())
+            diff, scale = check.tolist()
+            if self.n_el and diff > 1e-9 * scale:
                 raise ValueError("dN_dX does not match this package's reference gradients and quadrature; "
                                  "the reference-frame operator cannot be used for this problem")
-            packed = torch.zeros(nq, 2, S, 2, dtype=torch.float64, device=dev)
-            packed[:, :, :n, :] = Jinv.permute(1, 2, 0, 3)                                 # [q][row][e][col]
-            self.jinv = packed.contiguous()
+            self.jinv = jinv.view(nq, 2, S, 2)
             self.view.jinv = self.jinv.data_ptr()
         return self.jinv
 

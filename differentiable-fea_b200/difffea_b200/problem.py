@@ -11,7 +11,7 @@ built; the mapped quarter plate with a hole has its own builder (``build_quarter
 """
 import torch
 
-from difffea_b200.boundary_conditions import (boundary_edges, dofs_from_node_mask, edge_traction_load,
+from difffea_b200.boundary_conditions import (boundary_edges, bounding_box, dofs_from_node_mask, edge_traction_load,
                                               select_boundary_nodes)
 from difffea_b200.elements import element_quadrature, get_element, make_shape_fn, quadrature_gradients
 from difffea_b200.materials import lame_parameters, material_vector
@@ -64,11 +64,12 @@ def _assemble(nodes, conn, element_type, spec, dtype):
     dev = nodes.device
     GP, GW = element_quadrature(element_type, dtype=dtype, device=dev)
     N = nodes.shape[0]
-    fixed_nodes = select_boundary_nodes(nodes, spec["fixed_side"])
+    box = bounding_box(nodes)
+    fixed_nodes = select_boundary_nodes(nodes, spec["fixed_side"], box=box)
     comps = {"xy": (0, 1), "x": (0,), "y": (1,)}[spec.get("fixed_dofs", "xy")]
     fixed = dofs_from_node_mask(fixed_nodes, comps)
     u_D = torch.zeros(2 * N, dtype=dtype, device=dev)
-    load_nodes = select_boundary_nodes(nodes, spec["load_side"])
+    load_nodes = select_boundary_nodes(nodes, spec["load_side"], box=box)
     value = spec.get("load_value", (0.0, 0.0))
     f = torch.zeros(N, 2, dtype=dtype, device=dev)
     if spec.get("load_mode", "force") == "displacement":

@@ -171,6 +171,17 @@ int dfea_mesh_pack(int64_t n_el, int64_t stride, int32_t nen, int32_t n_q, int64
 /* FP32 copy of the packed gradients (the geometry of the FP32 inner operator). */
 int dfea_mesh_grad_to_f32(const dfea_mesh_view* mesh, float* grad32_out, void* stream);
 
+/*
+ * Inverse element Jacobians of the reference-frame FP32 operator (DFEA_F32REF), from the packed mesh and
+ * the node coordinates nodes (n_nodes, 2) float64 (problem.py `nodes`): jinv_out [n_q][2][stride][2]
+ * (row r of Jinv at Gauss point q as an f64 pair; zeros in the padding slots), 16-byte aligned.  check (2
+ * doubles) receives the largest |Jinv^T dN/dxi - dN/dX| and the largest |dN/dX| over the mesh: the caller
+ * accepts the problem's geometry when the first is within a tolerance of the second (the reference
+ * derives dN/dX the same way, operators.py:85-120).  No counterpart function in the reference.
+ */
+int dfea_mesh_ref_frame(const dfea_mesh_view* mesh, const double* nodes, double* jinv_out, double* check,
+                        void* stream);
+
 /* ---------------------------------------------------------------- kernels (a), (b) ------------ */
 
 /*

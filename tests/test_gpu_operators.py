@@ -246,6 +246,27 @@ def test_reference_frame_operator_at_size_is_symmetric(et, nx, ny):
     assert rel(Av, make_tangent_operator("cuda", u, th, p)(v)) < 2e-6
 
 
+@pytest.mark.parametrize("case", ["quad4", "quad9", "quad8", "tri3", "tri6", "plate_quad9"])
+def test_reference_frame_jacobians_match_the_node_geometry(case):
+    """The library's packed inverse Jacobians equal (dX/dxi)^-1 formed from the nodes with torch (the mapped
+    quarter plate: a different Jacobian in every element)."""
+    from difffea_b200.problem import build_quarter_plate_problem
+    p = (build_quarter_plate_problem("quad9", n_theta=6, n_radial=5, device=DEV) if case == "plate_quad9"
+         else build_rectangle_problem(case, 7, 3, 2.0, 1.1, device=DEV))
+    mesh = cuda_mesh(p)
+    jinv = mesh.ensure_ref_frame()
+    S, nq, nen, n = mesh.stride, mesh.n_q, mesh.nen, mesh.n_el
+    conn = (mesh.conn.view(nen, S)[:, :n] >> 2).to(torch.int64).t()
+    X = p["nodes"].to(torch.float64)[conn]                                   # (n, nen, 2), packed order
+    J = torch.einsum("eai,qaj->eqij", X, mesh.ref_grad.to(X.device))
+    det = J[..., 0, 0] * J[..., 1, 1] - J[..., 0, 1] * J[..., 1, 0]
+    inv = torch.stack([torch.stack([J[..., 1, 1], -J[..., 0, 1]], -1),
+                       torch.stack([-J[..., 1, 0], J[..., 0, 0]], -1)], -2) / det[..., None, None]
+    expect = torch.zeros(nq, 2, S, 2, dtype=torch.float64, device=X.device)
+    expect[:, :, :n, :] = inv.permute(1, 2, 0, 3)
+    assert float((jinv - expect).abs().max()) <= 1e-14 * float(expect.abs().max())
+
+
 def test_reference_frame_rejects_inconsistent_geometry():
     d, p, u, v, th = golden_case("operator_quad4_h0.5_unit")
     q = dict(p)
