@@ -9,7 +9,7 @@ equivalent nodal forces).
 """
 import torch
 
-from difffea_b200.elements import edge_shape, gauss_1d
+from difffea_b200.elements import edge_shape_at_rule, gauss_1d
 
 
 def bounding_box(nodes):
@@ -68,7 +68,7 @@ def edge_traction_load(nodes, edges, order, node_mask, total_force, n_gauss=3):
     if edges.shape[0] == 0:
         return f
     s, w = gauss_1d(n_gauss, dtype, device)   # (host leggauss values moved to the device)
-    N, dN = edge_shape(order, s)                                   # (g, k)
+    N, dN = edge_shape_at_rule(order, s)                           # (g, k)
     Xe = nodes[edges]                                              # (E, k, 2)
     tangent = torch.einsum("gk,ekd->egd", dN, Xe)                  # dX/ds at every Gauss point
     speed = torch.linalg.norm(tangent, dim=-1)                     # (E, g)

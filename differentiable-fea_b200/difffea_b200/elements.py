@@ -225,6 +225,24 @@ def edge_shape(order, s):
     return N, dN
 
 
+_EDGE_SHAPES = {}
+
+
+def edge_shape_at_rule(order, s):
+    """edge_shape(order, s); for a shared Gauss rule's points (gauss_1d) the result is computed once and shared
+    as well (do not modify), after its stream has finished computing it."""
+    key = (order, id(s))
+    hit = _EDGE_SHAPES.get(key)
+    if hit is not None and hit[0] is s:
+        return hit[1]
+    out = edge_shape(order, s)
+    if any(rule[0] is s for k, rule in list(_QUADRATURE.items()) if k[0] == "gauss_1d"):
+        if s.is_cuda:
+            torch.cuda.current_stream(s.device).synchronize()
+        _EDGE_SHAPES[key] = (s, out)
+    return out
+
+
 def reference_node_coordinates(name, dtype=torch.float64):
     coords = {
         "quad4": [(-1, -1), (1, -1), (1, 1), (-1, 1)],
