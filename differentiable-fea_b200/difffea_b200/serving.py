@@ -341,7 +341,7 @@ class ServingEngine:
                  pcg_max_iter=5000, prewarm_bytes=0, pcg_graph=0, pcg_form="gather",
                  fp32_moduli="ref", order="fifo", max_blocks=64, preconditioner="auto", batched=False,
                  driver="native", max_newton=25, max_cutbacks=8, pool_bytes=0, mg_graphs=False, mg_bounds_every=3,
-                 mg_gather=False):
+                 mg_gather=True):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if self.device.index is None:            # "cuda": the current device, by index (the slot threads set it)
             self.device = torch.device(self.device.type, torch.cuda.current_device())
@@ -359,7 +359,9 @@ class ServingEngine:
         # 59.4 vs 93.8 solves/s), although one request alone is faster with it (54.5 vs 72.9 ms).
         # mg_bounds_every=3: the smoother bounds are estimated at a request's first set-up and every third one
         # after it (measured: 101-113 vs 70-75 solves/s with estimates at every set-up, the same Newton and
-        # PCG iteration counts to 0.05 %).  mg_gather: off (no gain measured on the stream).
+        # PCG iteration counts to 0.05 %).  mg_gather: level 0 of the hierarchy in the gather form, whose node pass
+        # also does the smoothing update (2 launches per smoothing step instead of 6): 178.5 vs 166.1 solves/s on
+        # 320 requests of the stream (medians of three).
         # pcg_graph=0: the Jacobi PCG launches its kernels directly (status read every 16 iterations).  Capturing
         # and instantiating a graph per request made the 32-slot engine stall from run to run (80 small requests:
         # 42-181 solves/s with unrolled graphs, 168-178 with direct launches, 132-139 with the conditional loop);
