@@ -119,3 +119,21 @@ def test_pooled_meshes_give_the_fresh_results_bit_for_bit():
     again = eng.run(reqs)                                   # every mesh pooled now, several slots
     for a, b in zip(fresh, again):
         assert torch.equal(a.u, b.u)
+
+
+def test_host_built_requests_match_the_device_built_ones():
+    """source="host" (each problem built on the host, pinned, copied inside the slot) gives the results of the
+    same host dictionaries passed in, bit for bit, and those of problems built on the device to 1e-8 (host and
+    device geometry differ in the last bits)."""
+    from difffea_b200.serving import request_problem, request_stream
+    reqs = request_stream(12, seed=5)
+    eng = ServingEngine(n_slots=4, device=DEV, precision="fp32")
+    host = eng.run(reqs, source="host")
+    given = {r.rid: {k: (v.pin_memory() if torch.is_tensor(v) else v) for k, v in request_problem(r, "cpu").items()}
+             for r in reqs}
+    passed = eng.run(reqs, host_params=given)
+    built_on_device = eng.run(reqs)
+    for a, b, c in zip(host, passed, built_on_device):
+        assert a.converged and b.converged and c.converged
+        assert torch.equal(a.u, b.u), a.rid
+        assert rel(a.u, c.u) < 1e-8, a.rid
