@@ -488,6 +488,12 @@ __host__ __device__ static int mg_dot_blocks(int64_t n) {
     return (int)(b < 1 ? 1 : (b > kMgDotBlocks ? kMgDotBlocks : b));
 }
 
+// The library's own drivers take a dot product in ONE launch: every block stores its partial sum, and the last
+// block to arrive (an integer ticket after the partials in dot_work, zeroed at every set-up and reset by that
+// block) adds the partials with k_mg_dot_final's tree, so the result is bitwise that of the two-launch form.
+constexpr int kMgDotWork = kMgDotBlocks + 32;   // doubles: the partials, then the ticket (256-byte padded)
+__host__ __device__ inline unsigned* dot_ticket(double* work) { return reinterpret_cast<unsigned*>(work + kMgDotBlocks); }
+
 __global__ void __launch_bounds__(kMgDotThreads) k_mg_dot_part(int64_t n, const double* __restrict__ x,
                                                                 const double* __restrict__ y, double* __restrict__ part) {
     double a = 0.0;
@@ -497,13 +503,73 @@ __global__ void __launch_bounds__(kMgDotThreads) k_mg_dot_part(int64_t n, const 
     if (threadIdx.x == 0) part[blockIdx.x] = a;
 }
 
-// x += alpha p, r += neg q (neg = -alpha) and the per-block partial sums of r.r in the grid and accumulation
-// order of k_mg_dot_part: the PCG update of dfea_mg_pcg's host-driven loop (two axpys and the first pass of
-// its r.r) in one launch, with the same expressions, so the iterates and the norm are bitwise the same
+// thread 0 of the block that holds the total: what k_mg_dot_final stores (LANCZOS: the CG step's bookkeeping)
+template <bool LANCZOS>
+__device__ __forceinline__ void dot_store(double a, double* out, double* hist, int k) {
+    if (LANCZOS) {
+        const double alpha = out[1] / out[0], beta = a / out[1];
+        hist[2 * k] = alpha;
+        hist[2 * k + 1] = beta;
+        out[1] = a;
+        out[3] = beta;
+    } else {
+        *out = a;
+    }
+}
+
+// the block partial of a dot handed to the last-block sum; true in the block that stored the total
+template <bool LANCZOS>
+__device__ __forceinline__ void dot_finish(double a, double* work, double* out, double* hist, int k) {
+    const double vals[1] = {block_sum<kMgDotThreads>(a)};
+    double tot[1];
+    if (last_block_sum<kMgDotThreads, 1>(vals, RedSite{work, dot_ticket(work), nullptr}, tot) && threadIdx.x == 0)
+        dot_store<LANCZOS>(tot[0], out, hist, k);
+}
+
+// x.y in one launch (grid: mg_dot_blocks(n) blocks of kMgDotThreads)
+template <bool LANCZOS>
+__global__ void __launch_bounds__(kMgDotThreads) k_mg_dot1(int64_t n, const double* __restrict__ x,
+                                                            const double* __restrict__ y, double* __restrict__ work,
+                                                            double* __restrict__ out, double* __restrict__ hist, int k) {
+    double a = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a += x[i] * y[i];
+    dot_finish<LANCZOS>(a, work, out, hist, k);
+}
+
+// k_mg_lanczos_step and the following r.z in one launch: r -= alpha q, z = r / D with alpha = s[1] / s[0], then
+// the CG step's bookkeeping of k_mg_dot_final<true>
+__global__ void __launch_bounds__(kMgDotThreads) k_mg_lanczos_step_rz(int64_t n, const double* __restrict__ q,
+                                                                       double* __restrict__ r, double* __restrict__ z,
+                                                                       const double* __restrict__ diag,
+                                                                       double* __restrict__ s, double* __restrict__ work,
+                                                                       double* __restrict__ hist, int k) {
+    const double alpha = s[1] / s[0];
+    double a = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        const double zi = ri / diag[i];
+        z[i] = zi;
+        a += ri * zi;
+    }
+    dot_finish<true>(a, work, s, hist, k);
+}
+
+// the drivers' dot: x.y into *out in one launch (the ticket in work is zero, as every set-up leaves it)
+static int mg_dot1(int64_t n, const double* x, const double* y, double* out, double* work, cudaStream_t s) {
+    k_mg_dot1<false><<<mg_dot_blocks(n), kMgDotThreads, 0, s>>>(n, x, y, work, out, nullptr, 0);
+    note_launches(1);
+    return launch_check("multigrid dot");
+}
+
+// x += alpha p, r += neg q (neg = -alpha) and r.r in the grid and accumulation order of the dot: the PCG update
+// of dfea_mg_pcg's host-driven loop (two axpys and its r.r) in one launch, with the same expressions, so the
+// iterates and the norm are bitwise the same
 __global__ void __launch_bounds__(kMgDotThreads) k_mg_update_rr(int64_t n, double alpha, double neg,
                                                                  const double* __restrict__ p, const double* __restrict__ q,
                                                                  double* __restrict__ x, double* __restrict__ r,
-                                                                 double* __restrict__ part) {
+                                                                 double* __restrict__ work, double* __restrict__ out) {
     double a = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         x[i] += alpha * p[i];
@@ -512,8 +578,7 @@ __global__ void __launch_bounds__(kMgDotThreads) k_mg_update_rr(int64_t n, doubl
         r[i] = ri;
         a += ri * ri;
     }
-    a = block_sum<kMgDotThreads>(a);
-    if (threadIdx.x == 0) part[blockIdx.x] = a;
+    dot_finish<false>(a, work, out, nullptr, 0);
 }
 
 // LANCZOS: the sum is r.z of a CG step: alpha = s[1] / s[0], beta = sum / s[1] into hist, s[1] = sum, s[3] = beta
@@ -550,6 +615,17 @@ __global__ void k_mg_lanczos_p(int64_t n, double* __restrict__ p, const double* 
     const double beta = s[3];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = z[i] + beta * p[i];
+}
+
+// the drivers' Lanczos step: dfea_mg_lanczos_step's arithmetic in three launches instead of six
+static int mg_lanczos_step1(int64_t n, double* p, const double* q, double* r, double* z, const double* diag, double* sc,
+                            double* hist, int k, double* work, cudaStream_t s) {
+    const int nb = mg_dot_blocks(n);
+    k_mg_dot1<false><<<nb, kMgDotThreads, 0, s>>>(n, p, q, work, sc, nullptr, 0);
+    k_mg_lanczos_step_rz<<<nb, kMgDotThreads, 0, s>>>(n, q, r, z, diag, sc, work, hist, k);
+    k_mg_lanczos_p<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(n, p, z, sc);
+    note_launches(3);
+    return launch_check("multigrid Lanczos step");
 }
 
 // ------------------------------------------------------------------------------------------
@@ -982,7 +1058,7 @@ extern "C" int dfea_mg_dense_solve(int32_t n, const double* Ainv, const double* 
     return launch_check("dfea_mg_dense_solve");
 }
 
-extern "C" int64_t dfea_mg_dot_work(void) { return kMgDotBlocks; }
+extern "C" int64_t dfea_mg_dot_work(void) { return kMgDotWork; }
 
 extern "C" int dfea_mg_dot(int64_t n, const double* x, const double* y, double* out, double* work, void* stream) {
     if (n < 0 || !x || !y || !out || !work) return set_error(DFEA_ERR_INVALID, "dfea_mg_dot: bad arguments");
@@ -1271,7 +1347,8 @@ static int setup_device_part(const dfea_mesh_view* mesh, const dfea_mg* mg, cons
                              const double* diag, cudaStream_t s, bool lanczos) {
     int rc;
     const int L = mg->n_levels;
-    if ((rc = check_cuda(cudaMemcpyAsync(mg->level[0].diag, diag, mg->level[0].n * sizeof(double), cudaMemcpyDeviceToDevice, s),
+    if ((rc = check_cuda(cudaMemsetAsync(dot_ticket(mg->dot_work), 0, sizeof(unsigned), s), "cudaMemsetAsync")) ||
+        (rc = check_cuda(cudaMemcpyAsync(mg->level[0].diag, diag, mg->level[0].n * sizeof(double), cudaMemcpyDeviceToDevice, s),
                          "cudaMemcpyAsync")))
         return rc;
     for (int l = 1; l < L; ++l) {
@@ -1309,15 +1386,15 @@ static int setup_device_part(const dfea_mesh_view* mesh, const dfea_mg* mg, cons
         k_mg_div<<<grid_for(lv.n, kThreads, 8), kThreads, 0, s>>>(lv.n, lv.r, lv.diag, lv.d);
         note_launches(2);
         if ((rc = check_cuda(cudaMemcpyAsync(lv.x, lv.d, lv.n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")) ||
-            (rc = dfea_mg_dot(lv.n, lv.r, lv.d, mg->lscal + 4 * l + 1, mg->dot_work, s)))
+            (rc = mg_dot1(lv.n, lv.r, lv.d, mg->lscal + 4 * l + 1, mg->dot_work, s)))
             return rc;
     }
     for (int k = 0; k < mg->lanczos_steps; ++k)
         for (int l = 0; l < t; ++l) {
             const dfea_mg_level& lv = mg->level[l];
             if ((rc = mg_apply(mesh, mg, moduli, moduli_dtype, l, lv.x, lv.q, s)) ||
-                (rc = dfea_mg_lanczos_step(lv.n, lv.x, lv.q, lv.r, lv.d, lv.diag, mg->lscal + 4 * l,
-                                           mg->lhist + (int64_t)2 * mg->lanczos_steps * l, k, mg->dot_work, s)))
+                (rc = mg_lanczos_step1(lv.n, lv.x, lv.q, lv.r, lv.d, lv.diag, mg->lscal + 4 * l,
+                                       mg->lhist + (int64_t)2 * mg->lanczos_steps * l, k, mg->dot_work, s)))
                 return rc;
         }
     return DFEA_OK;
@@ -1426,14 +1503,14 @@ static int pcg_start_part(const dfea_mesh_view* mesh, const dfea_mg* mg, const v
     int rc;
     if ((rc = check_cuda(cudaMemsetAsync(x, 0, n * sizeof(double), s), "cudaMemsetAsync")) ||
         (rc = check_cuda(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")) ||
-        (rc = dfea_mg_dot(n, b, b, &st->nb2, mg->dot_work, s)))
+        (rc = mg_dot1(n, b, b, &st->nb2, mg->dot_work, s)))
         return rc;
     k_mgp_check<<<1, 1, 0, s>>>(st);
     note_launches(1);
     if ((rc = launch_check("dfea_mg_pcg: check")) || (rc = mg_vcycle(mesh, mg, moduli, code, 0, r, z, s)) ||
         (rc = check_cuda(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync")))
         return rc;
-    return dfea_mg_dot(n, r, z, &st->rz, mg->dot_work, s);
+    return mg_dot1(n, r, z, &st->rz, mg->dot_work, s);
 }
 
 // one iteration of the device-side loop
@@ -1443,12 +1520,12 @@ static int pcg_body_part(const dfea_mesh_view* mesh, const dfea_mg* mg, const vo
     double *r = mg->pcg, *z = mg->pcg + n, *p = mg->pcg + 2 * n, *q = mg->pcg + 3 * n;
     MgPcgState* st = reinterpret_cast<MgPcgState*>(mg->pcg_state);
     int rc;
-    if ((rc = mg_apply(mesh, mg, moduli, code, 0, p, q, s)) || (rc = dfea_mg_dot(n, p, q, &st->curv, mg->dot_work, s)))
+    if ((rc = mg_apply(mesh, mg, moduli, code, 0, p, q, s)) || (rc = mg_dot1(n, p, q, &st->curv, mg->dot_work, s)))
         return rc;
     k_mgp_update<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(n, st, x, r, p, q, z);
     note_launches(1);
-    if ((rc = launch_check("dfea_mg_pcg: update")) || (rc = dfea_mg_dot(n, r, r, &st->rr, mg->dot_work, s)) ||
-        (rc = mg_vcycle(mesh, mg, moduli, code, 0, r, z, s)) || (rc = dfea_mg_dot(n, r, z, &st->rz_new, mg->dot_work, s)))
+    if ((rc = launch_check("dfea_mg_pcg: update")) || (rc = mg_dot1(n, r, r, &st->rr, mg->dot_work, s)) ||
+        (rc = mg_vcycle(mesh, mg, moduli, code, 0, r, z, s)) || (rc = mg_dot1(n, r, z, &st->rz_new, mg->dot_work, s)))
         return rc;
     k_mgp_direction<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(n, st, p, z);
     k_mgp_end<<<1, 1, 0, s>>>(st, cond);
@@ -1648,7 +1725,7 @@ extern "C" int dfea_mg_pcg(const dfea_mesh_view* mesh, const dfea_mg* mg, const 
     double *r = mg->pcg, *z = mg->pcg + n, *p = mg->pcg + 2 * n, *q = mg->pcg + 3 * n;
     double h[1];
     auto dot = [&](const double* u, const double* v, double* out) -> int {
-        int e = dfea_mg_dot(n, u, v, mg->scal, mg->dot_work, s);
+        int e = mg_dot1(n, u, v, mg->scal, mg->dot_work, s);
         return e ? e : read_scalars(out, mg->scal, 1, s);
     };
     *iterations = 0;
@@ -1679,9 +1756,8 @@ extern "C" int dfea_mg_pcg(const dfea_mesh_view* mesh, const dfea_mg* mg, const 
         }
         const double alpha = rz / curv;
         const int nb = mg_dot_blocks(n);
-        k_mg_update_rr<<<nb, kMgDotThreads, 0, s>>>(n, alpha, -alpha, p, q, x, r, mg->dot_work);
-        k_mg_dot_final<false><<<1, kMgDotThreads, 0, s>>>(nb, mg->dot_work, mg->scal, nullptr, 0);
-        note_launches(2);
+        k_mg_update_rr<<<nb, kMgDotThreads, 0, s>>>(n, alpha, -alpha, p, q, x, r, mg->dot_work, mg->scal);
+        note_launches(1);
         if ((rc = launch_check("dfea_mg_pcg: update")) || (rc = read_scalars(h, mg->scal, 1, s))) return rc;
         if (h[0] <= tol2) {
             *iterations = k + 1;

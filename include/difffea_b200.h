@@ -358,7 +358,9 @@ int dfea_mg_cheb_step(int64_t n, double* x, double* r, double* d, const double* 
  * beta = r.z / s[1], p = z + beta p, s[1] = r.z, s[3] = beta, (alpha, beta) into hist[2k], hist[2k+1].
  * Start: r = b, z = r / diag, p = z, s[1] = r.z.  The eigenvalues of the tridiagonal matrix of the
  * coefficients approximate those of D^-1 A (Saad, Iterative Methods, section 6.7). */
-int64_t dfea_mg_dot_work(void); /* doubles of the work buffer of dfea_mg_dot and dfea_mg_lanczos_step */
+int64_t dfea_mg_dot_work(void); /* doubles of the work buffer of dfea_mg_dot, dfea_mg_lanczos_step and
+                                   dfea_mg.dot_work (the drivers keep a reduction ticket after the partials;
+                                   dfea_mg_setup zeroes it) */
 int dfea_mg_dot(int64_t n, const double* x, const double* y, double* out, double* work, void* stream);
 int dfea_mg_lanczos_step(int64_t n, double* p, const double* q, double* r, double* z, const double* diag,
                          double* s, double* hist, int32_t k, double* work, void* stream);
