@@ -815,7 +815,7 @@ __global__ void k_mg_dense_solve(int n, const double* __restrict__ Ainv, const d
 // between phases.  Each phase calls the per-node function of the kernel it replaces, so the result is
 // bitwise that of the separate launches.
 // ------------------------------------------------------------------------------------------
-constexpr int kMgTailThreads = 512;
+constexpr int kMgTailThreads = 1024;
 constexpr int kMgTailNodes = 1536;   // levels of at most this many nodes run in the tail
 
 struct MgTailLevel {
