@@ -225,12 +225,13 @@ def measure(kind, element, n_elements, precision, reps=20, flush=True, pcg_iters
     return row
 
 
-def vcycle_once(element, n_elements, precision, reps=10):
-    """Set-up and one V-cycle of the multigrid preconditioner on the microbench mesh (CUDA events)."""
+def vcycle_once(element, n_elements, precision, reps=10, gather=False):
+    """Set-up and one V-cycle of the multigrid preconditioner on the microbench mesh (CUDA events); ``gather``:
+    level 0 in the gather form (the serving engine's)."""
     from difffea_b200.multigrid import Multigrid
     st = State(element, n_elements, precision)
     code = _lib.DFEA_F32REF if precision == "ref" else (_lib.DFEA_F64 if st.C.dtype == torch.float64 else _lib.DFEA_F32)
-    mg = Multigrid(st.mesh, st.p)
+    mg = Multigrid(st.mesh, st.p, gather=gather)
     r = torch.randn(st.N2, dtype=torch.float64, generator=torch.Generator().manual_seed(1)).to(st.device)
     z = torch.empty_like(r)
     setup_ms, _ = time_launches(lambda: mg.setup(st.C, code, st.diag), reps=3, warmup=1)
@@ -240,7 +241,7 @@ def vcycle_once(element, n_elements, precision, reps=10):
 
 
 def solve_once(element, nx, precision, pcg_graph, form="auto", preconditioner="jacobi", mg_graphs=False,
-               mg_bounds_every=3):
+               mg_bounds_every=3, mg_gather=False):
     """Wall and device milliseconds of one serving-type request (the second of two identical solves)."""
     import time
     from difffea_b200.serving import Request, solve_request
@@ -254,7 +255,8 @@ def solve_once(element, nx, precision, pcg_graph, form="auto", preconditioner="j
         t = time.perf_counter()
         e0.record(s)
         u, info = solve_request(req, "cuda", precision=prec, pcg_graph=pcg_graph, pcg_form=form,
-                                preconditioner=preconditioner, mg_graphs=mg_graphs, mg_bounds_every=mg_bounds_every)
+                                preconditioner=preconditioner, mg_graphs=mg_graphs, mg_bounds_every=mg_bounds_every,
+                                mg_gather=mg_gather)
         e1.record(s)
         torch.cuda.synchronize()
         out = dict(kernel="solve", element=element, nx=nx, n_el=req.n_elements, precision=precision,
@@ -288,17 +290,18 @@ def main(argv=None):
     ap.add_argument("--mg-graphs", action="store_true", help="solve: graph-driven multigrid (default: host-driven, "
                     "as the serving engine)")
     ap.add_argument("--mg-bounds-every", type=int, default=3, help="solve: multigrid smoother bounds every k-th set-up")
+    ap.add_argument("--mg-gather", action="store_true", help="vcycle / solve: level 0 of the hierarchy in the gather form")
     ap.add_argument("--pcg-graph", type=int, default=None,
                     help="PCG form: 0 direct launches (solve's default), 1 loop graph (pcg's default), "
                          "2 unrolled graph")
     a = ap.parse_args(argv)
     if a.kind == "solve":
         print(json.dumps(solve_once(a.element, a.nx, a.precision, 0 if a.pcg_graph is None else a.pcg_graph,
-                                    a.form or "auto", a.preconditioner, a.mg_graphs, a.mg_bounds_every)),
+                                    a.form or "auto", a.preconditioner, a.mg_graphs, a.mg_bounds_every, a.mg_gather)),
               flush=True)
         return 0
     if a.kind == "vcycle":
-        print(json.dumps(vcycle_once(a.element, a.elements, a.precision, a.reps)), flush=True)
+        print(json.dumps(vcycle_once(a.element, a.elements, a.precision, a.reps, gather=a.mg_gather)), flush=True)
         return 0
     if a.kind == "sweep":
         for element in ("quad4", "quad9"):
