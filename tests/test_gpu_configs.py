@@ -64,7 +64,7 @@ def test_plain_100x100_solve_against_the_oracle():
     print(f"\nplain 100x100 Q4: rel err {err:.2e}; Newton {info['total_newton']} (oracle {info_ref['total_newton']}), "
           f"CG {info['total_cg']} (oracle {info_ref['total_cg']}), max u_x {float(u[0::2].max()):.4f}")
     assert info["converged"] and info_ref["converged"]
-    assert err <= 1e-9                                      # the north star's bar for complete solutions
+    assert err <= 1e-9                                      # the parity bar for complete solutions
     assert info["total_newton"] == info_ref["total_newton"]
     assert abs(info["total_cg"] - info_ref["total_cg"]) <= 0.01 * info_ref["total_cg"]
     assert 0.09 < float(u[0::2].max()) < 0.10               # ~10 % stretch

@@ -49,7 +49,7 @@ def test_moduli_and_diagonal_match_reference(name):
 def test_tangent_product_matches_qp_ew(name):
     d, p, u, v, th = golden_case(name)
     y = make_tangent_operator("cuda", u, th, p)(v)
-    assert rel(y, d["Av_qp_ew"]) < 1e-11           # the parity bar of the north star (per product)
+    assert rel(y, d["Av_qp_ew"]) < 1e-11           # the parity bar per product
     assert rel(y, d["Av_jvp"]) < 1e-11
     assert make_tangent_operator("auto", u, th, p)(v).equal(y)
 

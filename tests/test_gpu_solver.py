@@ -36,7 +36,7 @@ def test_complete_solve_matches_reference(name):
     u, info = newton_krylov_solve(p, _t(d, "theta"), int(d["n_load_steps"]), float(d["tol"]), verbose=False,
                                   preconditioner=device_pre)
     assert info["converged"] and info["load_factor"] == 1.0
-    assert rel(u, d["u_star"]) < 1e-9                      # complete solutions: the north star's bar
+    assert rel(u, d["u_star"]) < 1e-9                      # the parity bar for complete solutions
     if device_pre == pre:
         assert info["total_newton"] == int(d["total_newton"])
         assert abs(info["total_cg"] - int(d["total_cg"])) <= max(3, 0.03 * int(d["total_cg"]))
