@@ -546,6 +546,72 @@ __global__ void k_zero_tickets(unsigned* t, int n, double* results, int nr) {
     if (i < nr) results[i] = 0.0;
 }
 
+// Node -> (element, local node) incidence of the gather form, CSR: ptr[n_nodes + 1] and the slots
+// a * stride + e of every node in increasing order -- the arrays a stable sort of the slots by node gives.
+// Counting with integer atomics, an exclusive scan in one block, a fill at per-node cursors (in any order),
+// then each node's few slots sorted ascending: every step is exact, so the result is the same each time.
+__global__ void k_inc_count(int64_t n_slots, int64_t n_el, int64_t S, const int32_t* __restrict__ conn,
+                            int32_t* __restrict__ count) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_slots; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = t / n_el, e = t - a * n_el;
+        atomicAdd(&count[conn[a * S + e] >> 2], 1);
+    }
+}
+
+constexpr int kIncScanThreads = 1024;
+
+// ptr[i] = sum of count[0..i), ptr[N] = the total; the counts are replaced by the same prefix (the fill's
+// cursors).  One block: each thread scans its contiguous chunk, the chunk totals are scanned in shared memory.
+__global__ void __launch_bounds__(kIncScanThreads) k_inc_scan(int64_t N, int32_t* __restrict__ count_cursor,
+                                                              int32_t* __restrict__ ptr) {
+    __shared__ long long part[kIncScanThreads];
+    const int tid = threadIdx.x;
+    const int64_t chunk = (N + kIncScanThreads - 1) / kIncScanThreads;
+    const int64_t lo = tid * chunk, hi = lo + chunk < N ? lo + chunk : N;
+    long long s = 0;
+    for (int64_t i = lo; i < hi; ++i) s += count_cursor[i];
+    part[tid] = s;
+    __syncthreads();
+    for (int off = 1; off < kIncScanThreads; off <<= 1) {
+        const long long v = tid >= off ? part[tid - off] : 0;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    long long run = part[tid] - s;
+    for (int64_t i = lo; i < hi; ++i) {
+        const int32_t c = count_cursor[i];
+        ptr[i] = (int32_t)run;
+        count_cursor[i] = (int32_t)run;
+        run += c;
+    }
+    if (tid == kIncScanThreads - 1) ptr[N] = (int32_t)part[tid];
+}
+
+__global__ void k_inc_fill(int64_t n_slots, int64_t n_el, int64_t S, const int32_t* __restrict__ conn,
+                           int32_t* __restrict__ cursor, int32_t* __restrict__ inc) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_slots; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = t / n_el, e = t - a * n_el;
+        const int pos = atomicAdd(&cursor[conn[a * S + e] >> 2], 1);
+        inc[pos] = (int32_t)(a * S + e);
+    }
+}
+
+__global__ void k_inc_sort(int64_t N, const int32_t* __restrict__ ptr, int32_t* __restrict__ inc) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+        const int b = ptr[n], end = ptr[n + 1];
+        for (int i = b + 1; i < end; ++i) {
+            const int32_t v = inc[i];
+            int j = i - 1;
+            while (j >= b && inc[j] > v) {
+                inc[j + 1] = inc[j];
+                --j;
+            }
+            inc[j + 1] = v;
+        }
+    }
+}
+
 // Inverse element Jacobians of the reference-frame FP32 operator, packed [q][row][stride] as (col 0, col 1)
 // pairs (zeros in the padding slots), from the packed connectivity and the node coordinates:
 // J_ij = sum_a X_a,i dN_a/dxi_j, Jinv = J^-1.  check[0] and check[1] receive the largest |Jinv^T dN/dxi -
@@ -684,6 +750,28 @@ extern "C" int dfea_mesh_pack(int64_t n_el, int64_t stride, int32_t nen, int32_t
     k_node_fix<<<grid_for(n_nodes, kThreads, 8), kThreads, 0, s>>>(n_nodes, m, node_fix_out);
     note_launches(1);
     return launch_check("dfea_mesh_pack");
+}
+
+extern "C" int dfea_mesh_node_incidence(const dfea_mesh_view* mesh, int32_t* ptr_out, int32_t* inc_out, int32_t* work,
+                                        void* stream) {
+    int rc = validate_mesh(mesh, false);
+    if (rc) return rc;
+    if (!ptr_out || !inc_out || !work) return set_error(DFEA_ERR_INVALID, "dfea_mesh_node_incidence: NULL pointer");
+    if ((int64_t)mesh->nen * mesh->stride >= (int64_t(1) << 31))
+        return set_error(DFEA_ERR_INVALID, "dfea_mesh_node_incidence: mesh too large for 32-bit incidence indices");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t N = mesh->n_nodes, n_slots = (int64_t)mesh->nen * mesh->n_el;
+    if ((rc = check_cuda(cudaMemsetAsync(work, 0, N * sizeof(int32_t), s), "cudaMemsetAsync"))) return rc;
+    if (n_slots > 0)
+        k_inc_count<<<grid_for(n_slots, kThreads, 8), kThreads, 0, s>>>(n_slots, mesh->n_el, mesh->stride, mesh->conn, work);
+    k_inc_scan<<<1, kIncScanThreads, 0, s>>>(N, work, ptr_out);
+    if (n_slots > 0) {
+        k_inc_fill<<<grid_for(n_slots, kThreads, 8), kThreads, 0, s>>>(n_slots, mesh->n_el, mesh->stride, mesh->conn, work,
+                                                                        inc_out);
+        k_inc_sort<<<grid_for(N, kThreads, 8), kThreads, 0, s>>>(N, ptr_out, inc_out);
+    }
+    note_launches(n_slots > 0 ? 4 : 1);
+    return launch_check("dfea_mesh_node_incidence");
 }
 
 extern "C" int dfea_mesh_ref_frame(const dfea_mesh_view* mesh, const double* nodes, double* jinv_out, double* check,

@@ -112,6 +112,7 @@ _PROTOS = {
                                       c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "dfea_mesh_grad_to_f32": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp]),
     "dfea_mesh_ref_frame": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp]),
+    "dfea_mesh_node_incidence": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp]),
     "dfea_qp_moduli": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp, c_vp]),
     "dfea_qp_moduli_block": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp,
                                             c_vp, c_vp]),

@@ -159,13 +159,12 @@ class CudaMesh:
             S, nen, n, N, dev = self.stride, self.nen, self.n_el, self.n_nodes, self.device
             if nen * S >= 2 ** 31:
                 raise ValueError("mesh too large for 32-bit incidence indices")
-            nodes = (self.conn.view(nen, S)[:, :n] >> 2).to(torch.int64).reshape(-1)
-            flat = (torch.arange(nen, device=dev)[:, None] * S + torch.arange(n, device=dev)[None, :]).reshape(-1)
-            order = torch.sort(nodes, stable=True).indices
-            self.node_elem = flat[order].to(torch.int32).contiguous()
-            ptr_ = torch.zeros(N + 1, dtype=torch.int64, device=dev)
-            ptr_[1:] = torch.cumsum(torch.bincount(nodes, minlength=N), 0)
-            self.node_elem_ptr = ptr_.to(torch.int32).contiguous()
+            i32 = dict(dtype=torch.int32, device=dev)
+            ptr_, inc, work = torch.empty(N + 1, **i32), torch.empty(max(nen * n, 1), **i32), torch.empty(N, **i32)
+            with torch.cuda.device(dev):
+                _lib.call("dfea_mesh_node_incidence", self.view_ref, ptr(ptr_), ptr(inc), ptr(work), stream_handle())
+            self.node_elem = inc[:nen * n]
+            self.node_elem_ptr = ptr_
             self.view.node_elem_ptr = self.node_elem_ptr.data_ptr()
             self.view.node_elem = self.node_elem.data_ptr()
         return self.node_elem_ptr, self.node_elem

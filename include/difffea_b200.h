@@ -182,6 +182,15 @@ int dfea_mesh_grad_to_f32(const dfea_mesh_view* mesh, float* grad32_out, void* s
 int dfea_mesh_ref_frame(const dfea_mesh_view* mesh, const double* nodes, double* jinv_out, double* check,
                         void* stream);
 
+/*
+ * Node incidence of the gather form (the node_elem_ptr / node_elem arrays of dfea_mesh_view): ptr_out
+ * [n_nodes + 1] and inc_out [nen * n_el], the slots a * stride + e of each node in increasing order; work is
+ * n_nodes int32 of scratch.  Exact (integer counting, a scan and per-node sorts), so the same each time.
+ * No counterpart function in the reference (its products scatter through torch index_add, operators.py:385-412).
+ */
+int dfea_mesh_node_incidence(const dfea_mesh_view* mesh, int32_t* ptr_out, int32_t* inc_out, int32_t* work,
+                             void* stream);
+
 /* ---------------------------------------------------------------- kernels (a), (b) ------------ */
 
 /*

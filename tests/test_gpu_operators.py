@@ -267,6 +267,24 @@ def test_reference_frame_jacobians_match_the_node_geometry(case):
     assert float((jinv - expect).abs().max()) <= 1e-14 * float(expect.abs().max())
 
 
+@pytest.mark.parametrize("case", ["quad4", "quad9", "quad8", "tri6", "plate_quad9"])
+def test_node_incidence_is_the_stable_sort_of_the_slots_by_node(case):
+    """The library's node incidence (counting, scan, fill, per-node sort) equals the CSR a stable sort of the
+    packed slots a * stride + e by node gives, bit for bit."""
+    from difffea_b200.problem import build_quarter_plate_problem
+    p = (build_quarter_plate_problem("quad9", n_theta=6, n_radial=5, device=DEV) if case == "plate_quad9"
+         else build_rectangle_problem(case, 9, 4, 2.0, 1.1, device=DEV))
+    mesh = cuda_mesh(p)
+    ptr_, inc = mesh.ensure_node_incidence()
+    S, nen, n, N = mesh.stride, mesh.nen, mesh.n_el, mesh.n_nodes
+    nodes = (mesh.conn.view(nen, S)[:, :n] >> 2).to(torch.int64).reshape(-1)
+    flat = (torch.arange(nen, device=nodes.device)[:, None] * S + torch.arange(n, device=nodes.device)[None, :]).reshape(-1)
+    expect_inc = flat[torch.sort(nodes, stable=True).indices].to(torch.int32)
+    expect_ptr = torch.zeros(N + 1, dtype=torch.int64, device=nodes.device)
+    expect_ptr[1:] = torch.cumsum(torch.bincount(nodes, minlength=N), 0)
+    assert torch.equal(inc, expect_inc) and torch.equal(ptr_, expect_ptr.to(torch.int32))
+
+
 def test_reference_frame_rejects_inconsistent_geometry():
     d, p, u, v, th = golden_case("operator_quad4_h0.5_unit")
     q = dict(p)
