@@ -199,6 +199,7 @@ extern "C" int64_t dfea_struct_size(const char* name) {
         {"dfea_mg", (int64_t)sizeof(dfea_mg)},               {"dfea_newton", (int64_t)sizeof(dfea_newton)},
         {"dfea_newton_record", (int64_t)sizeof(dfea_newton_record)},
         {"dfea_newton_info", (int64_t)sizeof(dfea_newton_info)},
+        {"dfea_rect_spec", (int64_t)sizeof(dfea_rect_spec)},
     };
     for (const Entry& e : table)
         if (std::strcmp(e.name, name) == 0) return e.size;

@@ -100,6 +100,13 @@ class NewtonInfo(ctypes.Structure):
                 ("load_factor", c_f64), ("n_records", c_i32), ("reserved", c_i32)]
 
 
+class RectSpec(ctypes.Structure):
+    """Mirror of ``dfea_rect_spec``: a serving request's structured rectangle for ``dfea_build_rectangle``."""
+    _fields_ = [("nen", c_i32), ("n_q", c_i32), ("nx", c_i32), ("ny", c_i32), ("width", c_f64), ("height", c_f64),
+                ("load_x", c_f64), ("load_y", c_f64), ("ref_grad", c_f64 * (9 * 9 * 2)), ("gauss_w", c_f64 * 9),
+                ("edge_s", c_f64 * 3), ("edge_w", c_f64 * 3)]
+
+
 _PROTOS = {
     "dfea_last_error": (ctypes.c_char_p, []),
     "dfea_version": (ctypes.c_int, []),
@@ -113,6 +120,7 @@ _PROTOS = {
     "dfea_mesh_grad_to_f32": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp]),
     "dfea_mesh_ref_frame": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp]),
     "dfea_mesh_node_incidence": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp]),
+    "dfea_build_rectangle": (ctypes.c_int, [ctypes.POINTER(RectSpec)] + [c_vp] * 9),
     "dfea_qp_moduli": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp, c_vp]),
     "dfea_qp_moduli_block": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp,
                                             c_vp, c_vp]),

@@ -170,9 +170,70 @@ def pcg_iteration_bytes(req):
 
 
 def request_problem(req, device="cpu", build_on_device=False):
-    """The problem dictionary of a request (on ``device``)."""
+    """
+    The problem dictionary of a request (on ``device``).  Built on a GPU, a Q4 or Q9 request's arrays are written
+    by one library call (``dfea_build_rectangle``): the mesh, supports and load of build_rectangle_problem, its
+    geometry and load vector to rounding (the sums run in another order), in a few launches and no torch
+    operations -- the serving engine's slots then hold the interpreter lock for less of each request.
+    """
+    if build_on_device and req.element_type in _RECT_NEN and torch.device(device).type == "cuda":
+        return _device_request_problem(req, torch.device(device))
     return build_rectangle_problem(req.element_type, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu,
                                    load=(req.load * 1.0, 0.0), device=device, build_on_device=build_on_device)
+
+
+_RECT_NEN = {"quad4": 4, "quad9": 9}
+_RECT_TEMPLATES = {}
+
+
+def _rect_template(element_type):
+    """The element type's quadrature data in a ``dfea_rect_spec`` (built once per element type)."""
+    spec = _RECT_TEMPLATES.get(element_type)
+    if spec is None:
+        from difffea_b200 import _lib
+        from difffea_b200.elements import element_quadrature, gauss_1d, quadrature_gradients
+        GP, GW = element_quadrature(element_type)
+        s, w = gauss_1d(3)
+        spec = _lib.RectSpec()
+        spec.nen, spec.n_q = _RECT_NEN[element_type], GW.numel()
+        for i, x in enumerate(quadrature_gradients(element_type, GP).reshape(-1).tolist()):
+            spec.ref_grad[i] = x
+        for i, x in enumerate(GW.tolist()):
+            spec.gauss_w[i] = x
+        for i in range(3):
+            spec.edge_s[i], spec.edge_w[i] = float(s[i]), float(w[i])
+        spec = _RECT_TEMPLATES.setdefault(element_type, spec)
+    return spec
+
+
+def _device_request_problem(req, device):
+    import ctypes
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr, stream_handle
+    from difffea_b200.elements import element_quadrature, make_shape_fn
+    from difffea_b200.materials import lame_parameters, material_vector
+    if device.index is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    et = req.element_type
+    spec = _lib.RectSpec.from_buffer_copy(_rect_template(et))
+    spec.nx, spec.ny, spec.width, spec.height = req.nx, req.ny, 4.0, 1.0
+    spec.load_x, spec.load_y = req.load * 1.0, 0.0
+    nen, nq, span = spec.nen, spec.n_q, (2 if spec.nen == 9 else 1)
+    N, n_el = (span * req.nx + 1) * (span * req.ny + 1), req.nx * req.ny
+    f64 = dict(dtype=torch.float64, device=device)
+    nodes, conn = torch.empty(N, 2, **f64), torch.empty(n_el, nen, dtype=torch.int64, device=device)
+    dN_dX, w_detJ = torch.empty(n_el, nq, nen, 2, **f64), torch.empty(n_el, nq, **f64)
+    f, m, u_D = torch.empty(2 * N, **f64), torch.empty(2 * N, **f64), torch.empty(2 * N, **f64)
+    fixed = torch.empty(2 * N, dtype=torch.bool, device=device)
+    with torch.cuda.device(device):
+        _lib.call("dfea_build_rectangle", ctypes.byref(spec), ptr(nodes), ptr(conn), ptr(dN_dX), ptr(w_detJ), ptr(f),
+                  ptr(m), ptr(fixed), ptr(u_D), stream_handle())
+    GP, GW = element_quadrature(et, torch.float64, device)
+    mu0, lmbda0 = lame_parameters(req.E, req.nu)
+    mat_p, mat_scalable = material_vector("neo_hookean", {"mu": mu0, "lmbda": lmbda0})
+    return {"nodes": nodes, "conn": conn, "shape_fn": make_shape_fn(et), "GP": GP, "GW": GW, "material": "neo_hookean",
+            "mat_p": mat_p.to(device), "mat_scalable": mat_scalable.to(device), "f": f, "m": m, "fixed": fixed,
+            "u_D": u_D, "element_type": et, "dN_dX": dN_dX, "w_detJ": w_detJ}
 
 
 class PooledSolve:
@@ -192,13 +253,17 @@ class PooledSolve:
         self.order = el["order"]
         self.edges = boundary_edges(params["conn"], el["edges"])
         self.load_nodes = select_boundary_nodes(params["nodes"], "right")
+        self.native = req.element_type in _RECT_NEN and params["nodes"].is_cuda
 
     def retarget(self, req):
         """The problem dictionary of ``req`` on this mesh (new load vector and material), bound to the workspace."""
         from difffea_b200.boundary_conditions import edge_traction_load
         from difffea_b200.materials import lame_parameters, material_vector
         p = self.params
-        f = edge_traction_load(p["nodes"], self.edges, self.order, self.load_nodes, (float(req.load * 1.0), 0.0))
+        if self.native:       # the load vector the fresh build of this request would have
+            f = request_problem(req, p["nodes"].device, build_on_device=True)["f"].reshape(-1, 2)
+        else:
+            f = edge_traction_load(p["nodes"], self.edges, self.order, self.load_nodes, (float(req.load * 1.0), 0.0))
         mu0, lmbda0 = lame_parameters(req.E, req.nu)
         mat_p, _ = material_vector("neo_hookean", {"mu": mu0, "lmbda": lmbda0}, dtype=p["nodes"].dtype)
         self.params = {**p, "f": f.reshape(-1), "mat_p": mat_p.to(p["nodes"].device)}

@@ -191,6 +191,29 @@ int dfea_mesh_ref_frame(const dfea_mesh_view* mesh, const double* nodes, double*
 int dfea_mesh_node_incidence(const dfea_mesh_view* mesh, int32_t* ptr_out, int32_t* inc_out, int32_t* work,
                              void* stream);
 
+/*
+ * The problem of a serving request, written on the device: a structured rectangle [0, width] x [0, height]
+ * of nx x ny Q4 (nen 4) or Q9 (nen 9) cells, both displacement components fixed on x = 0, a uniform traction
+ * of total (load_x, load_y) on x = width -- the arrays problem.build_rectangle_problem builds (the
+ * reference's rectangle mesher, boundary conditions and precompute_geometry, problem.py:115-194 and
+ * operators.py:85-120): nodes (N, 2), conn (n_el, nen) int64 in the mesher's numbering, dN_dX
+ * (n_el, n_q, nen, 2), w_detJ (n_el, n_q), f, m and u_D (2N), fixed (2N bytes 0/1).  The reference gradients,
+ * Gauss weights and the 3-point edge rule come from the caller.  No counterpart function in the reference.
+ */
+typedef struct {
+    int32_t nen;                                        /* 4 or 9 */
+    int32_t n_q;                                        /* Gauss points per element */
+    int32_t nx, ny;                                     /* cells */
+    double width, height;
+    double load_x, load_y;                              /* total traction force on x = width */
+    double ref_grad[DFEA_MAX_NQ * DFEA_MAX_NEN * 2];    /* dN_a/dxi_alpha at the Gauss points, [q][a][alpha] */
+    double gauss_w[DFEA_MAX_NQ];                        /* Gauss weights */
+    double edge_s[3], edge_w[3];                        /* the edge rule on [-1, 1] */
+} dfea_rect_spec;
+
+int dfea_build_rectangle(const dfea_rect_spec* spec, double* nodes, int64_t* conn, double* dN_dX, double* w_detJ,
+                         double* f, double* m, uint8_t* fixed, double* u_D, void* stream);
+
 /* ---------------------------------------------------------------- kernels (a), (b) ------------ */
 
 /*

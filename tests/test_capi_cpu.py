@@ -85,7 +85,8 @@ def test_ctypes_mirrors_match_the_library_struct_layouts():
     lib = _lib.load()
     mirrors = {"dfea_material": _lib.Material, "dfea_mesh_view": _lib.MeshView, "dfea_mg_grid": _lib.MgGrid,
                "dfea_mg_level": _lib.MgLevel, "dfea_mg": _lib.Mg, "dfea_newton": _lib.Newton,
-               "dfea_newton_record": _lib.NewtonRecord, "dfea_newton_info": _lib.NewtonInfo}
+               "dfea_newton_record": _lib.NewtonRecord, "dfea_newton_info": _lib.NewtonInfo,
+               "dfea_rect_spec": _lib.RectSpec}
     for name, cls in mirrors.items():
         assert lib.dfea_struct_size(name.encode()) == ctypes.sizeof(cls), name
     assert lib.dfea_struct_size(b"no_such_struct") == -1

@@ -137,3 +137,23 @@ def test_host_built_requests_match_the_device_built_ones():
         assert a.converged and b.converged and c.converged
         assert torch.equal(a.u, b.u), a.rid
         assert rel(a.u, c.u) < 1e-8, a.rid
+
+
+@pytest.mark.parametrize("et,nx", [("quad4", 16), ("quad9", 12), ("quad4", 100), ("quad9", 64)])
+def test_device_request_problem_matches_the_builder(et, nx):
+    """A request built on the GPU by the library (dfea_build_rectangle) has build_rectangle_problem's keys, mesh,
+    supports and material exactly, and its geometry and load to rounding; its solution agrees to 1e-9."""
+    from difffea_b200.problem import build_rectangle_problem
+    from difffea_b200.serving import request_problem, solve_request
+    req = Request(0, et, nx, 1.3, 0.31, 0.04)
+    p = request_problem(req, DEV, build_on_device=True)
+    q = build_rectangle_problem(et, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu, load=(req.load, 0.0), device=DEV,
+                                build_on_device=True)
+    assert list(p) == list(q)
+    for k in ("conn", "fixed", "m", "u_D", "mat_p", "mat_scalable", "GP", "GW"):
+        assert torch.equal(p[k], q[k]), k
+    for k in ("nodes", "dN_dX", "w_detJ", "f"):
+        assert p[k].shape == q[k].shape and rel(p[k], q[k]) < 1e-13, k
+    u, info = solve_request(req, DEV, preconditioner="auto")
+    u_ref, info_ref = solve_request(req, DEV, preconditioner="auto", host_params=request_problem(req, "cpu"))
+    assert info["converged"] and info_ref["converged"] and rel(u, u_ref) < 1e-9
