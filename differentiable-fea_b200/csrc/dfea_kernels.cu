@@ -552,81 +552,74 @@ __global__ void k_zero_tickets(unsigned* t, int n, double* results, int nr) {
 // lines; element e = I ny + J.
 // ------------------------------------------------------------------------------------------
 // torch.linspace's value at ind: from the start below the halfway point, from the end above it
-__device__ __forceinline__ double lin_value(double start, double end, int64_t steps, int64_t ind) {
+__host__ __device__ inline double lin_value(double start, double end, int64_t steps, int64_t ind) {
     const double step = (end - start) / (steps - 1);
     return ind < steps / 2 ? start + step * ind : end - step * (steps - ind - 1);
 }
 
 struct RectGrid {
     int64_t gx, gy;
-    __device__ int64_t id(int64_t i, int64_t j) const { return i * (gy + 1) + j; }
+    __host__ __device__ int64_t id(int64_t i, int64_t j) const { return i * (gy + 1) + j; }
 };
 
-__device__ __forceinline__ RectGrid rect_grid(const dfea_rect_spec& p) {
+__host__ __device__ inline RectGrid rect_grid(const dfea_rect_spec& p) {
     const int64_t span = p.nen == 9 ? 2 : 1;
     return RectGrid{span * p.nx, span * p.ny};
 }
 
-__global__ void k_rect_nodes(dfea_rect_spec p, double* __restrict__ nodes, double* __restrict__ m,
-                             uint8_t* __restrict__ fixed, double* __restrict__ u_D, double* __restrict__ f) {
-    const RectGrid g = rect_grid(p);
-    const int64_t N = (g.gx + 1) * (g.gy + 1);
-    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < N; id += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = id / (g.gy + 1), j = id - i * (g.gy + 1);
-        nodes[2 * id] = lin_value(0.0, p.width, g.gx + 1, i);
-        nodes[2 * id + 1] = lin_value(0.0, p.height, g.gy + 1, j);
-        const bool clamped = i == 0;       // the side x = 0 (the next line lies a cell width away)
-        for (int c = 0; c < 2; ++c) {
-            fixed[2 * id + c] = clamped ? 1 : 0;
-            m[2 * id + c] = clamped ? 0.0 : 1.0;
-            u_D[2 * id + c] = 0.0;
-            f[2 * id + c] = 0.0;
-        }
+// grid node id: coordinates, supports (the side x = 0; the next line lies a cell width away), zero load
+__host__ __device__ inline void rect_node(const dfea_rect_spec& p, const RectGrid& g, int64_t id, double* nodes,
+                                          double* m, uint8_t* fixed, double* u_D, double* f) {
+    const int64_t i = id / (g.gy + 1), j = id - i * (g.gy + 1);
+    nodes[2 * id] = lin_value(0.0, p.width, g.gx + 1, i);
+    nodes[2 * id + 1] = lin_value(0.0, p.height, g.gy + 1, j);
+    const bool clamped = i == 0;
+    for (int c = 0; c < 2; ++c) {
+        fixed[2 * id + c] = clamped ? 1 : 0;
+        m[2 * id + c] = clamped ? 0.0 : 1.0;
+        u_D[2 * id + c] = 0.0;
+        f[2 * id + c] = 0.0;
     }
 }
 
-// element connectivity in the element library's local order, and dN/dX = J^-T dN/dxi, w detJ at its Gauss points
-__global__ void k_rect_elements(dfea_rect_spec p, int64_t* __restrict__ conn, double* __restrict__ dN_dX,
-                                double* __restrict__ w_detJ) {
-    const RectGrid g = rect_grid(p);
-    const int nen = p.nen, nq = p.n_q;
-    const int64_t n_el = (int64_t)p.nx * p.ny;
+// element e: connectivity in the element library's local order, dN/dX = J^-T dN/dxi and w detJ at its Gauss points
+__host__ __device__ inline void rect_element(const dfea_rect_spec& p, const RectGrid& g, int64_t e, int64_t* conn,
+                                             double* dN_dX, double* w_detJ) {
     // grid offsets of the nine Q9 nodes in their 2 x 2 block of grid cells; the four Q4 corners
     const int di9[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1}, dj9[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
     const int di4[4] = {0, 1, 1, 0}, dj4[4] = {0, 0, 1, 1};
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_el; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t I = e / p.ny, J = e - I * p.ny;
-        double X[DFEA_MAX_NEN][2];
+    const int nen = p.nen, nq = p.n_q;
+    const int64_t I = e / p.ny, J = e - I * p.ny;
+    double X[DFEA_MAX_NEN][2];
+    for (int a = 0; a < nen; ++a) {
+        const int64_t i = nen == 9 ? 2 * I + di9[a] : I + di4[a], j = nen == 9 ? 2 * J + dj9[a] : J + dj4[a];
+        conn[e * nen + a] = g.id(i, j);
+        X[a][0] = lin_value(0.0, p.width, g.gx + 1, i);
+        X[a][1] = lin_value(0.0, p.height, g.gy + 1, j);
+    }
+    for (int q = 0; q < nq; ++q) {
+        const double* dNr = p.ref_grad + q * nen * 2;
+        double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
         for (int a = 0; a < nen; ++a) {
-            const int64_t i = nen == 9 ? 2 * I + di9[a] : I + di4[a], j = nen == 9 ? 2 * J + dj9[a] : J + dj4[a];
-            conn[e * nen + a] = g.id(i, j);
-            X[a][0] = lin_value(0.0, p.width, g.gx + 1, i);
-            X[a][1] = lin_value(0.0, p.height, g.gy + 1, j);
+            J00 += X[a][0] * dNr[2 * a];
+            J01 += X[a][0] * dNr[2 * a + 1];
+            J10 += X[a][1] * dNr[2 * a];
+            J11 += X[a][1] * dNr[2 * a + 1];
         }
-        for (int q = 0; q < nq; ++q) {
-            const double* dNr = p.ref_grad + q * nen * 2;
-            double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
-            for (int a = 0; a < nen; ++a) {
-                J00 += X[a][0] * dNr[2 * a];
-                J01 += X[a][0] * dNr[2 * a + 1];
-                J10 += X[a][1] * dNr[2 * a];
-                J11 += X[a][1] * dNr[2 * a + 1];
-            }
-            const double det = J00 * J11 - J01 * J10;
-            const double i00 = J11 / det, i01 = -J01 / det, i10 = -J10 / det, i11 = J00 / det;
-            double* out = dN_dX + (e * nq + q) * nen * 2;
-            for (int a = 0; a < nen; ++a) {
-                out[2 * a] = dNr[2 * a] * i00 + dNr[2 * a + 1] * i10;
-                out[2 * a + 1] = dNr[2 * a] * i01 + dNr[2 * a + 1] * i11;
-            }
-            w_detJ[e * nq + q] = p.gauss_w[q] * det;
+        const double det = J00 * J11 - J01 * J10;
+        const double i00 = J11 / det, i01 = -J01 / det, i10 = -J10 / det, i11 = J00 / det;
+        double* out = dN_dX + (e * nq + q) * nen * 2;
+        for (int a = 0; a < nen; ++a) {
+            out[2 * a] = dNr[2 * a] * i00 + dNr[2 * a + 1] * i10;
+            out[2 * a + 1] = dNr[2 * a] * i01 + dNr[2 * a + 1] * i11;
         }
+        w_detJ[e * nq + q] = p.gauss_w[q] * det;
     }
 }
 
-// the consistent nodal forces of the uniform traction on x = W (one block): edge J joins grid nodes (gx, k J) and
+// the consistent nodal forces of the uniform traction on x = W: edge J joins grid nodes (gx, k J) and
 // (gx, k J + k) (k = 1 for Q4, 2 for Q9 with its mid node at k J + 1); t = load / total edge length
-__device__ __forceinline__ void edge_shape_at(int order, double s, double (&N)[3], double (&dN)[3]) {
+__host__ __device__ inline void edge_shape_at(int order, double s, double (&N)[3], double (&dN)[3]) {
     if (order == 1) {
         N[0] = 0.5 * (1.0 - s); N[1] = 0.5 * (1.0 + s); N[2] = 0.0;
         dN[0] = -0.5; dN[1] = 0.5; dN[2] = 0.0;
@@ -636,7 +629,7 @@ __device__ __forceinline__ void edge_shape_at(int order, double s, double (&N)[3
     }
 }
 
-__device__ double edge_speed(const dfea_rect_spec& p, const RectGrid& g, int64_t J, int gpt) {
+__host__ __device__ inline double edge_speed(const dfea_rect_spec& p, const RectGrid& g, int64_t J, int gpt) {
     const int order = p.nen == 9 ? 2 : 1, k = order;
     double N[3], dN[3];
     edge_shape_at(order, p.edge_s[gpt], N, dN);
@@ -649,48 +642,69 @@ __device__ double edge_speed(const dfea_rect_spec& p, const RectGrid& g, int64_t
     return sqrt(t0 * t0 + t1 * t1);
 }
 
+__host__ __device__ inline double rect_edge_length(const dfea_rect_spec& p, const RectGrid& g) {
+    double L = 0.0;
+    for (int64_t J = 0; J < p.ny; ++J)
+        for (int gpt = 0; gpt < 3; ++gpt) L += edge_speed(p, g, J, gpt) * p.edge_w[gpt];
+    return L;
+}
+
+// the load of grid node (gx, j): the contributions of the (at most two) edges that hold it, in edge order
+__host__ __device__ inline void rect_load_node(const dfea_rect_spec& p, const RectGrid& g, int64_t j, double tx,
+                                               double ty, double* f) {
+    const int order = p.nen == 9 ? 2 : 1;
+    int64_t edge[2];
+    int local[2], n_edges = 0;
+    if (order == 1) {
+        if (j > 0) { edge[n_edges] = j - 1; local[n_edges++] = 1; }
+        if (j < p.ny) { edge[n_edges] = j; local[n_edges++] = 0; }
+    } else if (j % 2) {
+        edge[n_edges] = (j - 1) / 2; local[n_edges++] = 2;
+    } else {
+        if (j > 0) { edge[n_edges] = j / 2 - 1; local[n_edges++] = 1; }
+        if (j / 2 < p.ny) { edge[n_edges] = j / 2; local[n_edges++] = 0; }
+    }
+    double fx = 0.0, fy = 0.0;
+    for (int k = 0; k < n_edges; ++k) {
+        double cx = 0.0, cy = 0.0;
+        for (int gpt = 0; gpt < 3; ++gpt) {
+            double N[3], dN[3];
+            edge_shape_at(order, p.edge_s[gpt], N, dN);
+            const double w = p.edge_w[gpt] * N[local[k]] * edge_speed(p, g, edge[k], gpt);
+            cx += w * tx;
+            cy += w * ty;
+        }
+        fx += cx;
+        fy += cy;
+    }
+    const int64_t id = g.id(g.gx, j);
+    f[2 * id] = fx;
+    f[2 * id + 1] = fy;
+}
+
+__global__ void k_rect_nodes(dfea_rect_spec p, double* __restrict__ nodes, double* __restrict__ m,
+                             uint8_t* __restrict__ fixed, double* __restrict__ u_D, double* __restrict__ f) {
+    const RectGrid g = rect_grid(p);
+    const int64_t N = (g.gx + 1) * (g.gy + 1);
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < N; id += (int64_t)gridDim.x * blockDim.x)
+        rect_node(p, g, id, nodes, m, fixed, u_D, f);
+}
+
+__global__ void k_rect_elements(dfea_rect_spec p, int64_t* __restrict__ conn, double* __restrict__ dN_dX,
+                                double* __restrict__ w_detJ) {
+    const RectGrid g = rect_grid(p);
+    const int64_t n_el = (int64_t)p.nx * p.ny;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_el; e += (int64_t)gridDim.x * blockDim.x)
+        rect_element(p, g, e, conn, dN_dX, w_detJ);
+}
+
 __global__ void __launch_bounds__(256) k_rect_load(dfea_rect_spec p, double* __restrict__ f) {
     const RectGrid g = rect_grid(p);
-    const int order = p.nen == 9 ? 2 : 1;
     __shared__ double length;
-    if (threadIdx.x == 0) {
-        double L = 0.0;
-        for (int64_t J = 0; J < p.ny; ++J)
-            for (int gpt = 0; gpt < 3; ++gpt) L += edge_speed(p, g, J, gpt) * p.edge_w[gpt];
-        length = L;
-    }
+    if (threadIdx.x == 0) length = rect_edge_length(p, g);
     __syncthreads();
     const double tx = p.load_x / length, ty = p.load_y / length;
-    for (int64_t j = threadIdx.x; j <= g.gy; j += blockDim.x) {
-        // the edges that hold grid node (gx, j), in edge order, and the node's place on each
-        int64_t edge[2];
-        int local[2], n_edges = 0;
-        if (order == 1) {
-            if (j > 0) { edge[n_edges] = j - 1; local[n_edges++] = 1; }
-            if (j < p.ny) { edge[n_edges] = j; local[n_edges++] = 0; }
-        } else if (j % 2) {
-            edge[n_edges] = (j - 1) / 2; local[n_edges++] = 2;
-        } else {
-            if (j > 0) { edge[n_edges] = j / 2 - 1; local[n_edges++] = 1; }
-            if (j / 2 < p.ny) { edge[n_edges] = j / 2; local[n_edges++] = 0; }
-        }
-        double fx = 0.0, fy = 0.0;
-        for (int k = 0; k < n_edges; ++k) {
-            double cx = 0.0, cy = 0.0;
-            for (int gpt = 0; gpt < 3; ++gpt) {
-                double N[3], dN[3];
-                edge_shape_at(order, p.edge_s[gpt], N, dN);
-                const double w = p.edge_w[gpt] * N[local[k]] * edge_speed(p, g, edge[k], gpt);
-                cx += w * tx;
-                cy += w * ty;
-            }
-            fx += cx;
-            fy += cy;
-        }
-        const int64_t id = g.id(g.gx, j);
-        f[2 * id] = fx;
-        f[2 * id + 1] = fy;
-    }
+    for (int64_t j = threadIdx.x; j <= g.gy; j += blockDim.x) rect_load_node(p, g, j, tx, ty, f);
 }
 
 // Node -> (element, local node) incidence of the gather form, CSR: ptr[n_nodes + 1] and the slots
@@ -899,16 +913,40 @@ extern "C" int dfea_mesh_pack(int64_t n_el, int64_t stride, int32_t nen, int32_t
     return launch_check("dfea_mesh_pack");
 }
 
+static int validate_rect(const dfea_rect_spec* spec, const char* what) {
+    if (!spec) return set_error(DFEA_ERR_INVALID, "%s: NULL spec", what);
+    const dfea_rect_spec& p = *spec;
+    if (!((p.nen == 4 && p.n_q == 4) || (p.nen == 9 && p.n_q == 9)) || p.nx < 1 || p.ny < 1 || !(p.width > 0.0) ||
+        !(p.height > 0.0))
+        return set_error(DFEA_ERR_INVALID, "%s: a Q4 or Q9 rectangle of at least one cell", what);
+    const int64_t span = p.nen == 9 ? 2 : 1;
+    if ((span * p.nx + 1) * (span * p.ny + 1) >= (int64_t(1) << 29)) return set_error(DFEA_ERR_INVALID, "%s: too many nodes", what);
+    return DFEA_OK;
+}
+
+extern "C" int dfea_build_rectangle_host(const dfea_rect_spec* spec, double* nodes, int64_t* conn, double* dN_dX,
+                                         double* w_detJ, double* f, double* m, uint8_t* fixed, double* u_D) {
+    int rc = validate_rect(spec, "dfea_build_rectangle_host");
+    if (rc) return rc;
+    if (!nodes || !conn || !dN_dX || !w_detJ || !f || !m || !fixed || !u_D)
+        return set_error(DFEA_ERR_INVALID, "dfea_build_rectangle_host: NULL pointer");
+    const dfea_rect_spec& p = *spec;
+    const RectGrid g = rect_grid(p);
+    const int64_t N = (g.gx + 1) * (g.gy + 1), n_el = (int64_t)p.nx * p.ny;
+    for (int64_t id = 0; id < N; ++id) rect_node(p, g, id, nodes, m, fixed, u_D, f);
+    for (int64_t e = 0; e < n_el; ++e) rect_element(p, g, e, conn, dN_dX, w_detJ);
+    const double L = rect_edge_length(p, g);
+    for (int64_t j = 0; j <= g.gy; ++j) rect_load_node(p, g, j, p.load_x / L, p.load_y / L, f);
+    return DFEA_OK;
+}
+
 extern "C" int dfea_build_rectangle(const dfea_rect_spec* spec, double* nodes, int64_t* conn, double* dN_dX,
                                     double* w_detJ, double* f, double* m, uint8_t* fixed, double* u_D, void* stream) {
-    if (!spec) return set_error(DFEA_ERR_INVALID, "dfea_build_rectangle: NULL spec");
+    int rc = validate_rect(spec, "dfea_build_rectangle");
+    if (rc) return rc;
     const dfea_rect_spec& p = *spec;
-    if (!((p.nen == 4 && p.n_q == 4) || (p.nen == 9 && p.n_q == 9)) || p.nx < 1 || p.ny < 1 ||
-        !(p.width > 0.0) || !(p.height > 0.0))
-        return set_error(DFEA_ERR_INVALID, "dfea_build_rectangle: a Q4 or Q9 rectangle of at least one cell");
     const int64_t span = p.nen == 9 ? 2 : 1;
     const int64_t N = (span * p.nx + 1) * (span * p.ny + 1), n_el = (int64_t)p.nx * p.ny;
-    if (N >= (int64_t(1) << 29)) return set_error(DFEA_ERR_INVALID, "dfea_build_rectangle: too many nodes");
     if (!nodes || !conn || !dN_dX || !w_detJ || !f || !m || !fixed || !u_D)
         return set_error(DFEA_ERR_INVALID, "dfea_build_rectangle: NULL pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -121,6 +121,7 @@ _PROTOS = {
     "dfea_mesh_ref_frame": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp]),
     "dfea_mesh_node_incidence": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_vp, c_vp]),
     "dfea_build_rectangle": (ctypes.c_int, [ctypes.POINTER(RectSpec)] + [c_vp] * 9),
+    "dfea_build_rectangle_host": (ctypes.c_int, [ctypes.POINTER(RectSpec)] + [c_vp] * 8),
     "dfea_qp_moduli": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp, c_vp]),
     "dfea_qp_moduli_block": (ctypes.c_int, [ctypes.POINTER(MeshView), c_vp, c_vp, c_f64, c_f64, c_vp, c_i32, c_vp,
                                             c_vp, c_vp]),

@@ -169,17 +169,24 @@ def pcg_iteration_bytes(req):
     return req.n_elements * per_el + req.n_nodes * per_node
 
 
-def request_problem(req, device="cpu", build_on_device=False):
+def request_problem(req, device="cpu", build_on_device=False, pin_memory=False):
     """
-    The problem dictionary of a request (on ``device``).  Built on a GPU, a Q4 or Q9 request's arrays are written
-    by one library call (``dfea_build_rectangle``): the mesh, supports and load of build_rectangle_problem, its
-    geometry and load vector to rounding (the sums run in another order), in a few launches and no torch
-    operations -- the serving engine's slots then hold the interpreter lock for less of each request.
+    The problem dictionary of a request (on ``device``).  A Q4 or Q9 request's arrays are written by one library
+    call -- on the GPU (``dfea_build_rectangle``, with ``build_on_device``) or on the host
+    (``dfea_build_rectangle_host``, ``device="cpu"``; into page-locked memory with ``pin_memory``, ready to be
+    copied): the mesh, supports and load of build_rectangle_problem, its geometry and load vector to rounding
+    (the sums run in another order), with no torch operations -- the serving engine's slots then hold the
+    interpreter lock for less of each request.
     """
-    if build_on_device and req.element_type in _RECT_NEN and torch.device(device).type == "cuda":
-        return _device_request_problem(req, torch.device(device))
-    return build_rectangle_problem(req.element_type, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu,
-                                   load=(req.load * 1.0, 0.0), device=device, build_on_device=build_on_device)
+    dev = torch.device(device)
+    if req.element_type in _RECT_NEN:
+        if dev.type == "cuda" and build_on_device:
+            return _device_request_problem(req, dev)
+        if dev.type == "cpu":
+            return _host_request_problem(req, pin_memory)
+    p = build_rectangle_problem(req.element_type, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu,
+                                load=(req.load * 1.0, 0.0), device=device, build_on_device=build_on_device)
+    return {k: (v.pin_memory() if torch.is_tensor(v) else v) for k, v in p.items()} if pin_memory else p
 
 
 _RECT_NEN = {"quad4": 4, "quad9": 9}
@@ -206,34 +213,62 @@ def _rect_template(element_type):
     return spec
 
 
-def _device_request_problem(req, device):
-    import ctypes
+def _rect_arrays(req, **kw):
+    """A request's dfea_rect_spec and empty arrays for the builder (torch.empty keywords ``kw``)."""
     from difffea_b200 import _lib
-    from difffea_b200.cuda_mesh import ptr, stream_handle
-    from difffea_b200.elements import element_quadrature, make_shape_fn
-    from difffea_b200.materials import lame_parameters, material_vector
-    if device.index is None:
-        device = torch.device("cuda", torch.cuda.current_device())
-    et = req.element_type
-    spec = _lib.RectSpec.from_buffer_copy(_rect_template(et))
+    spec = _lib.RectSpec.from_buffer_copy(_rect_template(req.element_type))
     spec.nx, spec.ny, spec.width, spec.height = req.nx, req.ny, 4.0, 1.0
     spec.load_x, spec.load_y = req.load * 1.0, 0.0
     nen, nq, span = spec.nen, spec.n_q, (2 if spec.nen == 9 else 1)
     N, n_el = (span * req.nx + 1) * (span * req.ny + 1), req.nx * req.ny
-    f64 = dict(dtype=torch.float64, device=device)
-    nodes, conn = torch.empty(N, 2, **f64), torch.empty(n_el, nen, dtype=torch.int64, device=device)
-    dN_dX, w_detJ = torch.empty(n_el, nq, nen, 2, **f64), torch.empty(n_el, nq, **f64)
-    f, m, u_D = torch.empty(2 * N, **f64), torch.empty(2 * N, **f64), torch.empty(2 * N, **f64)
-    fixed = torch.empty(2 * N, dtype=torch.bool, device=device)
-    with torch.cuda.device(device):
-        _lib.call("dfea_build_rectangle", ctypes.byref(spec), ptr(nodes), ptr(conn), ptr(dN_dX), ptr(w_detJ), ptr(f),
-                  ptr(m), ptr(fixed), ptr(u_D), stream_handle())
-    GP, GW = element_quadrature(et, torch.float64, device)
+    f64 = dict(dtype=torch.float64, **kw)
+    arrays = dict(nodes=torch.empty(N, 2, **f64), conn=torch.empty(n_el, nen, dtype=torch.int64, **kw),
+                  dN_dX=torch.empty(n_el, nq, nen, 2, **f64), w_detJ=torch.empty(n_el, nq, **f64),
+                  f=torch.empty(2 * N, **f64), m=torch.empty(2 * N, **f64),
+                  fixed=torch.empty(2 * N, dtype=torch.bool, **kw), u_D=torch.empty(2 * N, **f64))
+    return spec, arrays
+
+
+def _rect_problem(req, a, GP, GW, mat_device=None):
+    """The problem dictionary (build_rectangle_problem's keys, in its order) of the builder's arrays ``a``."""
+    from difffea_b200.elements import make_shape_fn
+    from difffea_b200.materials import lame_parameters, material_vector
     mu0, lmbda0 = lame_parameters(req.E, req.nu)
     mat_p, mat_scalable = material_vector("neo_hookean", {"mu": mu0, "lmbda": lmbda0})
-    return {"nodes": nodes, "conn": conn, "shape_fn": make_shape_fn(et), "GP": GP, "GW": GW, "material": "neo_hookean",
-            "mat_p": mat_p.to(device), "mat_scalable": mat_scalable.to(device), "f": f, "m": m, "fixed": fixed,
-            "u_D": u_D, "element_type": et, "dN_dX": dN_dX, "w_detJ": w_detJ}
+    if mat_device is not None:
+        mat_p, mat_scalable = mat_p.to(mat_device), mat_scalable.to(mat_device)
+    return {"nodes": a["nodes"], "conn": a["conn"], "shape_fn": make_shape_fn(req.element_type), "GP": GP, "GW": GW,
+            "material": "neo_hookean", "mat_p": mat_p, "mat_scalable": mat_scalable, "f": a["f"], "m": a["m"],
+            "fixed": a["fixed"], "u_D": a["u_D"], "element_type": req.element_type, "dN_dX": a["dN_dX"],
+            "w_detJ": a["w_detJ"]}
+
+
+def _host_request_problem(req, pin_memory=False):
+    import ctypes
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr
+    from difffea_b200.elements import element_quadrature
+    spec, a = _rect_arrays(req, pin_memory=True) if pin_memory else _rect_arrays(req)
+    _lib.call("dfea_build_rectangle_host", ctypes.byref(spec), *(ptr(a[k]) for k in _RECT_ARGS))
+    GP, GW = element_quadrature(req.element_type)
+    return _rect_problem(req, a, GP, GW)
+
+
+_RECT_ARGS = ("nodes", "conn", "dN_dX", "w_detJ", "f", "m", "fixed", "u_D")
+
+
+def _device_request_problem(req, device):
+    import ctypes
+    from difffea_b200 import _lib
+    from difffea_b200.cuda_mesh import ptr, stream_handle
+    from difffea_b200.elements import element_quadrature
+    if device.index is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    spec, a = _rect_arrays(req, device=device)
+    with torch.cuda.device(device):
+        _lib.call("dfea_build_rectangle", ctypes.byref(spec), *(ptr(a[k]) for k in _RECT_ARGS), stream_handle())
+    GP, GW = element_quadrature(req.element_type, torch.float64, device)
+    return _rect_problem(req, a, GP, GW, mat_device=device)
 
 
 class PooledSolve:
@@ -538,8 +573,7 @@ class ServingEngine:
                     with torch.cuda.stream(stream):
                         hp = host_params.get(req.rid) if host_params is not None else None
                         if hp is None and source == "host":
-                            hp = {k: (v.pin_memory() if torch.is_tensor(v) else v)
-                                  for k, v in request_problem(req, "cpu").items()}
+                            hp = request_problem(req, "cpu", pin_memory=True)
                         u, info = solve_request(req, self.device, host_params=hp, **self.solve_kw)
                         res.u = u.to("cpu") if keep_solutions else None
                         stream.synchronize()

@@ -214,6 +214,10 @@ typedef struct {
 int dfea_build_rectangle(const dfea_rect_spec* spec, double* nodes, int64_t* conn, double* dN_dX, double* w_detJ,
                          double* f, double* m, uint8_t* fixed, double* u_D, void* stream);
 
+/* The same arrays computed on the host into host memory (a problem submitted from host memory). */
+int dfea_build_rectangle_host(const dfea_rect_spec* spec, double* nodes, int64_t* conn, double* dN_dX, double* w_detJ,
+                              double* f, double* m, uint8_t* fixed, double* u_D);
+
 /* ---------------------------------------------------------------- kernels (a), (b) ------------ */
 
 /*

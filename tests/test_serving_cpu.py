@@ -160,3 +160,19 @@ def test_two_rank_bench_helpers_over_gloo():
         assert len(sample_ids[0]) == len(sample_ids[1]) == (3 + 2) * 4
         assert max_nx <= 64
         assert config == out[0][5]                            # both arms and all ranks print one config
+
+
+@pytest.mark.parametrize("et,nx", [("quad4", 16), ("quad9", 12), ("quad4", 100), ("quad9", 64), ("quad4", 4)])
+def test_host_request_problem_matches_the_builder(et, nx):
+    """A request built on the host by the library (dfea_build_rectangle_host) has build_rectangle_problem's keys,
+    connectivity, supports and material exactly, and its coordinates, geometry and load to rounding."""
+    from difffea_b200.problem import build_rectangle_problem
+    req = Request(0, et, nx, 1.3, 0.31, 0.04)
+    p = request_problem(req, "cpu")
+    q = build_rectangle_problem(et, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu, load=(req.load, 0.0))
+    assert list(p) == list(q)
+    for k in ("conn", "fixed", "m", "u_D", "mat_p", "mat_scalable", "GP", "GW"):
+        assert torch.equal(p[k], q[k]), k
+    for k in ("nodes", "dN_dX", "w_detJ", "f"):
+        assert p[k].shape == q[k].shape, k
+        assert float((p[k] - q[k]).abs().max()) <= 1e-13 * float(q[k].abs().max()), k
