@@ -270,8 +270,8 @@ def full_windows(rank, world, steps, warmup):
 
 def oracle_request_solve(req):
     """One request by the oracle on this host's cores (tangent "qp", Jacobi-PCG): (seconds, u, info)."""
-    from difffea_b200.serving import request_problem
-    p = request_problem(req, "cpu")
+    from difffea_b200.serving import reference_request_problem
+    p = reference_request_problem(req)
     tol = 1e-10 * float(torch.linalg.vector_norm(p["f"]))
     return cpu_oracle_solve(p, torch.ones(p["conn"].shape[0], dtype=torch.float64), 1, tol, 5000)
 

@@ -189,6 +189,14 @@ def request_problem(req, device="cpu", build_on_device=False, pin_memory=False):
     return {k: (v.pin_memory() if torch.is_tensor(v) else v) for k, v in p.items()} if pin_memory else p
 
 
+def reference_request_problem(req):
+    """The problem dictionary of a request built on the host by build_rectangle_problem (torch operations, the
+    reference's problem construction restated), independently of the library's builders: the input of the
+    reference arm and of the parity checks."""
+    return build_rectangle_problem(req.element_type, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu,
+                                   load=(req.load * 1.0, 0.0))
+
+
 _RECT_NEN = {"quad4": 4, "quad9": 9}
 _RECT_TEMPLATES = {}
 

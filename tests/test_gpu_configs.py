@@ -170,13 +170,13 @@ def _big_requests():
 
 
 def test_serving_requests_nx256_plus_against_the_oracle():
-    from difffea_b200.serving import ServingEngine, request_problem
+    from difffea_b200.serving import ServingEngine, reference_request_problem
     reqs = _big_requests()
     eng = ServingEngine(n_slots=4, device=DEV, precision="fp32")
     results = eng.run(reqs)
     for r, res in zip(reqs, results):
         assert res.converged and not res.error, res.error
-        p = request_problem(r, "cpu")
+        p = reference_request_problem(r)           # the oracle's input: built independently of the library
         P = oracle.as_problem(p)
         tol = 1e-10 * float(torch.linalg.vector_norm(p["f"]))
         th = torch.ones(p["conn"].shape[0], dtype=torch.float64)

@@ -144,7 +144,7 @@ def test_device_request_problem_matches_the_builder(et, nx):
     """A request built on the GPU by the library (dfea_build_rectangle) has build_rectangle_problem's keys, mesh,
     supports and material exactly, and its geometry and load to rounding; its solution agrees to 1e-9."""
     from difffea_b200.problem import build_rectangle_problem
-    from difffea_b200.serving import request_problem, solve_request
+    from difffea_b200.serving import reference_request_problem, request_problem, solve_request
     req = Request(0, et, nx, 1.3, 0.31, 0.04)
     p = request_problem(req, DEV, build_on_device=True)
     q = build_rectangle_problem(et, req.nx, req.ny, 4.0, 1.0, E=req.E, nu=req.nu, load=(req.load, 0.0), device=DEV,
@@ -155,5 +155,5 @@ def test_device_request_problem_matches_the_builder(et, nx):
     for k in ("nodes", "dN_dX", "w_detJ", "f"):
         assert p[k].shape == q[k].shape and rel(p[k], q[k]) < 1e-13, k
     u, info = solve_request(req, DEV, preconditioner="auto")
-    u_ref, info_ref = solve_request(req, DEV, preconditioner="auto", host_params=request_problem(req, "cpu"))
+    u_ref, info_ref = solve_request(req, DEV, preconditioner="auto", host_params=reference_request_problem(req))
     assert info["converged"] and info_ref["converged"] and rel(u, u_ref) < 1e-9
