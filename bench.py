@@ -412,8 +412,9 @@ def run_serve(args):
                "warmup": args.warmup, "ms_per_step": sample_ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32 operator / f64 Newton and Krylov vectors",
                "data": "synthetic (seeded request stream)", "config": serve_config(args.steps),
-               "engine": f"{SERVE['slots']} slots, largest waiting request first, multigrid-preconditioned from "
-                         f"2500 nodes, Jacobi below, host sync "
+               "engine": f"{SERVE['slots']} slots, largest waiting request first, problems written by the library "
+                         f"on the device, multigrid-preconditioned from 2500 nodes (gather-form level 0), Jacobi "
+                         f"below (direct launches), the C++ Newton driver per request, host sync "
                          f"{'blocking' if blocking else 'spin (blocking sync refused)'}",
                "all_converged": ok and lat_ok,
                "e2e": {"value": world * len(timed_s) / e2e_s, "unit": "solves/s", "requests": len(timed_s),
