@@ -176,3 +176,19 @@ def test_host_request_problem_matches_the_builder(et, nx):
     for k in ("nodes", "dN_dX", "w_detJ", "f"):
         assert p[k].shape == q[k].shape, k
         assert float((p[k] - q[k]).abs().max()) <= 1e-13 * float(q[k].abs().max()), k
+
+
+@pytest.mark.parametrize("et,nx", [("quad4", 24), ("quad9", 20)])
+def test_library_built_requests_are_recognised_as_structured_grids(et, nx):
+    """The multigrid hierarchy needs the mesher's numbering: the library-built connectivity is recognised as the
+    nx x ny grid, with every node at its grid position."""
+    from difffea_b200.multigrid import structured_grid
+    req = Request(0, et, nx, 1.0, 0.3, 0.02)
+    p = request_problem(req, "cpu")
+    g = structured_grid(p["conn"], p["nodes"].shape[0])
+    assert g is not None and (g["ncx"], g["ncy"]) == (req.nx, req.ny)
+    span = 2 if et == "quad9" else 1
+    x = p["nodes"][:, 0] * (span * req.nx / 4.0)
+    y = p["nodes"][:, 1] * (span * req.ny / 1.0)
+    assert torch.equal(torch.round(x).to(torch.int32), g["node_ij"][:, 0])
+    assert torch.equal(torch.round(y).to(torch.int32), g["node_ij"][:, 1])
