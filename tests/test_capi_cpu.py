@@ -98,3 +98,21 @@ def test_newton_driver_validates_before_touching_the_gpu():
     assert lib.dfea_newton_solve(None, 1, 1e-8, 25, 8, 500, ctypes.byref(info), None, 0, None) == 1
     nw = _lib.Newton()                 # no mesh, no buffers
     assert lib.dfea_newton_solve(ctypes.byref(nw), 1, 1e-8, 25, 8, 500, ctypes.byref(info), None, 0, None) == 1
+
+
+def test_rectangle_builder_rejects_bad_specs():
+    """dfea_build_rectangle_host (the host builder of the serving requests' problems) refuses element types other
+    than Q4 / Q9, empty rectangles and NULL outputs with an error code and a message, writing nothing."""
+    from difffea_b200.serving import Request, _rect_arrays
+    lib = _lib.load()
+    invalid = int(re.search(r"#define DFEA_ERR_INVALID (\d+)", open(HEADER).read()).group(1))
+    spec, a = _rect_arrays(Request(0, "quad4", 8, 1.0, 0.3, 0.02))
+    ptrs = [ctypes.c_void_p(a[k].data_ptr()) for k in ("nodes", "conn", "dN_dX", "w_detJ", "f", "m", "fixed", "u_D")]
+    assert lib.dfea_build_rectangle_host(ctypes.byref(spec), *ptrs) == _lib.DFEA_OK
+    for field, value in (("nen", 8), ("nx", 0), ("ny", -1), ("width", 0.0)):
+        bad = _lib.RectSpec.from_buffer_copy(spec)
+        setattr(bad, field, value)
+        assert lib.dfea_build_rectangle_host(ctypes.byref(bad), *ptrs) == invalid, field
+        assert b"rectangle" in lib.dfea_last_error(), field
+    assert lib.dfea_build_rectangle_host(ctypes.byref(spec), *ptrs[:-1], ctypes.c_void_p(0)) == invalid
+    assert lib.dfea_build_rectangle_host(None, *ptrs) == invalid
