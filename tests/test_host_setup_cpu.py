@@ -73,3 +73,33 @@ def test_step_by_step_pcg_matches_oracle_on_closures():
         assert k1 == k2 and torch.equal(x1, x2)
     x, k = newton_krylov.pcg(A, torch.zeros_like(b), lambda r: r / dg)
     assert k == 0 and float(x.abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("name", ["operator_quad4_h0.5_unit", "operator_quad4_h0.25_theta", "operator_quad4_h0.1_theta",
+                                  "operator_quad9_h0.5_unit", "operator_quad9_h0.25_theta"])
+def test_library_rectangle_builder_matches_reference(name):
+    """The library's rectangle builder (dfea_build_rectangle_host, which writes the serving requests' problems)
+    reproduces the reference's own problem arrays for its rectangle cantilever: the mesh, supports and
+    prescribed values exactly, geometry and load to rounding."""
+    import ctypes
+    from difffea_b200 import _lib, serving
+    from difffea_b200.cuda_mesh import ptr
+    d = load(name)
+    et = "quad9" if "quad9" in name else "quad4"
+    h = float(name.split("_h")[1].split("_")[0])
+    spec = _lib.RectSpec.from_buffer_copy(serving._rect_template(et))
+    spec.nx, spec.ny, spec.width, spec.height = round(2.0 / h), round(1.0 / h), 2.0, 1.0
+    spec.load_x, spec.load_y = 60.0, 0.0
+    N, n_el, nen, nq = d["nodes"].shape[0], d["conn"].shape[0], d["conn"].shape[1], d["w_detJ"].shape[1]
+    f64 = dict(dtype=torch.float64)
+    a = dict(nodes=torch.empty(N, 2, **f64), conn=torch.empty(n_el, nen, dtype=torch.int64),
+             dN_dX=torch.empty(n_el, nq, nen, 2, **f64), w_detJ=torch.empty(n_el, nq, **f64),
+             f=torch.empty(2 * N, **f64), m=torch.empty(2 * N, **f64), fixed=torch.empty(2 * N, dtype=torch.bool),
+             u_D=torch.empty(2 * N, **f64))
+    assert _lib.load().dfea_build_rectangle_host(ctypes.byref(spec), *(ptr(a[k]) for k in serving._RECT_ARGS)) == 0
+    for k in ("conn", "m", "u_D"):
+        assert torch.equal(a[k].double(), torch.as_tensor(d[k]).double()), k
+    assert torch.equal(a["fixed"], torch.as_tensor(d["fixed"]))
+    assert rel(a["nodes"], d["nodes"]) < 1e-15
+    assert rel(a["dN_dX"], d["dN_dX"]) < 1e-13 and rel(a["w_detJ"], d["w_detJ"]) < 1e-13
+    assert rel(a["f"], d["f"]) < 1e-13
